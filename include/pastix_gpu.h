@@ -1,0 +1,187 @@
+/*
+ * pastix_gpu.h -- C ABI of the B200 numerical factorization and solve.
+ *
+ * This library replaces the numerical part of PaStiX ("sopalin") on one
+ * NVIDIA B200: the coeftab lives in device memory and the diagonal-block
+ * factorizations, panel TRSMs, update GEMMs with their indexed scatter-add,
+ * the forward/backward solves and the iterative refinement run as CUDA
+ * kernels.  Ordering, symbolic factorization and blend analysis stay on the
+ * host: their output (the SolverMatrix cblk/blok/browtab arrays and the
+ * ordering) is handed over once through pastix_gpu_structure().
+ *
+ * Every entry point takes plain pointers and sizes.  Integer tables are
+ * int64_t (PaStiX built with PASTIX_INT64, its default); numerical arrays are
+ * double / double _Complex as the reference's PastixDouble / PastixComplex64
+ * data.  Return values are the reference's pastix_error_t codes
+ * (include/pastix/api.h:368-376).
+ *
+ * The one reference-side plug point per entry point is named in its comment.
+ */
+#ifndef PASTIX_GPU_H
+#define PASTIX_GPU_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define PASTIX_GPU_API __attribute__((visibility("default")))
+#else
+#define PASTIX_GPU_API
+#endif
+
+/* pastix_error_t (include/pastix/api.h:368-376) */
+#define PASTIX_GPU_SUCCESS          0
+#define PASTIX_GPU_ERR_ALLOC        2
+#define PASTIX_GPU_ERR_NOTIMPLEMENTED 3
+#define PASTIX_GPU_ERR_OUTOFMEMORY  4
+#define PASTIX_GPU_ERR_INTERNAL     6
+#define PASTIX_GPU_ERR_BADPARAMETER 7
+
+/* iparm / dparm indices used here, same values as include/pastix/api.h:35-186 */
+#define PGPU_IPARM_VERBOSE          0
+#define PGPU_IPARM_NNZEROS          2
+#define PGPU_IPARM_FACTORIZATION   43
+#define PGPU_IPARM_STATIC_PIVOTING 45
+#define PGPU_IPARM_REFINEMENT      51
+#define PGPU_IPARM_NBITER          52
+#define PGPU_IPARM_ITERMAX         53
+#define PGPU_IPARM_GMRES_IM        54
+#define PGPU_IPARM_MIXED           71
+#define PGPU_IPARM_SIZE            80
+#define PGPU_DPARM_EPSILON_REFINEMENT 1
+#define PGPU_DPARM_RELATIVE_ERROR     2
+#define PGPU_DPARM_EPSILON_MAGN_CTRL  3
+#define PGPU_DPARM_FACT_TIME         10
+#define PGPU_DPARM_FACT_FLOPS        11
+#define PGPU_DPARM_FACT_THFLOPS      12
+#define PGPU_DPARM_SOLV_TIME         17
+#define PGPU_DPARM_REFINE_TIME       22
+#define PGPU_DPARM_A_NORM            23
+#define PGPU_DPARM_SIZE              26
+
+/* pastix_factotype_t (include/pastix/api.h:313-324) */
+#define PGPU_FACT_POTRF 0
+#define PGPU_FACT_SYTRF 1
+#define PGPU_FACT_GETRF 2
+#define PGPU_FACT_HETRF 4
+/* spm_mtxtype_t values (PastixGeneral/Symmetric/Hermitian) */
+#define PGPU_GENERAL   111
+#define PGPU_SYMMETRIC 112
+#define PGPU_HERMITIAN 113
+/* spm_coeftype_t values of the input matrix */
+#define PGPU_DOUBLE    3
+#define PGPU_COMPLEX64 5
+/* pastix_refine_t (include/pastix/api.h:273-278) */
+#define PGPU_REFINE_GMRES 0
+#define PGPU_REFINE_CG    1
+
+typedef struct pastix_gpu_s pastix_gpu_t;
+
+/*
+ * Create a context on CUDA device `device`, copying the caller's iparm/dparm
+ * arrays (IPARM_SIZE / DPARM_SIZE entries in the reference's order; NULL
+ * keeps the reference defaults of common/api.c:411-560).
+ * Replaces the GPU side of pastixInit (common/api.c:891).
+ */
+PASTIX_GPU_API int pastix_gpu_init( pastix_gpu_t **ctx, int device,
+                     const int64_t *iparm, const double *dparm );
+
+/*
+ * Hand over the analysis result: the SolverMatrix of blend/solver.h:137-273
+ * produced by pastix_subtask_blend (blend/pastix_subtask_blend.c:121).
+ *   cblktab : (cblknbr+1) x 4  {fcolnum, lcolnum, first blok index, brownum}
+ *   bloktab : bloknbr x 4      {frownum, lrownum, lcblknm, fcblknm}
+ *   browtab : brownbr          (blend/solver.h:222)
+ *   permtab, peritab : n       (pastix_order_t, include/pastix/order.h)
+ * All indices 0-based.  The device coeftab is laid out and allocated here
+ * (plug point: coeftabInit, sopalin/coeftab.c:204).
+ */
+PASTIX_GPU_API int pastix_gpu_structure( pastix_gpu_t *ctx, int64_t n,
+                          int64_t cblknbr, const int64_t *cblktab,
+                          int64_t bloknbr, const int64_t *bloktab,
+                          int64_t brownbr, const int64_t *browtab,
+                          const int64_t *permtab, const int64_t *peritab );
+
+/*
+ * Hand over the pattern of the user's matrix (0-based CSC; Symmetric and
+ * Hermitian matrices give one triangle).  Builds the device-side bcsc
+ * equivalents: the fill-in map into the coeftab and the permuted matrix the
+ * refinement multiplies by.  Replaces pastix_subtask_spm2bcsc
+ * (sopalin/pastix_task_sopalin.c:93) / bcscInit (bcsc/bcsc.c:1887).
+ */
+PASTIX_GPU_API int pastix_gpu_spm( pastix_gpu_t *ctx, int mtxtype, int flttype, int64_t n,
+                    const int64_t *colptr, const int64_t *rowptr );
+
+/*
+ * Numerical factorization of the matrix whose values (in the order of the
+ * pattern given to pastix_gpu_spm) are at `values` -- host or device memory.
+ * iparm[IPARM_FACTORIZATION] selects POTRF / GETRF / HETRF, and
+ * iparm[IPARM_MIXED] = 1 factorizes in single precision.  Copies the values
+ * in, scatters them into the coeftab and factorizes it.
+ * Replaces pastix_task_numfact (sopalin/pastix_task_sopalin.c:637), i.e. the
+ * bcsc2ctab and sopalin subtasks (plug point: sopalinFacto,
+ * sopalin/pastix_task_sopalin.c:51-58).
+ */
+PASTIX_GPU_API int pastix_gpu_numfact( pastix_gpu_t *ctx, const void *values );
+
+/*
+ * Solve A X = B in place for `nrhs` right-hand sides (column-major, leading
+ * dimension ldb, host or device memory).  Replaces pastix_task_solve
+ * (sopalin/pastix_task_solve.c:753; plug point: ztrsm_table,
+ * sopalin/sequential_ztrsm.c:536-552).
+ */
+PASTIX_GPU_API int pastix_gpu_solve( pastix_gpu_t *ctx, int64_t nrhs, void *B, int64_t ldb );
+
+/*
+ * Iterative refinement of X for A X = B (CG or GMRES, per
+ * iparm[IPARM_REFINEMENT]; FP64 residuals, preconditioned by the factors)
+ * to dparm[DPARM_EPSILON_REFINEMENT].  Replaces pastix_task_refine
+ * (refinement/pastix_task_refine.c:231).
+ */
+PASTIX_GPU_API int pastix_gpu_refine( pastix_gpu_t *ctx, int64_t nrhs, const void *B, int64_t ldb,
+                       void *X, int64_t ldx );
+
+/*
+ * Solve then refine; replaces pastix_task_solve_and_refine
+ * (refinement/pastix_task_refine.c:354).  X receives the solution.
+ */
+PASTIX_GPU_API int pastix_gpu_solve_and_refine( pastix_gpu_t *ctx, int64_t nrhs, const void *B,
+                                 int64_t ldb, void *X, int64_t ldx );
+
+/* Copy the output parameters (iparm/dparm, reference indices) out. */
+PASTIX_GPU_API int pastix_gpu_get_params( pastix_gpu_t *ctx, int64_t *iparm, double *dparm );
+/* Change one parameter between calls (e.g. IPARM_MIXED, IPARM_REFINEMENT). */
+PASTIX_GPU_API int pastix_gpu_set_iparm( pastix_gpu_t *ctx, int index, int64_t value );
+PASTIX_GPU_API int pastix_gpu_set_dparm( pastix_gpu_t *ctx, int index, double value );
+
+/*
+ * Download the factors in the reference's 1D panel layout: cblk after cblk,
+ * a column-major stride x width panel whose rows follow the cblk's blocks
+ * (the layout of cpucblk_zalloc_fr for a 1D cblk, kernels/cpucblk_zinit.c:220).
+ * Element type: the factor type (double/float, complex for Hermitian).
+ * U receives U^T for LU (may be NULL otherwise).
+ */
+PASTIX_GPU_API int pastix_gpu_coeftab( pastix_gpu_t *ctx, void *L, void *U );
+
+/*
+ * Launch statistics of the last numfact / solve / refine: number of kernel
+ * launches issued and the device time (ms) each phase took.
+ *   stats[0] numfact launches, stats[1] solve launches, stats[2] refine launches
+ *   stats[3] numfact ms, stats[4] solve ms, stats[5] refine ms
+ *   stats[6] update-GEMM ms inside numfact (CUDA events around those launches)
+ *   stats[7] update-GEMM launches inside numfact
+ */
+PASTIX_GPU_API int pastix_gpu_stats( pastix_gpu_t *ctx, double *stats );
+
+/* Release the device memory and the context (pastixFinalize, common/api.c:914). */
+PASTIX_GPU_API void pastix_gpu_finalize( pastix_gpu_t **ctx );
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PASTIX_GPU_H */

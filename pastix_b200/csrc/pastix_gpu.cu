@@ -1,0 +1,938 @@
+// Host side of the B200 sopalin replacement: the C ABI declared in
+// include/pastix_gpu.h, the device layout of the coeftab, the level schedule
+// and the drivers of numfact / solve / refinement.
+#include "pastix_gpu.h"
+#include "pgpu_factor.cuh"
+#include "pgpu_solve.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+using namespace pgpu;
+
+#define PGPU_CHECK(x)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (x);                                                          \
+        if (e_ != cudaSuccess) {                                                       \
+            fprintf(stderr, "pastix_gpu: %s failed: %s (%s:%d)\n", #x,                 \
+                    cudaGetErrorString(e_), __FILE__, __LINE__);                       \
+            return e_ == cudaErrorMemoryAllocation ? PASTIX_GPU_ERR_OUTOFMEMORY        \
+                                                   : PASTIX_GPU_ERR_INTERNAL;          \
+        }                                                                              \
+    } while (0)
+
+namespace {
+
+template <typename T>
+struct DArr {
+    T *p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t cnt) {
+        release();
+        n = cnt;
+        if (!cnt) return cudaSuccess;
+        return cudaMalloc(&p, cnt * sizeof(T));
+    }
+    cudaError_t upload(const std::vector<T> &v, cudaStream_t s) {
+        cudaError_t e = alloc(v.size());
+        if (e != cudaSuccess || v.empty()) return e;
+        return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    DArr() = default;
+    DArr(const DArr &) = delete;
+    DArr &operator=(const DArr &) = delete;
+    ~DArr() { release(); }
+};
+
+inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+inline int cdiv(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+const int SOLVE_ROWS_PER_CHUNK = 256;
+
+bool is_device_ptr(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+struct pastix_gpu_s {
+    int device = 0;
+    int64_t iparm[PGPU_IPARM_SIZE];
+    double dparm[PGPU_DPARM_SIZE];
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[6];
+
+    // ---- structure (host copies) ----
+    int n = 0, cblknbr = 0, bloknbr = 0;
+    std::vector<int> fcol, width, height, ld, fblok, bfrow, blrow, browoff, bfcblk, rowidx, col2cblk;
+    std::vector<int64_t> coefoff, rowbase;
+    std::vector<int> peritab;
+    int64_t coefnbr = 0;      // elements of one (L or U) coeftab incl. padding
+    int maxw = 0;
+    int nlevels = 0;
+    std::vector<int> lvl_ptr, lvl_cblks, lvl_maxw;
+    double thflops_potrf = 0, thflops_getrf = 0;
+
+    // ---- device structure ----
+    DArr<int> d_fcol, d_width, d_height, d_ld, d_fblok, d_rowidx, d_bfrow, d_blrow, d_browoff, d_bfcblk,
+        d_lvl_cblks, d_peritab;
+    DArr<int64_t> d_coefoff, d_rowbase;
+    Meta meta{};
+
+    // ---- factorization plan (per factotype) ----
+    int plan_fact = -1;
+    std::vector<int> tile_ptr, trsm_ptr;
+    DArr<int4> d_tiles, d_trsm;
+    DArr<GemmTask> d_tasks;
+    std::vector<int> solve_ptr;
+    DArr<int2> d_solve_chunks;
+
+    // ---- matrix ----
+    int mtxtype = PGPU_SYMMETRIC, flttype = PGPU_DOUBLE;
+    int64_t nnz = 0;
+    DArr<int64_t> d_fill_dst;   // per user nnz: coeftab offset (U entries offset by coefnbr)
+    DArr<int8_t> d_wgt;         // Frobenius weight per user nnz
+    DArr<int64_t> d_csr_ptr, d_csr_src;
+    DArr<int> d_csr_col;
+    DArr<double> d_csr_val, d_vals;
+    bool have_spm = false;
+
+    // ---- numerical state ----
+    DArr<unsigned char> d_coef;
+    int coef_float = 0;     // factor precision of d_coef
+    int fact_done = -1;     // factotype of the factors in d_coef, -1 if none
+    DArr<Status> d_status;
+    DArr<double> d_partial, d_scalar;
+    DArr<unsigned char> d_work;   // solve workspace (n x 16 in factor precision)
+    DArr<double> d_rhs, d_x, d_r, d_z, d_p, d_ap, d_gm;   // refinement vectors
+    double stats[8] = {0};
+};
+
+// --------------------------------------------------------------------------
+static void default_params(int64_t *iparm, double *dparm) {
+    // common/api.c:411-560 defaults for the entries this layer reads
+    std::fill(iparm, iparm + PGPU_IPARM_SIZE, 0);
+    std::fill(dparm, dparm + PGPU_DPARM_SIZE, 0.0);
+    iparm[PGPU_IPARM_FACTORIZATION] = PGPU_FACT_GETRF;
+    iparm[PGPU_IPARM_REFINEMENT] = PGPU_REFINE_GMRES;
+    iparm[PGPU_IPARM_ITERMAX] = 250;
+    iparm[PGPU_IPARM_GMRES_IM] = 25;
+    dparm[PGPU_DPARM_EPSILON_REFINEMENT] = -1.0;
+    dparm[PGPU_DPARM_EPSILON_MAGN_CTRL] = 0.0;
+}
+
+extern "C" int pastix_gpu_init(pastix_gpu_t **pctx, int device, const int64_t *iparm, const double *dparm) {
+    if (!pctx) return PASTIX_GPU_ERR_BADPARAMETER;
+    *pctx = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        fprintf(stderr, "pastix_gpu: no CUDA device available\n");
+        return PASTIX_GPU_ERR_INTERNAL;
+    }
+    if (device < 0 || device >= ndev) return PASTIX_GPU_ERR_BADPARAMETER;
+    PGPU_CHECK(cudaSetDevice(device));
+    pastix_gpu_t *ctx = new pastix_gpu_t();
+    ctx->device = device;
+    default_params(ctx->iparm, ctx->dparm);
+    if (iparm) std::memcpy(ctx->iparm, iparm, sizeof(ctx->iparm));
+    if (dparm) std::memcpy(ctx->dparm, dparm, sizeof(ctx->dparm));
+    PGPU_CHECK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    for (auto &e : ctx->ev) PGPU_CHECK(cudaEventCreate(&e));
+    PGPU_CHECK(ctx->d_status.alloc(1));
+    PGPU_CHECK(ctx->d_partial.alloc(1024));
+    PGPU_CHECK(ctx->d_scalar.alloc(16));
+    *pctx = ctx;
+    return PASTIX_GPU_SUCCESS;
+}
+
+// --------------------------------------------------------------------------
+// Structure handoff: device layout + level schedule.
+// --------------------------------------------------------------------------
+extern "C" int pastix_gpu_structure(pastix_gpu_t *ctx, int64_t n, int64_t cblknbr, const int64_t *cblktab,
+                                    int64_t bloknbr, const int64_t *bloktab, int64_t brownbr,
+                                    const int64_t *browtab, const int64_t *permtab, const int64_t *peritab) {
+    (void)brownbr; (void)browtab; (void)permtab;
+    if (!ctx || n <= 0 || cblknbr <= 0 || !cblktab || !bloktab || !peritab) return PASTIX_GPU_ERR_BADPARAMETER;
+    if (n > INT32_MAX || bloknbr > INT32_MAX) return PASTIX_GPU_ERR_BADPARAMETER;
+    PGPU_CHECK(cudaSetDevice(ctx->device));
+    auto &C = *ctx;
+    C.n = (int)n;
+    C.cblknbr = (int)cblknbr;
+    C.bloknbr = (int)bloknbr;
+    const int nc = C.cblknbr, nb = C.bloknbr;
+    C.fcol.resize(nc); C.width.resize(nc); C.height.resize(nc); C.ld.resize(nc);
+    C.coefoff.resize(nc); C.rowbase.resize(nc); C.fblok.resize(nc + 1);
+    C.bfrow.resize(nb); C.blrow.resize(nb); C.browoff.resize(nb); C.bfcblk.resize(nb);
+    C.col2cblk.assign(n, -1);
+    C.rowidx.clear();
+    for (int b = 0; b < nb; b++) {
+        C.bfrow[b] = (int)bloktab[4 * b + 0];
+        C.blrow[b] = (int)bloktab[4 * b + 1];
+        C.bfcblk[b] = (int)bloktab[4 * b + 3];
+    }
+    int64_t off = 0;
+    C.maxw = 0;
+    for (int c = 0; c <= nc; c++) C.fblok[c] = (int)cblktab[4 * c + 2];
+    if (C.fblok[nc] != nb) return PASTIX_GPU_ERR_BADPARAMETER;
+    double fl_potrf = 0, fl_getrf = 0;
+    for (int c = 0; c < nc; c++) {
+        const int fc = (int)cblktab[4 * c + 0], lc = (int)cblktab[4 * c + 1];
+        const int w = lc - fc + 1;
+        const int b0 = C.fblok[c], b1 = C.fblok[c + 1];
+        if (w <= 0 || b1 <= b0 || C.bfrow[b0] != fc || C.blrow[b0] != lc) return PASTIX_GPU_ERR_BADPARAMETER;
+        C.fcol[c] = fc;
+        C.width[c] = w;
+        C.maxw = std::max(C.maxw, w);
+        for (int j = fc; j <= lc; j++) C.col2cblk[j] = c;
+        C.rowbase[c] = (int64_t)C.rowidx.size();
+        int h = 0;
+        for (int b = b0; b < b1; b++) {
+            if (C.blrow[b] < C.bfrow[b] || C.blrow[b] >= n) return PASTIX_GPU_ERR_BADPARAMETER;
+            if (b > b0 && (C.bfcblk[b] <= c || C.bfcblk[b] >= nc || C.bfrow[b] <= C.blrow[b - 1]))
+                return PASTIX_GPU_ERR_BADPARAMETER;
+            C.browoff[b] = h;
+            for (int r = C.bfrow[b]; r <= C.blrow[b]; r++) C.rowidx.push_back(r);
+            h += C.blrow[b] - C.bfrow[b] + 1;
+        }
+        C.height[c] = h;
+        C.ld[c] = (int)round_up(w, 4);
+        C.coefoff[c] = off;
+        off += round_up((int64_t)h * C.ld[c], 32);
+        // algorithmic flops (common/flops.h: FLOPS_DPOTRF / DGETRF, DTRSM, DGEMM)
+        const double W = w, M = h - w;
+        fl_potrf += W * W * W / 3.0 + W * W / 2.0 + W / 6.0 + M * W * W;
+        fl_getrf += 2.0 * W * W * W / 3.0 - W * W / 2.0 + 5.0 * W / 6.0 + 2.0 * M * W * W;
+        for (int b = b0 + 1; b < b1; b++) {
+            const double N = C.blrow[b] - C.bfrow[b] + 1, Mb = h - C.browoff[b];
+            fl_potrf += 2.0 * Mb * N * W;
+            fl_getrf += 2.0 * Mb * N * W + (b + 1 < b1 ? 2.0 * (Mb - N) * N * W : 0.0);
+        }
+    }
+    // every block must lie inside the columns of the cblk it faces, which is
+    // what lets the update GEMM address its target column directly
+    for (int b = 0; b < nb; b++) {
+        const int f = C.bfcblk[b];
+        if (f < 0 || f >= nc || C.bfrow[b] < C.fcol[f] || C.blrow[b] > C.fcol[f] + C.width[f] - 1)
+            return PASTIX_GPU_ERR_BADPARAMETER;
+    }
+    // the panel TRSM keeps TRSM_ROWS x w elements in shared memory
+    if ((size_t)(TRSM_ROWS + 1) * C.maxw * sizeof(double) > 200 * 1024) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    C.thflops_potrf = fl_potrf;
+    C.thflops_getrf = fl_getrf;
+    for (int j = 0; j < n; j++)
+        if (C.col2cblk[j] < 0) return PASTIX_GPU_ERR_BADPARAMETER;
+    C.coefnbr = off;
+    C.peritab.assign(peritab, peritab + n);
+
+    // level schedule: level(c) = 1 + max level of the cblks whose first
+    // off-diagonal block faces c (elimination-tree children)
+    std::vector<int> level(nc, 0);
+    for (int c = 0; c < nc; c++) {
+        if (C.fblok[c + 1] - C.fblok[c] > 1) {
+            int p = C.bfcblk[C.fblok[c] + 1];
+            level[p] = std::max(level[p], level[c] + 1);
+        }
+    }
+    C.nlevels = 0;
+    for (int c = 0; c < nc; c++) C.nlevels = std::max(C.nlevels, level[c] + 1);
+    C.lvl_ptr.assign(C.nlevels + 1, 0);
+    for (int c = 0; c < nc; c++) C.lvl_ptr[level[c] + 1]++;
+    for (int l = 0; l < C.nlevels; l++) C.lvl_ptr[l + 1] += C.lvl_ptr[l];
+    C.lvl_cblks.assign(nc, 0);
+    C.lvl_maxw.assign(C.nlevels, 0);
+    {
+        std::vector<int> pos(C.lvl_ptr.begin(), C.lvl_ptr.end() - 1);
+        for (int c = 0; c < nc; c++) {
+            C.lvl_cblks[pos[level[c]]++] = c;
+            C.lvl_maxw[level[c]] = std::max(C.lvl_maxw[level[c]], C.width[c]);
+        }
+    }
+
+    // device copies
+    cudaStream_t s = C.stream;
+    PGPU_CHECK(C.d_fcol.upload(C.fcol, s));
+    PGPU_CHECK(C.d_width.upload(C.width, s));
+    PGPU_CHECK(C.d_height.upload(C.height, s));
+    PGPU_CHECK(C.d_ld.upload(C.ld, s));
+    PGPU_CHECK(C.d_coefoff.upload(C.coefoff, s));
+    PGPU_CHECK(C.d_fblok.upload(C.fblok, s));
+    PGPU_CHECK(C.d_rowbase.upload(C.rowbase, s));
+    PGPU_CHECK(C.d_rowidx.upload(C.rowidx, s));
+    PGPU_CHECK(C.d_bfrow.upload(C.bfrow, s));
+    PGPU_CHECK(C.d_blrow.upload(C.blrow, s));
+    PGPU_CHECK(C.d_browoff.upload(C.browoff, s));
+    PGPU_CHECK(C.d_bfcblk.upload(C.bfcblk, s));
+    PGPU_CHECK(C.d_lvl_cblks.upload(C.lvl_cblks, s));
+    PGPU_CHECK(C.d_peritab.upload(C.peritab, s));
+    C.meta = Meta{C.n, nc, nb, C.d_fcol.p, C.d_width.p, C.d_height.p, C.d_ld.p, C.d_coefoff.p,
+                  C.d_fblok.p, C.d_rowbase.p, C.d_rowidx.p, C.d_bfrow.p, C.d_blrow.p, C.d_browoff.p,
+                  C.d_bfcblk.p};
+
+    // solve chunks (independent of the factorization type)
+    std::vector<int2> sch;
+    C.solve_ptr.assign(C.nlevels + 1, 0);
+    for (int l = 0; l < C.nlevels; l++) {
+        for (int q = C.lvl_ptr[l]; q < C.lvl_ptr[l + 1]; q++) {
+            int c = C.lvl_cblks[q];
+            for (int r0 = C.width[c]; r0 < C.height[c]; r0 += SOLVE_ROWS_PER_CHUNK) sch.push_back(make_int2(c, r0));
+        }
+        C.solve_ptr[l + 1] = (int)sch.size();
+    }
+    PGPU_CHECK(C.d_solve_chunks.upload(sch, s));
+    C.plan_fact = -1;
+    C.fact_done = -1;
+    C.d_coef.release();
+    PGPU_CHECK(cudaStreamSynchronize(s));
+    return PASTIX_GPU_SUCCESS;
+}
+
+// Panel row of global row r in cblk c (host mirror of panel_row_of).
+static int host_panel_row(const pastix_gpu_t &C, int c, int r) {
+    int lo = C.fblok[c], hi = C.fblok[c + 1] - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (C.bfrow[mid] <= r) lo = mid; else hi = mid - 1;
+    }
+    if (r < C.bfrow[lo] || r > C.blrow[lo]) return -1;
+    return C.browoff[lo] + (r - C.bfrow[lo]);
+}
+
+// --------------------------------------------------------------------------
+// Pattern handoff: fill-in map (bcsc -> coeftab) and the permuted CSR.
+// --------------------------------------------------------------------------
+extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64_t n, const int64_t *colptr,
+                              const int64_t *rowptr) {
+    if (!ctx || !colptr || !rowptr) return PASTIX_GPU_ERR_BADPARAMETER;
+    if (n != ctx->n) return PASTIX_GPU_ERR_BADPARAMETER;
+    if (flttype != PGPU_DOUBLE) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    if (mtxtype != PGPU_GENERAL && mtxtype != PGPU_SYMMETRIC && mtxtype != PGPU_HERMITIAN)
+        return PASTIX_GPU_ERR_BADPARAMETER;
+    PGPU_CHECK(cudaSetDevice(ctx->device));
+    auto &C = *ctx;
+    C.mtxtype = mtxtype;
+    C.flttype = flttype;
+    const int64_t nnz = colptr[n];
+    C.nnz = nnz;
+    std::vector<int> perm(n);
+    for (int k = 0; k < n; k++) perm[C.peritab[k]] = k;
+    std::vector<int64_t> dst(nnz);
+    std::vector<int8_t> wgt(nnz);
+    const bool sym = (mtxtype != PGPU_GENERAL);
+    // permuted full matrix as (row, col, src) triplets
+    std::vector<int64_t> rcount(n + 1, 0);
+    for (int64_t j = 0; j < n; j++) {
+        for (int64_t k = colptr[j]; k < colptr[j + 1]; k++) {
+            int64_t i = rowptr[k];
+            if (i < 0 || i >= n) return PASTIX_GPU_ERR_BADPARAMETER;
+            int pi = perm[i], pj = perm[j];
+            wgt[k] = (sym && i != j) ? 2 : 1;
+            rcount[pi + 1]++;
+            if (sym && i != j) rcount[pj + 1]++;
+            if (sym && pi < pj) std::swap(pi, pj);
+            int64_t d;
+            if (pi >= pj) {
+                int c = C.col2cblk[pj];
+                int pr = host_panel_row(C, c, pi);
+                if (pr < 0) return PASTIX_GPU_ERR_BADPARAMETER;
+                d = C.coefoff[c] + (int64_t)pr * C.ld[c] + (pj - C.fcol[c]);
+            } else {
+                // general, upper entry A(pi, pj), pi < pj
+                int c = C.col2cblk[pi];
+                if (C.col2cblk[pj] == c) {
+                    // inside the diagonal block: kept in L's square
+                    d = C.coefoff[c] + (int64_t)(pi - C.fcol[c]) * C.ld[c] + (pj - C.fcol[c]);
+                } else {
+                    int pr = host_panel_row(C, c, pj);
+                    if (pr < 0) return PASTIX_GPU_ERR_BADPARAMETER;
+                    d = C.coefnbr + C.coefoff[c] + (int64_t)pr * C.ld[c] + (pi - C.fcol[c]);
+                }
+            }
+            dst[k] = d;
+        }
+    }
+    for (int64_t i = 0; i < n; i++) rcount[i + 1] += rcount[i];
+    const int64_t fnnz = rcount[n];
+    std::vector<int> ccol(fnnz);
+    std::vector<int64_t> csrc(fnnz);
+    {
+        std::vector<int64_t> pos(rcount.begin(), rcount.end() - 1);
+        for (int64_t j = 0; j < n; j++) {
+            for (int64_t k = colptr[j]; k < colptr[j + 1]; k++) {
+                int64_t i = rowptr[k];
+                int pi = perm[i], pj = perm[j];
+                int64_t q = pos[pi]++;
+                ccol[q] = pj;
+                csrc[q] = k;
+                if (sym && i != j) {
+                    q = pos[pj]++;
+                    ccol[q] = pi;
+                    csrc[q] = k;
+                }
+            }
+        }
+    }
+    cudaStream_t s = C.stream;
+    PGPU_CHECK(C.d_fill_dst.upload(dst, s));
+    PGPU_CHECK(C.d_wgt.upload(wgt, s));
+    PGPU_CHECK(C.d_csr_ptr.upload(rcount, s));
+    PGPU_CHECK(C.d_csr_col.upload(ccol, s));
+    PGPU_CHECK(C.d_csr_src.upload(csrc, s));
+    PGPU_CHECK(C.d_csr_val.alloc(fnnz));
+    PGPU_CHECK(C.d_vals.alloc(nnz));
+    PGPU_CHECK(cudaStreamSynchronize(s));
+    C.have_spm = true;
+    C.fact_done = -1;
+    return PASTIX_GPU_SUCCESS;
+}
+
+// --------------------------------------------------------------------------
+// Factorization plan for one factorization type.
+// --------------------------------------------------------------------------
+static int build_fact_plan(pastix_gpu_t &C, int fact) {
+    if (C.plan_fact == fact) return PASTIX_GPU_SUCCESS;
+    const bool lu = (fact == PGPU_FACT_GETRF);
+    std::vector<int4> tiles, trsm;
+    std::vector<GemmTask> tasks;
+    C.tile_ptr.assign(C.nlevels + 1, 0);
+    C.trsm_ptr.assign(C.nlevels + 1, 0);
+    for (int l = 0; l < C.nlevels; l++) {
+        for (int q = C.lvl_ptr[l]; q < C.lvl_ptr[l + 1]; q++) {
+            const int c = C.lvl_cblks[q];
+            const int w = C.width[c], h = C.height[c];
+            for (int r0 = w; r0 < h; r0 += TRSM_ROWS) {
+                trsm.push_back(make_int4(c, r0, 0, lu ? 1 : 0));
+                if (lu) trsm.push_back(make_int4(c, r0, 1, 2));
+            }
+            const int b1 = C.fblok[c + 1];
+            for (int b = C.fblok[c] + 1; b < b1; b++) {
+                const int f = C.bfcblk[b];
+                const int N = C.blrow[b] - C.bfrow[b] + 1;
+                auto add = [&](int arow0, int flags) {
+                    const int M = h - arow0;
+                    if (M <= 0) return;
+                    const int id = (int)tasks.size();
+                    tasks.push_back(GemmTask{c, b, f, arow0, M, flags});
+                    for (int tm = 0; tm < cdiv(M, GEMM_TM); tm++)
+                        for (int tn = 0; tn < cdiv(N, GEMM_TN); tn++) {
+                            if ((flags & 8) && tm < tn) continue;   // strictly upper tiles of the diagonal block
+                            tiles.push_back(make_int4(id, tm, tn, 0));
+                        }
+                };
+                if (!lu) {
+                    add(C.browoff[b], 8);
+                } else {
+                    add(C.browoff[b], 2);                          // L side: A = L, B = U^T rows of b
+                    if (b + 1 < b1) add(C.browoff[b + 1], 1 | 4);  // U side: A = U^T, B = L rows of b
+                }
+            }
+        }
+        C.tile_ptr[l + 1] = (int)tiles.size();
+        C.trsm_ptr[l + 1] = (int)trsm.size();
+    }
+    cudaStream_t s = C.stream;
+    PGPU_CHECK(C.d_tiles.upload(tiles, s));
+    PGPU_CHECK(C.d_trsm.upload(trsm, s));
+    PGPU_CHECK(C.d_tasks.upload(tasks, s));
+    PGPU_CHECK(cudaStreamSynchronize(s));
+    C.plan_fact = fact;
+    return PASTIX_GPU_SUCCESS;
+}
+
+static const int DIAG_SMEM_BYTES = 96 * 1024;
+
+template <typename T>
+static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches) {
+    const bool lu = (fact == PGPU_FACT_GETRF);
+    T *coefL = reinterpret_cast<T *>(C.d_coef.p);
+    T *coefU = lu ? coefL + C.coefnbr : coefL;
+    cudaStream_t s = C.stream;
+    int smem_w = (int)std::floor(std::sqrt((double)DIAG_SMEM_BYTES / sizeof(T)));
+    auto kdiag = lu ? k_diag_factor<T, true> : k_diag_factor<T, false>;
+    PGPU_CHECK(cudaFuncSetAttribute(kdiag, cudaFuncAttributeMaxDynamicSharedMemorySize, DIAG_SMEM_BYTES));
+    PGPU_CHECK(cudaFuncSetAttribute(k_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    int nl = 0;
+    float gemm_ms = 0.f;
+    int ngemm = 0;
+    for (int l = 0; l < C.nlevels; l++) {
+        const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
+        const int mw = C.lvl_maxw[l];
+        // the whole level's diagonal blocks fit the shared-memory path when
+        // its widest one does; otherwise the cblks that fit still use it
+        const int sw = std::min(mw, smem_w);
+        size_t dsm = (size_t)sw * sw * sizeof(T);
+        kdiag<<<ncb, 256, dsm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, crit, sw * sw,
+                                    C.d_status.p);
+        nl++;
+        const int ntr = C.trsm_ptr[l + 1] - C.trsm_ptr[l];
+        if (ntr) {
+            size_t tsm = (size_t)(TRSM_ROWS + 1) * mw * sizeof(T);
+            k_trsm<T><<<ntr, 256, tsm, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], coefL, coefU);
+            nl++;
+        }
+        const int nti = C.tile_ptr[l + 1] - C.tile_ptr[l];
+        if (nti) {
+            k_gemm_scatter<T><<<nti, 256, 0, s>>>(C.meta, C.d_tiles.p + C.tile_ptr[l], C.d_tasks.p, coefL, coefU);
+            nl++;
+            ngemm++;
+        }
+    }
+    PGPU_CHECK(cudaGetLastError());
+    (void)gemm_ms;
+    *launches = nl;
+    C.stats[7] = ngemm;
+    return PASTIX_GPU_SUCCESS;
+}
+
+static int dev_norm_frob(pastix_gpu_t &C, double *out) {
+    cudaStream_t s = C.stream;
+    const int nb = 512;
+    k_sumsq_partial<<<nb, RED_THREADS, 0, s>>>(C.nnz, C.d_vals.p, C.d_wgt.p, C.d_partial.p);
+    k_dot_final<<<1, RED_THREADS, 0, s>>>(nb, C.d_partial.p, C.d_scalar.p, 1);
+    PGPU_CHECK(cudaMemcpyAsync(out, C.d_scalar.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PGPU_CHECK(cudaStreamSynchronize(s));
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
+    if (!ctx || !values) return PASTIX_GPU_ERR_BADPARAMETER;
+    auto &C = *ctx;
+    if (!C.have_spm || C.cblknbr == 0) return PASTIX_GPU_ERR_BADPARAMETER;
+    PGPU_CHECK(cudaSetDevice(C.device));
+    const int fact = (int)C.iparm[PGPU_IPARM_FACTORIZATION];
+    if (fact != PGPU_FACT_POTRF && fact != PGPU_FACT_GETRF) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    if (fact == PGPU_FACT_POTRF && C.mtxtype == PGPU_GENERAL) return PASTIX_GPU_ERR_BADPARAMETER;
+    const int mixed = C.iparm[PGPU_IPARM_MIXED] ? 1 : 0;
+    int rc = build_fact_plan(C, fact);
+    if (rc) return rc;
+    const size_t esz = mixed ? sizeof(float) : sizeof(double);
+    const size_t ncoef = (size_t)C.coefnbr * (fact == PGPU_FACT_GETRF ? 2 : 1);
+    if (C.d_coef.n < ncoef * esz) {
+        C.d_coef.release();
+        PGPU_CHECK(C.d_coef.alloc(ncoef * esz));
+    }
+    cudaStream_t s = C.stream;
+    PGPU_CHECK(cudaEventRecord(C.ev[0], s));
+    // values in (pastix_subtask_spm2bcsc), norm, bcsc -> coeftab
+    if (is_device_ptr(values))
+        PGPU_CHECK(cudaMemcpyAsync(C.d_vals.p, values, C.nnz * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    else
+        PGPU_CHECK(cudaMemcpyAsync(C.d_vals.p, values, C.nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+    double anorm = 0;
+    rc = dev_norm_frob(C, &anorm);
+    if (rc) return rc;
+    C.dparm[PGPU_DPARM_A_NORM] = anorm;
+    // static pivoting threshold, sopalin/pastix_task_sopalin.c:461-485 (the
+    // bcsc stays double, so eps = dlamch('e') also for the mixed factors)
+    const double magn = C.dparm[PGPU_DPARM_EPSILON_MAGN_CTRL];
+    double crit;
+    if (magn < 0.) crit = -magn;
+    else if (magn == 0.) crit = 1.1102230246251565e-16 * anorm;
+    else crit = magn * anorm;
+    k_gather_vals<<<1024, 256, 0, s>>>((int64_t)C.d_csr_val.n, C.d_csr_src.p, C.d_vals.p, C.d_csr_val.p);
+    PGPU_CHECK(cudaMemsetAsync(C.d_status.p, 0, sizeof(Status), s));
+    PGPU_CHECK(cudaMemsetAsync(C.d_coef.p, 0, ncoef * esz, s));
+    int launches = 4;
+    if (mixed)
+        k_fillin<float><<<2048, 256, 0, s>>>(C.nnz, C.d_vals.p, C.d_fill_dst.p, (float *)C.d_coef.p, C.d_status.p);
+    else
+        k_fillin<double><<<2048, 256, 0, s>>>(C.nnz, C.d_vals.p, C.d_fill_dst.p, (double *)C.d_coef.p, C.d_status.p);
+    int nl = 0;
+    rc = mixed ? run_factor<float>(C, fact, crit, &nl) : run_factor<double>(C, fact, crit, &nl);
+    if (rc) return rc;
+    PGPU_CHECK(cudaEventRecord(C.ev[1], s));
+    Status st;
+    PGPU_CHECK(cudaMemcpyAsync(&st, C.d_status.p, sizeof(Status), cudaMemcpyDeviceToHost, s));
+    PGPU_CHECK(cudaStreamSynchronize(s));
+    float ms = 0;
+    PGPU_CHECK(cudaEventElapsedTime(&ms, C.ev[0], C.ev[1]));
+    C.stats[0] = launches + nl;
+    C.stats[3] = ms;
+    C.iparm[PGPU_IPARM_STATIC_PIVOTING] = st.nbpivots;
+    const double fl = (fact == PGPU_FACT_GETRF) ? C.thflops_getrf : C.thflops_potrf;
+    C.dparm[PGPU_DPARM_FACT_TIME] = ms * 1e-3;
+    C.dparm[PGPU_DPARM_FACT_THFLOPS] = fl;
+    C.dparm[PGPU_DPARM_FACT_FLOPS] = fl / (ms * 1e-3) / 1e9;
+    C.coef_float = mixed;
+    C.fact_done = fact;
+    if (st.overflow) {
+        fprintf(stderr, "pastix_gpu: mixed-precision overflow during the matrix initialization\n");
+        C.fact_done = -1;
+        return PASTIX_GPU_ERR_INTERNAL;
+    }
+    if (st.negpivots) fprintf(stderr, "pastix_gpu: Negative diagonal term (%d)\n", st.negpivots);
+    if (st.nonfinite) {
+        fprintf(stderr, "pastix_gpu: non-finite diagonal term met in the factorization (%d)\n", st.nonfinite);
+        return PASTIX_GPU_ERR_INTERNAL;
+    }
+    return PASTIX_GPU_SUCCESS;
+}
+
+// --------------------------------------------------------------------------
+// Solve on a permuted device RHS block W (factor precision, ld = n).
+// --------------------------------------------------------------------------
+template <typename T>
+static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
+    const bool lu = (C.fact_done == PGPU_FACT_GETRF);
+    const T *coefL = reinterpret_cast<const T *>(C.d_coef.p);
+    const T *coefU = lu ? coefL + C.coefnbr : coefL;
+    cudaStream_t s = C.stream;
+    const int ldb = C.n;
+    int nl = 0;
+    for (int l = 0; l < C.nlevels; l++) {
+        const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
+        const int mw = C.lvl_maxw[l];
+        k_fwd_diag<T><<<ncb, 128, (size_t)mw * nrhs * sizeof(T), s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l],
+                                                                      coefL, W, ldb, nrhs, lu ? 1 : 0);
+        nl++;
+        const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
+        if (nch) {
+            k_fwd_off<T><<<nch, 256, (size_t)mw * nrhs * sizeof(T), s>>>(
+                C.meta, C.d_solve_chunks.p + C.solve_ptr[l], coefL, W, ldb, nrhs, SOLVE_ROWS_PER_CHUNK);
+            nl++;
+        }
+    }
+    for (int l = C.nlevels - 1; l >= 0; l--) {
+        const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
+        const int mw = C.lvl_maxw[l];
+        const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
+        if (nch) {
+            k_bwd_off<T><<<nch, 128, 0, s>>>(C.meta, C.d_solve_chunks.p + C.solve_ptr[l], coefU, W, ldb, nrhs,
+                                              SOLVE_ROWS_PER_CHUNK);
+            nl++;
+        }
+        k_bwd_diag<T><<<ncb, 128, (size_t)mw * nrhs * sizeof(T), s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l],
+                                                                      coefL, W, ldb, nrhs, lu ? 1 : 0);
+        nl++;
+    }
+    PGPU_CHECK(cudaGetLastError());
+    *launches += nl;
+    return PASTIX_GPU_SUCCESS;
+}
+
+static int ensure_work(pastix_gpu_t &C) {
+    const size_t need = (size_t)C.n * SOLVE_MAXRHS * sizeof(double);
+    if (C.d_work.n < need) {
+        C.d_work.release();
+        PGPU_CHECK(C.d_work.alloc(need));
+    }
+    if (C.d_rhs.n < (size_t)C.n * SOLVE_MAXRHS) PGPU_CHECK(C.d_rhs.alloc((size_t)C.n * SOLVE_MAXRHS));
+    return PASTIX_GPU_SUCCESS;
+}
+
+// Solve in place on a device FP64 block (user order, ld = ldb).
+static int solve_device_block(pastix_gpu_t &C, double *dB, int64_t ldb, int nrhs, int *launches) {
+    cudaStream_t s = C.stream;
+    const int n = C.n;
+    const int grid = std::min(4096, cdiv((int64_t)n * nrhs, 256));
+    int rc;
+    if (C.coef_float) {
+        float *W = reinterpret_cast<float *>(C.d_work.p);
+        k_permute<double, float><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, dB, ldb, W, n, 0);
+        rc = solve_permuted<float>(C, W, nrhs, launches);
+        if (rc) return rc;
+        k_permute<float, double><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, W, n, dB, ldb, 1);
+    } else {
+        double *W = reinterpret_cast<double *>(C.d_work.p);
+        k_permute<double, double><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, dB, ldb, W, n, 0);
+        rc = solve_permuted<double>(C, W, nrhs, launches);
+        if (rc) return rc;
+        k_permute<double, double><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, W, n, dB, ldb, 1);
+    }
+    *launches += 2;
+    PGPU_CHECK(cudaGetLastError());
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_solve(pastix_gpu_t *ctx, int64_t nrhs, void *B, int64_t ldb) {
+    if (!ctx || !B || nrhs <= 0 || ldb < ctx->n) return PASTIX_GPU_ERR_BADPARAMETER;
+    auto &C = *ctx;
+    if (C.fact_done < 0) return PASTIX_GPU_ERR_BADPARAMETER;
+    PGPU_CHECK(cudaSetDevice(C.device));
+    int rc = ensure_work(C);
+    if (rc) return rc;
+    cudaStream_t s = C.stream;
+    const bool dev = is_device_ptr(B);
+    int launches = 0;
+    PGPU_CHECK(cudaEventRecord(C.ev[2], s));
+    for (int64_t r0 = 0; r0 < nrhs; r0 += SOLVE_MAXRHS) {
+        const int nr = (int)std::min<int64_t>(SOLVE_MAXRHS, nrhs - r0);
+        double *hb = reinterpret_cast<double *>(B) + r0 * ldb;
+        double *db;
+        int64_t dld;
+        if (dev) {
+            db = hb;
+            dld = ldb;
+        } else {
+            db = C.d_rhs.p;
+            dld = C.n;
+            PGPU_CHECK(cudaMemcpy2DAsync(db, C.n * sizeof(double), hb, ldb * sizeof(double), C.n * sizeof(double),
+                                         nr, cudaMemcpyHostToDevice, s));
+        }
+        rc = solve_device_block(C, db, dld, nr, &launches);
+        if (rc) return rc;
+        if (!dev)
+            PGPU_CHECK(cudaMemcpy2DAsync(hb, ldb * sizeof(double), db, C.n * sizeof(double), C.n * sizeof(double),
+                                         nr, cudaMemcpyDeviceToHost, s));
+    }
+    PGPU_CHECK(cudaEventRecord(C.ev[3], s));
+    PGPU_CHECK(cudaStreamSynchronize(s));
+    float ms = 0;
+    PGPU_CHECK(cudaEventElapsedTime(&ms, C.ev[2], C.ev[3]));
+    C.stats[1] = launches;
+    C.stats[4] = ms;
+    C.dparm[PGPU_DPARM_SOLV_TIME] = ms * 1e-3;
+    return PASTIX_GPU_SUCCESS;
+}
+
+// --------------------------------------------------------------------------
+// Refinement (refinement/z_refine_grad.c:49 z_grad_smp, preconditioned CG).
+// Vectors in the user numbering (the SpMV matrix is permuted, so vectors are
+// permuted in and out of it).
+// --------------------------------------------------------------------------
+struct VecOps {
+    pastix_gpu_t &C;
+    int launches = 0;
+    double dot(const double *x, const double *y) {
+        const int nb = 256;
+        k_dot_partial<<<nb, RED_THREADS, 0, C.stream>>>(C.n, x, y, C.d_partial.p);
+        k_dot_final<<<1, RED_THREADS, 0, C.stream>>>(nb, C.d_partial.p, C.d_scalar.p, 0);
+        launches += 2;
+        double v = 0;
+        cudaMemcpyAsync(&v, C.d_scalar.p, sizeof(double), cudaMemcpyDeviceToHost, C.stream);
+        cudaStreamSynchronize(C.stream);
+        return v;
+    }
+    double norm(const double *x) { return std::sqrt(dot(x, nullptr)); }
+    void axpy(double a, const double *x, double *y) {
+        k_axpy<<<1024, 256, 0, C.stream>>>(C.n, a, x, y);
+        launches++;
+    }
+    void xpby(const double *z, double beta, double *p) {
+        k_xpby<<<1024, 256, 0, C.stream>>>(C.n, z, beta, p);
+        launches++;
+    }
+    void copy(const double *x, double *y) {
+        cudaMemcpyAsync(y, x, C.n * sizeof(double), cudaMemcpyDeviceToDevice, C.stream);
+    }
+    // y = alpha A x + beta y, in the user numbering: the CSR is permuted, so
+    // work on permuted copies held in d_gm.
+    void spmv(double alpha, const double *x, double beta, double *y) {
+        const int n = C.n;
+        double *xp = C.d_gm.p, *yp = C.d_gm.p + n;
+        const int grid = cdiv(n, 256);
+        k_permute<double, double><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, x, n, xp, n, 0);
+        if (beta != 0.0) k_permute<double, double><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, y, n, yp, n, 0);
+        k_spmv<<<cdiv((int64_t)n * 32, 256), 256, 0, C.stream>>>(n, C.d_csr_ptr.p, C.d_csr_col.p, C.d_csr_val.p,
+                                                                alpha, xp, beta, yp);
+        k_permute<double, double><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, yp, n, y, n, 1);
+        launches += 3 + (beta != 0.0);
+    }
+    int spsv(double *z) { return solve_device_block(C, z, C.n, 1, &launches); }
+};
+
+static int refine_cg(pastix_gpu_t &C, VecOps &V, const double *b, double *x, double eps, int itermax, int *iters,
+                     double *resid) {
+    const int n = C.n;
+    double *r = C.d_r.p, *z = C.d_z.p, *p = C.d_p.p, *ap = C.d_ap.p;
+    double normb = V.norm(b);
+    if (normb == 0.) normb = 1;
+    const double normx = V.norm(x);
+    V.copy(b, r);
+    if (normx > 0.) V.spmv(-1.0, x, 1.0, r);
+    double normr = V.norm(r);
+    double resid_b = normr / normb;
+    V.copy(r, z);
+    int rc = V.spsv(z);
+    if (rc) return rc;
+    V.copy(z, p);
+    int it = 0;
+    (void)n;
+    while (resid_b > eps && it < itermax) {
+        it++;
+        V.spmv(1.0, p, 0.0, ap);
+        double beta = V.dot(r, z);
+        double alpha = V.dot(ap, p);
+        alpha = beta / alpha;
+        V.axpy(alpha, p, x);
+        V.axpy(-alpha, ap, r);
+        V.copy(r, z);
+        rc = V.spsv(z);
+        if (rc) return rc;
+        alpha = V.dot(r, z);
+        beta = alpha / beta;
+        V.xpby(z, beta, p);
+        normr = V.norm(r);
+        resid_b = normr / normb;
+    }
+    *iters = it;
+    *resid = resid_b;
+    return PASTIX_GPU_SUCCESS;
+}
+
+static int ensure_refine_vectors(pastix_gpu_t &C) {
+    const size_t n = C.n;
+    if (C.d_r.n < n) {
+        PGPU_CHECK(C.d_r.alloc(n));
+        PGPU_CHECK(C.d_z.alloc(n));
+        PGPU_CHECK(C.d_p.alloc(n));
+        PGPU_CHECK(C.d_ap.alloc(n));
+        PGPU_CHECK(C.d_x.alloc(n));
+        PGPU_CHECK(C.d_gm.alloc(2 * n));
+    }
+    return ensure_work(C);
+}
+
+static int refine_impl(pastix_gpu_t &C, int64_t nrhs, const void *B, int64_t ldb, void *X, int64_t ldx) {
+    int rc = ensure_refine_vectors(C);
+    if (rc) return rc;
+    cudaStream_t s = C.stream;
+    double eps = C.dparm[PGPU_DPARM_EPSILON_REFINEMENT];
+    if (eps < 0.) eps = 1e-12;   // refinement/pastix_task_refine.c:131-140 (double input)
+    const int itermax = (int)C.iparm[PGPU_IPARM_ITERMAX];
+    const int method = (int)C.iparm[PGPU_IPARM_REFINEMENT];
+    if (method != PGPU_REFINE_CG) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    const bool bdev = is_device_ptr(B), xdev = is_device_ptr(X);
+    VecOps V{C};
+    int maxit = 0;
+    double maxres = 0;
+    PGPU_CHECK(cudaEventRecord(C.ev[4], s));
+    for (int64_t r = 0; r < nrhs; r++) {
+        const double *bcol = reinterpret_cast<const double *>(B) + r * ldb;
+        double *xcol = reinterpret_cast<double *>(X) + r * ldx;
+        double *db = C.d_rhs.p, *dx = C.d_x.p;
+        PGPU_CHECK(cudaMemcpyAsync(db, bcol, C.n * sizeof(double),
+                                   bdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+        PGPU_CHECK(cudaMemcpyAsync(dx, xcol, C.n * sizeof(double),
+                                   xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+        int it = 0;
+        double res = 0;
+        rc = refine_cg(C, V, db, dx, eps, itermax, &it, &res);
+        if (rc) return rc;
+        PGPU_CHECK(cudaMemcpyAsync(xcol, dx, C.n * sizeof(double),
+                                   xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+        maxit = std::max(maxit, it);
+        maxres = std::max(maxres, res);
+    }
+    PGPU_CHECK(cudaEventRecord(C.ev[5], s));
+    PGPU_CHECK(cudaStreamSynchronize(s));
+    float ms = 0;
+    PGPU_CHECK(cudaEventElapsedTime(&ms, C.ev[4], C.ev[5]));
+    C.stats[2] = V.launches;
+    C.stats[5] = ms;
+    C.iparm[PGPU_IPARM_NBITER] = maxit;
+    C.dparm[PGPU_DPARM_RELATIVE_ERROR] = maxres;
+    C.dparm[PGPU_DPARM_REFINE_TIME] = ms * 1e-3;
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_refine(pastix_gpu_t *ctx, int64_t nrhs, const void *B, int64_t ldb, void *X,
+                                 int64_t ldx) {
+    if (!ctx || !B || !X || nrhs <= 0 || ldb < ctx->n || ldx < ctx->n) return PASTIX_GPU_ERR_BADPARAMETER;
+    if (ctx->fact_done < 0) return PASTIX_GPU_ERR_BADPARAMETER;
+    PGPU_CHECK(cudaSetDevice(ctx->device));
+    return refine_impl(*ctx, nrhs, B, ldb, X, ldx);
+}
+
+extern "C" int pastix_gpu_solve_and_refine(pastix_gpu_t *ctx, int64_t nrhs, const void *B, int64_t ldb, void *X,
+                                           int64_t ldx) {
+    if (!ctx || !B || !X || nrhs <= 0 || ldb < ctx->n || ldx < ctx->n) return PASTIX_GPU_ERR_BADPARAMETER;
+    auto &C = *ctx;
+    if (C.fact_done < 0) return PASTIX_GPU_ERR_BADPARAMETER;
+    PGPU_CHECK(cudaSetDevice(C.device));
+    // X := B, solve in place, then refine
+    const bool bdev = is_device_ptr(B), xdev = is_device_ptr(X);
+    cudaMemcpyKind k = bdev ? (xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost)
+                            : (xdev ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost);
+    PGPU_CHECK(cudaMemcpy2DAsync(X, ldx * sizeof(double), B, ldb * sizeof(double), C.n * sizeof(double), nrhs, k,
+                                 C.stream));
+    PGPU_CHECK(cudaStreamSynchronize(C.stream));
+    int rc = pastix_gpu_solve(ctx, nrhs, X, ldx);
+    if (rc) return rc;
+    return refine_impl(C, nrhs, B, ldb, X, ldx);
+}
+
+extern "C" int pastix_gpu_get_params(pastix_gpu_t *ctx, int64_t *iparm, double *dparm) {
+    if (!ctx) return PASTIX_GPU_ERR_BADPARAMETER;
+    if (iparm) std::memcpy(iparm, ctx->iparm, sizeof(ctx->iparm));
+    if (dparm) std::memcpy(dparm, ctx->dparm, sizeof(ctx->dparm));
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_set_iparm(pastix_gpu_t *ctx, int index, int64_t value) {
+    if (!ctx || index < 0 || index >= PGPU_IPARM_SIZE) return PASTIX_GPU_ERR_BADPARAMETER;
+    ctx->iparm[index] = value;
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_set_dparm(pastix_gpu_t *ctx, int index, double value) {
+    if (!ctx || index < 0 || index >= PGPU_DPARM_SIZE) return PASTIX_GPU_ERR_BADPARAMETER;
+    ctx->dparm[index] = value;
+    return PASTIX_GPU_SUCCESS;
+}
+
+// Factors in the reference's 1D layout (column-major stride x width panels).
+template <typename T>
+static void host_relayout(const pastix_gpu_t &C, const std::vector<T> &dev, T *L, T *U, bool lu) {
+    int64_t off = 0;
+    for (int c = 0; c < C.cblknbr; c++) {
+        const int w = C.width[c], h = C.height[c], ld = C.ld[c];
+        const T *P = dev.data() + C.coefoff[c];
+        const T *PU = dev.data() + C.coefnbr + C.coefoff[c];
+        for (int j = 0; j < w; j++)
+            for (int i = 0; i < h; i++) {
+                if (L) L[off + (int64_t)j * h + i] = P[(int64_t)i * ld + j];
+                if (lu && U) U[off + (int64_t)j * h + i] = (i < w) ? P[(int64_t)j * ld + i] : PU[(int64_t)i * ld + j];
+            }
+        off += (int64_t)h * w;
+    }
+}
+
+extern "C" int pastix_gpu_coeftab(pastix_gpu_t *ctx, void *L, void *U) {
+    if (!ctx || ctx->fact_done < 0) return PASTIX_GPU_ERR_BADPARAMETER;
+    auto &C = *ctx;
+    PGPU_CHECK(cudaSetDevice(C.device));
+    const bool lu = (C.fact_done == PGPU_FACT_GETRF);
+    const size_t ncoef = (size_t)C.coefnbr * (lu ? 2 : 1);
+    if (C.coef_float) {
+        std::vector<float> h(ncoef);
+        PGPU_CHECK(cudaMemcpy(h.data(), C.d_coef.p, ncoef * sizeof(float), cudaMemcpyDeviceToHost));
+        host_relayout<float>(C, h, (float *)L, (float *)U, lu);
+    } else {
+        std::vector<double> h(ncoef);
+        PGPU_CHECK(cudaMemcpy(h.data(), C.d_coef.p, ncoef * sizeof(double), cudaMemcpyDeviceToHost));
+        host_relayout<double>(C, h, (double *)L, (double *)U, lu);
+    }
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_stats(pastix_gpu_t *ctx, double *stats) {
+    if (!ctx || !stats) return PASTIX_GPU_ERR_BADPARAMETER;
+    std::memcpy(stats, ctx->stats, sizeof(ctx->stats));
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" void pastix_gpu_finalize(pastix_gpu_t **pctx) {
+    if (!pctx || !*pctx) return;
+    pastix_gpu_t *C = *pctx;
+    cudaSetDevice(C->device);
+    if (C->stream) cudaStreamSynchronize(C->stream);
+    for (auto &e : C->ev) cudaEventDestroy(e);
+    if (C->stream) cudaStreamDestroy(C->stream);
+    delete C;   // every DArr member frees its device memory
+    *pctx = nullptr;
+}

@@ -1,0 +1,102 @@
+"""GPU parity: the CUDA factorization/solve against the reference's own CPU
+path (oracle/_ref) and the numpy restatement, on the same structure and
+seeded inputs.  Tolerances: FP64 factors agree to 1e-12 relative (max-norm
+over the factor); FP32 (mixed) factors to 5e-5 relative against the
+reference's own mixed factorization."""
+import numpy as np
+import pytest
+
+from pastix_b200 import matrices as M
+from tests import refutil as U
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ("lap6", lambda: M.laplacian_7pt(6), "potrf"),
+    ("lap20", lambda: M.laplacian_7pt(20), "potrf"),
+    ("diff14", lambda: M.diffusion_lognormal(14, 14, 14, 1.0, np.random.default_rng(3)), "potrf"),
+    ("diff2d", lambda: M.diffusion_lognormal(40, 33, 1, 0.5, np.random.default_rng(4)), "potrf"),
+    ("cd10", lambda: M.convdiff_upwind(10, 10, 10, 10.0), "getrf"),
+    ("cd9x7x5", lambda: M.convdiff_upwind(9, 7, 5, 10.0), "getrf"),
+]
+
+
+def _gpu_solver(system, st, fact, mixed=False, refine=None):
+    from pastix_b200 import gpu as G
+    s = G.Solver()
+    s.set_iparm(G.IPARM_FACTORIZATION, G.FACT[fact])
+    s.set_iparm(G.IPARM_MIXED, 1 if mixed else 0)
+    if refine:
+        s.set_iparm(G.IPARM_REFINEMENT, G.REFINE[refine])
+    s.set_structure(U.gpu_structure(system, st))
+    s.set_spm(system)
+    return s
+
+
+@pytest.mark.parametrize("name,make,fact", CASES, ids=[c[0] for c in CASES])
+def test_factor_matches_reference(name, make, fact):
+    A = make()
+    ref, st = U.run_reference(A, fact)
+    g = U.gpu_structure(A, st)
+    lay = U.layout_of(g)
+    Lr, Ur = U.ref_coeftab_1d(ref, st, lay)
+    s = _gpu_solver(A, st, fact)
+    s.numfact(A.values)
+    Lg, Ug = s.coeftab()
+    mask = U.lower_mask(lay) if fact == "potrf" else np.ones(lay.off[-1], bool)
+    scale = np.abs(Lr).max()
+    assert np.abs(Lg - Lr)[mask].max() <= 1e-12 * scale
+    if fact == "getrf":
+        assert np.abs(Ug - Ur).max() <= 1e-12 * np.abs(Ur).max()
+    ip, dp = s.params()
+    assert ip[45] == ref.iparm("STATIC_PIVOTING")
+    assert abs(dp[23] - ref.dparm("A_NORM")) <= 1e-12 * ref.dparm("A_NORM")
+
+
+@pytest.mark.parametrize("name,make,fact", CASES, ids=[c[0] for c in CASES])
+def test_solve_matches_reference(name, make, fact):
+    A = make()
+    ref, st = U.run_reference(A, fact)
+    s = _gpu_solver(A, st, fact)
+    s.numfact(A.values)
+    rng = np.random.default_rng(7)
+    x, b = M.rhs_from_xtrue(A, 4, rng)
+    xg = s.solve(b)
+    xr = ref.solve(b)
+    assert np.abs(xg - xr).max() <= 1e-11 * np.abs(xr).max()
+    assert np.abs(xg - x).max() <= 1e-9
+
+
+@pytest.mark.parametrize("name,make,fact", [c for c in CASES if c[2] == "potrf"],
+                         ids=[c[0] for c in CASES if c[2] == "potrf"])
+def test_mixed_factor_matches_reference_mixed(name, make, fact):
+    A = make()
+    ref, st = U.run_reference(A, fact, mixed=True)
+    g = U.gpu_structure(A, st)
+    lay = U.layout_of(g)
+    Lr, _ = U.ref_coeftab_1d(ref, st, lay)
+    assert Lr.dtype == np.float32
+    s = _gpu_solver(A, st, fact, mixed=True)
+    s.numfact(A.values)
+    Lg, _ = s.coeftab()
+    assert Lg.dtype == np.float32
+    mask = U.lower_mask(lay)
+    assert np.abs(Lg.astype(np.float64) - Lr)[mask].max() <= 5e-5 * np.abs(Lr).max()
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_cg_refinement_reaches_1e12(mixed):
+    A = M.diffusion_lognormal(16, 16, 16, 1.0, np.random.default_rng(11))
+    ref, st = U.run_reference(A, "potrf", numfact=False)
+    s = _gpu_solver(A, st, "potrf", mixed=mixed, refine="cg")
+    s.numfact(A.values)
+    rng = np.random.default_rng(5)
+    x, b = M.rhs_from_xtrue(A, 2, rng)
+    xs = s.solve_and_refine(b)
+    Af = A.to_scipy_full()
+    r = b - Af @ xs
+    assert np.linalg.norm(r, axis=0).max() / np.linalg.norm(b, axis=0).min() <= 1e-12
+    bwd = np.abs(r).max() / (abs(Af).sum(axis=1).max() * np.abs(xs).max() + np.abs(b).max())
+    assert bwd <= 1e-12
+    ip, dp = s.params()
+    assert ip[52] >= (1 if mixed else 0)
