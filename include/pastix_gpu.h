@@ -177,6 +177,29 @@ PASTIX_GPU_API int pastix_gpu_coeftab( pastix_gpu_t *ctx, void *L, void *U );
  */
 PASTIX_GPU_API int pastix_gpu_stats( pastix_gpu_t *ctx, double *stats );
 
+/*
+ * Host analysis for a matrix on an nx x ny x nz grid (vertex x + nx*(y + ny*z)):
+ * the reference's grid nested dissection (pastixOrderGrid,
+ * order/order_grids.c:303) with the personal-ordering analysis that follows
+ * it (pastix_subtask_order, _symbfact, _reordering, _blend; the call sequence
+ * of example/ordering_grid.c:107-123).  Produces the tables
+ * pastix_gpu_structure() takes.  iparm may be NULL (reference defaults);
+ * IPARM_MIN/MAX_BLOCKSIZE, IPARM_TASKS2D_WIDTH, IPARM_REORDERING_SPLIT/STOP
+ * are read.  colptr/rowptr: 0-based CSC pattern (one triangle or both).
+ */
+typedef struct pastix_gpu_analysis_s pastix_gpu_analysis_t;
+PASTIX_GPU_API int pastix_gpu_analyze_grid( pastix_gpu_analysis_t **an, int64_t nx, int64_t ny, int64_t nz,
+                                            int64_t n, const int64_t *colptr, const int64_t *rowptr,
+                                            const int64_t *iparm );
+/* sizes[0..4] = n, cblknbr, bloknbr, brownbr, supernodes of the ordering */
+PASTIX_GPU_API int pastix_gpu_analysis_sizes( const pastix_gpu_analysis_t *an, int64_t *sizes );
+/* cblktab (cblknbr+1) x 4, bloktab bloknbr x 4, browtab, permtab/peritab (n),
+ * rangtab (supernodes+1) and treetab (supernodes) of the ordering; any may be NULL */
+PASTIX_GPU_API int pastix_gpu_analysis_export( const pastix_gpu_analysis_t *an, int64_t *cblktab,
+                                               int64_t *bloktab, int64_t *browtab, int64_t *permtab,
+                                               int64_t *peritab, int64_t *rangtab, int64_t *treetab );
+PASTIX_GPU_API void pastix_gpu_analysis_free( pastix_gpu_analysis_t **an );
+
 /* Release the device memory and the context (pastixFinalize, common/api.c:914). */
 PASTIX_GPU_API void pastix_gpu_finalize( pastix_gpu_t **ctx );
 
