@@ -1,0 +1,358 @@
+#!/usr/bin/env python3
+"""Benchmark: time-to-solution at backward error <= 1e-12 on one B200,
+FP32 factorization + FP64 CG refinement ("mixed") vs the FP64 factorization.
+
+Workload (default): 3D 7-point variable-coefficient diffusion on a 100^3 grid
+(n = 1e6, SPD, face coefficients lognormal(0, 1) per edge, seeded), Cholesky,
+one right-hand side b = A x_true with x_true ~ U[-1, 1].  The analysis is the
+grid nested dissection of the reference (done once, not timed).  One step =
+numerical factorization + solve + refinement to ||r||_2/||b||_2 <= 1e-12.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config 1..5] [--scale S]
+
+Prints one JSON line (rank 0).  `value`: mixed-arm time-to-solution with the
+matrix values and b already in HBM (CUDA events on the library's stream);
+`e2e`: the same through the C ABI with host buffers (values, b in; x out).
+With --impl reference the reference's own CPU path (oracle/_ref, static
+scheduler, all host cores) is timed on a bounded sample (the same problem on
+a smaller grid) and scaled to the full problem by the ratio of factorization
+flops; N > 1 runs independent replicas (the single-system path does not
+shard), rank 0 reports the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from pastix_b200 import matrices as M  # noqa: E402
+
+METRIC = "time-to-solution at backward err <=1e-12: mixed vs FP64 factor, 1 B200"
+CONFIG_DESC = {
+    1: "laplacian_7pt 20^3 (n=8000), LLt, CG to 1e-12, nrhs 1",
+    2: "diffusion_lognormal(sigma=1) 100^3 (n=1e6), LLt, FP32 factor + FP64 CG vs FP64 factor, nrhs 1",
+    3: "convdiff_upwind(Pe=10) 80^3 (n=512000), LU, GMRES(30), nrhs 4",
+    4: "512 x diffusion_lognormal(sigma=0.5) 2D sides U{32..256}, LLt, nrhs 8",
+    5: "magnetic_laplacian 60^3 - 0.5 I, LDLh complex, GMRES, nrhs 4",
+}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", type=int, default=2)
+    p.add_argument("--scale", type=float, default=1.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-scale", type=float, default=0.5)
+    return p.parse_args()
+
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def reduce_max(pg, v, local):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda:%d" % local)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.rows = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            for line in out.strip().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    self.rows.append(f)
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def errors(A, b, x, xtrue):
+    Af = A.to_scipy_full()
+    r = b - Af @ x
+    anorm_inf = abs(Af).sum(axis=1).max()
+    bwd = float(np.abs(r).max() / (anorm_inf * np.abs(x).max() + np.abs(b).max()))
+    rel = float((np.linalg.norm(r, axis=0) / np.linalg.norm(b, axis=0)).max())
+    fwd = float(np.abs(x - xtrue).max() / np.abs(xtrue).max())
+    return {"backward_error": bwd, "relative_residual": rel, "forward_error": fwd}
+
+
+def fma_peaks():
+    import ctypes as C
+    lib = C.CDLL(os.path.join(ROOT, "pastix_b200", "lib", "libpgpu_peak.so"))
+    lib.pgpu_peak_fma_tflops.restype = C.c_double
+    lib.pgpu_peak_fma_tflops.argtypes = [C.c_int, C.c_int]
+    return {"fp64_fma_tflops": lib.pgpu_peak_fma_tflops(0, 20000),
+            "fp32_fma_tflops": lib.pgpu_peak_fma_tflops(1, 40000)}
+
+
+# ---------------------------------------------------------------------------
+def run_arm(A, st, b, mixed, steps, warmup, fact, refine):
+    """One arm (mixed or FP64): device-resident timing, then e2e timing."""
+    import torch
+    from pastix_b200 import gpu as G
+    s = G.Solver(device=torch.cuda.current_device())
+    s.set_iparm(G.IPARM_FACTORIZATION, G.FACT[fact])
+    s.set_iparm(G.IPARM_MIXED, 1 if mixed else 0)
+    s.set_iparm(G.IPARM_REFINEMENT, G.REFINE[refine])
+    s.set_dparm(G.DPARM_EPSILON_REFINEMENT, 1e-12)
+    s.set_structure(st)
+    s.set_spm(A)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_vals = torch.from_numpy(np.ascontiguousarray(A.values)).to(dev)
+    d_b = torch.from_numpy(np.asfortranarray(b).reshape(-1, order="F").copy()).to(dev)
+    d_x = torch.zeros_like(d_b)
+    nrhs = b.shape[1]
+
+    def step_resident():
+        s.numfact(d_vals)
+        from pastix_b200.gpu import load, _p, _check
+        rc = load().pastix_gpu_solve_and_refine(s._h, nrhs, _p(d_b), A.n, _p(d_x), A.n)
+        _check("pastix_gpu_solve_and_refine", rc)
+        st_ = s.stats()
+        ip, dp = s.params()
+        return st_, ip, dp
+
+    for _ in range(warmup):
+        step_resident()
+    torch.cuda.synchronize()
+    per = []
+    launches = 0
+    gemm_ms = gemm_flops = 0.0
+    iters = []
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        st_, ip, dp = step_resident()
+        per.append(st_["numfact_ms"] + st_["solve_ms"] + st_["refine_ms"])
+        launches += int(st_["numfact_launches"] + st_["solve_launches"] + st_["refine_launches"])
+        gemm_ms += st_["gemm_ms"]
+        gemm_flops += st_["gemm_flops"]
+        iters.append(int(ip[G.IPARM_NBITER]))
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / steps
+    last = dict(st_)
+    x = d_x.cpu().numpy().reshape(A.n, nrhs, order="F")
+    # e2e through the C ABI with host buffers
+    e2e = []
+    xh = None
+    for _ in range(max(1, steps)):
+        t = time.perf_counter()
+        s.numfact(A.values)
+        xh = s.solve_and_refine(b)
+        e2e.append(time.perf_counter() - t)
+    s.close()
+    return {
+        "device_s": float(np.median(per)) / 1e3, "device_s_all": [p / 1e3 for p in per], "wall_s": wall,
+        "e2e_s": float(np.median(e2e)), "launches_per_step": launches / steps, "launches": launches,
+        "gemm_ms_per_step": gemm_ms / steps, "gemm_flops_per_step": gemm_flops / steps,
+        "refine_iters": iters[-1], "factor_ms": last["numfact_ms"], "solve_ms": last["solve_ms"],
+        "refine_ms": last["refine_ms"], "diag_ms": last["diag_ms"], "trsm_ms": last["trsm_ms"],
+        "fact_gflops": float(dp[G.DPARM_FACT_FLOPS]), "thflops": float(dp[G.DPARM_FACT_THFLOPS]),
+        "x": x, "x_e2e": xh,
+    }
+
+
+def cpu_reference_sample(cfg, scale, sample_scale, fact, refine, mixed, steps, warmup, nthreads):
+    """Reference CPU path on the same problem at `sample_scale` of the grid,
+    scaled to the full problem by the factorization-flop ratio."""
+    from oracle import pastix_ref as R
+    systems, _ = M.config(cfg, scale=scale * sample_scale, seed=0)
+    As = systems[0]
+    rng = np.random.default_rng(1)
+    xs, bs = M.rhs_from_xtrue(As, 1, rng)
+    r = R.RefSolver(As, fact=fact, nthreads=nthreads, mixed=mixed, refine=refine, eps_refine=1e-12)
+    r.analyze()
+    times = []
+    for i in range(warmup + steps):
+        t = time.perf_counter()
+        r.numfact()
+        x0 = r.solve(bs)
+        x1 = r.refine(bs, x0)
+        dt = time.perf_counter() - t
+        if i >= warmup:
+            times.append(dt)
+    thf = r.dparm("FACT_THFLOPS")
+    err = errors(As, bs, x1, xs)
+    r.close()
+    return float(np.median(times)), thf, As.grid, err
+
+
+def main():
+    args = parse()
+    rank, world, local, pg = dist_setup(args)
+    cfg = args.config
+    fact = {1: "potrf", 2: "potrf", 3: "getrf", 4: "potrf", 5: "hetrf"}[cfg]
+    refine = {1: "cg", 2: "cg", 3: "gmres", 4: "cg", 5: "gmres"}[cfg]
+    systems, meta = M.config(cfg, scale=args.scale, seed=0)
+    A = systems[0]
+    rng = np.random.default_rng(1)
+    xtrue, b = M.rhs_from_xtrue(A, meta["nrhs"] if cfg != 2 else 1, rng)
+    config = {"workload": CONFIG_DESC[cfg] + ("" if args.scale == 1.0 else " scaled %.2f" % args.scale),
+              "grid": list(A.grid), "n": A.n, "nnz": A.nnz, "nrhs": int(b.shape[1]),
+              "ordering": "reference grid nested dissection (pastixOrderGrid; Scotch unavailable)",
+              "l2": "inputs larger than L2 (coeftab > 126 MB), no flush",
+              "parallelism": "replicas" if world > 1 else "1 GPU"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        nth = os.cpu_count() or 1
+        t, thf_s, grid_s, err = cpu_reference_sample(cfg, args.scale, args.cpu_sample_scale, fact, refine, True,
+                                                     args.steps, args.warmup, nth)
+        # full-problem flops from the reference's own analysis (DPARM_FACT_THFLOPS)
+        from oracle import pastix_ref as R
+        rf = R.RefSolver(A, fact=fact, nthreads=nth)
+        rf.analyze()
+        thf_full = rf.dparm("FACT_THFLOPS")
+        rf.close()
+        value = t * thf_full / thf_s
+        line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 factor + f64 refine",
+                "data": "synthetic (seeded)", "config": config,
+                "cpu_baseline": {"value": value, "unit": "s", "cores": nth, "kind": "reference",
+                                 "sample": "reference CPU path (static scheduler, %d threads, OpenBLAS seq.) on the "
+                                           "same problem on a %s grid: %.2f s measured, scaled by factorization "
+                                           "flops %.3e/%.3e" % (nth, "x".join(map(str, grid_s)), t, thf_full, thf_s),
+                                 "errors": err},
+                "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    from pastix_b200 import analysis
+    t_an = time.perf_counter()
+    st = analysis.analyze(A)
+    t_an = time.perf_counter() - t_an
+    peaks = fma_peaks() if rank == 0 else {}
+    barrier(pg)
+    with ClockSampler(local) as clk:
+        mixed = run_arm(A, st, b, True, args.steps, args.warmup, fact, refine)
+        fp64 = run_arm(A, st, b, False, args.steps, args.warmup, fact, refine)
+    barrier(pg)
+    value = reduce_max(pg, mixed["device_s"], local)
+    e2e_v = reduce_max(pg, mixed["e2e_s"], local)
+    fp64_v = reduce_max(pg, fp64["device_s"], local)
+    if rank != 0:
+        return
+    err_m = errors(A, b, mixed["x"], xtrue)
+    err_d = errors(A, b, fp64["x"], xtrue)
+    err_e = errors(A, b, mixed["x_e2e"], xtrue)
+    g_ach = mixed["gemm_flops_per_step"] / (mixed["gemm_ms_per_step"] * 1e-3) / 1e12
+    peak32 = peaks.get("fp32_fma_tflops")
+    g64 = fp64["gemm_flops_per_step"] / (fp64["gemm_ms_per_step"] * 1e-3) / 1e12
+    peak64 = peaks.get("fp64_fma_tflops")
+    line = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 factor + f64 refine", "data": "synthetic (seeded)",
+        "config": config,
+        "fp64": {"value": fp64_v, "unit": "s", "e2e_s": fp64["e2e_s"], "factor_ms": fp64["factor_ms"],
+                 "solve_ms": fp64["solve_ms"], "refine_ms": fp64["refine_ms"], "refine_iters": fp64["refine_iters"],
+                 "fact_gflops": fp64["fact_gflops"], "errors": err_d,
+                 "roofline_gemm": {"bound": "fp64 fma", "achieved": g64, "peak": peak64, "unit": "TFLOP/s",
+                                   "frac": g64 / peak64 if peak64 else None,
+                                   "peak_source": "measured FP64 FMA microbenchmark (pastix_b200/csrc/peak.cu)"}},
+        "mixed": {"factor_ms": mixed["factor_ms"], "solve_ms": mixed["solve_ms"], "refine_ms": mixed["refine_ms"],
+                  "diag_ms": mixed["diag_ms"], "trsm_ms": mixed["trsm_ms"], "gemm_ms": mixed["gemm_ms_per_step"],
+                  "refine_iters": mixed["refine_iters"], "fact_gflops": mixed["fact_gflops"], "errors": err_m,
+                  "wall_s": mixed["wall_s"], "device_s_all": mixed["device_s_all"]},
+        "mixed_speedup_vs_fp64": fp64_v / value,
+        "roofline": {"bound": "tensor", "kernel": "k_gemm_scatter (update GEMM + scatter-add), FP32 FMA",
+                     "achieved": g_ach, "peak": peak32, "unit": "TFLOP/s",
+                     "frac": g_ach / peak32 if peak32 else None, "traffic": None,
+                     "peak_source": "measured FP32 FMA microbenchmark (pastix_b200/csrc/peak.cu); "
+                                    "MEASURED_PEAKS.json has no FP32/FP64 CUDA-core peak",
+                     "algorithmic_flops_per_step": mixed["gemm_flops_per_step"]},
+        "e2e": {"value": e2e_v, "unit": "s", "h2d_bytes_per_step": int(A.nnz * 8 + b.size * 8),
+                "d2h_bytes_per_step": int(b.size * 8), "errors": err_e},
+        "gpu_launches": int(mixed["launches"]),
+        "analysis_s": t_an, "peaks": peaks,
+    }
+    line["clocks"] = clk.summary()
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            nth = os.cpu_count() or 1
+            t, thf_s, grid_s, err = cpu_reference_sample(cfg, args.scale, args.cpu_sample_scale, fact, refine,
+                                                         True, 1, 0, nth)
+            v = t * mixed["thflops"] / thf_s
+            line["cpu_baseline"] = {"value": v, "unit": "s", "cores": nth, "kind": "reference",
+                                    "sample": "reference CPU mixed path (static scheduler, %d threads) on the same "
+                                              "problem on a %s grid: %.2f s, scaled by factorization flops "
+                                              "%.3e/%.3e" % (nth, "x".join(map(str, grid_s)), t,
+                                                             mixed["thflops"], thf_s),
+                                    "errors": err}
+        except Exception as e:  # the oracle may be absent on a fresh checkout
+            line["cpu_baseline"] = {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": "unavailable: %s" % e}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -174,6 +174,10 @@ PASTIX_GPU_API int pastix_gpu_coeftab( pastix_gpu_t *ctx, void *L, void *U );
  *   stats[3] numfact ms, stats[4] solve ms, stats[5] refine ms
  *   stats[6] update-GEMM ms inside numfact (CUDA events around those launches)
  *   stats[7] update-GEMM launches inside numfact
+ *   stats[8] diagonal-factorization ms, stats[9] panel-TRSM ms inside numfact
+ *   stats[10] algorithmic flops of the update GEMMs (sum of 2 M N K)
+ *   stats[11] reserved
+ * (12 doubles)
  */
 PASTIX_GPU_API int pastix_gpu_stats( pastix_gpu_t *ctx, double *stats );
 

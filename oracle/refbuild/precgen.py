@@ -50,6 +50,7 @@ NORMAL = [
     ("LAPACKE_sorgqr", "LAPACKE_dorgqr", "LAPACKE_cungqr", r"\bLAPACKE_zungqr"),
     ("LAPACKE_sorglq", "LAPACKE_dorglq", "LAPACKE_cunglq", r"\bLAPACKE_zunglq"),
     ("LAPACKE_slag2d", "LAPACKE_dlag2s", "LAPACKE_clag2z", r"\bLAPACKE_zlag2c"),
+    ("LAPACKE_slag2d", "LAPACKE_slag2d", "LAPACKE_clag2z", r"\bLAPACKE_clag2z"),
     ("FLOPS_SORMQR", "FLOPS_DORMQR", "FLOPS_CUNMQR", r"\bFLOPS_ZUNMQR\b"),
     ("FLOPS_SORMLQ", "FLOPS_DORMLQ", "FLOPS_CUNMLQ", r"\bFLOPS_ZUNMLQ\b"),
     ("FLOPS_SORGQR", "FLOPS_DORGQR", "FLOPS_CUNGQR", r"\bFLOPS_ZUNGQR\b"),

@@ -14,6 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libpastix_gpu.so")
+PEAKLIB = os.path.join(LIBDIR, "libpgpu_peak.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["pastix_gpu.cu", "pgpu_analysis.cpp"]
@@ -49,6 +50,8 @@ def build(force=False, verbose=False):
     os.replace(tmp, LIB)
     for o in objs:
         os.remove(o)
+    # bench-only helper: FMA peak microbenchmark
+    subprocess.check_call([NVCC] + ARCH + FLAGS + ["-shared", "-o", PEAKLIB, os.path.join(CSRC, "peak.cu")])
     return LIB
 
 

@@ -119,7 +119,10 @@ struct pastix_gpu_s {
     DArr<double> d_partial, d_scalar;
     DArr<unsigned char> d_work;   // solve workspace (n x 16 in factor precision)
     DArr<double> d_rhs, d_x, d_r, d_z, d_p, d_ap, d_gm;   // refinement vectors
-    double stats[8] = {0};
+    DArr<double> d_sr_b, d_sr_x;   // solve_and_refine staging of host B / X
+    std::vector<cudaEvent_t> evpool;   // per-launch timing events
+    double gemm_flops[5] = {0};        // update-GEMM flops per factotype
+    double stats[12] = {0};
 };
 
 // --------------------------------------------------------------------------
@@ -408,6 +411,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fact) {
     const bool lu = (fact == PGPU_FACT_GETRF);
     std::vector<int4> tiles, trsm;
     std::vector<GemmTask> tasks;
+    double gflops = 0;
     C.tile_ptr.assign(C.nlevels + 1, 0);
     C.trsm_ptr.assign(C.nlevels + 1, 0);
     for (int l = 0; l < C.nlevels; l++) {
@@ -427,6 +431,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fact) {
                     if (M <= 0) return;
                     const int id = (int)tasks.size();
                     tasks.push_back(GemmTask{c, b, f, arow0, M, flags});
+                    gflops += 2.0 * M * N * w;
                     for (int tm = 0; tm < cdiv(M, GEMM_TM); tm++)
                         for (int tn = 0; tn < cdiv(N, GEMM_TN); tn++) {
                             if ((flags & 8) && tm < tn) continue;   // strictly upper tiles of the diagonal block
@@ -450,13 +455,44 @@ static int build_fact_plan(pastix_gpu_t &C, int fact) {
     PGPU_CHECK(C.d_tasks.upload(tasks, s));
     PGPU_CHECK(cudaStreamSynchronize(s));
     C.plan_fact = fact;
+    C.gemm_flops[fact] = gflops;
     return PASTIX_GPU_SUCCESS;
 }
 
 static const int DIAG_SMEM_BYTES = 96 * 1024;
 
+// Per-launch timing: one event recorded before every launch (and one after
+// the last), so launch i took ev[i+1] - ev[i]; kinds[i] says which phase.
+struct LaunchTimer {
+    pastix_gpu_t &C;
+    std::vector<int> kinds;
+    int used = 0;
+    explicit LaunchTimer(pastix_gpu_t &c) : C(c) {}
+    cudaError_t mark(int kind) {
+        if (used >= (int)C.evpool.size()) {
+            cudaEvent_t e;
+            cudaError_t r = cudaEventCreate(&e);
+            if (r != cudaSuccess) return r;
+            C.evpool.push_back(e);
+        }
+        kinds.push_back(kind);
+        return cudaEventRecord(C.evpool[used++], C.stream);
+    }
+    // after the stream was synchronized: accumulate ms per kind
+    void collect(double *ms, int nkind) {
+        for (int k = 0; k < nkind; k++) ms[k] = 0;
+        for (int i = 0; i + 1 < used; i++) {
+            float t = 0;
+            if (kinds[i] >= 0 && kinds[i] < nkind && cudaEventElapsedTime(&t, C.evpool[i], C.evpool[i + 1]) == cudaSuccess)
+                ms[kinds[i]] += t;
+        }
+    }
+};
+
+enum { PH_DIAG = 0, PH_TRSM = 1, PH_GEMM = 2, PH_END = 3 };
+
 template <typename T>
-static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches) {
+static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, LaunchTimer &tm) {
     const bool lu = (fact == PGPU_FACT_GETRF);
     T *coefL = reinterpret_cast<T *>(C.d_coef.p);
     T *coefU = lu ? coefL + C.coefnbr : coefL;
@@ -465,9 +501,7 @@ static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches) {
     auto kdiag = lu ? k_diag_factor<T, true> : k_diag_factor<T, false>;
     PGPU_CHECK(cudaFuncSetAttribute(kdiag, cudaFuncAttributeMaxDynamicSharedMemorySize, DIAG_SMEM_BYTES));
     PGPU_CHECK(cudaFuncSetAttribute(k_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    int nl = 0;
-    float gemm_ms = 0.f;
-    int ngemm = 0;
+    int nl = 0, ngemm = 0;
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
@@ -475,24 +509,27 @@ static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches) {
         // its widest one does; otherwise the cblks that fit still use it
         const int sw = std::min(mw, smem_w);
         size_t dsm = (size_t)sw * sw * sizeof(T);
+        PGPU_CHECK(tm.mark(PH_DIAG));
         kdiag<<<ncb, 256, dsm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, crit, sw * sw,
                                     C.d_status.p);
         nl++;
         const int ntr = C.trsm_ptr[l + 1] - C.trsm_ptr[l];
         if (ntr) {
             size_t tsm = (size_t)(TRSM_ROWS + 1) * mw * sizeof(T);
+            PGPU_CHECK(tm.mark(PH_TRSM));
             k_trsm<T><<<ntr, 256, tsm, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], coefL, coefU);
             nl++;
         }
         const int nti = C.tile_ptr[l + 1] - C.tile_ptr[l];
         if (nti) {
+            PGPU_CHECK(tm.mark(PH_GEMM));
             k_gemm_scatter<T><<<nti, 256, 0, s>>>(C.meta, C.d_tiles.p + C.tile_ptr[l], C.d_tasks.p, coefL, coefU);
             nl++;
             ngemm++;
         }
     }
+    PGPU_CHECK(tm.mark(PH_END));
     PGPU_CHECK(cudaGetLastError());
-    (void)gemm_ms;
     *launches = nl;
     C.stats[7] = ngemm;
     return PASTIX_GPU_SUCCESS;
@@ -552,7 +589,8 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     else
         k_fillin<double><<<2048, 256, 0, s>>>(C.nnz, C.d_vals.p, C.d_fill_dst.p, (double *)C.d_coef.p, C.d_status.p);
     int nl = 0;
-    rc = mixed ? run_factor<float>(C, fact, crit, &nl) : run_factor<double>(C, fact, crit, &nl);
+    LaunchTimer tm(C);
+    rc = mixed ? run_factor<float>(C, fact, crit, &nl, tm) : run_factor<double>(C, fact, crit, &nl, tm);
     if (rc) return rc;
     PGPU_CHECK(cudaEventRecord(C.ev[1], s));
     Status st;
@@ -562,6 +600,14 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     PGPU_CHECK(cudaEventElapsedTime(&ms, C.ev[0], C.ev[1]));
     C.stats[0] = launches + nl;
     C.stats[3] = ms;
+    {
+        double ph[3];
+        tm.collect(ph, 3);
+        C.stats[8] = ph[PH_DIAG];
+        C.stats[9] = ph[PH_TRSM];
+        C.stats[6] = ph[PH_GEMM];
+        C.stats[10] = C.gemm_flops[fact];
+    }
     C.iparm[PGPU_IPARM_STATIC_PIVOTING] = st.nbpivots;
     const double fl = (fact == PGPU_FACT_GETRF) ? C.thflops_getrf : C.thflops_potrf;
     C.dparm[PGPU_DPARM_FACT_TIME] = ms * 1e-3;
@@ -854,16 +900,32 @@ extern "C" int pastix_gpu_solve_and_refine(pastix_gpu_t *ctx, int64_t nrhs, cons
     auto &C = *ctx;
     if (C.fact_done < 0) return PASTIX_GPU_ERR_BADPARAMETER;
     PGPU_CHECK(cudaSetDevice(C.device));
-    // X := B, solve in place, then refine
     const bool bdev = is_device_ptr(B), xdev = is_device_ptr(X);
-    cudaMemcpyKind k = bdev ? (xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost)
-                            : (xdev ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost);
-    PGPU_CHECK(cudaMemcpy2DAsync(X, ldx * sizeof(double), B, ldb * sizeof(double), C.n * sizeof(double), nrhs, k,
-                                 C.stream));
-    PGPU_CHECK(cudaStreamSynchronize(C.stream));
-    int rc = pastix_gpu_solve(ctx, nrhs, X, ldx);
+    if (bdev && xdev) {
+        // X := B, solve in place, then refine -- all on the device
+        PGPU_CHECK(cudaMemcpy2DAsync(X, ldx * sizeof(double), B, ldb * sizeof(double), C.n * sizeof(double), nrhs,
+                                     cudaMemcpyDeviceToDevice, C.stream));
+        int rc = pastix_gpu_solve(ctx, nrhs, X, ldx);
+        if (rc) return rc;
+        return refine_impl(C, nrhs, B, ldb, X, ldx);
+    }
+    // host buffers: B crosses once, X comes back once
+    if (C.d_sr_b.n < (size_t)C.n * nrhs) {
+        PGPU_CHECK(C.d_sr_b.alloc((size_t)C.n * nrhs));
+        PGPU_CHECK(C.d_sr_x.alloc((size_t)C.n * nrhs));
+    }
+    double *db = C.d_sr_b.p, *dx = C.d_sr_x.p;
+    PGPU_CHECK(cudaMemcpy2DAsync(db, C.n * sizeof(double), B, ldb * sizeof(double), C.n * sizeof(double), nrhs,
+                                 bdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, C.stream));
+    PGPU_CHECK(cudaMemcpyAsync(dx, db, (size_t)C.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, C.stream));
+    int rc = pastix_gpu_solve(ctx, nrhs, dx, C.n);
     if (rc) return rc;
-    return refine_impl(C, nrhs, B, ldb, X, ldx);
+    rc = refine_impl(C, nrhs, db, C.n, dx, C.n);
+    if (rc) return rc;
+    PGPU_CHECK(cudaMemcpy2DAsync(X, ldx * sizeof(double), dx, C.n * sizeof(double), C.n * sizeof(double), nrhs,
+                                 xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, C.stream));
+    PGPU_CHECK(cudaStreamSynchronize(C.stream));
+    return PASTIX_GPU_SUCCESS;
 }
 
 extern "C" int pastix_gpu_get_params(pastix_gpu_t *ctx, int64_t *iparm, double *dparm) {
@@ -932,6 +994,7 @@ extern "C" void pastix_gpu_finalize(pastix_gpu_t **pctx) {
     cudaSetDevice(C->device);
     if (C->stream) cudaStreamSynchronize(C->stream);
     for (auto &e : C->ev) cudaEventDestroy(e);
+    for (auto &e : C->evpool) cudaEventDestroy(e);
     if (C->stream) cudaStreamDestroy(C->stream);
     delete C;   // every DArr member frees its device memory
     *pctx = nullptr;

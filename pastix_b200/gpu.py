@@ -125,10 +125,10 @@ class Solver:
         return ip, dp
 
     def stats(self):
-        s = np.zeros(8, np.float64)
+        s = np.zeros(12, np.float64)
         _check("pastix_gpu_stats", load().pastix_gpu_stats(self._h, _p(s)))
         keys = ["numfact_launches", "solve_launches", "refine_launches", "numfact_ms", "solve_ms",
-                "refine_ms", "gemm_ms", "gemm_launches"]
+                "refine_ms", "gemm_ms", "gemm_launches", "diag_ms", "trsm_ms", "gemm_flops", "reserved"]
         return dict(zip(keys, s.tolist()))
 
     # -- structure / pattern -----------------------------------------------
