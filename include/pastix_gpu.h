@@ -137,6 +137,33 @@ PASTIX_GPU_API int pastix_gpu_numfact( pastix_gpu_t *ctx, const void *values );
 PASTIX_GPU_API int pastix_gpu_solve( pastix_gpu_t *ctx, int64_t nrhs, void *B, int64_t ldb );
 
 /*
+ * Allocation-free solve: A X = B in place for `nrhs` right-hand sides that
+ * already live in device memory (dB, column-major, leading dimension ldb),
+ * using the factors of the last pastix_gpu_numfact.  No counterpart in the
+ * reference: it exists for callers that cannot let a library allocate device
+ * memory in the middle of their work -- applications whose own pool
+ * allocator has already reserved the GPU's memory, and solve loops that must
+ * not be stalled by cudaMalloc/cudaFree, which can synchronize the device.
+ *
+ * The call allocates nothing.  Its scratch (the permuted right-hand sides in
+ * factor precision) is a fixed array of PASTIX_GPU_NOALLOC_SCRATCH_BYTES
+ * (16 MiB) in the library's device memory, which every GPU that loads the
+ * library holds until the process exits.  It holds up to 16 right-hand sides
+ * at a time, so n * min(nrhs, 16) * (8 for FP64 factors, 4 for FP32) must not
+ * exceed 16 MiB (e.g. n <= 131072 for 16 FP64 right-hand sides, n <= 2097152
+ * for one); larger requests return PASTIX_GPU_ERR_BADPARAMETER without doing
+ * any work.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, once per device); make that first call before any
+ * stream capture.  All calls share the one array and it keeps the contents of
+ * the last call (nothing needs clearing: every element used is written first),
+ * so calls that overlap on the GPU -- from two contexts, threads or streams on
+ * the same device -- race and must be serialized by the caller.
+ * Returns when the solution is in dB.
+ */
+#define PASTIX_GPU_NOALLOC_SCRATCH_BYTES ( (size_t)16 << 20 )
+PASTIX_GPU_API int pastix_gpu_solve_noalloc( pastix_gpu_t *ctx, int64_t nrhs, void *dB, int64_t ldb );
+
+/*
  * Iterative refinement of X for A X = B (CG or GMRES, per
  * iparm[IPARM_REFINEMENT]; FP64 residuals, preconditioned by the factors)
  * to dparm[DPARM_EPSILON_REFINEMENT].  Replaces pastix_task_refine

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 using namespace pgpu;
@@ -742,6 +743,83 @@ extern "C" int pastix_gpu_solve(pastix_gpu_t *ctx, int64_t nrhs, void *B, int64_
     C.stats[1] = launches;
     C.stats[4] = ms;
     C.dparm[PGPU_DPARM_SOLV_TIME] = ms * 1e-3;
+    return PASTIX_GPU_SUCCESS;
+}
+
+// --------------------------------------------------------------------------
+// Allocation-free solve (pastix_gpu_solve_noalloc): the permuted right-hand
+// sides live in this file-scope device array instead of a cudaMalloc'ed
+// workspace.  In host code `g_noalloc_scratch` only names the symbol; its
+// device address comes from cudaGetSymbolAddress, looked up once per device
+// (with that device current) on the first call there.
+// --------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[PASTIX_GPU_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+const int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
+}  // namespace
+
+// Device address of the scratch array on `dev` (the current device).
+static int noalloc_scratch_address(int dev, void **addr) {
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return PASTIX_GPU_ERR_INTERNAL;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            fprintf(stderr, "pastix_gpu_solve_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+            return PASTIX_GPU_ERR_INTERNAL;
+        }
+        g_noalloc_addr[dev] = p;
+    }
+    *addr = g_noalloc_addr[dev];
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_solve_noalloc(pastix_gpu_t *ctx, int64_t nrhs, void *dB, int64_t ldb) {
+    if (!ctx || !dB || nrhs <= 0 || ldb < ctx->n) return PASTIX_GPU_ERR_BADPARAMETER;
+    auto &C = *ctx;
+    if (C.fact_done < 0) return PASTIX_GPU_ERR_BADPARAMETER;
+    const size_t esz = C.coef_float ? sizeof(float) : sizeof(double);
+    const size_t need = (size_t)C.n * (size_t)std::min<int64_t>(nrhs, SOLVE_MAXRHS) * esz;
+    if (need > PASTIX_GPU_NOALLOC_SCRATCH_BYTES) {
+        fprintf(stderr,
+                "pastix_gpu_solve_noalloc: n=%d x %lld right-hand sides x %zu bytes = %zu bytes exceeds the "
+                "%zu-byte scratch array\n",
+                C.n, (long long)std::min<int64_t>(nrhs, SOLVE_MAXRHS), esz, need,
+                (size_t)PASTIX_GPU_NOALLOC_SCRATCH_BYTES);
+        return PASTIX_GPU_ERR_BADPARAMETER;
+    }
+    PGPU_CHECK(cudaSetDevice(C.device));
+    if (!is_device_ptr(dB)) return PASTIX_GPU_ERR_BADPARAMETER;
+    void *scratch = nullptr;
+    int rc = noalloc_scratch_address(C.device, &scratch);
+    if (rc) return rc;
+    cudaStream_t s = C.stream;
+    const int n = C.n;
+    int launches = 0;
+    for (int64_t r0 = 0; r0 < nrhs; r0 += SOLVE_MAXRHS) {
+        const int nr = (int)std::min<int64_t>(SOLVE_MAXRHS, nrhs - r0);
+        double *db = reinterpret_cast<double *>(dB) + r0 * ldb;
+        const int grid = std::min(4096, cdiv((int64_t)n * nr, 256));
+        if (C.coef_float) {
+            float *W = reinterpret_cast<float *>(scratch);
+            k_permute<double, float><<<grid, 256, 0, s>>>(n, nr, C.d_peritab.p, db, ldb, W, n, 0);
+            rc = solve_permuted<float>(C, W, nr, &launches);
+            if (rc) return rc;
+            k_permute<float, double><<<grid, 256, 0, s>>>(n, nr, C.d_peritab.p, W, n, db, ldb, 1);
+        } else {
+            double *W = reinterpret_cast<double *>(scratch);
+            k_permute<double, double><<<grid, 256, 0, s>>>(n, nr, C.d_peritab.p, db, ldb, W, n, 0);
+            rc = solve_permuted<double>(C, W, nr, &launches);
+            if (rc) return rc;
+            k_permute<double, double><<<grid, 256, 0, s>>>(n, nr, C.d_peritab.p, W, n, db, ldb, 1);
+        }
+    }
+    PGPU_CHECK(cudaGetLastError());
+    PGPU_CHECK(cudaStreamSynchronize(s));
     return PASTIX_GPU_SUCCESS;
 }
 
