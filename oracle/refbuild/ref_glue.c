@@ -24,8 +24,13 @@ typedef struct ref_handle_s {
     int            has_spm;
 } ref_handle_t;
 
+/* OpenBLAS entry point: PaStiX requires a sequential BLAS (README.md:76-77);
+ * the bundled OpenBLAS is the pthreads build, so pin it to one thread. */
+void openblas_set_num_threads( int );
+
 ref_handle_t *ref_create( int nthreads, int verbose )
 {
+    openblas_set_num_threads( 1 );
     ref_handle_t *h = calloc( 1, sizeof( ref_handle_t ) );
     pastixInitParam( h->iparm, h->dparm );
     h->iparm[IPARM_VERBOSE]    = verbose;

@@ -4,6 +4,7 @@
 #include "pastix_gpu.h"
 #include "pgpu_factor.cuh"
 #include "pgpu_solve.cuh"
+#include "pgpu_panel.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -96,7 +97,7 @@ struct pastix_gpu_s {
 
     // ---- factorization plan (per factotype) ----
     int plan_fact = -1;
-    std::vector<int> tile_ptr, trsm_ptr;
+    std::vector<int> tile_ptr, trsm_ptr, lvl_plrows, lvl_porows;
     DArr<int4> d_tiles, d_trsm;
     DArr<GemmTask> d_tasks;
     std::vector<int> solve_ptr;
@@ -235,7 +236,7 @@ extern "C" int pastix_gpu_structure(pastix_gpu_t *ctx, int64_t n, int64_t cblknb
             return PASTIX_GPU_ERR_BADPARAMETER;
     }
     // the panel TRSM keeps TRSM_ROWS x w elements in shared memory
-    if ((size_t)(TRSM_ROWS + 1) * C.maxw * sizeof(double) > 200 * 1024) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    if (C.maxw > 400) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
     C.thflops_potrf = fl_potrf;
     C.thflops_getrf = fl_getrf;
     for (int j = 0; j < n; j++)
@@ -407,22 +408,38 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
 // --------------------------------------------------------------------------
 // Factorization plan for one factorization type.
 // --------------------------------------------------------------------------
-static int build_fact_plan(pastix_gpu_t &C, int fact) {
-    if (C.plan_fact == fact) return PASTIX_GPU_SUCCESS;
+// Off-diagonal rows of cblks taller than fuse_rows are solved by
+// k_trsm_rows; shorter panels are factorized whole by k_panel_factor.
+static int fuse_rows_for(bool lu, bool fp32) {
+    if (lu) return fp32 ? 256 : 96;
+    return fp32 ? 1024 : 512;
+}
+static const int TRSM_TR = 32;   // panel rows per k_trsm_rows CTA
+
+static int build_fact_plan(pastix_gpu_t &C, int fact, bool fp32) {
+    const int key = fact * 2 + (fp32 ? 1 : 0);
+    if (C.plan_fact == key) return PASTIX_GPU_SUCCESS;
     const bool lu = (fact == PGPU_FACT_GETRF);
+    const int fuse = fuse_rows_for(lu, fp32);
     std::vector<int4> tiles, trsm;
     std::vector<GemmTask> tasks;
     double gflops = 0;
     C.tile_ptr.assign(C.nlevels + 1, 0);
     C.trsm_ptr.assign(C.nlevels + 1, 0);
+    C.lvl_plrows.assign(C.nlevels, 0);
+    C.lvl_porows.assign(C.nlevels, 0);
     for (int l = 0; l < C.nlevels; l++) {
         for (int q = C.lvl_ptr[l]; q < C.lvl_ptr[l + 1]; q++) {
             const int c = C.lvl_cblks[q];
             const int w = C.width[c], h = C.height[c];
-            for (int r0 = w; r0 < h; r0 += TRSM_ROWS) {
-                trsm.push_back(make_int4(c, r0, 0, lu ? 1 : 0));
-                if (lu) trsm.push_back(make_int4(c, r0, 1, 2));
-            }
+            const int rows = (h <= fuse) ? h : w;
+            C.lvl_plrows[l] = std::max(C.lvl_plrows[l], rows);
+            C.lvl_porows[l] = std::max(C.lvl_porows[l], rows - w);
+            if (h > fuse)
+                for (int r0 = w; r0 < h; r0 += TRSM_TR) {
+                    trsm.push_back(make_int4(c, r0, 0, lu ? 1 : 0));
+                    if (lu) trsm.push_back(make_int4(c, r0, 1, 2));
+                }
             const int b1 = C.fblok[c + 1];
             for (int b = C.fblok[c] + 1; b < b1; b++) {
                 const int f = C.bfcblk[b];
@@ -455,12 +472,12 @@ static int build_fact_plan(pastix_gpu_t &C, int fact) {
     PGPU_CHECK(C.d_trsm.upload(trsm, s));
     PGPU_CHECK(C.d_tasks.upload(tasks, s));
     PGPU_CHECK(cudaStreamSynchronize(s));
-    C.plan_fact = fact;
+    C.plan_fact = key;
     C.gemm_flops[fact] = gflops;
     return PASTIX_GPU_SUCCESS;
 }
 
-static const int DIAG_SMEM_BYTES = 96 * 1024;
+static const int SMEM_LIMIT = 227 * 1024;
 
 // Per-launch timing: one event recorded before every launch (and one after
 // the last), so launch i took ev[i+1] - ev[i]; kinds[i] says which phase.
@@ -498,27 +515,28 @@ static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, Lau
     T *coefL = reinterpret_cast<T *>(C.d_coef.p);
     T *coefU = lu ? coefL + C.coefnbr : coefL;
     cudaStream_t s = C.stream;
-    int smem_w = (int)std::floor(std::sqrt((double)DIAG_SMEM_BYTES / sizeof(T)));
-    auto kdiag = lu ? k_diag_factor<T, true> : k_diag_factor<T, false>;
-    PGPU_CHECK(cudaFuncSetAttribute(kdiag, cudaFuncAttributeMaxDynamicSharedMemorySize, DIAG_SMEM_BYTES));
-    PGPU_CHECK(cudaFuncSetAttribute(k_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    const int fuse = fuse_rows_for(lu, sizeof(T) == 4);
+    auto kpanel = lu ? k_panel_factor<T, true> : k_panel_factor<T, false>;
+    PGPU_CHECK(cudaFuncSetAttribute(kpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
+    PGPU_CHECK(cudaFuncSetAttribute(k_trsm_rows<T, TRSM_TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    SMEM_LIMIT));
     int nl = 0, ngemm = 0;
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
-        // the whole level's diagonal blocks fit the shared-memory path when
-        // its widest one does; otherwise the cblks that fit still use it
-        const int sw = std::min(mw, smem_w);
-        size_t dsm = (size_t)sw * sw * sizeof(T);
+        const int pl = C.lvl_plrows[l], pu = lu ? mw : 0, po = lu ? C.lvl_porows[l] : 0;
+        const size_t psm = (size_t)(PB * PBL + (size_t)(pl + pu + po) * PBL) * sizeof(T);
+        if (psm > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
         PGPU_CHECK(tm.mark(PH_DIAG));
-        kdiag<<<ncb, 256, dsm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, crit, sw * sw,
-                                    C.d_status.p);
+        kpanel<<<ncb, 256, psm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, coefU, crit, fuse, pl, pu,
+                                     C.d_status.p);
         nl++;
         const int ntr = C.trsm_ptr[l + 1] - C.trsm_ptr[l];
         if (ntr) {
-            size_t tsm = (size_t)(TRSM_ROWS + 1) * mw * sizeof(T);
+            const size_t tsm = ((size_t)TRSM_TR * (mw + 1) + PB * PBL + (size_t)mw * PBL) * sizeof(T);
+            if (tsm > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
             PGPU_CHECK(tm.mark(PH_TRSM));
-            k_trsm<T><<<ntr, 256, tsm, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], coefL, coefU);
+            k_trsm_rows<T, TRSM_TR><<<ntr, 256, tsm, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], coefL, coefU, mw);
             nl++;
         }
         const int nti = C.tile_ptr[l + 1] - C.tile_ptr[l];
@@ -555,7 +573,7 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     if (fact != PGPU_FACT_POTRF && fact != PGPU_FACT_GETRF) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
     if (fact == PGPU_FACT_POTRF && C.mtxtype == PGPU_GENERAL) return PASTIX_GPU_ERR_BADPARAMETER;
     const int mixed = C.iparm[PGPU_IPARM_MIXED] ? 1 : 0;
-    int rc = build_fact_plan(C, fact);
+    int rc = build_fact_plan(C, fact, mixed != 0);
     if (rc) return rc;
     const size_t esz = mixed ? sizeof(float) : sizeof(double);
     const size_t ncoef = (size_t)C.coefnbr * (fact == PGPU_FACT_GETRF ? 2 : 1);

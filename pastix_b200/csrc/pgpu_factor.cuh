@@ -28,142 +28,6 @@ __global__ void k_fillin(int64_t nnz, const double *__restrict__ vals,
 }
 
 // ---------------------------------------------------------------------------
-// Diagonal block factorization, one CTA per cblk of the level.
-//   POTRF: kernels/core_zpotrfsp.c:68 core_zpotf2sp -- |a_kk| < crit gives
-//          a_kk := crit (a static pivot); a negative pivot is reported.
-//   GETRF: kernels/core_zgetrfsp.c:64 core_zgetf2sp -- |a_kk| < crit gives
-//          a_kk := +-crit with the sign of a_kk; no row pivoting.
-// The w x w block is factorized in shared memory when it fits, in place in
-// global memory otherwise.  Column k is scaled by the reciprocal of the
-// pivot, as the reference does (alpha = 1/a_kk; scal).
-// ---------------------------------------------------------------------------
-template <typename T, bool LU>
-__global__ void k_diag_factor(Meta m, const int *__restrict__ cblks, T *__restrict__ coef,
-                              double crit, int smem_cap, Status *st) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *S = reinterpret_cast<T *>(smem_raw);
-    __shared__ T piv_s;
-    const int c = cblks[blockIdx.x];
-    const int w = m.width[c];
-    const int ldg = m.ld[c];
-    T *G = coef + m.coefoff[c];
-    // smem_cap: elements of dynamic shared memory this launch was given
-    const bool in_smem = (w * w <= smem_cap);
-    T *A = in_smem ? S : G;
-    const int lda = in_smem ? w : ldg;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    if (in_smem) {
-        for (int e = tid; e < w * w; e += nt) {
-            int i = e / w, j = e - i * w;
-            S[e] = (LU || j <= i) ? G[(int64_t)i * ldg + j] : T(0);
-        }
-        __syncthreads();
-    }
-    int npiv = 0, nneg = 0, nbad = 0;
-    for (int k = 0; k < w; k++) {
-        if (tid == 0) {
-            T akk = A[k * lda + k];
-            if (!isfinite(akk)) nbad++;
-            if (ScalarOps<T>::absval(akk) < T(crit)) {
-                if (LU) akk = (akk < T(0)) ? T(-crit) : T(crit);
-                else akk = T(crit);
-                npiv++;
-            }
-            if (!LU) {
-                if (akk < T(0)) nneg++;
-                akk = ScalarOps<T>::sqrtv(akk);
-            }
-            A[k * lda + k] = akk;
-            piv_s = T(1) / akk;
-        }
-        __syncthreads();
-        const T alpha = piv_s;
-        for (int i = k + 1 + tid; i < w; i += nt) A[i * lda + k] *= alpha;
-        __syncthreads();
-        const int r = w - k - 1;
-        if (LU) {
-            for (int e = tid; e < r * r; e += nt) {
-                int i = k + 1 + e / r, j = k + 1 + e % r;
-                A[i * lda + j] -= A[i * lda + k] * A[k * lda + j];
-            }
-        } else {
-            // lower triangle of the trailing block, rows i >= j
-            for (int e = tid; e < r * r; e += nt) {
-                int i = k + 1 + e / r, j = k + 1 + e % r;
-                if (j <= i) A[i * lda + j] -= A[i * lda + k] * A[j * lda + k];
-            }
-        }
-        __syncthreads();
-    }
-    if (in_smem) {
-        for (int e = tid; e < w * w; e += nt) {
-            int i = e / w, j = e - i * w;
-            if (LU || j <= i) G[(int64_t)i * ldg + j] = S[e];
-        }
-    }
-    if (tid == 0) {
-        if (npiv) atomicAdd(&st->nbpivots, npiv);
-        if (nneg) atomicAdd(&st->negpivots, nneg);
-        if (nbad) atomicAdd(&st->nonfinite, nbad);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Panel TRSM (kernels/core_ztrsmsp.c:71 core_ztrsmsp_1d): every panel row
-// below the diagonal block is an independent solve against the factorized
-// diagonal block D (w x w, row-major).  Three forms:
-//   mode 0  POTRF       X := X L^{-T}        (Right, Lower, ConjTrans, NonUnit)
-//   mode 1  GETRF on L  X := X U^{-1}        (Right, Upper, NoTrans,  NonUnit)
-//   mode 2  GETRF on U  X := X L^{-T}, unit  (Right, Upper, NoTrans,  Unit) on U^T
-// A CTA owns TRSM_ROWS rows kept in shared memory and eliminates column by
-// column; the coefficient vector of step j is staged in shared memory.
-// chunks[i] = {cblk, first panel row, panel select (0 L / 1 U), mode}.
-// ---------------------------------------------------------------------------
-constexpr int TRSM_ROWS = 32;
-
-template <typename T>
-__global__ void k_trsm(Meta m, const int4 *__restrict__ chunks, T *__restrict__ coefL,
-                       T *__restrict__ coefU) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int4 ch = chunks[blockIdx.x];
-    const int c = ch.x, r0 = ch.y, mode = ch.w;
-    const int w = m.width[c], h = m.height[c], ld = m.ld[c];
-    const int nrows = min(TRSM_ROWS, h - r0);
-    T *X = reinterpret_cast<T *>(smem_raw);            // [TRSM_ROWS][w]
-    T *v = X + TRSM_ROWS * w;                            // [w] coefficients of step j
-    const T *D = coefL + m.coefoff[c];                   // diagonal block lives in L
-    T *P = (ch.z ? coefU : coefL) + m.coefoff[c] + (int64_t)r0 * ld;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int e = tid; e < nrows * w; e += nt) {
-        int i = e / w, j = e - i * w;
-        X[e] = P[(int64_t)i * ld + j];
-    }
-    for (int j = 0; j < w; j++) {
-        // stage coefficients: v[l] for l > j, v[j] = 1/d_jj
-        for (int l = j + tid; l < w; l += nt) {
-            T cval;
-            if (mode == 1) cval = D[j * ld + l];   // U[j][l]
-            else cval = D[l * ld + j];             // L[l][j]
-            v[l] = (l == j) ? (mode == 2 ? T(1) : T(1) / cval) : cval;
-        }
-        __syncthreads();
-        if (mode != 2)
-            for (int i = tid; i < nrows; i += nt) X[i * w + j] *= v[j];
-        __syncthreads();
-        const int r = w - j - 1;
-        for (int e = tid; e < nrows * r; e += nt) {
-            int i = e / r, l = j + 1 + (e - (e / r) * r);
-            X[i * w + l] -= X[i * w + j] * v[l];
-        }
-        __syncthreads();
-    }
-    for (int e = tid; e < nrows * w; e += nt) {
-        int i = e / w, j = e - i * w;
-        P[(int64_t)i * ld + j] = X[e];
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Update GEMM with indexed scatter-add (kernels/core_zgemmsp.c:104
 // core_zgemmsp_1d1d: W = A B^T then core_zgeadd into the facing cblk).
 // Task t: source cblk c, block b facing cblk f.  A = panel rows

@@ -14,7 +14,9 @@ constexpr int SOLVE_MAXRHS = 16;
 // Forward, diagonal part (kernels/solve_ztrsmsp.c:75 solve_blok_ztrsm with
 // Left, Lower, NoTrans): B[fcol:fcol+w, :] := D^{-1} B[...], D = L_kk
 // (POTRF, non-unit) or the unit lower part of the LU diagonal block.  One CTA
-// per cblk of the level, column-oriented elimination in shared memory.
+// per cblk of the level, blocked by 32 columns: warp 0 substitutes through
+// the 32x32 tile (shuffles, no block barrier), then all threads update the
+// rows below inside the diagonal block.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
@@ -24,21 +26,33 @@ __global__ void k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
     const int c = cblks[blockIdx.x];
     const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c];
     const T *D = coefL + m.coefoff[c];
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
     for (int e = tid; e < w * nrhs; e += nt) {
         int j = e / nrhs, r = e - j * nrhs;
         y[e] = B[(int64_t)r * ldb + fc + j];
     }
     __syncthreads();
-    for (int j = 0; j < w; j++) {
-        if (!unit) {
-            if (tid < nrhs) y[j * nrhs + tid] *= T(1) / D[j * ld + j];
-            __syncthreads();
+    for (int jb = 0; jb < w; jb += 32) {
+        const int nb = min(32, w - jb);
+        if (tid < 32) {
+            for (int r = 0; r < nrhs; r++) {
+                T v = (lane < nb) ? y[(jb + lane) * nrhs + r] : T(0);
+                for (int j = 0; j < nb; j++) {
+                    if (!unit && lane == j) v *= T(1) / D[(int64_t)(jb + j) * ld + jb + j];
+                    const T xj = __shfl_sync(0xffffffffu, v, j);
+                    if (lane > j && lane < nb) v -= D[(int64_t)(jb + lane) * ld + jb + j] * xj;
+                }
+                if (lane < nb) y[(jb + lane) * nrhs + r] = v;
+            }
         }
-        const int rem = (w - j - 1) * nrhs;
+        __syncthreads();
+        const int rem = (w - jb - nb) * nrhs;
         for (int e = tid; e < rem; e += nt) {
-            int l = j + 1 + e / nrhs, r = e % nrhs;
-            y[l * nrhs + r] -= D[l * ld + j] * y[j * nrhs + r];
+            const int i = jb + nb + e / nrhs, r = e % nrhs;
+            const T *row = D + (int64_t)i * ld + jb;
+            T s = T(0);
+            for (int l = 0; l < nb; l++) s += row[l] * y[(jb + l) * nrhs + r];
+            y[i * nrhs + r] -= s;
         }
         __syncthreads();
     }
@@ -116,6 +130,8 @@ __global__ void k_bwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
 // Backward, diagonal part: B[fcol:fcol+w, :] := D^{-1} B[...] with
 // D = L_kk^T (POTRF, Left, Lower, ConjTrans/Trans, NonUnit) or the upper
 // triangle U_kk of the LU diagonal block (Left, Upper, NoTrans, NonUnit).
+// Blocked by 32 columns from the last block up: warp 0 substitutes through
+// the tile, then all threads update the rows above.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
@@ -125,21 +141,43 @@ __global__ void k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
     const int c = cblks[blockIdx.x];
     const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c];
     const T *D = coefL + m.coefoff[c];
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
     for (int e = tid; e < w * nrhs; e += nt) {
         int j = e / nrhs, r = e - j * nrhs;
         x[e] = B[(int64_t)r * ldb + fc + j];
     }
     __syncthreads();
-    for (int j = w - 1; j >= 0; j--) {
-        if (tid < nrhs) x[j * nrhs + tid] *= T(1) / D[j * ld + j];
+    const int nblk = (w + 31) / 32;
+    for (int bi = nblk - 1; bi >= 0; bi--) {
+        const int jb = bi * 32, nb = min(32, w - jb);
+        if (tid < 32) {
+            for (int r = 0; r < nrhs; r++) {
+                T v = (lane < nb) ? x[(jb + lane) * nrhs + r] : T(0);
+                for (int j = nb - 1; j >= 0; j--) {
+                    if (lane == j) v *= T(1) / D[(int64_t)(jb + j) * ld + jb + j];
+                    const T xj = __shfl_sync(0xffffffffu, v, j);
+                    if (lane < j) {
+                        // upper: U[l][j]; Cholesky: L^T[l][j] = L[j][l]
+                        const T dlj = upper ? D[(int64_t)(jb + lane) * ld + jb + j]
+                                            : D[(int64_t)(jb + j) * ld + jb + lane];
+                        v -= dlj * xj;
+                    }
+                }
+                if (lane < nb) x[(jb + lane) * nrhs + r] = v;
+            }
+        }
         __syncthreads();
-        const int rem = j * nrhs;
+        const int rem = jb * nrhs;
         for (int e = tid; e < rem; e += nt) {
-            int l = e / nrhs, r = e % nrhs;
-            // upper: U[l][j] (column j of the row-major block); Cholesky: L^T[l][j] = L[j][l]
-            const T dlj = upper ? D[l * ld + j] : D[j * ld + l];
-            x[l * nrhs + r] -= dlj * x[j * nrhs + r];
+            const int i = e / nrhs, r = e % nrhs;
+            T s = T(0);
+            if (upper) {
+                const T *row = D + (int64_t)i * ld + jb;
+                for (int l = 0; l < nb; l++) s += row[l] * x[(jb + l) * nrhs + r];
+            } else {
+                for (int l = 0; l < nb; l++) s += D[(int64_t)(jb + l) * ld + i] * x[(jb + l) * nrhs + r];
+            }
+            x[i * nrhs + r] -= s;
         }
         __syncthreads();
     }
