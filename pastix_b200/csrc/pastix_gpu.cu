@@ -58,7 +58,7 @@ struct DArr {
 inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 inline int cdiv(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
-const int SOLVE_ROWS_PER_CHUNK = 256;
+const int SOLVE_ROWS_PER_CHUNK = 32;
 
 bool is_device_ptr(const void *p) {
     cudaPointerAttributes at;
@@ -658,10 +658,13 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
     cudaStream_t s = C.stream;
     const int ldb = C.n;
     int nl = 0;
+    PGPU_CHECK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
+    PGPU_CHECK(cudaFuncSetAttribute(k_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
+    PGPU_CHECK(cudaFuncSetAttribute(k_fwd_off<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
-        k_fwd_diag<T><<<ncb, 128, (size_t)mw * nrhs * sizeof(T), s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l],
+        k_fwd_diag<T><<<ncb, 128, ((size_t)mw * nrhs + 32 * 33) * sizeof(T), s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l],
                                                                       coefL, W, ldb, nrhs, lu ? 1 : 0);
         nl++;
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
@@ -680,7 +683,7 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
                                               SOLVE_ROWS_PER_CHUNK);
             nl++;
         }
-        k_bwd_diag<T><<<ncb, 128, (size_t)mw * nrhs * sizeof(T), s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l],
+        k_bwd_diag<T><<<ncb, 128, ((size_t)mw * nrhs + 32 * 33) * sizeof(T), s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l],
                                                                       coefL, W, ldb, nrhs, lu ? 1 : 0);
         nl++;
     }

@@ -32,15 +32,22 @@ __global__ void k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
         y[e] = B[(int64_t)r * ldb + fc + j];
     }
     __syncthreads();
+    T *tile = y + w * nrhs;                   // [32][33] diagonal tile
     for (int jb = 0; jb < w; jb += 32) {
         const int nb = min(32, w - jb);
+        for (int e = tid; e < nb * nb; e += nt) {
+            const int i = e / nb, j = e - i * nb;
+            tile[i * 33 + j] = D[(int64_t)(jb + i) * ld + jb + j];
+        }
+        __syncthreads();
         if (tid < 32) {
+            const T dinv = (lane < nb) ? T(1) / tile[lane * 33 + lane] : T(1);
             for (int r = 0; r < nrhs; r++) {
                 T v = (lane < nb) ? y[(jb + lane) * nrhs + r] : T(0);
                 for (int j = 0; j < nb; j++) {
-                    if (!unit && lane == j) v *= T(1) / D[(int64_t)(jb + j) * ld + jb + j];
+                    if (!unit && lane == j) v *= dinv;
                     const T xj = __shfl_sync(0xffffffffu, v, j);
-                    if (lane > j && lane < nb) v -= D[(int64_t)(jb + lane) * ld + jb + j] * xj;
+                    if (lane > j && lane < nb) v -= tile[lane * 33 + j] * xj;
                 }
                 if (lane < nb) y[(jb + lane) * nrhs + r] = v;
             }
@@ -147,19 +154,25 @@ __global__ void k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
         x[e] = B[(int64_t)r * ldb + fc + j];
     }
     __syncthreads();
+    T *tile = x + w * nrhs;                   // [32][33] diagonal tile
     const int nblk = (w + 31) / 32;
     for (int bi = nblk - 1; bi >= 0; bi--) {
         const int jb = bi * 32, nb = min(32, w - jb);
+        for (int e = tid; e < nb * nb; e += nt) {
+            const int i = e / nb, j = e - i * nb;
+            tile[i * 33 + j] = D[(int64_t)(jb + i) * ld + jb + j];
+        }
+        __syncthreads();
         if (tid < 32) {
+            const T dinv = (lane < nb) ? T(1) / tile[lane * 33 + lane] : T(1);
             for (int r = 0; r < nrhs; r++) {
                 T v = (lane < nb) ? x[(jb + lane) * nrhs + r] : T(0);
                 for (int j = nb - 1; j >= 0; j--) {
-                    if (lane == j) v *= T(1) / D[(int64_t)(jb + j) * ld + jb + j];
+                    if (lane == j) v *= dinv;
                     const T xj = __shfl_sync(0xffffffffu, v, j);
                     if (lane < j) {
                         // upper: U[l][j]; Cholesky: L^T[l][j] = L[j][l]
-                        const T dlj = upper ? D[(int64_t)(jb + lane) * ld + jb + j]
-                                            : D[(int64_t)(jb + j) * ld + jb + lane];
+                        const T dlj = upper ? tile[lane * 33 + j] : tile[j * 33 + lane];
                         v -= dlj * xj;
                     }
                 }
