@@ -203,8 +203,14 @@ PASTIX_GPU_API int pastix_gpu_coeftab( pastix_gpu_t *ctx, void *L, void *U );
  *   stats[7] update-GEMM launches inside numfact
  *   stats[8] diagonal-factorization ms, stats[9] panel-TRSM ms inside numfact
  *   stats[10] algorithmic flops of the update GEMMs (sum of 2 M N K)
- *   stats[11] reserved
- * (12 doubles)
+ *   stats[11] ms of the tensor-core (tcgen05) update-GEMM launches (part of stats[6])
+ *   stats[12] algorithmic flops of the GEMM tasks that ran on the tensor cores
+ *   stats[13] tensor-core tiles whose bounded MMA wait timed out (0 when healthy)
+ *   stats[14..15] reserved
+ * (16 doubles)
+ * The single-precision (mixed) factorization runs its large update GEMMs on
+ * the tensor cores with TF32 operands; environment PASTIX_GPU_MIXED_GEMM=fp32
+ * keeps them on FP32 FMA instead.
  */
 PASTIX_GPU_API int pastix_gpu_stats( pastix_gpu_t *ctx, double *stats );
 

@@ -5,6 +5,7 @@
 #include "pgpu_factor.cuh"
 #include "pgpu_solve.cuh"
 #include "pgpu_panel.cuh"
+#include "pgpu_gemm_tc.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -97,8 +98,9 @@ struct pastix_gpu_s {
 
     // ---- factorization plan (per factotype) ----
     int plan_fact = -1;
-    std::vector<int> tile_ptr, trsm_ptr, lvl_plrows, lvl_porows;
-    DArr<int4> d_tiles, d_trsm;
+    std::vector<int> tile_ptr, tctile_ptr, trsm_ptr, lvl_plrows, lvl_porows;
+    DArr<int4> d_tiles, d_tctiles, d_trsm;
+    double tc_flops = 0;   // update-GEMM flops on the tensor-core path
     DArr<GemmTask> d_tasks;
     std::vector<int> solve_ptr;
     DArr<int2> d_solve_chunks;
@@ -124,7 +126,7 @@ struct pastix_gpu_s {
     DArr<double> d_sr_b, d_sr_x;   // solve_and_refine staging of host B / X
     std::vector<cudaEvent_t> evpool;   // per-launch timing events
     double gemm_flops[5] = {0};        // update-GEMM flops per factotype
-    double stats[12] = {0};
+    double stats[16] = {0};
 };
 
 // --------------------------------------------------------------------------
@@ -416,15 +418,25 @@ static int fuse_rows_for(bool lu, bool fp32) {
 }
 static const int TRSM_TR = 32;   // panel rows per k_trsm_rows CTA
 
+// Single-precision update GEMMs large enough for a 128 x 128 tensor-core tile
+// go to k_gemm_scatter_tc (TF32 operands) unless PASTIX_GPU_MIXED_GEMM=fp32.
+static bool tc_enabled() {
+    const char *e = getenv("PASTIX_GPU_MIXED_GEMM");
+    return !(e && std::strcmp(e, "fp32") == 0);
+}
+static bool tc_task(int M, int N, int K) { return K >= 32 && M >= 64 && N >= 32 && (int64_t)M * N >= 128 * 64; }
+
 static int build_fact_plan(pastix_gpu_t &C, int fact, bool fp32) {
-    const int key = fact * 2 + (fp32 ? 1 : 0);
+    const bool use_tc = fp32 && tc_enabled();
+    const int key = fact * 4 + (fp32 ? 1 : 0) + (use_tc ? 2 : 0);
     if (C.plan_fact == key) return PASTIX_GPU_SUCCESS;
     const bool lu = (fact == PGPU_FACT_GETRF);
     const int fuse = fuse_rows_for(lu, fp32);
-    std::vector<int4> tiles, trsm;
+    std::vector<int4> tiles, trsm, tctiles;
     std::vector<GemmTask> tasks;
-    double gflops = 0;
+    double gflops = 0, tcflops = 0;
     C.tile_ptr.assign(C.nlevels + 1, 0);
+    C.tctile_ptr.assign(C.nlevels + 1, 0);
     C.trsm_ptr.assign(C.nlevels + 1, 0);
     C.lvl_plrows.assign(C.nlevels, 0);
     C.lvl_porows.assign(C.nlevels, 0);
@@ -450,6 +462,15 @@ static int build_fact_plan(pastix_gpu_t &C, int fact, bool fp32) {
                     const int id = (int)tasks.size();
                     tasks.push_back(GemmTask{c, b, f, arow0, M, flags});
                     gflops += 2.0 * M * N * w;
+                    if (use_tc && tc_task(M, N, w)) {
+                        tcflops += 2.0 * M * N * w;
+                        for (int tm = 0; tm < cdiv(M, TC_BM); tm++)
+                            for (int tn = 0; tn < cdiv(N, TC_BN); tn++) {
+                                if ((flags & 8) && tm < tn) continue;
+                                tctiles.push_back(make_int4(id, tm, tn, 0));
+                            }
+                        return;
+                    }
                     for (int tm = 0; tm < cdiv(M, GEMM_TM); tm++)
                         for (int tn = 0; tn < cdiv(N, GEMM_TN); tn++) {
                             if ((flags & 8) && tm < tn) continue;   // strictly upper tiles of the diagonal block
@@ -465,15 +486,18 @@ static int build_fact_plan(pastix_gpu_t &C, int fact, bool fp32) {
             }
         }
         C.tile_ptr[l + 1] = (int)tiles.size();
+        C.tctile_ptr[l + 1] = (int)tctiles.size();
         C.trsm_ptr[l + 1] = (int)trsm.size();
     }
     cudaStream_t s = C.stream;
     PGPU_CHECK(C.d_tiles.upload(tiles, s));
+    PGPU_CHECK(C.d_tctiles.upload(tctiles, s));
     PGPU_CHECK(C.d_trsm.upload(trsm, s));
     PGPU_CHECK(C.d_tasks.upload(tasks, s));
     PGPU_CHECK(cudaStreamSynchronize(s));
     C.plan_fact = key;
     C.gemm_flops[fact] = gflops;
+    C.tc_flops = tcflops;
     return PASTIX_GPU_SUCCESS;
 }
 
@@ -507,7 +531,7 @@ struct LaunchTimer {
     }
 };
 
-enum { PH_DIAG = 0, PH_TRSM = 1, PH_GEMM = 2, PH_END = 3 };
+enum { PH_DIAG = 0, PH_TRSM = 1, PH_GEMM = 2, PH_TC = 3, PH_END = 4 };
 
 template <typename T>
 static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, LaunchTimer &tm) {
@@ -520,6 +544,8 @@ static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, Lau
     PGPU_CHECK(cudaFuncSetAttribute(kpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(k_trsm_rows<T, TRSM_TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     SMEM_LIMIT));
+    if constexpr (sizeof(T) == 4)
+        PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
     int nl = 0, ngemm = 0;
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
@@ -545,6 +571,16 @@ static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, Lau
             k_gemm_scatter<T><<<nti, 256, 0, s>>>(C.meta, C.d_tiles.p + C.tile_ptr[l], C.d_tasks.p, coefL, coefU);
             nl++;
             ngemm++;
+        }
+        if constexpr (sizeof(T) == 4) {
+            const int ntc = C.tctile_ptr[l + 1] - C.tctile_ptr[l];
+            if (ntc) {
+                PGPU_CHECK(tm.mark(PH_TC));
+                k_gemm_scatter_tc<<<ntc, TC_THREADS, TC_SMEM, s>>>(C.meta, C.d_tctiles.p + C.tctile_ptr[l],
+                                                                  C.d_tasks.p, coefL, coefU, C.d_status.p);
+                nl++;
+                ngemm++;
+            }
         }
     }
     PGPU_CHECK(tm.mark(PH_END));
@@ -620,12 +656,20 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     C.stats[0] = launches + nl;
     C.stats[3] = ms;
     {
-        double ph[3];
-        tm.collect(ph, 3);
+        double ph[4];
+        tm.collect(ph, 4);
         C.stats[8] = ph[PH_DIAG];
         C.stats[9] = ph[PH_TRSM];
-        C.stats[6] = ph[PH_GEMM];
+        C.stats[6] = ph[PH_GEMM] + ph[PH_TC];
         C.stats[10] = C.gemm_flops[fact];
+        C.stats[11] = ph[PH_TC];
+        C.stats[12] = mixed ? C.tc_flops : 0.0;
+        C.stats[13] = st.timeout;
+    }
+    if (st.timeout) {
+        fprintf(stderr, "pastix_gpu: %d tensor-core GEMM tiles timed out waiting for their MMAs\n", st.timeout);
+        C.fact_done = -1;
+        return PASTIX_GPU_ERR_INTERNAL;
     }
     C.iparm[PGPU_IPARM_STATIC_PIVOTING] = st.nbpivots;
     const double fl = (fact == PGPU_FACT_GETRF) ? C.thflops_getrf : C.thflops_potrf;

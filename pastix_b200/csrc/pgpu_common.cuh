@@ -41,6 +41,7 @@ struct Status {
     int negpivots;     // negative/zero diagonal met in a Cholesky pivot
     int nonfinite;     // NaN/Inf met on a diagonal
     int overflow;      // FP32 down-cast overflow in the mixed fill-in
+    int timeout;       // a bounded wait inside a kernel gave up (tile skipped)
 };
 
 template <typename T> struct ScalarOps;

@@ -1,0 +1,268 @@
+// Update GEMM with indexed scatter-add on the 5th-generation tensor cores
+// (tcgen05, sm_100a) for the single-precision factorization: C = A B^T with
+// A = panel rows [arow0 + i0, +128) of cblk c, B = rows [browoff_b + j0, +128)
+// of block b, K = w_c, FP32 operands read as TF32, FP32 accumulation in TMEM;
+// C is subtracted from the facing cblk f at (panel row of the source row in
+// f, frownum_b + j - fcolnum_f), as kernels/core_zgemmsp.c:104
+// core_zgemmsp_1d1d + core_zgeadd do.
+//
+// Per CTA (128 threads, one 128 x 128 output tile):
+//   * A and B k-blocks (128 rows x 32 floats = 128 B per row) are staged in
+//     shared memory with cp.async in the canonical K-major SWIZZLE_128B layout
+//     (8-row groups of 1024 B, 16-byte chunk c of row r stored at chunk
+//     c ^ (r & 7)), TC_STAGES deep;
+//   * one thread issues 4 tcgen05.mma.kind::tf32 (K = 8 each) per k-block and
+//     commits them to the stage's mbarrier, which frees the stage;
+//   * the accumulator (128 lanes x 128 fp32 columns of TMEM) is read back with
+//     tcgen05.ld by the 4 warps (warp w owns lanes 32w..32w+31), transposed
+//     through shared memory so a warp's atomics hit 32 consecutive columns.
+// Every mbarrier wait is bounded; on time-out the CTA records the failure in
+// Status::timeout, frees its TMEM and leaves the tile untouched.
+#pragma once
+
+#include "pgpu_common.cuh"
+#include "pgpu_factor.cuh"
+
+namespace pgpu {
+
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_STAGES = 3, TC_THREADS = 128;
+constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 4;              // 16 KB per operand per stage
+constexpr int TC_SMEM = TC_STAGES * 2 * TC_TILE_BYTES + 1024;  // + alignment slack
+constexpr int TC_TMEM_COLS = 128;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: K-major, SWIZZLE_128B, 8-row groups
+// 1024 B apart (stride byte offset), version 1 (sm_100).
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+    d |= static_cast<uint64_t>(1u) << 16;                 // leading byte offset (unused, swizzled K-major)
+    d |= static_cast<uint64_t>(1024u >> 4) << 32;         // stride byte offset
+    d |= static_cast<uint64_t>(1u) << 46;                 // descriptor version
+    d |= static_cast<uint64_t>(2u) << 61;                 // SWIZZLE_128B
+    return d;
+}
+
+// Instruction descriptor: D fp32, A/B tf32, both K-major, M = 128, N = 128.
+__device__ __forceinline__ uint32_t tc_idesc() {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
+}
+
+// Bounded wait on an mbarrier phase; false on time-out (about 2 s).
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > 4000000000LL) return false;
+    }
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void *gptr, bool valid) {
+    const int sz = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr), "l"(gptr), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void tc_fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+          "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+          "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const int4 *__restrict__ tiles,
+                                                                const GemmTask *__restrict__ tasks,
+                                                                float *__restrict__ coefL,
+                                                                float *__restrict__ coefU, Status *st) {
+    extern __shared__ __align__(16) unsigned char tc_smem_raw[];
+    __shared__ __align__(8) uint64_t mbar[TC_STAGES];
+    __shared__ uint32_t tmem_base_s;
+    __shared__ int trow_s[TC_BM];
+    __shared__ int fail_s;
+
+    // 1024-byte aligned operand area (SWIZZLE_128B atoms)
+    const uint32_t raw = smem_u32(tc_smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char *sbase = tc_smem_raw + (base - raw);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int4 tl = tiles[blockIdx.x];
+    const GemmTask t = tasks[tl.x];
+    const int c = t.c, b = t.b, f = t.f;
+    const int K = m.width[c], ld = m.ld[c];
+    const int N = m.blrow[b] - m.bfrow[b] + 1;
+    const int i0 = tl.y * TC_BM, j0 = tl.z * TC_BN;
+    const float *A = ((t.flags & 1) ? coefU : coefL) + m.coefoff[c] + (int64_t)(t.arow0 + i0) * ld;
+    const float *B = ((t.flags & 2) ? coefU : coefL) + m.coefoff[c] + (int64_t)(m.browoff[b] + j0) * ld;
+    const int mrows = min(TC_BM, t.M - i0), ncols = min(TC_BN, N - j0);
+    const int nk = (K + TC_BK - 1) / TC_BK;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < TC_STAGES; s++) mbar_init(smem_u32(&mbar[s]), 1);
+        fail_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    {
+        int tr = -1;
+        if (tid < mrows) tr = panel_row_of(m, f, m.rowidx[m.rowbase[c] + t.arow0 + i0 + tid]);
+        trow_s[tid] = tr;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_s;
+
+    auto stageA = [&](int s) { return base + (uint32_t)(s * 2) * TC_TILE_BYTES; };
+    auto stageB = [&](int s) { return base + (uint32_t)(s * 2 + 1) * TC_TILE_BYTES; };
+    auto load_stage = [&](int s, int kb) {
+        const int k0 = kb * TC_BK;
+        // 128 rows x 8 chunks of 16 B for each operand; 16 chunks per thread
+#pragma unroll
+        for (int q = 0; q < (TC_BM * 8) / TC_THREADS; q++) {
+            const int e = tid + q * TC_THREADS;
+            const int r = e >> 3, ch = e & 7;
+            const int kc = k0 + ch * 4;
+            const uint32_t soff = (uint32_t)(r * 128 + ((ch ^ (r & 7)) << 4));
+            const bool va = (r < mrows) && (kc < K);
+            cp_async16(stageA(s) + soff, va ? (const void *)(A + (int64_t)r * ld + kc) : (const void *)A, va);
+            const bool vb = (r < ncols) && (kc < K);
+            cp_async16(stageB(s) + soff, vb ? (const void *)(B + (int64_t)r * ld + kc) : (const void *)B, vb);
+        }
+    };
+
+    const uint32_t idesc = tc_idesc();
+#pragma unroll
+    for (int s = 0; s < TC_STAGES - 1; s++) {
+        if (s < nk) load_stage(s, s);
+        cp_async_commit();
+    }
+    bool ok = true;
+    for (int kb = 0; kb < nk; kb++) {
+        const int s = kb % TC_STAGES;
+        const int pk = kb + TC_STAGES - 1;
+        if (pk < nk) {
+            const int ps = pk % TC_STAGES;
+            if (kb >= 1) {
+                // stage ps was last read by the MMAs of k-block kb-1
+                if (!mbar_wait(smem_u32(&mbar[ps]), (uint32_t)(((kb - 1) / TC_STAGES) & 1))) ok = false;
+            }
+            if (ok) load_stage(ps, pk);
+        }
+        cp_async_commit();
+        cp_async_wait<TC_STAGES - 1>();
+        tc_fence_async_smem();
+        if (!__syncthreads_and(ok ? 1 : 0)) {
+            ok = false;
+            break;
+        }
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int kk = 0; kk < TC_BK / 8; kk++) {
+                const uint64_t ad = tc_sdesc(stageA(s) + kk * 32);
+                const uint64_t bd = tc_sdesc(stageB(s) + kk * 32);
+                tc_mma(tmem, ad, bd, idesc, (kb > 0 || kk > 0) ? 1u : 0u);
+            }
+            tc_commit(smem_u32(&mbar[s]));
+        }
+    }
+    // all MMAs done when the last commit's barrier flips
+    if (ok && nk > 0) {
+        if (!mbar_wait(smem_u32(&mbar[(nk - 1) % TC_STAGES]), (uint32_t)(((nk - 1) / TC_STAGES) & 1))) ok = false;
+    }
+    cp_async_wait<0>();
+    if (!ok) atomicExch(&fail_s, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!fail_s) {
+        // epilogue: TMEM -> registers -> transpose in shared memory -> atomics
+        float *E = reinterpret_cast<float *>(sbase) + warp * 32 * 33;
+        float *C = ((t.flags & 4) ? coefU : coefL) + m.coefoff[f];
+        const int ldf = m.ld[f], wf = m.width[f];
+        const int tcol0 = m.bfrow[b] + j0 - m.fcol[f];
+        const bool lower_only = (t.flags & 8) != 0;
+        for (int cb = 0; cb < TC_BN; cb += 32) {
+            uint32_t v[32];
+            tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 32; q++) E[lane * 33 + q] = __uint_as_float(v[q]);
+            __syncwarp();
+            const int j = cb + lane;
+            if (j < ncols) {
+                const int tc = tcol0 + j;
+                for (int rr = 0; rr < 32; rr++) {
+                    const int i = warp * 32 + rr;
+                    if (i >= mrows) break;
+                    const int tr = trow_s[i];
+                    if (tr < 0) continue;
+                    if (lower_only && tr < wf && tc > tr) continue;
+                    atomicAdd(&C[(int64_t)tr * ldf + tc], -E[rr * 33 + lane]);
+                }
+            }
+            __syncwarp();
+        }
+    } else if (tid == 0) {
+        atomicAdd(&st->timeout, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS)
+                     : "memory");
+    }
+}
+
+}  // namespace pgpu

@@ -69,7 +69,7 @@ def test_solve_matches_reference(name, make, fact):
 
 @pytest.mark.parametrize("name,make,fact", [c for c in CASES if c[2] == "potrf"],
                          ids=[c[0] for c in CASES if c[2] == "potrf"])
-def test_mixed_factor_matches_reference_mixed(name, make, fact):
+def test_mixed_factor_matches_reference_mixed(name, make, fact, fp32_gemm):
     A = make()
     ref, st = U.run_reference(A, fact, mixed=True)
     g = U.gpu_structure(A, st)
@@ -100,3 +100,32 @@ def test_cg_refinement_reaches_1e12(mixed):
     assert bwd <= 1e-12
     ip, dp = s.params()
     assert ip[52] >= (1 if mixed else 0)
+
+
+@pytest.fixture
+def fp32_gemm(monkeypatch):
+    monkeypatch.setenv("PASTIX_GPU_MIXED_GEMM", "fp32")
+
+
+def test_tf32_tensor_core_factor_and_refinement():
+    """The mixed factorization's large update GEMMs run on tcgen05 with TF32
+    operands: the factor stays within TF32 accuracy of the reference's FP32
+    factor and CG refinement still reaches 1e-12."""
+    A = M.diffusion_lognormal(26, 25, 24, 1.0, np.random.default_rng(12))
+    ref, st = U.run_reference(A, "potrf", mixed=True)
+    g = U.gpu_structure(A, st)
+    lay = U.layout_of(g)
+    Lr, _ = U.ref_coeftab_1d(ref, st, lay)
+    s = _gpu_solver(A, st, "potrf", mixed=True, refine="cg")
+    s.numfact(A.values)
+    stats = s.stats()
+    assert stats["tc_flops"] > 0.3 * stats["gemm_flops"], stats
+    assert stats["tc_timeouts"] == 0
+    Lg, _ = s.coeftab()
+    mask = U.lower_mask(lay)
+    err = np.abs(Lg.astype(np.float64) - Lr)[mask].max() / np.abs(Lr).max()
+    assert err <= 2e-2, err
+    x, b = M.rhs_from_xtrue(A, 1, np.random.default_rng(6))
+    xs = s.solve_and_refine(b)
+    r = b - A.to_scipy_full() @ xs
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1e-12
