@@ -147,8 +147,30 @@ def fma_peaks():
     lib = C.CDLL(os.path.join(ROOT, "pastix_b200", "lib", "libpgpu_peak.so"))
     lib.pgpu_peak_fma_tflops.restype = C.c_double
     lib.pgpu_peak_fma_tflops.argtypes = [C.c_int, C.c_int]
-    return {"fp64_fma_tflops": lib.pgpu_peak_fma_tflops(0, 20000),
-            "fp32_fma_tflops": lib.pgpu_peak_fma_tflops(1, 40000)}
+    out = {"fp64_fma_tflops": lib.pgpu_peak_fma_tflops(0, 20000),
+           "fp32_fma_tflops": lib.pgpu_peak_fma_tflops(1, 40000)}
+    # TF32 tensor-core rate of cuBLAS (fp32 matmul with TF32 allowed), 8192^3,
+    # best of 10 -- the denominator for the tcgen05 TF32 update GEMM
+    import torch
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    a = torch.randn(8192, 8192, device="cuda")
+    bm = torch.randn(8192, 8192, device="cuda")
+    for _ in range(3):
+        a @ bm
+    best = 1e30
+    for _ in range(10):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ bm
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    out["tf32_cublas_tflops"] = 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+    del a, bm
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -183,7 +205,7 @@ def run_arm(A, st, b, mixed, steps, warmup, fact, refine):
     torch.cuda.synchronize()
     per = []
     launches = 0
-    gemm_ms = gemm_flops = 0.0
+    gemm_ms = gemm_flops = tc_ms = tc_flops = 0.0
     iters = []
     t0 = time.perf_counter()
     for _ in range(steps):
@@ -192,6 +214,8 @@ def run_arm(A, st, b, mixed, steps, warmup, fact, refine):
         launches += int(st_["numfact_launches"] + st_["solve_launches"] + st_["refine_launches"])
         gemm_ms += st_["gemm_ms"]
         gemm_flops += st_["gemm_flops"]
+        tc_ms += st_["tc_ms"]
+        tc_flops += st_["tc_flops"]
         iters.append(int(ip[G.IPARM_NBITER]))
     torch.cuda.synchronize()
     wall = (time.perf_counter() - t0) / steps
@@ -210,6 +234,7 @@ def run_arm(A, st, b, mixed, steps, warmup, fact, refine):
         "device_s": float(np.median(per)) / 1e3, "device_s_all": [p / 1e3 for p in per], "wall_s": wall,
         "e2e_s": float(np.median(e2e)), "launches_per_step": launches / steps, "launches": launches,
         "gemm_ms_per_step": gemm_ms / steps, "gemm_flops_per_step": gemm_flops / steps,
+        "tc_ms_per_step": tc_ms / steps, "tc_flops_per_step": tc_flops / steps,
         "refine_iters": iters[-1], "factor_ms": last["numfact_ms"], "solve_ms": last["solve_ms"],
         "refine_ms": last["refine_ms"], "diag_ms": last["diag_ms"], "trsm_ms": last["trsm_ms"],
         "fact_gflops": float(dp[G.DPARM_FACT_FLOPS]), "thflops": float(dp[G.DPARM_FACT_THFLOPS]),
@@ -309,7 +334,14 @@ def main():
     err_d = errors(A, b, fp64["x"], xtrue)
     err_e = errors(A, b, mixed["x_e2e"], xtrue)
     g_ach = mixed["gemm_flops_per_step"] / (mixed["gemm_ms_per_step"] * 1e-3) / 1e12
-    peak32 = peaks.get("fp32_fma_tflops")
+    tc_ach = (mixed["tc_flops_per_step"] / (mixed["tc_ms_per_step"] * 1e-3) / 1e12
+              if mixed["tc_ms_per_step"] > 0 else None)
+    peak_tf32 = peaks.get("tf32_cublas_tflops")
+    bf16_peak = None
+    try:
+        bf16_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]
+    except Exception:
+        bf16_peak = 1590.0
     g64 = fp64["gemm_flops_per_step"] / (fp64["gemm_ms_per_step"] * 1e-3) / 1e12
     peak64 = peaks.get("fp64_fma_tflops")
     line = {
@@ -328,12 +360,17 @@ def main():
                   "refine_iters": mixed["refine_iters"], "fact_gflops": mixed["fact_gflops"], "errors": err_m,
                   "wall_s": mixed["wall_s"], "device_s_all": mixed["device_s_all"]},
         "mixed_speedup_vs_fp64": fp64_v / value,
-        "roofline": {"bound": "tensor", "kernel": "k_gemm_scatter (update GEMM + scatter-add), FP32 FMA",
-                     "achieved": g_ach, "peak": peak32, "unit": "TFLOP/s",
-                     "frac": g_ach / peak32 if peak32 else None, "traffic": None,
-                     "peak_source": "measured FP32 FMA microbenchmark (pastix_b200/csrc/peak.cu); "
-                                    "MEASURED_PEAKS.json has no FP32/FP64 CUDA-core peak",
-                     "algorithmic_flops_per_step": mixed["gemm_flops_per_step"]},
+        "roofline": {"bound": "tensor",
+                     "kernel": "k_gemm_scatter_tc<3xTF32> (tcgen05 update GEMM + scatter-add)",
+                     "achieved": tc_ach, "peak": peak_tf32, "unit": "TFLOP/s",
+                     "frac": tc_ach / peak_tf32 if (peak_tf32 and tc_ach) else None, "traffic": None,
+                     "peak_source": "measured cuBLAS TF32 GEMM 8192^3 on this GPU (torch.matmul, allow_tf32); "
+                                    "MEASURED_PEAKS.json has BF16 only (%.1f TFLOP/s)" % bf16_peak,
+                     "frac_of_bf16_measured": tc_ach / bf16_peak if (bf16_peak and tc_ach) else None,
+                     "algorithmic_flops_per_step": mixed["tc_flops_per_step"],
+                     "tc_ms_per_step": mixed["tc_ms_per_step"],
+                     "all_gemm": {"achieved": g_ach, "algorithmic_flops_per_step": mixed["gemm_flops_per_step"],
+                                  "ms_per_step": mixed["gemm_ms_per_step"]}},
         "e2e": {"value": e2e_v, "unit": "s", "h2d_bytes_per_step": int(A.nnz * 8 + b.size * 8),
                 "d2h_bytes_per_step": int(b.size * 8), "errors": err_e},
         "gpu_launches": int(mixed["launches"]),

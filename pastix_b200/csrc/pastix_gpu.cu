@@ -419,11 +419,17 @@ static int fuse_rows_for(bool lu, bool fp32) {
 static const int TRSM_TR = 32;   // panel rows per k_trsm_rows CTA
 
 // Single-precision update GEMMs large enough for a 128 x 128 tensor-core tile
-// go to k_gemm_scatter_tc (TF32 operands) unless PASTIX_GPU_MIXED_GEMM=fp32.
-static bool tc_enabled() {
+// go to k_gemm_scatter_tc.  PASTIX_GPU_MIXED_GEMM selects the operand mode:
+// "3xtf32" (default; split products, about FP32 accuracy), "tf32" (one TF32
+// product) or "fp32" (no tensor cores: FP32 FMA tiles only).
+enum { MG_FP32 = 0, MG_TF32 = 1, MG_3XTF32 = 2 };
+static int mixed_gemm_mode() {
     const char *e = getenv("PASTIX_GPU_MIXED_GEMM");
-    return !(e && std::strcmp(e, "fp32") == 0);
+    if (e && std::strcmp(e, "fp32") == 0) return MG_FP32;
+    if (e && std::strcmp(e, "tf32") == 0) return MG_TF32;
+    return MG_3XTF32;
 }
+static bool tc_enabled() { return mixed_gemm_mode() != MG_FP32; }
 static bool tc_task(int M, int N, int K) { return K >= 32 && M >= 64 && N >= 32 && (int64_t)M * N >= 128 * 64; }
 
 static int build_fact_plan(pastix_gpu_t &C, int fact, bool fp32) {
@@ -544,8 +550,13 @@ static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, Lau
     PGPU_CHECK(cudaFuncSetAttribute(kpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(k_trsm_rows<T, TRSM_TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     SMEM_LIMIT));
-    if constexpr (sizeof(T) == 4)
-        PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    const bool split = (mixed_gemm_mode() == MG_3XTF32);
+    if constexpr (sizeof(T) == 4) {
+        PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        tc_smem_bytes<false>()));
+        PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        tc_smem_bytes<true>()));
+    }
     int nl = 0, ngemm = 0;
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
@@ -576,8 +587,12 @@ static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, Lau
             const int ntc = C.tctile_ptr[l + 1] - C.tctile_ptr[l];
             if (ntc) {
                 PGPU_CHECK(tm.mark(PH_TC));
-                k_gemm_scatter_tc<<<ntc, TC_THREADS, TC_SMEM, s>>>(C.meta, C.d_tctiles.p + C.tctile_ptr[l],
-                                                                  C.d_tasks.p, coefL, coefU, C.d_status.p);
+                if (split)
+                    k_gemm_scatter_tc<true><<<ntc, TC_THREADS, tc_smem_bytes<true>(), s>>>(
+                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p);
+                else
+                    k_gemm_scatter_tc<false><<<ntc, TC_THREADS, tc_smem_bytes<false>(), s>>>(
+                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p);
                 nl++;
                 ngemm++;
             }

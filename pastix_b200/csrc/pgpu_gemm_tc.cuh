@@ -1,18 +1,26 @@
 // Update GEMM with indexed scatter-add on the 5th-generation tensor cores
 // (tcgen05, sm_100a) for the single-precision factorization: C = A B^T with
 // A = panel rows [arow0 + i0, +128) of cblk c, B = rows [browoff_b + j0, +128)
-// of block b, K = w_c, FP32 operands read as TF32, FP32 accumulation in TMEM;
-// C is subtracted from the facing cblk f at (panel row of the source row in
-// f, frownum_b + j - fcolnum_f), as kernels/core_zgemmsp.c:104
-// core_zgemmsp_1d1d + core_zgeadd do.
+// of block b, K = w_c, FP32 accumulation in TMEM; C is subtracted from the
+// facing cblk f at (panel row of the source row in f, frownum_b + j -
+// fcolnum_f), as kernels/core_zgemmsp.c:104 core_zgemmsp_1d1d + core_zgeadd do.
+//
+// Two operand modes:
+//   SPLIT = false: the FP32 operands are read as TF32 (one MMA per k-step);
+//   SPLIT = true : "3xTF32" -- every operand is split into x = hi + lo with
+//                  hi = tf32(x) (round to nearest) and lo = x - hi, and
+//                  A B^T ~ lo_a hi_b + hi_a lo_b + hi_a hi_b (three MMAs per
+//                  k-step, small terms first), which keeps about FP32 accuracy.
 //
 // Per CTA (128 threads, one 128 x 128 output tile):
 //   * A and B k-blocks (128 rows x 32 floats = 128 B per row) are staged in
-//     shared memory with cp.async in the canonical K-major SWIZZLE_128B layout
-//     (8-row groups of 1024 B, 16-byte chunk c of row r stored at chunk
-//     c ^ (r & 7)), TC_STAGES deep;
-//   * one thread issues 4 tcgen05.mma.kind::tf32 (K = 8 each) per k-block and
-//     commits them to the stage's mbarrier, which frees the stage;
+//     shared memory in the canonical K-major SWIZZLE_128B layout (8-row groups
+//     of 1024 B, 16-byte chunk c of row r stored at chunk c ^ (r & 7)):
+//     with cp.async TC_STAGES deep (TF32), or through registers where the
+//     split happens, double-buffered with the next k-block's global loads in
+//     flight while the current MMAs run (3xTF32);
+//   * one thread issues the tcgen05.mma (K = 8 each) of a k-block and commits
+//     them to the stage's mbarrier, which frees the stage;
 //   * the accumulator (128 lanes x 128 fp32 columns of TMEM) is read back with
 //     tcgen05.ld by the 4 warps (warp w owns lanes 32w..32w+31), transposed
 //     through shared memory so a warp's atomics hit 32 consecutive columns.
@@ -25,9 +33,19 @@
 
 namespace pgpu {
 
-constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_STAGES = 3, TC_THREADS = 128;
-constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 4;              // 16 KB per operand per stage
-constexpr int TC_SMEM = TC_STAGES * 2 * TC_TILE_BYTES + 1024;  // + alignment slack
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_THREADS = 128;
+constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 4;                     // 16 KB per operand tile
+template <bool SPLIT> struct TcCfg;
+template <> struct TcCfg<false> {
+    static constexpr int STAGES = 3, TILES = 2;                        // A, B
+};
+template <> struct TcCfg<true> {
+    static constexpr int STAGES = 2, TILES = 4;                        // A hi, A lo, B hi, B lo
+};
+template <bool SPLIT>
+constexpr int tc_smem_bytes() {
+    return TcCfg<SPLIT>::STAGES * TcCfg<SPLIT>::TILES * TC_TILE_BYTES + 1024;   // + alignment slack
+}
 constexpr int TC_TMEM_COLS = 128;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -114,12 +132,26 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Round to TF32 (nearest, ties away) -- the "hi" part of the 3xTF32 split.
+__device__ __forceinline__ float tf32_hi(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void sts128(uint32_t saddr, float4 v) {
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(saddr), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+                 : "memory");
+}
+
+template <bool SPLIT>
 __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const int4 *__restrict__ tiles,
                                                                 const GemmTask *__restrict__ tasks,
                                                                 float *__restrict__ coefL,
                                                                 float *__restrict__ coefU, Status *st) {
+    constexpr int S = TcCfg<SPLIT>::STAGES, NT = TcCfg<SPLIT>::TILES;
     extern __shared__ __align__(16) unsigned char tc_smem_raw[];
-    __shared__ __align__(8) uint64_t mbar[TC_STAGES];
+    __shared__ __align__(8) uint64_t mbar[S];
     __shared__ uint32_t tmem_base_s;
     __shared__ int trow_s[TC_BM];
     __shared__ int fail_s;
@@ -148,7 +180,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int s = 0; s < TC_STAGES; s++) mbar_init(smem_u32(&mbar[s]), 1);
+        for (int s = 0; s < S; s++) mbar_init(smem_u32(&mbar[s]), 1);
         fail_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -162,65 +194,134 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_s;
 
-    auto stageA = [&](int s) { return base + (uint32_t)(s * 2) * TC_TILE_BYTES; };
-    auto stageB = [&](int s) { return base + (uint32_t)(s * 2 + 1) * TC_TILE_BYTES; };
-    auto load_stage = [&](int s, int kb) {
-        const int k0 = kb * TC_BK;
-        // 128 rows x 8 chunks of 16 B for each operand; 16 chunks per thread
+    // operand tile q (0 A / 1 B for TF32; 0 A hi, 1 A lo, 2 B hi, 3 B lo split) of stage s
+    auto tile_addr = [&](int s, int q) { return base + (uint32_t)(s * NT + q) * TC_TILE_BYTES; };
+    const uint32_t idesc = tc_idesc();
+    auto issue = [&](int s, int kb) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-        for (int q = 0; q < (TC_BM * 8) / TC_THREADS; q++) {
-            const int e = tid + q * TC_THREADS;
-            const int r = e >> 3, ch = e & 7;
-            const int kc = k0 + ch * 4;
-            const uint32_t soff = (uint32_t)(r * 128 + ((ch ^ (r & 7)) << 4));
-            const bool va = (r < mrows) && (kc < K);
-            cp_async16(stageA(s) + soff, va ? (const void *)(A + (int64_t)r * ld + kc) : (const void *)A, va);
-            const bool vb = (r < ncols) && (kc < K);
-            cp_async16(stageB(s) + soff, vb ? (const void *)(B + (int64_t)r * ld + kc) : (const void *)B, vb);
+        for (int kk = 0; kk < TC_BK / 8; kk++) {
+            const uint32_t first = (kb > 0 || kk > 0) ? 1u : 0u;
+            if (SPLIT) {
+                const uint64_t ah = tc_sdesc(tile_addr(s, 0) + kk * 32), al = tc_sdesc(tile_addr(s, 1) + kk * 32);
+                const uint64_t bh = tc_sdesc(tile_addr(s, 2) + kk * 32), bl = tc_sdesc(tile_addr(s, 3) + kk * 32);
+                tc_mma(tmem, al, bh, idesc, first);
+                tc_mma(tmem, ah, bl, idesc, 1u);
+                tc_mma(tmem, ah, bh, idesc, 1u);
+            } else {
+                tc_mma(tmem, tc_sdesc(tile_addr(s, 0) + kk * 32), tc_sdesc(tile_addr(s, 1) + kk * 32), idesc, first);
+            }
         }
+        tc_commit(smem_u32(&mbar[s]));
     };
 
-    const uint32_t idesc = tc_idesc();
-#pragma unroll
-    for (int s = 0; s < TC_STAGES - 1; s++) {
-        if (s < nk) load_stage(s, s);
-        cp_async_commit();
-    }
     bool ok = true;
-    for (int kb = 0; kb < nk; kb++) {
-        const int s = kb % TC_STAGES;
-        const int pk = kb + TC_STAGES - 1;
-        if (pk < nk) {
-            const int ps = pk % TC_STAGES;
-            if (kb >= 1) {
-                // stage ps was last read by the MMAs of k-block kb-1
-                if (!mbar_wait(smem_u32(&mbar[ps]), (uint32_t)(((kb - 1) / TC_STAGES) & 1))) ok = false;
-            }
-            if (ok) load_stage(ps, pk);
-        }
-        cp_async_commit();
-        cp_async_wait<TC_STAGES - 1>();
-        tc_fence_async_smem();
-        if (!__syncthreads_and(ok ? 1 : 0)) {
-            ok = false;
-            break;
-        }
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if constexpr (!SPLIT) {
+        auto load_stage = [&](int s, int kb) {
+            const int k0 = kb * TC_BK;
+            // 128 rows x 8 chunks of 16 B for each operand; 8 chunks per thread each
 #pragma unroll
-            for (int kk = 0; kk < TC_BK / 8; kk++) {
-                const uint64_t ad = tc_sdesc(stageA(s) + kk * 32);
-                const uint64_t bd = tc_sdesc(stageB(s) + kk * 32);
-                tc_mma(tmem, ad, bd, idesc, (kb > 0 || kk > 0) ? 1u : 0u);
+            for (int q = 0; q < (TC_BM * 8) / TC_THREADS; q++) {
+                const int e = tid + q * TC_THREADS;
+                const int r = e >> 3, ch = e & 7;
+                const int kc = k0 + ch * 4;
+                const uint32_t soff = (uint32_t)(r * 128 + ((ch ^ (r & 7)) << 4));
+                const bool va = (r < mrows) && (kc < K);
+                cp_async16(tile_addr(s, 0) + soff, va ? (const void *)(A + (int64_t)r * ld + kc) : (const void *)A,
+                           va);
+                const bool vb = (r < ncols) && (kc < K);
+                cp_async16(tile_addr(s, 1) + soff, vb ? (const void *)(B + (int64_t)r * ld + kc) : (const void *)B,
+                           vb);
             }
-            tc_commit(smem_u32(&mbar[s]));
+        };
+#pragma unroll
+        for (int s = 0; s < S - 1; s++) {
+            if (s < nk) load_stage(s, s);
+            cp_async_commit();
+        }
+        for (int kb = 0; kb < nk; kb++) {
+            const int s = kb % S;
+            const int pk = kb + S - 1;
+            if (pk < nk) {
+                const int ps = pk % S;
+                if (kb >= 1) {
+                    // stage ps was last read by the MMAs of k-block kb-1
+                    if (!mbar_wait(smem_u32(&mbar[ps]), (uint32_t)(((kb - 1) / S) & 1))) ok = false;
+                }
+                if (ok) load_stage(ps, pk);
+            }
+            cp_async_commit();
+            cp_async_wait<S - 1>();
+            tc_fence_async_smem();
+            if (!__syncthreads_and(ok ? 1 : 0)) {
+                ok = false;
+                break;
+            }
+            if (tid == 0) issue(s, kb);
+        }
+    } else {
+        // 3xTF32: global -> registers -> (hi, lo) -> swizzled shared memory
+        constexpr int CH = (TC_BM * 8) / TC_THREADS;     // 8 chunks of 16 B per operand per thread
+        float4 ra[CH], rb[CH];
+        auto gload = [&](int kb) {
+            const int k0 = kb * TC_BK;
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                const int e = tid + q * TC_THREADS;
+                const int r = e >> 3, ch = e & 7;
+                const int kc = k0 + ch * 4;
+                ra[q] = ((r < mrows) && (kc < K)) ? __ldg(reinterpret_cast<const float4 *>(A + (int64_t)r * ld + kc))
+                                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+                rb[q] = ((r < ncols) && (kc < K)) ? __ldg(reinterpret_cast<const float4 *>(B + (int64_t)r * ld + kc))
+                                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        };
+        auto split_store = [&](int s) {
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                const int e = tid + q * TC_THREADS;
+                const int r = e >> 3, ch = e & 7;
+                const uint32_t soff = (uint32_t)(r * 128 + ((ch ^ (r & 7)) << 4));
+                float4 h, l;
+                h.x = tf32_hi(ra[q].x); h.y = tf32_hi(ra[q].y); h.z = tf32_hi(ra[q].z); h.w = tf32_hi(ra[q].w);
+                l.x = ra[q].x - h.x; l.y = ra[q].y - h.y; l.z = ra[q].z - h.z; l.w = ra[q].w - h.w;
+                sts128(tile_addr(s, 0) + soff, h);
+                sts128(tile_addr(s, 1) + soff, l);
+                h.x = tf32_hi(rb[q].x); h.y = tf32_hi(rb[q].y); h.z = tf32_hi(rb[q].z); h.w = tf32_hi(rb[q].w);
+                l.x = rb[q].x - h.x; l.y = rb[q].y - h.y; l.z = rb[q].z - h.z; l.w = rb[q].w - h.w;
+                sts128(tile_addr(s, 2) + soff, h);
+                sts128(tile_addr(s, 3) + soff, l);
+            }
+        };
+        if (nk > 0) {
+            gload(0);
+            split_store(0);
+        }
+        tc_fence_async_smem();
+        __syncthreads();
+        for (int kb = 0; kb < nk; kb++) {
+            const int s = kb & 1;
+            if (tid == 0) issue(s, kb);
+            if (kb + 1 < nk) {
+                gload(kb + 1);                       // in flight while the MMAs of kb run
+                if (kb >= 1) {
+                    // stage s^1 was last read by the MMAs of k-block kb-1
+                    if (!mbar_wait(smem_u32(&mbar[s ^ 1]), (uint32_t)(((kb - 1) >> 1) & 1))) ok = false;
+                }
+                if (ok) split_store(s ^ 1);
+                tc_fence_async_smem();
+            }
+            if (!__syncthreads_and(ok ? 1 : 0)) {
+                ok = false;
+                break;
+            }
         }
     }
     // all MMAs done when the last commit's barrier flips
     if (ok && nk > 0) {
-        if (!mbar_wait(smem_u32(&mbar[(nk - 1) % TC_STAGES]), (uint32_t)(((nk - 1) / TC_STAGES) & 1))) ok = false;
+        if (!mbar_wait(smem_u32(&mbar[(nk - 1) % S]), (uint32_t)(((nk - 1) / S) & 1))) ok = false;
     }
-    cp_async_wait<0>();
+    if constexpr (!SPLIT) cp_async_wait<0>();
     if (!ok) atomicExch(&fail_s, 1);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

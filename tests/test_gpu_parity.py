@@ -107,10 +107,13 @@ def fp32_gemm(monkeypatch):
     monkeypatch.setenv("PASTIX_GPU_MIXED_GEMM", "fp32")
 
 
-def test_tf32_tensor_core_factor_and_refinement():
+@pytest.mark.parametrize("mode,tol", [("3xtf32", 5e-4), ("tf32", 2e-2)])
+def test_tf32_tensor_core_factor_and_refinement(mode, tol, monkeypatch):
     """The mixed factorization's large update GEMMs run on tcgen05 with TF32
-    operands: the factor stays within TF32 accuracy of the reference's FP32
-    factor and CG refinement still reaches 1e-12."""
+    operands (one product, or the 3xTF32 split): the factor stays within that
+    mode's accuracy of the reference's FP32 factor and CG refinement still
+    reaches 1e-12."""
+    monkeypatch.setenv("PASTIX_GPU_MIXED_GEMM", mode)
     A = M.diffusion_lognormal(26, 25, 24, 1.0, np.random.default_rng(12))
     ref, st = U.run_reference(A, "potrf", mixed=True)
     g = U.gpu_structure(A, st)
@@ -124,7 +127,7 @@ def test_tf32_tensor_core_factor_and_refinement():
     Lg, _ = s.coeftab()
     mask = U.lower_mask(lay)
     err = np.abs(Lg.astype(np.float64) - Lr)[mask].max() / np.abs(Lr).max()
-    assert err <= 2e-2, err
+    assert err <= tol, err
     x, b = M.rhs_from_xtrue(A, 1, np.random.default_rng(6))
     xs = s.solve_and_refine(b)
     r = b - A.to_scipy_full() @ xs
