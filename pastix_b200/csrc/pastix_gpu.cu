@@ -124,6 +124,7 @@ struct pastix_gpu_s {
     DArr<unsigned char> d_work;   // solve workspace (n x 16 in factor precision)
     DArr<double> d_rhs, d_x, d_r, d_z, d_p, d_ap, d_gm;   // refinement vectors
     DArr<double> d_sr_b, d_sr_x;   // solve_and_refine staging of host B / X
+    DArr<double> d_gmV, d_gmW, d_gmh;   // GMRES basis, preconditioned basis, projections
     std::vector<cudaEvent_t> evpool;   // per-launch timing events
     double gemm_flops[5] = {0};        // update-GEMM flops per factotype
     double stats[16] = {0};
@@ -988,6 +989,104 @@ static int refine_cg(pastix_gpu_t &C, VecOps &V, const double *b, double *x, dou
     return PASTIX_GPU_SUCCESS;
 }
 
+// --------------------------------------------------------------------------
+// GMRES(im), right preconditioned (refinement/z_refine_gmres.c:49
+// z_gmres_smp, Saad Alg. 9.5): V holds the Krylov basis, W = M^{-1} V so the
+// solution update needs no extra solve; modified Gram-Schmidt with the
+// projections h_{j,i} kept in device memory (one host round trip per inner
+// iteration, for the Givens rotations on the small Hessenberg matrix).
+// --------------------------------------------------------------------------
+static int refine_gmres(pastix_gpu_t &C, VecOps &V, const double *b, double *x, double eps, int itermax, int im,
+                        int *iters_out, double *resid_out) {
+    const int64_t n = C.n;
+    const int im1 = im + 1;
+    if (C.d_gmV.n < (size_t)n * im1) {
+        PGPU_CHECK(C.d_gmV.alloc((size_t)n * im1));
+        PGPU_CHECK(C.d_gmW.alloc((size_t)n * im));
+    }
+    if (C.d_gmh.n < (size_t)2 * im1) PGPU_CHECK(C.d_gmh.alloc((size_t)2 * im1));
+    cudaStream_t s = C.stream;
+    double *gV = C.d_gmV.p, *gW = C.d_gmW.p, *dh = C.d_gmh.p;
+    std::vector<double> H((size_t)im * im1, 0.0), cs(im, 0.0), sn(im, 0.0), G(im1, 0.0), hcol(im1, 0.0);
+    double normb = V.norm(b);
+    if (normb == 0.) normb = 1;
+    const double normx = V.norm(x);
+    int iters = 0;
+    double resid_b = 0;
+    bool outflag = true;
+    while (outflag) {
+        // r0 = b - A x
+        V.copy(b, gV);
+        if (normx > 0. || iters > 0) V.spmv(-1.0, x, 1.0, gV);
+        double resid = V.norm(gV);
+        resid_b = resid / normb;
+        if (resid_b <= eps) break;
+        k_scal<<<1024, 256, 0, s>>>(n, 1.0 / resid, gV);
+        V.launches++;
+        std::fill(G.begin(), G.end(), 0.0);
+        G[0] = resid;
+        int i = -1;
+        bool inflag = true;
+        while (inflag) {
+            i++;
+            double *vi = gV + (int64_t)i * n, *wi = gW + (int64_t)i * n, *vn = gV + (int64_t)(i + 1) * n;
+            V.copy(vi, wi);
+            int rc = V.spsv(wi);                       // w_i = M^{-1} v_i
+            if (rc) return rc;
+            V.spmv(1.0, wi, 0.0, vn);                  // v_{i+1} = A w_i
+            for (int j = 0; j <= i; j++) {             // modified Gram-Schmidt
+                k_dot_partial<<<256, RED_THREADS, 0, s>>>(n, vn, gV + (int64_t)j * n, C.d_partial.p);
+                k_dot_final<<<1, RED_THREADS, 0, s>>>(256, C.d_partial.p, dh + j, 0);
+                k_axpy_dev<<<1024, 256, 0, s>>>(n, dh + j, -1.0, gV + (int64_t)j * n, vn);
+                V.launches += 3;
+            }
+            k_dot_partial<<<256, RED_THREADS, 0, s>>>(n, vn, nullptr, C.d_partial.p);
+            k_dot_final<<<1, RED_THREADS, 0, s>>>(256, C.d_partial.p, dh + i + 1, 1);
+            V.launches += 2;
+            PGPU_CHECK(cudaMemcpyAsync(hcol.data(), dh, (i + 2) * sizeof(double), cudaMemcpyDeviceToHost, s));
+            PGPU_CHECK(cudaStreamSynchronize(s));
+            const double norm = hcol[i + 1];
+            if (norm > 1e-50) {
+                k_scal<<<1024, 256, 0, s>>>(n, 1.0 / norm, vn);
+                V.launches++;
+            }
+            double *Hi = H.data() + (size_t)i * im1;
+            for (int j = 0; j <= i + 1; j++) Hi[j] = hcol[j];
+            for (int j = 0; j < i; j++) {              // previous Givens rotations
+                const double tmp = Hi[j];
+                Hi[j] = cs[j] * tmp + sn[j] * Hi[j + 1];
+                Hi[j + 1] = cs[j] * Hi[j + 1] - sn[j] * tmp;
+            }
+            double t = std::sqrt(Hi[i] * Hi[i] + Hi[i + 1] * Hi[i + 1]);
+            if (std::fabs(t) <= eps) t = eps;
+            cs[i] = Hi[i] / t;
+            sn[i] = Hi[i + 1] / t;
+            G[i + 1] = -sn[i] * G[i];
+            G[i] = cs[i] * G[i];
+            Hi[i] = cs[i] * Hi[i] + sn[i] * Hi[i + 1];
+            resid = std::fabs(G[i + 1]);
+            resid_b = resid / normb;
+            iters++;
+            if (i + 1 >= im || resid_b <= eps || iters >= itermax) inflag = false;
+        }
+        // y = H^{-1} g (upper triangular, size i+1), x += W y
+        const int k = i + 1;
+        for (int r = k - 1; r >= 0; r--) {
+            double sum = G[r];
+            for (int j = r + 1; j < k; j++) sum -= H[(size_t)j * im1 + r] * G[j];
+            G[r] = sum / H[(size_t)r * im1 + r];
+        }
+        PGPU_CHECK(cudaMemcpyAsync(dh, G.data(), k * sizeof(double), cudaMemcpyHostToDevice, s));
+        k_gemv_acc<<<1024, 256, 0, s>>>(n, k, gW, n, dh, x);
+        V.launches++;
+        PGPU_CHECK(cudaStreamSynchronize(s));
+        if (iters >= itermax) outflag = false;
+    }
+    *iters_out = iters;
+    *resid_out = resid_b;
+    return PASTIX_GPU_SUCCESS;
+}
+
 static int ensure_refine_vectors(pastix_gpu_t &C) {
     const size_t n = C.n;
     if (C.d_r.n < n) {
@@ -1009,7 +1108,8 @@ static int refine_impl(pastix_gpu_t &C, int64_t nrhs, const void *B, int64_t ldb
     if (eps < 0.) eps = 1e-12;   // refinement/pastix_task_refine.c:131-140 (double input)
     const int itermax = (int)C.iparm[PGPU_IPARM_ITERMAX];
     const int method = (int)C.iparm[PGPU_IPARM_REFINEMENT];
-    if (method != PGPU_REFINE_CG) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    if (method != PGPU_REFINE_CG && method != PGPU_REFINE_GMRES) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    const int im = std::max<int>(1, (int)C.iparm[PGPU_IPARM_GMRES_IM]);
     const bool bdev = is_device_ptr(B), xdev = is_device_ptr(X);
     VecOps V{C};
     int maxit = 0;
@@ -1025,7 +1125,8 @@ static int refine_impl(pastix_gpu_t &C, int64_t nrhs, const void *B, int64_t ldb
                                    xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
         int it = 0;
         double res = 0;
-        rc = refine_cg(C, V, db, dx, eps, itermax, &it, &res);
+        rc = (method == PGPU_REFINE_CG) ? refine_cg(C, V, db, dx, eps, itermax, &it, &res)
+                                        : refine_gmres(C, V, db, dx, eps, itermax, im, &it, &res);
         if (rc) return rc;
         PGPU_CHECK(cudaMemcpyAsync(xcol, dx, C.n * sizeof(double),
                                    xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));

@@ -292,6 +292,33 @@ __global__ void k_xpby(int64_t n, const double *__restrict__ z, double beta, dou
         p[i] = z[i] + beta * p[i];
 }
 
+// y += sign * (*alpha) * x with the scalar read from device memory (GMRES
+// orthogonalization without a host round trip per projection).
+__global__ void k_axpy_dev(int64_t n, const double *__restrict__ alpha, double sign, const double *__restrict__ x,
+                           double *__restrict__ y) {
+    const double a = sign * (*alpha);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        y[i] += a * x[i];
+}
+
+__global__ void k_scal(int64_t n, double a, double *__restrict__ x) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        x[i] *= a;
+}
+
+// x += W(:, 0:k) y  (bvec_zgemv, bcsc/bvec_zcompute.c; W column-major, ld ldw)
+__global__ void k_gemv_acc(int64_t n, int k, const double *__restrict__ W, int64_t ldw,
+                           const double *__restrict__ y, double *__restrict__ x) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int j = 0; j < k; j++) s += W[i + j * ldw] * y[j];
+        x[i] += s;
+    }
+}
+
 // Gather the permuted-matrix values from the user's values.
 __global__ void k_gather_vals(int64_t nnz, const int64_t *__restrict__ src, const double *__restrict__ vals,
                               double *__restrict__ out) {

@@ -132,3 +132,38 @@ def test_tf32_tensor_core_factor_and_refinement(mode, tol, monkeypatch):
     xs = s.solve_and_refine(b)
     r = b - A.to_scipy_full() @ xs
     assert np.linalg.norm(r) / np.linalg.norm(b) <= 1e-12
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_lu_gmres_refinement_reaches_1e12(mixed):
+    """GETRF + GMRES(30) (refinement/z_refine_gmres.c) on the upwind
+    convection-diffusion operator; FP32 factors use the tensor-core GEMM."""
+    A = M.convdiff_upwind(18, 17, 16, 10.0)
+    ref, st = U.run_reference(A, "getrf", numfact=False)
+    s = _gpu_solver(A, st, "getrf", mixed=mixed, refine="gmres")
+    from pastix_b200 import gpu as G
+    s.set_iparm(G.IPARM_GMRES_IM, 30)
+    s.numfact(A.values)
+    x, b = M.rhs_from_xtrue(A, 4, np.random.default_rng(9))
+    xs = s.solve_and_refine(b)
+    Af = A.to_scipy_full()
+    r = b - Af @ xs
+    assert (np.linalg.norm(r, axis=0) / np.linalg.norm(b, axis=0)).max() <= 1e-12
+    bwd = np.abs(r).max() / (abs(Af).sum(axis=1).max() * np.abs(xs).max() + np.abs(b).max())
+    assert bwd <= 1e-12
+    assert np.abs(xs - x).max() <= 1e-8
+
+
+@pytest.mark.parametrize("name,make", [("cd10", lambda: M.convdiff_upwind(10, 10, 10, 10.0)),
+                                       ("cd20x18x16", lambda: M.convdiff_upwind(20, 18, 16, 10.0))])
+def test_mixed_lu_factor_matches_reference_mixed(name, make, fp32_gemm):
+    A = make()
+    ref, st = U.run_reference(A, "getrf", mixed=True)
+    g = U.gpu_structure(A, st)
+    lay = U.layout_of(g)
+    Lr, Ur = U.ref_coeftab_1d(ref, st, lay)
+    s = _gpu_solver(A, st, "getrf", mixed=True)
+    s.numfact(A.values)
+    Lg, Ug = s.coeftab()
+    assert np.abs(Lg.astype(np.float64) - Lr).max() <= 5e-5 * np.abs(Lr).max()
+    assert np.abs(Ug.astype(np.float64) - Ur).max() <= 5e-5 * np.abs(Ur).max()
