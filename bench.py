@@ -377,8 +377,8 @@ def main():
                      "tc_ms_per_step": mixed["tc_ms_per_step"],
                      "all_gemm": {"achieved": g_ach, "algorithmic_flops_per_step": mixed["gemm_flops_per_step"],
                                   "ms_per_step": mixed["gemm_ms_per_step"]}},
-        "e2e": {"value": e2e_v, "unit": "s", "h2d_bytes_per_step": int(A.nnz * 8 + b.size * 8),
-                "d2h_bytes_per_step": int(b.size * 8), "errors": err_e},
+        "e2e": {"value": e2e_v, "unit": "s", "h2d_bytes_per_step": int(A.values.nbytes + b.nbytes),
+                "d2h_bytes_per_step": int(b.nbytes), "errors": err_e},
         "gpu_launches": int(mixed["launches"]),
         "analysis_s": t_an, "peaks": peaks,
     }

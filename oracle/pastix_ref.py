@@ -12,6 +12,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_ref", "libpastix_ref.so")
+# the same build with the one-increment fix of core_zhetf2sp (see
+# oracle/refbuild/build_ref.py HEFIX): pins the LDL^h of complex matrices
+LIB_HEFIX = os.path.join(HERE, "_ref", "libpastix_ref_hefix.so")
 
 # include/pastix/api.h enumerations (iparm / dparm indices, values)
 IPARM = {k: i for i, k in enumerate("""VERBOSE IO_STRATEGY NNZEROS NNZEROS_BLOCK_LOCAL ALLOCATED_TERMS
@@ -39,19 +42,18 @@ SCHED_STATIC = 1
 
 NC, NB = 10, 8     # columns of the exported cblk / blok tables (ref_glue.c)
 
-_lib = None
+_libs = {}
 
 
-def available():
-    return os.path.exists(LIB)
+def available(variant=None):
+    return os.path.exists(LIB_HEFIX if variant == "hefix" else LIB)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not available():
+def lib(variant=None):
+    if variant not in _libs:
+        if not available(variant):
             raise RuntimeError("reference oracle not built: run oracle/refbuild/build_ref.py")
-        L = C.CDLL(LIB)
+        L = C.CDLL(LIB_HEFIX if variant == "hefix" else LIB)
         P, I64, I = C.c_void_p, C.c_int64, C.c_int
         L.ref_create.restype = P
         L.ref_create.argtypes = [I, I]
@@ -74,8 +76,8 @@ def lib():
         L.ref_order_dump.argtypes = [P, P, P]
         L.ref_coeftab_dump.argtypes = [P, P, P]
         L.ref_destroy.argtypes = [P]
-        _lib = L
-    return _lib
+        _libs[variant] = L
+    return _libs[variant]
 
 
 def _ptr(a):
@@ -86,8 +88,10 @@ class RefSolver:
     """One reference pastix instance (pastix_data_t) on one matrix."""
 
     def __init__(self, system, fact="potrf", nthreads=1, mixed=False, refine=None,
-                 eps_refine=None, itermax=None, gmres_im=None, verbose=0, iparm=None, dparm=None):
-        L = lib()
+                 eps_refine=None, itermax=None, gmres_im=None, verbose=0, iparm=None, dparm=None,
+                 variant=None):
+        self.variant = variant
+        L = lib(variant)
         self.sys = system
         self.h = L.ref_create(nthreads, verbose)
         self.set_iparm("FACTORIZATION", FACT[fact])
@@ -116,32 +120,32 @@ class RefSolver:
             raise RuntimeError("ref_set_matrix failed")
 
     def set_iparm(self, k, v):
-        lib().ref_set_iparm(self.h, IPARM[k], int(v))
+        lib(self.variant).ref_set_iparm(self.h, IPARM[k], int(v))
 
     def set_dparm(self, k, v):
-        lib().ref_set_dparm(self.h, DPARM[k], float(v))
+        lib(self.variant).ref_set_dparm(self.h, DPARM[k], float(v))
 
     def iparm(self, k):
-        return lib().ref_get_iparm(self.h, IPARM[k])
+        return lib(self.variant).ref_get_iparm(self.h, IPARM[k])
 
     def dparm(self, k):
-        return lib().ref_get_dparm(self.h, DPARM[k])
+        return lib(self.variant).ref_get_dparm(self.h, DPARM[k])
 
     def analyze(self):
         nx, ny, nz = self.sys.grid
-        rc = lib().ref_analyze_grid(self.h, nx, ny, nz)
+        rc = lib(self.variant).ref_analyze_grid(self.h, nx, ny, nz)
         if rc:
             raise RuntimeError("analysis failed: %d" % rc)
 
     def numfact(self):
-        rc = lib().ref_numfact(self.h)
+        rc = lib(self.variant).ref_numfact(self.h)
         if rc:
             raise RuntimeError("numfact failed: %d" % rc)
 
     def solve(self, b):
         x = np.asfortranarray(b.copy())
         nrhs = x.shape[1] if x.ndim == 2 else 1
-        rc = lib().ref_solve(self.h, nrhs, _ptr(x), self.sys.n)
+        rc = lib(self.variant).ref_solve(self.h, nrhs, _ptr(x), self.sys.n)
         if rc:
             raise RuntimeError("solve failed: %d" % rc)
         return x
@@ -150,14 +154,14 @@ class RefSolver:
         b = np.asfortranarray(b.copy())
         x = np.asfortranarray(x.copy())
         nrhs = x.shape[1] if x.ndim == 2 else 1
-        rc = lib().ref_refine(self.h, nrhs, _ptr(b), self.sys.n, _ptr(x), self.sys.n)
+        rc = lib(self.variant).ref_refine(self.h, nrhs, _ptr(b), self.sys.n, _ptr(x), self.sys.n)
         if rc:
             raise RuntimeError("refine failed: %d" % rc)
         return x
 
     def structure(self):
         """The SolverMatrix and ordering, as integer tables (ref_glue.c)."""
-        L = lib()
+        L = lib(self.variant)
         sz = np.zeros(16, np.int64)
         if L.ref_struct_sizes(self.h, _ptr(sz)):
             raise RuntimeError("no solver matrix")
@@ -187,12 +191,12 @@ class RefSolver:
         dt = {2: np.float32, 3: np.float64, 4: np.complex64, 5: np.complex128}[st["flttype"]]
         Lc = np.zeros(size, dt)
         Uc = np.zeros(size, dt) if st["factotype"] == FACT["getrf"] else None
-        lib().ref_coeftab_dump(self.h, _ptr(Lc), _ptr(Uc))
+        lib(self.variant).ref_coeftab_dump(self.h, _ptr(Lc), _ptr(Uc))
         return Lc, Uc
 
     def close(self):
         if self.h:
-            lib().ref_destroy(self.h)
+            lib(self.variant).ref_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -163,6 +163,46 @@ def compile_one(args):
     return obj, None
 
 
+# The reference's unblocked LDL^h kernel (kernels/core_zhetrfsp.c:91-92
+# core_zhetf2sp) copies column k of the diagonal block into row k with
+# cblas_zcopy(m, Amk, 1, Akm, lda) and then conjugates it with
+# LAPACKE_zlacgv_work(m, Akm, 1): increment 1 instead of lda, so it
+# conjugates m entries of column k+1 (the new diagonal and the lower
+# entries below it) instead of row k.  For a Hermitian matrix with non-real
+# off-diagonal entries the factors are then not those of A (real-valued
+# Hermitian matrices are unaffected).  libpastix_ref_hefix.so is the same
+# build with that one increment set to lda (in generated copies under
+# oracle/_ref/gen/hefix/), used to pin the GPU LDL^h on complex data.
+HEFIX = [("kernels/core_zhetrfsp.c", "z", "LAPACKE_zlacgv_work( m, Akm, 1 )", "LAPACKE_zlacgv_work( m, Akm, lda )"),
+         ("kernels/core_chetrfsp.c", "c", "LAPACKE_clacgv_work( m, Akm, 1 )", "LAPACKE_clacgv_work( m, Akm, lda )")]
+
+
+def build_hefix(units, blas):
+    fixdir = os.path.join(GEN, "hefix", "kernels")
+    os.makedirs(fixdir, exist_ok=True)
+    repl = {}
+    for rel, prec, old, new in HEFIX:
+        src = os.path.join(REF if prec == "z" else GEN, rel)
+        text = open(src).read()
+        if text.count(old) != 1:
+            raise RuntimeError("hefix: pattern not found once in %s" % src)
+        dst = os.path.join(fixdir, os.path.basename(rel))
+        with open(dst, "w") as f:
+            f.write(text.replace(old, new))
+        obj = os.path.join(OBJ, "hefix__" + os.path.basename(rel) + "." + prec + ".o")
+        o, err = compile_one((dst, prec, obj))
+        if err:
+            raise RuntimeError(err)
+        repl[src] = obj
+    objs = [repl.get(u[0], u[2]) for u in units]
+    if len([u for u in units if u[0] in repl]) != len(HEFIX):
+        raise RuntimeError("hefix: kernels not found among the compiled units")
+    so = os.path.join(OUT, "libpastix_ref_hefix.so")
+    subprocess.check_call(["gcc", "-shared", "-o", so] + objs +
+                          [blas, "-Wl,-Bsymbolic", "-Wl,--disable-new-dtags", "-Wl,-rpath," + os.path.dirname(blas),
+                           "-lm", "-pthread"])
+
+
 def main():
     if not os.path.isdir(REF):
         print("reference tree not present; skipping the reference build")
@@ -198,6 +238,7 @@ def main():
     cmd = ["gcc", "-shared", "-o", so] + objs + [blas, "-Wl,--disable-new-dtags", "-Wl,-rpath," + os.path.dirname(blas),
                                                  "-lm", "-pthread"]
     subprocess.check_call(cmd)
+    build_hefix(units, blas)
     drv = os.path.join(OUT, "pastix_ref_driver")
     cmd = ["gcc"] + CFLAGS + includes() + [os.path.join(HERE, "ref_driver.c"), "-o", drv,
                                            "-L" + OUT, "-lpastix_ref", "-Wl,-rpath,$ORIGIN",

@@ -11,10 +11,17 @@ after cblk, a column-major panel of `stride` rows and `width` columns; the
 diagonal block is rows [0, width), off-diagonal block b follows at the row
 offset given by the blocks before it.
 
-Algorithms followed:
+Algorithms followed (real or complex data; the Hermitian forms POTRF = LL^h
+and HETRF = LDL^h conjugate the transposed operand):
   fill-in      kernels/cpucblk_zinit.c:393  cpucblk_zfillin_fr
   POTRF        kernels/core_zpotrfsp.c:68,144,334 (core_zpotf2sp, static pivot)
   GETRF        kernels/core_zgetrfsp.c:64,217,355 (core_zgetf2sp, geadd/getmo)
+  SYTRF/HETRF  kernels/core_zsytrfsp.c:63,141,482 and core_zhetrfsp.c:63,144,491
+               (unit L, D on the diagonal; off-diagonal rows X (D op(L)^t) = A;
+               update C -= A D op(B)^t, core_zgemdm); for HETRF the
+               mathematically intended conjugation of core_zhetf2sp (the
+               reference's kernels/core_zhetrfsp.c:92 passes increment 1 where
+               the row has stride lda -- see oracle/refbuild/build_ref.py)
   TRSM         kernels/core_ztrsmsp.c:71  core_ztrsmsp_1d
   update GEMM  kernels/core_zgemmsp.c:104 core_zgemmsp_1d1d (GEMM + scatter-add)
   solve        kernels/solve_ztrsmsp.c:301,450 forward / backward
@@ -112,10 +119,10 @@ def _potf2(A, crit):
         if abs(A[k, k]) < crit:
             A[k, k] = crit
             piv += 1
-        A[k, k] = np.sqrt(A[k, k])
+        A[k, k] = np.sqrt(A[k, k].real)
         alpha = 1.0 / A[k, k]
         A[k + 1:, k] *= alpha
-        A[k + 1:, k + 1:] -= np.tril(np.outer(A[k + 1:, k], A[k + 1:, k]))
+        A[k + 1:, k + 1:] -= np.tril(np.outer(A[k + 1:, k], np.conj(A[k + 1:, k])))
     return piv
 
 
@@ -133,11 +140,39 @@ def _getf2(A, crit):
     return piv
 
 
+def _ldlf2(A, crit, herm):
+    """core_zsytf2sp / core_zhetf2sp on the lower triangle of a square block
+    (in place): unit L below the diagonal, D on it.  Returns #static pivots."""
+    n = A.shape[0]
+    piv = 0
+    for k in range(n):
+        if abs(A[k, k]) < crit:
+            A[k, k] = -crit if A[k, k].real < 0 else crit
+            piv += 1
+        d = A[k, k]
+        l = A[k + 1:, k] / d
+        A[k + 1:, k] = l
+        if herm:
+            A[k + 1:, k + 1:] -= np.tril(np.outer(l, np.conj(l))) * d.real       # zher, real alpha
+            i = np.arange(k + 1, n)
+            A[i, i] = A[i, i].real
+        else:
+            A[k + 1:, k + 1:] -= np.tril(np.outer(l * d, l))
+    return piv
+
+
+def _cj(herm):
+    return np.conj if herm else (lambda v: v)
+
+
 def factorize(layout, L, U, fact, crit):
     """Right-looking supernodal factorization in cblk order (in place).
     Returns the number of static pivots."""
     nbpiv = 0
     lu = fact == "getrf"
+    ldl = fact in ("sytrf", "hetrf")
+    herm = fact in ("potrf", "hetrf")
+    cj = _cj(herm)
     for c in range(layout.cblknbr):
         P = layout.panel(L, c)
         w = int(layout.width[c])
@@ -151,12 +186,23 @@ def factorize(layout, L, U, fact, crit):
                 P[w:, :] = solve_triangular(np.triu(D), P[w:, :].T, trans="T", lower=False).T
                 Lu = np.tril(D, -1) + np.eye(w)
                 PU[w:, :] = solve_triangular(Lu, PU[w:, :].T, lower=True, unit_diagonal=True).T
+        elif ldl:
+            Dl = np.tril(D)
+            nbpiv += _ldlf2(Dl, crit, fact == "hetrf")
+            D[:, :] = Dl + np.triu(D, 1)
+            if P.shape[0] > w:
+                Lu = np.tril(D, -1) + np.eye(w)
+                # X (D op(L)^t) = A  ->  Y op(L)^t = A, X = Y D^{-1}
+                Y = cj(solve_triangular(Lu, cj(P[w:, :]).T, lower=True, unit_diagonal=True).T)
+                P[w:, :] = Y / np.diag(D)[None, :]
         else:
             Dl = np.tril(D)
             nbpiv += _potf2(Dl, crit)
             D[:, :] = np.tril(Dl) + np.triu(D, 1)
             if P.shape[0] > w:
-                P[w:, :] = solve_triangular(np.tril(D), P[w:, :].T, lower=True).T
+                # X op(L)^t = A  ->  L conj(X)^t = conj(A)^t for LL^h
+                P[w:, :] = cj(solve_triangular(np.tril(D), cj(P[w:, :]).T, lower=True).T)
+        dg = np.diag(D).copy() if ldl else None
         rows = layout.rows(c)
         b0, b1 = layout.fblok[c], layout.fblok[c + 1]
         for b in range(b0 + 1, b1):
@@ -172,33 +218,46 @@ def factorize(layout, L, U, fact, crit):
                 if b + 1 < b1:
                     FU = layout.panel(U, f)
                     FU[np.ix_(tr[mb:], cols)] -= PU[r0 + mb:, :] @ P[r0:r0 + mb, :].T
+            elif ldl:
+                F[np.ix_(tr, cols)] -= (P[r0:, :] * dg[None, :]) @ cj(P[r0:r0 + mb, :]).T
             else:
-                F[np.ix_(tr, cols)] -= P[r0:, :] @ P[r0:r0 + mb, :].T
+                F[np.ix_(tr, cols)] -= P[r0:, :] @ cj(P[r0:r0 + mb, :]).T
     return nbpiv
 
 
 def solve(layout, L, U, fact, b):
-    """Forward/backward supernodal solve in the permuted numbering."""
+    """Forward/backward supernodal solve in the permuted numbering
+    (sopalin/sequential_ztrsm.c; LDL: the diagonal solve of
+    sopalin/sequential_zdiag.c between the two passes)."""
     x = np.array(b, dtype=np.result_type(L.dtype, b.dtype), copy=True)
     lu = fact == "getrf"
+    ldl = fact in ("sytrf", "hetrf")
+    herm = fact in ("potrf", "hetrf")
+    cj = _cj(herm)
     for c in range(layout.cblknbr):
         P = layout.panel(L, c)
         w, fc = int(layout.width[c]), int(layout.fcol[c])
         D = P[:w, :]
-        x[fc:fc + w] = solve_triangular(np.tril(D), x[fc:fc + w], lower=True, unit_diagonal=lu)
+        x[fc:fc + w] = solve_triangular(np.tril(D), x[fc:fc + w], lower=True, unit_diagonal=lu or ldl)
         if P.shape[0] > w:
             rows = layout.rows(c)[w:]
             np.subtract.at(x, rows, P[w:, :] @ x[fc:fc + w])
+    if ldl:
+        for c in range(layout.cblknbr):
+            P = layout.panel(L, c)
+            w, fc = int(layout.width[c]), int(layout.fcol[c])
+            x[fc:fc + w] /= np.diag(P[:w, :])
     for c in range(layout.cblknbr - 1, -1, -1):
         P = layout.panel(L, c)
         Q = layout.panel(U, c) if lu else P
         w, fc = int(layout.width[c]), int(layout.fcol[c])
         if P.shape[0] > w:
             rows = layout.rows(c)[w:]
-            x[fc:fc + w] -= Q[w:, :].T @ x[rows]
+            x[fc:fc + w] -= (Q[w:, :].T if lu else cj(Q[w:, :]).T) @ x[rows]
         D = P[:w, :]
         if lu:
             x[fc:fc + w] = solve_triangular(np.triu(D), x[fc:fc + w], lower=False)
         else:
-            x[fc:fc + w] = solve_triangular(np.tril(D), x[fc:fc + w], lower=True, trans="T")
+            x[fc:fc + w] = solve_triangular(np.tril(D), x[fc:fc + w], lower=True, trans="C" if herm else "T",
+                                            unit_diagonal=ldl)
     return x

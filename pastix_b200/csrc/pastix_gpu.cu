@@ -10,9 +10,11 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 using namespace pgpu;
@@ -88,7 +90,7 @@ struct pastix_gpu_s {
     int maxw = 0;
     int nlevels = 0;
     std::vector<int> lvl_ptr, lvl_cblks, lvl_maxw;
-    double thflops_potrf = 0, thflops_getrf = 0;
+    double thflops[2][3] = {{0}};   // [complex][POTRF, GETRF, LDL] algorithmic flops
 
     // ---- device structure ----
     DArr<int> d_fcol, d_width, d_height, d_ld, d_fblok, d_rowidx, d_bfrow, d_blrow, d_browoff, d_bfcblk,
@@ -107,8 +109,8 @@ struct pastix_gpu_s {
 
     // ---- matrix ----
     int mtxtype = PGPU_SYMMETRIC, flttype = PGPU_DOUBLE;
-    int64_t nnz = 0;
-    DArr<int64_t> d_fill_dst;   // per user nnz: coeftab offset (U entries offset by coefnbr)
+    int64_t nnz = 0, csr_nnz = 0;
+    DArr<int64_t> d_fill_dst;   // per user nnz: coeftab offset (U entries offset by coefnbr), ~offset: conjugate
     DArr<int8_t> d_wgt;         // Frobenius weight per user nnz
     DArr<int64_t> d_csr_ptr, d_csr_src;
     DArr<int> d_csr_col;
@@ -119,6 +121,7 @@ struct pastix_gpu_s {
     DArr<unsigned char> d_coef;
     int coef_float = 0;     // factor precision of d_coef
     int fact_done = -1;     // factotype of the factors in d_coef, -1 if none
+    int fact_mode = -1;     // kernel form (FM_*) of those factors
     DArr<Status> d_status;
     DArr<double> d_partial, d_scalar;
     DArr<unsigned char> d_work;   // solve workspace (n x 16 in factor precision)
@@ -126,7 +129,7 @@ struct pastix_gpu_s {
     DArr<double> d_sr_b, d_sr_x;   // solve_and_refine staging of host B / X
     DArr<double> d_gmV, d_gmW, d_gmh;   // GMRES basis, preconditioned basis, projections
     std::vector<cudaEvent_t> evpool;   // per-launch timing events
-    double gemm_flops[5] = {0};        // update-GEMM flops per factotype
+    double plan_gemm_flops = 0;        // update-GEMM flops of the current plan
     double stats[16] = {0};
 };
 
@@ -169,6 +172,34 @@ extern "C" int pastix_gpu_init(pastix_gpu_t **pctx, int device, const int64_t *i
 }
 
 // --------------------------------------------------------------------------
+// Algorithmic flops of the factorization (DPARM_FACT_THFLOPS), the
+// reference's model: symbol/symbol_cost.c:422 pastixSymbolGetFlops sums
+// sum1d per cblk -- diag(N) + trsm(M, N) + update(N, M) with N = width,
+// M = off-diagonal rows -- over symbol/symbol_cost_flops.c flopstable, with
+// the operation counts of common/flops.h (complex: 6 flops per multiply, 2
+// per add).  form: 0 POTRF, 1 GETRF, 2 LDL.
+// --------------------------------------------------------------------------
+static double structure_flops(const pastix_gpu_t &C, int form, bool z) {
+    auto fl = [z](double mul, double add) { return z ? 6.0 * mul + 2.0 * add : mul + add; };
+    const double scalw = z ? 6.0 : 1.0;
+    double tot = 0;
+    for (int c = 0; c < C.cblknbr; c++) {
+        const double N = C.width[c], M = C.height[c] - C.width[c];
+        if (form == 0) tot += fl(N * ((N / 6.0 + 0.5) * N + 1.0 / 3.0), N * ((N / 6.0) * N - 1.0 / 6.0));
+        else if (form == 1) tot += fl(0.5 * N * (N * (N - N / 3.0 - 1.0) + N) + 2.0 / 3.0 * N,
+                                     0.5 * N * (N * (N - N / 3.0) - N) + N / 6.0);
+        else tot += fl(N * ((N / 6.0 + 0.5) * N + 10.0 / 3.0), N * ((N / 6.0) * N - 1.0 / 6.0));
+        if (M <= 0) continue;
+        const double trsm = fl(0.5 * M * N * (N + 1), 0.5 * M * N * (N + 1));   // FLOPS_TRSM(Right, M, N)
+        const double syrk = fl(0.5 * N * M * (M + 1), 0.5 * N * M * (M + 1));   // FLOPS_SYRK(N, M)
+        if (form == 0) tot += trsm + syrk;
+        else if (form == 1) tot += 2.0 * trsm + fl(M * M * N, M * M * N);     // + FLOPS_GEMM(M, M, N)
+        else tot += trsm + scalw * N * M + syrk + scalw * M * M;
+    }
+    return tot;
+}
+
+// --------------------------------------------------------------------------
 // Structure handoff: device layout + level schedule.
 // --------------------------------------------------------------------------
 extern "C" int pastix_gpu_structure(pastix_gpu_t *ctx, int64_t n, int64_t cblknbr, const int64_t *cblktab,
@@ -197,7 +228,6 @@ extern "C" int pastix_gpu_structure(pastix_gpu_t *ctx, int64_t n, int64_t cblknb
     C.maxw = 0;
     for (int c = 0; c <= nc; c++) C.fblok[c] = (int)cblktab[4 * c + 2];
     if (C.fblok[nc] != nb) return PASTIX_GPU_ERR_BADPARAMETER;
-    double fl_potrf = 0, fl_getrf = 0;
     for (int c = 0; c < nc; c++) {
         const int fc = (int)cblktab[4 * c + 0], lc = (int)cblktab[4 * c + 1];
         const int w = lc - fc + 1;
@@ -221,15 +251,6 @@ extern "C" int pastix_gpu_structure(pastix_gpu_t *ctx, int64_t n, int64_t cblknb
         C.ld[c] = (int)round_up(w, 4);
         C.coefoff[c] = off;
         off += round_up((int64_t)h * C.ld[c], 32);
-        // algorithmic flops (common/flops.h: FLOPS_DPOTRF / DGETRF, DTRSM, DGEMM)
-        const double W = w, M = h - w;
-        fl_potrf += W * W * W / 3.0 + W * W / 2.0 + W / 6.0 + M * W * W;
-        fl_getrf += 2.0 * W * W * W / 3.0 - W * W / 2.0 + 5.0 * W / 6.0 + 2.0 * M * W * W;
-        for (int b = b0 + 1; b < b1; b++) {
-            const double N = C.blrow[b] - C.bfrow[b] + 1, Mb = h - C.browoff[b];
-            fl_potrf += 2.0 * Mb * N * W;
-            fl_getrf += 2.0 * Mb * N * W + (b + 1 < b1 ? 2.0 * (Mb - N) * N * W : 0.0);
-        }
     }
     // every block must lie inside the columns of the cblk it faces, which is
     // what lets the update GEMM address its target column directly
@@ -240,8 +261,8 @@ extern "C" int pastix_gpu_structure(pastix_gpu_t *ctx, int64_t n, int64_t cblknb
     }
     // the panel TRSM keeps TRSM_ROWS x w elements in shared memory
     if (C.maxw > 400) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
-    C.thflops_potrf = fl_potrf;
-    C.thflops_getrf = fl_getrf;
+    for (int z = 0; z < 2; z++)
+        for (int f = 0; f < 3; f++) C.thflops[z][f] = structure_flops(C, f, z != 0);
     for (int j = 0; j < n; j++)
         if (C.col2cblk[j] < 0) return PASTIX_GPU_ERR_BADPARAMETER;
     C.coefnbr = off;
@@ -327,7 +348,7 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
                               const int64_t *rowptr) {
     if (!ctx || !colptr || !rowptr) return PASTIX_GPU_ERR_BADPARAMETER;
     if (n != ctx->n) return PASTIX_GPU_ERR_BADPARAMETER;
-    if (flttype != PGPU_DOUBLE) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    if (flttype != PGPU_DOUBLE && flttype != PGPU_COMPLEX64) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
     if (mtxtype != PGPU_GENERAL && mtxtype != PGPU_SYMMETRIC && mtxtype != PGPU_HERMITIAN)
         return PASTIX_GPU_ERR_BADPARAMETER;
     PGPU_CHECK(cudaSetDevice(ctx->device));
@@ -341,6 +362,8 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
     std::vector<int64_t> dst(nnz);
     std::vector<int8_t> wgt(nnz);
     const bool sym = (mtxtype != PGPU_GENERAL);
+    // a Hermitian entry that lands in the other triangle is stored conjugated
+    const bool herm = (mtxtype == PGPU_HERMITIAN && flttype == PGPU_COMPLEX64);
     // permuted full matrix as (row, col, src) triplets
     std::vector<int64_t> rcount(n + 1, 0);
     for (int64_t j = 0; j < n; j++) {
@@ -351,7 +374,11 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
             wgt[k] = (sym && i != j) ? 2 : 1;
             rcount[pi + 1]++;
             if (sym && i != j) rcount[pj + 1]++;
-            if (sym && pi < pj) std::swap(pi, pj);
+            bool flip = false;
+            if (sym && pi < pj) {
+                std::swap(pi, pj);
+                flip = herm;
+            }
             int64_t d;
             if (pi >= pj) {
                 int c = C.col2cblk[pj];
@@ -370,7 +397,7 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
                     d = C.coefnbr + C.coefoff[c] + (int64_t)pr * C.ld[c] + (pi - C.fcol[c]);
                 }
             }
-            dst[k] = d;
+            dst[k] = flip ? ~d : d;
         }
     }
     for (int64_t i = 0; i < n; i++) rcount[i + 1] += rcount[i];
@@ -389,7 +416,7 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
                 if (sym && i != j) {
                     q = pos[pj]++;
                     ccol[q] = pi;
-                    csrc[q] = k;
+                    csrc[q] = herm ? ~k : k;
                 }
             }
         }
@@ -400,8 +427,10 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
     PGPU_CHECK(C.d_csr_ptr.upload(rcount, s));
     PGPU_CHECK(C.d_csr_col.upload(ccol, s));
     PGPU_CHECK(C.d_csr_src.upload(csrc, s));
-    PGPU_CHECK(C.d_csr_val.alloc(fnnz));
-    PGPU_CHECK(C.d_vals.alloc(nnz));
+    const int ncomp = (flttype == PGPU_COMPLEX64) ? 2 : 1;
+    C.csr_nnz = fnnz;
+    PGPU_CHECK(C.d_csr_val.alloc(fnnz * ncomp));
+    PGPU_CHECK(C.d_vals.alloc(nnz * ncomp));
     PGPU_CHECK(cudaStreamSynchronize(s));
     C.have_spm = true;
     C.fact_done = -1;
@@ -412,10 +441,13 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
 // Factorization plan for one factorization type.
 // --------------------------------------------------------------------------
 // Off-diagonal rows of cblks taller than fuse_rows are solved by
-// k_trsm_rows; shorter panels are factorized whole by k_panel_factor.
-static int fuse_rows_for(bool lu, bool fp32) {
-    if (lu) return fp32 ? 256 : 96;
-    return fp32 ? 1024 : 512;
+// k_trsm_rows; shorter panels are factorized whole by k_panel_factor (the
+// bound keeps the panel's shared-memory staging under the 227 KB limit for
+// the element size).
+static int fuse_rows_for(bool lu, size_t esz) {
+    if (esz <= 4) return lu ? 256 : 1024;
+    if (esz <= 8) return lu ? 96 : 512;
+    return lu ? 48 : 256;
 }
 static const int TRSM_TR = 32;   // panel rows per k_trsm_rows CTA
 
@@ -433,12 +465,29 @@ static int mixed_gemm_mode() {
 static bool tc_enabled() { return mixed_gemm_mode() != MG_FP32; }
 static bool tc_task(int M, int N, int K) { return K >= 32 && M >= 64 && N >= 32 && (int64_t)M * N >= 128 * 64; }
 
-static int build_fact_plan(pastix_gpu_t &C, int fact, bool fp32) {
-    const bool use_tc = fp32 && tc_enabled();
-    const int key = fact * 4 + (fp32 ? 1 : 0) + (use_tc ? 2 : 0);
+// Kernel form of a factorization request (pastix_factotype_t on a real or
+// complex matrix): the real LDL^h is the LDL^t, LL^t of a complex symmetric
+// matrix (PXTRF) is not provided.  -1 when unsupported.
+static int fact_mode_of(int fact, bool zc) {
+    switch (fact) {
+    case PGPU_FACT_POTRF: return FM_POTRF;
+    case PGPU_FACT_GETRF: return FM_GETRF;
+    case PGPU_FACT_SYTRF: return FM_SYTRF;
+    case PGPU_FACT_HETRF: return zc ? FM_HETRF : FM_SYTRF;
+    case 3: return zc ? -1 : FM_POTRF;
+    default: return -1;
+    }
+}
+
+static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
+    const bool use_tc = fp32 && !zc && tc_enabled() && (fmode == FM_POTRF || fmode == FM_GETRF);
+    const int key = ((fmode * 2 + (fp32 ? 1 : 0)) * 2 + (use_tc ? 1 : 0)) * 2 + (zc ? 1 : 0);
     if (C.plan_fact == key) return PASTIX_GPU_SUCCESS;
-    const bool lu = (fact == PGPU_FACT_GETRF);
-    const int fuse = fuse_rows_for(lu, fp32);
+    const bool lu = (fmode == FM_GETRF), ldl = fm_ldl(fmode);
+    const size_t esz = (fp32 ? 4 : 8) * (zc ? 2 : 1);
+    const int fuse = fuse_rows_for(lu, esz);
+    const int sym_flags = 8 | (ldl ? 16 : 0) | ((zc && fm_conj(fmode)) ? 32 : 0);
+    const double fma_flops = zc ? 8.0 : 2.0;
     std::vector<int4> tiles, trsm, tctiles;
     std::vector<GemmTask> tasks;
     double gflops = 0, tcflops = 0;
@@ -456,7 +505,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fact, bool fp32) {
             C.lvl_porows[l] = std::max(C.lvl_porows[l], rows - w);
             if (h > fuse)
                 for (int r0 = w; r0 < h; r0 += TRSM_TR) {
-                    trsm.push_back(make_int4(c, r0, 0, lu ? 1 : 0));
+                    trsm.push_back(make_int4(c, r0, 0, lu ? 1 : (ldl ? 3 : 0)));
                     if (lu) trsm.push_back(make_int4(c, r0, 1, 2));
                 }
             const int b1 = C.fblok[c + 1];
@@ -468,7 +517,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fact, bool fp32) {
                     if (M <= 0) return;
                     const int id = (int)tasks.size();
                     tasks.push_back(GemmTask{c, b, f, arow0, M, flags});
-                    gflops += 2.0 * M * N * w;
+                    gflops += fma_flops * M * N * w;
                     if (use_tc && tc_task(M, N, w)) {
                         tcflops += 2.0 * M * N * w;
                         for (int tm = 0; tm < cdiv(M, TC_BM); tm++)
@@ -485,7 +534,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fact, bool fp32) {
                         }
                 };
                 if (!lu) {
-                    add(C.browoff[b], 8);
+                    add(C.browoff[b], sym_flags);
                 } else {
                     add(C.browoff[b], 2);                          // L side: A = L, B = U^T rows of b
                     if (b + 1 < b1) add(C.browoff[b + 1], 1 | 4);  // U side: A = U^T, B = L rows of b
@@ -503,7 +552,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fact, bool fp32) {
     PGPU_CHECK(C.d_tasks.upload(tasks, s));
     PGPU_CHECK(cudaStreamSynchronize(s));
     C.plan_fact = key;
-    C.gemm_flops[fact] = gflops;
+    C.plan_gemm_flops = gflops;
     C.tc_flops = tcflops;
     return PASTIX_GPU_SUCCESS;
 }
@@ -541,18 +590,36 @@ struct LaunchTimer {
 enum { PH_DIAG = 0, PH_TRSM = 1, PH_GEMM = 2, PH_TC = 3, PH_END = 4 };
 
 template <typename T>
-static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, LaunchTimer &tm) {
-    const bool lu = (fact == PGPU_FACT_GETRF);
+using PanelKernel = void (*)(Meta, const int *, T *, T *, double, int, int, int, Status *);
+
+template <typename T>
+static PanelKernel<T> panel_kernel(int fmode) {
+    switch (fmode) {
+    case FM_GETRF: return k_panel_factor<T, FM_GETRF>;
+    case FM_SYTRF: return k_panel_factor<T, FM_SYTRF>;
+    case FM_HETRF:
+        if constexpr (is_cplx<T>::value) return k_panel_factor<T, FM_HETRF>;
+        return nullptr;
+    default: return k_panel_factor<T, FM_POTRF>;
+    }
+}
+
+template <typename T>
+static int run_factor(pastix_gpu_t &C, int fmode, double crit, int *launches, LaunchTimer &tm) {
+    const bool lu = (fmode == FM_GETRF);
     T *coefL = reinterpret_cast<T *>(C.d_coef.p);
     T *coefU = lu ? coefL + C.coefnbr : coefL;
     cudaStream_t s = C.stream;
-    const int fuse = fuse_rows_for(lu, sizeof(T) == 4);
-    auto kpanel = lu ? k_panel_factor<T, true> : k_panel_factor<T, false>;
+    const int fuse = fuse_rows_for(lu, sizeof(T));
+    PanelKernel<T> kpanel = panel_kernel<T>(fmode);
+    if (!kpanel) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    // the Hermitian forms conjugate the L coefficients in the row solves
+    constexpr bool CPX = is_cplx<T>::value;
+    auto ktrsm = (CPX && fm_conj(fmode)) ? k_trsm_rows<T, TRSM_TR, CPX> : k_trsm_rows<T, TRSM_TR, false>;
     PGPU_CHECK(cudaFuncSetAttribute(kpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
-    PGPU_CHECK(cudaFuncSetAttribute(k_trsm_rows<T, TRSM_TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    SMEM_LIMIT));
+    PGPU_CHECK(cudaFuncSetAttribute(ktrsm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     const bool split = (mixed_gemm_mode() == MG_3XTF32);
-    if constexpr (sizeof(T) == 4) {
+    if constexpr (std::is_same<T, float>::value) {
         PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         tc_smem_bytes<false>()));
         PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -563,7 +630,7 @@ static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, Lau
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
         const int pl = C.lvl_plrows[l], pu = lu ? mw : 0, po = lu ? C.lvl_porows[l] : 0;
-        const size_t psm = (size_t)(PB * PBL + (size_t)(pl + pu + po) * PBL) * sizeof(T);
+        const size_t psm = (size_t)(PB * PBL + PB + (size_t)(pl + pu + po) * PBL) * sizeof(T);
         if (psm > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
         PGPU_CHECK(tm.mark(PH_DIAG));
         kpanel<<<ncb, 256, psm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, coefU, crit, fuse, pl, pu,
@@ -571,10 +638,13 @@ static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, Lau
         nl++;
         const int ntr = C.trsm_ptr[l + 1] - C.trsm_ptr[l];
         if (ntr) {
-            const size_t tsm = ((size_t)TRSM_TR * (mw + 1) + PB * PBL + (size_t)mw * PBL) * sizeof(T);
-            if (tsm > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+            const size_t fixed = ((size_t)TRSM_TR * (mw + 1) + PB * PBL) * sizeof(T);
+            const int pch = (int)std::min<size_t>(mw, (SMEM_LIMIT - std::min<size_t>(fixed, SMEM_LIMIT)) /
+                                                          (PBL * sizeof(T)));
+            if (pch < PB) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+            const size_t tsm = fixed + (size_t)pch * PBL * sizeof(T);
             PGPU_CHECK(tm.mark(PH_TRSM));
-            k_trsm_rows<T, TRSM_TR><<<ntr, 256, tsm, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], coefL, coefU, mw);
+            ktrsm<<<ntr, 256, tsm, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], coefL, coefU, mw, pch);
             nl++;
         }
         const int nti = C.tile_ptr[l + 1] - C.tile_ptr[l];
@@ -584,7 +654,7 @@ static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, Lau
             nl++;
             ngemm++;
         }
-        if constexpr (sizeof(T) == 4) {
+        if constexpr (std::is_same<T, float>::value) {
             const int ntc = C.tctile_ptr[l + 1] - C.tctile_ptr[l];
             if (ntc) {
                 PGPU_CHECK(tm.mark(PH_TC));
@@ -606,14 +676,25 @@ static int run_factor(pastix_gpu_t &C, int fact, double crit, int *launches, Lau
     return PASTIX_GPU_SUCCESS;
 }
 
+template <typename S>
 static int dev_norm_frob(pastix_gpu_t &C, double *out) {
     cudaStream_t s = C.stream;
     const int nb = 512;
-    k_sumsq_partial<<<nb, RED_THREADS, 0, s>>>(C.nnz, C.d_vals.p, C.d_wgt.p, C.d_partial.p);
-    k_dot_final<<<1, RED_THREADS, 0, s>>>(nb, C.d_partial.p, C.d_scalar.p, 1);
+    k_sumsq_partial<S><<<nb, RED_THREADS, 0, s>>>(C.nnz, reinterpret_cast<const S *>(C.d_vals.p), C.d_wgt.p,
+                                                  C.d_partial.p);
+    k_dot_final<double><<<1, RED_THREADS, 0, s>>>(nb, C.d_partial.p, C.d_scalar.p, 1);
     PGPU_CHECK(cudaMemcpyAsync(out, C.d_scalar.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     PGPU_CHECK(cudaStreamSynchronize(s));
     return PASTIX_GPU_SUCCESS;
+}
+
+// bcsc -> coeftab in the factor precision, then the level loop
+template <typename T, typename S>
+static int fill_and_factor(pastix_gpu_t &C, int fmode, double crit, int *nl, LaunchTimer &tm) {
+    cudaStream_t s = C.stream;
+    k_fillin<T, S><<<2048, 256, 0, s>>>(C.nnz, reinterpret_cast<const S *>(C.d_vals.p), C.d_fill_dst.p,
+                                        reinterpret_cast<T *>(C.d_coef.p), C.d_status.p);
+    return run_factor<T>(C, fmode, crit, nl, tm);
 }
 
 extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
@@ -622,13 +703,16 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     if (!C.have_spm || C.cblknbr == 0) return PASTIX_GPU_ERR_BADPARAMETER;
     PGPU_CHECK(cudaSetDevice(C.device));
     const int fact = (int)C.iparm[PGPU_IPARM_FACTORIZATION];
-    if (fact != PGPU_FACT_POTRF && fact != PGPU_FACT_GETRF) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
-    if (fact == PGPU_FACT_POTRF && C.mtxtype == PGPU_GENERAL) return PASTIX_GPU_ERR_BADPARAMETER;
+    const bool zc = (C.flttype == PGPU_COMPLEX64);
+    const int fmode = fact_mode_of(fact, zc);
+    if (fmode < 0) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    if (fmode != FM_GETRF && C.mtxtype == PGPU_GENERAL) return PASTIX_GPU_ERR_BADPARAMETER;
     const int mixed = C.iparm[PGPU_IPARM_MIXED] ? 1 : 0;
-    int rc = build_fact_plan(C, fact, mixed != 0);
+    int rc = build_fact_plan(C, fmode, mixed != 0, zc);
     if (rc) return rc;
-    const size_t esz = mixed ? sizeof(float) : sizeof(double);
-    const size_t ncoef = (size_t)C.coefnbr * (fact == PGPU_FACT_GETRF ? 2 : 1);
+    const size_t esz = (mixed ? 4 : 8) * (zc ? 2 : 1);
+    const size_t vsz = zc ? 16 : 8;
+    const size_t ncoef = (size_t)C.coefnbr * (fmode == FM_GETRF ? 2 : 1);
     if (C.d_coef.n < ncoef * esz) {
         C.d_coef.release();
         PGPU_CHECK(C.d_coef.alloc(ncoef * esz));
@@ -636,12 +720,10 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     cudaStream_t s = C.stream;
     PGPU_CHECK(cudaEventRecord(C.ev[0], s));
     // values in (pastix_subtask_spm2bcsc), norm, bcsc -> coeftab
-    if (is_device_ptr(values))
-        PGPU_CHECK(cudaMemcpyAsync(C.d_vals.p, values, C.nnz * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    else
-        PGPU_CHECK(cudaMemcpyAsync(C.d_vals.p, values, C.nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+    PGPU_CHECK(cudaMemcpyAsync(C.d_vals.p, values, C.nnz * vsz,
+                               is_device_ptr(values) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
     double anorm = 0;
-    rc = dev_norm_frob(C, &anorm);
+    rc = zc ? dev_norm_frob<cdouble>(C, &anorm) : dev_norm_frob<double>(C, &anorm);
     if (rc) return rc;
     C.dparm[PGPU_DPARM_A_NORM] = anorm;
     // static pivoting threshold, sopalin/pastix_task_sopalin.c:461-485 (the
@@ -651,17 +733,22 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     if (magn < 0.) crit = -magn;
     else if (magn == 0.) crit = 1.1102230246251565e-16 * anorm;
     else crit = magn * anorm;
-    k_gather_vals<<<1024, 256, 0, s>>>((int64_t)C.d_csr_val.n, C.d_csr_src.p, C.d_vals.p, C.d_csr_val.p);
+    if (zc)
+        k_gather_vals<cdouble><<<1024, 256, 0, s>>>(C.csr_nnz, C.d_csr_src.p, (const cdouble *)C.d_vals.p,
+                                                    (cdouble *)C.d_csr_val.p);
+    else
+        k_gather_vals<double><<<1024, 256, 0, s>>>(C.csr_nnz, C.d_csr_src.p, C.d_vals.p, C.d_csr_val.p);
     PGPU_CHECK(cudaMemsetAsync(C.d_status.p, 0, sizeof(Status), s));
     PGPU_CHECK(cudaMemsetAsync(C.d_coef.p, 0, ncoef * esz, s));
     int launches = 4;
-    if (mixed)
-        k_fillin<float><<<2048, 256, 0, s>>>(C.nnz, C.d_vals.p, C.d_fill_dst.p, (float *)C.d_coef.p, C.d_status.p);
-    else
-        k_fillin<double><<<2048, 256, 0, s>>>(C.nnz, C.d_vals.p, C.d_fill_dst.p, (double *)C.d_coef.p, C.d_status.p);
     int nl = 0;
     LaunchTimer tm(C);
-    rc = mixed ? run_factor<float>(C, fact, crit, &nl, tm) : run_factor<double>(C, fact, crit, &nl, tm);
+    if (zc)
+        rc = mixed ? fill_and_factor<cfloat, cdouble>(C, fmode, crit, &nl, tm)
+                   : fill_and_factor<cdouble, cdouble>(C, fmode, crit, &nl, tm);
+    else
+        rc = mixed ? fill_and_factor<float, double>(C, fmode, crit, &nl, tm)
+                   : fill_and_factor<double, double>(C, fmode, crit, &nl, tm);
     if (rc) return rc;
     PGPU_CHECK(cudaEventRecord(C.ev[1], s));
     Status st;
@@ -677,7 +764,7 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
         C.stats[8] = ph[PH_DIAG];
         C.stats[9] = ph[PH_TRSM];
         C.stats[6] = ph[PH_GEMM] + ph[PH_TC];
-        C.stats[10] = C.gemm_flops[fact];
+        C.stats[10] = C.plan_gemm_flops;
         C.stats[11] = ph[PH_TC];
         C.stats[12] = mixed ? C.tc_flops : 0.0;
         C.stats[13] = st.timeout;
@@ -688,12 +775,13 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
         return PASTIX_GPU_ERR_INTERNAL;
     }
     C.iparm[PGPU_IPARM_STATIC_PIVOTING] = st.nbpivots;
-    const double fl = (fact == PGPU_FACT_GETRF) ? C.thflops_getrf : C.thflops_potrf;
+    const double fl = C.thflops[zc ? 1 : 0][fmode == FM_GETRF ? 1 : (fm_ldl(fmode) ? 2 : 0)];
     C.dparm[PGPU_DPARM_FACT_TIME] = ms * 1e-3;
     C.dparm[PGPU_DPARM_FACT_THFLOPS] = fl;
     C.dparm[PGPU_DPARM_FACT_FLOPS] = fl / (ms * 1e-3) / 1e9;
     C.coef_float = mixed;
     C.fact_done = fact;
+    C.fact_mode = fmode;
     if (st.overflow) {
         fprintf(stderr, "pastix_gpu: mixed-precision overflow during the matrix initialization\n");
         C.fact_done = -1;
@@ -708,11 +796,16 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
 }
 
 // --------------------------------------------------------------------------
-// Solve on a permuted device RHS block W (factor precision, ld = n).
+// Solve on a permuted device RHS block W (factor precision, ld = n):
+// sopalin/sequential_ztrsm.c:591 with the uplo/trans/diag choice of
+// sopalin/pastix_task_solve.c:600-650 (forward L; for LDL the diagonal
+// solve, sequential_zdiag.c; backward op(L)^t or U).
 // --------------------------------------------------------------------------
 template <typename T>
 static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
-    const bool lu = (C.fact_done == PGPU_FACT_GETRF);
+    const int fm = C.fact_mode;
+    const bool lu = (fm == FM_GETRF), ldl = fm_ldl(fm);
+    const int cjp = fm_conj(fm) ? 1 : 0;
     const T *coefL = reinterpret_cast<const T *>(C.d_coef.p);
     const T *coefU = lu ? coefL + C.coefnbr : coefL;
     cudaStream_t s = C.stream;
@@ -724,8 +817,8 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
-        k_fwd_diag<T><<<ncb, 128, ((size_t)mw * nrhs + 32 * 33) * sizeof(T), s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l],
-                                                                      coefL, W, ldb, nrhs, lu ? 1 : 0);
+        k_fwd_diag<T><<<ncb, 128, ((size_t)mw * nrhs + 32 * 33) * sizeof(T), s>>>(
+            C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs, (lu || ldl) ? 1 : 0);
         nl++;
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
@@ -734,17 +827,21 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
             nl++;
         }
     }
+    if (ldl) {
+        k_diag_scale<T><<<std::min(C.cblknbr, 4096), 128, 0, s>>>(C.meta, coefL, W, ldb, nrhs);
+        nl++;
+    }
     for (int l = C.nlevels - 1; l >= 0; l--) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
             k_bwd_off<T><<<nch, 128, 0, s>>>(C.meta, C.d_solve_chunks.p + C.solve_ptr[l], coefU, W, ldb, nrhs,
-                                              SOLVE_ROWS_PER_CHUNK);
+                                              SOLVE_ROWS_PER_CHUNK, lu ? 0 : cjp);
             nl++;
         }
-        k_bwd_diag<T><<<ncb, 128, ((size_t)mw * nrhs + 32 * 33) * sizeof(T), s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l],
-                                                                      coefL, W, ldb, nrhs, lu ? 1 : 0);
+        k_bwd_diag<T><<<ncb, 128, ((size_t)mw * nrhs + 32 * 33) * sizeof(T), s>>>(
+            C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs, lu ? 1 : 0, ldl ? 1 : 0, lu ? 0 : cjp);
         nl++;
     }
     PGPU_CHECK(cudaGetLastError());
@@ -752,38 +849,45 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
     return PASTIX_GPU_SUCCESS;
 }
 
+// bytes of one right-hand-side element (FP64 real or complex)
+static size_t rhs_esz(const pastix_gpu_t &C) { return C.flttype == PGPU_COMPLEX64 ? 16 : 8; }
+// bytes of one factor element
+static size_t coef_esz(const pastix_gpu_t &C) { return (C.coef_float ? 4 : 8) * (C.flttype == PGPU_COMPLEX64 ? 2 : 1); }
+
 static int ensure_work(pastix_gpu_t &C) {
-    const size_t need = (size_t)C.n * SOLVE_MAXRHS * sizeof(double);
+    const size_t need = (size_t)C.n * SOLVE_MAXRHS * 16;
     if (C.d_work.n < need) {
         C.d_work.release();
         PGPU_CHECK(C.d_work.alloc(need));
     }
-    if (C.d_rhs.n < (size_t)C.n * SOLVE_MAXRHS) PGPU_CHECK(C.d_rhs.alloc((size_t)C.n * SOLVE_MAXRHS));
+    if (C.d_rhs.n < (size_t)C.n * SOLVE_MAXRHS * 2) PGPU_CHECK(C.d_rhs.alloc((size_t)C.n * SOLVE_MAXRHS * 2));
     return PASTIX_GPU_SUCCESS;
 }
 
-// Solve in place on a device FP64 block (user order, ld = ldb).
-static int solve_device_block(pastix_gpu_t &C, double *dB, int64_t ldb, int nrhs, int *launches) {
+// Permute in (down-casting for single-precision factors), solve, permute out.
+template <typename S, typename T>
+static int solve_block_t(pastix_gpu_t &C, S *dB, int64_t ldb, int nrhs, T *W, int *launches) {
     cudaStream_t s = C.stream;
     const int n = C.n;
     const int grid = std::min(4096, cdiv((int64_t)n * nrhs, 256));
-    int rc;
-    if (C.coef_float) {
-        float *W = reinterpret_cast<float *>(C.d_work.p);
-        k_permute<double, float><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, dB, ldb, W, n, 0);
-        rc = solve_permuted<float>(C, W, nrhs, launches);
-        if (rc) return rc;
-        k_permute<float, double><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, W, n, dB, ldb, 1);
-    } else {
-        double *W = reinterpret_cast<double *>(C.d_work.p);
-        k_permute<double, double><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, dB, ldb, W, n, 0);
-        rc = solve_permuted<double>(C, W, nrhs, launches);
-        if (rc) return rc;
-        k_permute<double, double><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, W, n, dB, ldb, 1);
-    }
+    k_permute<S, T><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, dB, ldb, W, n, 0);
+    int rc = solve_permuted<T>(C, W, nrhs, launches);
+    if (rc) return rc;
+    k_permute<T, S><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, W, n, dB, ldb, 1);
     *launches += 2;
     PGPU_CHECK(cudaGetLastError());
     return PASTIX_GPU_SUCCESS;
+}
+
+// Solve in place on a device FP64 (real or complex) block, user order,
+// ld = ldb elements, with W as the permuted work block.
+static int solve_device_block(pastix_gpu_t &C, void *dB, int64_t ldb, int nrhs, void *W, int *launches) {
+    if (C.flttype == PGPU_COMPLEX64) {
+        if (C.coef_float) return solve_block_t<cdouble, cfloat>(C, (cdouble *)dB, ldb, nrhs, (cfloat *)W, launches);
+        return solve_block_t<cdouble, cdouble>(C, (cdouble *)dB, ldb, nrhs, (cdouble *)W, launches);
+    }
+    if (C.coef_float) return solve_block_t<double, float>(C, (double *)dB, ldb, nrhs, (float *)W, launches);
+    return solve_block_t<double, double>(C, (double *)dB, ldb, nrhs, (double *)W, launches);
 }
 
 extern "C" int pastix_gpu_solve(pastix_gpu_t *ctx, int64_t nrhs, void *B, int64_t ldb) {
@@ -797,10 +901,11 @@ extern "C" int pastix_gpu_solve(pastix_gpu_t *ctx, int64_t nrhs, void *B, int64_
     const bool dev = is_device_ptr(B);
     int launches = 0;
     PGPU_CHECK(cudaEventRecord(C.ev[2], s));
+    const size_t es = rhs_esz(C);
     for (int64_t r0 = 0; r0 < nrhs; r0 += SOLVE_MAXRHS) {
         const int nr = (int)std::min<int64_t>(SOLVE_MAXRHS, nrhs - r0);
-        double *hb = reinterpret_cast<double *>(B) + r0 * ldb;
-        double *db;
+        char *hb = reinterpret_cast<char *>(B) + r0 * ldb * es;
+        void *db;
         int64_t dld;
         if (dev) {
             db = hb;
@@ -808,14 +913,11 @@ extern "C" int pastix_gpu_solve(pastix_gpu_t *ctx, int64_t nrhs, void *B, int64_
         } else {
             db = C.d_rhs.p;
             dld = C.n;
-            PGPU_CHECK(cudaMemcpy2DAsync(db, C.n * sizeof(double), hb, ldb * sizeof(double), C.n * sizeof(double),
-                                         nr, cudaMemcpyHostToDevice, s));
+            PGPU_CHECK(cudaMemcpy2DAsync(db, C.n * es, hb, ldb * es, C.n * es, nr, cudaMemcpyHostToDevice, s));
         }
-        rc = solve_device_block(C, db, dld, nr, &launches);
+        rc = solve_device_block(C, db, dld, nr, C.d_work.p, &launches);
         if (rc) return rc;
-        if (!dev)
-            PGPU_CHECK(cudaMemcpy2DAsync(hb, ldb * sizeof(double), db, C.n * sizeof(double), C.n * sizeof(double),
-                                         nr, cudaMemcpyDeviceToHost, s));
+        if (!dev) PGPU_CHECK(cudaMemcpy2DAsync(hb, ldb * es, db, C.n * es, C.n * es, nr, cudaMemcpyDeviceToHost, s));
     }
     PGPU_CHECK(cudaEventRecord(C.ev[3], s));
     PGPU_CHECK(cudaStreamSynchronize(s));
@@ -863,7 +965,7 @@ extern "C" int pastix_gpu_solve_noalloc(pastix_gpu_t *ctx, int64_t nrhs, void *d
     if (!ctx || !dB || nrhs <= 0 || ldb < ctx->n) return PASTIX_GPU_ERR_BADPARAMETER;
     auto &C = *ctx;
     if (C.fact_done < 0) return PASTIX_GPU_ERR_BADPARAMETER;
-    const size_t esz = C.coef_float ? sizeof(float) : sizeof(double);
+    const size_t esz = coef_esz(C);
     const size_t need = (size_t)C.n * (size_t)std::min<int64_t>(nrhs, SOLVE_MAXRHS) * esz;
     if (need > PASTIX_GPU_NOALLOC_SCRATCH_BYTES) {
         fprintf(stderr,
@@ -879,25 +981,12 @@ extern "C" int pastix_gpu_solve_noalloc(pastix_gpu_t *ctx, int64_t nrhs, void *d
     int rc = noalloc_scratch_address(C.device, &scratch);
     if (rc) return rc;
     cudaStream_t s = C.stream;
-    const int n = C.n;
     int launches = 0;
     for (int64_t r0 = 0; r0 < nrhs; r0 += SOLVE_MAXRHS) {
         const int nr = (int)std::min<int64_t>(SOLVE_MAXRHS, nrhs - r0);
-        double *db = reinterpret_cast<double *>(dB) + r0 * ldb;
-        const int grid = std::min(4096, cdiv((int64_t)n * nr, 256));
-        if (C.coef_float) {
-            float *W = reinterpret_cast<float *>(scratch);
-            k_permute<double, float><<<grid, 256, 0, s>>>(n, nr, C.d_peritab.p, db, ldb, W, n, 0);
-            rc = solve_permuted<float>(C, W, nr, &launches);
-            if (rc) return rc;
-            k_permute<float, double><<<grid, 256, 0, s>>>(n, nr, C.d_peritab.p, W, n, db, ldb, 1);
-        } else {
-            double *W = reinterpret_cast<double *>(scratch);
-            k_permute<double, double><<<grid, 256, 0, s>>>(n, nr, C.d_peritab.p, db, ldb, W, n, 0);
-            rc = solve_permuted<double>(C, W, nr, &launches);
-            if (rc) return rc;
-            k_permute<double, double><<<grid, 256, 0, s>>>(n, nr, C.d_peritab.p, W, n, db, ldb, 1);
-        }
+        char *db = reinterpret_cast<char *>(dB) + r0 * ldb * rhs_esz(C);
+        rc = solve_device_block(C, db, ldb, nr, scratch, &launches);
+        if (rc) return rc;
     }
     PGPU_CHECK(cudaGetLastError());
     PGPU_CHECK(cudaStreamSynchronize(s));
@@ -905,55 +994,73 @@ extern "C" int pastix_gpu_solve_noalloc(pastix_gpu_t *ctx, int64_t nrhs, void *d
 }
 
 // --------------------------------------------------------------------------
-// Refinement (refinement/z_refine_grad.c:49 z_grad_smp, preconditioned CG).
-// Vectors in the user numbering (the SpMV matrix is permuted, so vectors are
-// permuted in and out of it).
+// Refinement (refinement/z_refine_grad.c:49 z_grad_smp, preconditioned CG;
+// refinement/z_refine_gmres.c:49 z_gmres_smp).  Vectors in the user
+// numbering (the SpMV matrix is permuted, so vectors are permuted in and out
+// of it).  S is the device scalar (double / cdouble), HS its host twin.
 // --------------------------------------------------------------------------
+template <typename S> struct HostScalar { typedef double type; };
+template <> struct HostScalar<cdouble> { typedef std::complex<double> type; };
+static inline double to_dev(double v) { return v; }
+static inline cdouble to_dev(const std::complex<double> &v) { return cdouble(v.real(), v.imag()); }
+static inline double to_host(double v) { return v; }
+static inline std::complex<double> to_host(const cdouble &v) { return std::complex<double>(v.re, v.im); }
+
+template <typename S>
 struct VecOps {
+    typedef typename HostScalar<S>::type HS;
     pastix_gpu_t &C;
     int launches = 0;
-    double dot(const double *x, const double *y) {
+    S *partial() { return reinterpret_cast<S *>(C.d_partial.p); }
+    S *scalar() { return reinterpret_cast<S *>(C.d_scalar.p); }
+    // sum conj(x) y (bvec_zdotc); x . x when y == nullptr
+    HS dot(const S *x, const S *y) {
         const int nb = 256;
-        k_dot_partial<<<nb, RED_THREADS, 0, C.stream>>>(C.n, x, y, C.d_partial.p);
-        k_dot_final<<<1, RED_THREADS, 0, C.stream>>>(nb, C.d_partial.p, C.d_scalar.p, 0);
+        k_dot_partial<S><<<nb, RED_THREADS, 0, C.stream>>>(C.n, x, y, partial());
+        k_dot_final<S><<<1, RED_THREADS, 0, C.stream>>>(nb, partial(), scalar(), 0);
         launches += 2;
-        double v = 0;
-        cudaMemcpyAsync(&v, C.d_scalar.p, sizeof(double), cudaMemcpyDeviceToHost, C.stream);
+        S v;
+        cudaMemcpyAsync(&v, scalar(), sizeof(S), cudaMemcpyDeviceToHost, C.stream);
         cudaStreamSynchronize(C.stream);
-        return v;
+        return to_host(v);
     }
-    double norm(const double *x) { return std::sqrt(dot(x, nullptr)); }
-    void axpy(double a, const double *x, double *y) {
-        k_axpy<<<1024, 256, 0, C.stream>>>(C.n, a, x, y);
+    double norm(const S *x) { return std::sqrt(std::real(dot(x, nullptr))); }
+    void axpy(HS a, const S *x, S *y) {
+        k_axpy<S><<<1024, 256, 0, C.stream>>>(C.n, to_dev(a), x, y);
         launches++;
     }
-    void xpby(const double *z, double beta, double *p) {
-        k_xpby<<<1024, 256, 0, C.stream>>>(C.n, z, beta, p);
+    void xpby(const S *z, HS beta, S *p) {
+        k_xpby<S><<<1024, 256, 0, C.stream>>>(C.n, z, to_dev(beta), p);
         launches++;
     }
-    void copy(const double *x, double *y) {
-        cudaMemcpyAsync(y, x, C.n * sizeof(double), cudaMemcpyDeviceToDevice, C.stream);
+    void copy(const S *x, S *y) { cudaMemcpyAsync(y, x, C.n * sizeof(S), cudaMemcpyDeviceToDevice, C.stream); }
+    void scal(double a, S *x) {
+        k_scal<S><<<1024, 256, 0, C.stream>>>(C.n, a, x);
+        launches++;
     }
     // y = alpha A x + beta y, in the user numbering: the CSR is permuted, so
     // work on permuted copies held in d_gm.
-    void spmv(double alpha, const double *x, double beta, double *y) {
+    void spmv(double alpha, const S *x, double beta, S *y) {
         const int n = C.n;
-        double *xp = C.d_gm.p, *yp = C.d_gm.p + n;
+        S *xp = reinterpret_cast<S *>(C.d_gm.p), *yp = xp + n;
+        const S *val = reinterpret_cast<const S *>(C.d_csr_val.p);
         const int grid = cdiv(n, 256);
-        k_permute<double, double><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, x, n, xp, n, 0);
-        if (beta != 0.0) k_permute<double, double><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, y, n, yp, n, 0);
-        k_spmv<<<cdiv((int64_t)n * 32, 256), 256, 0, C.stream>>>(n, C.d_csr_ptr.p, C.d_csr_col.p, C.d_csr_val.p,
-                                                                alpha, xp, beta, yp);
-        k_permute<double, double><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, yp, n, y, n, 1);
+        k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, x, n, xp, n, 0);
+        if (beta != 0.0) k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, y, n, yp, n, 0);
+        k_spmv<S><<<cdiv((int64_t)n * 32, 256), 256, 0, C.stream>>>(n, C.d_csr_ptr.p, C.d_csr_col.p, val, alpha, xp,
+                                                                     beta, yp);
+        k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, yp, n, y, n, 1);
         launches += 3 + (beta != 0.0);
     }
-    int spsv(double *z) { return solve_device_block(C, z, C.n, 1, &launches); }
+    int spsv(S *z) { return solve_device_block(C, z, C.n, 1, C.d_work.p, &launches); }
 };
 
-static int refine_cg(pastix_gpu_t &C, VecOps &V, const double *b, double *x, double eps, int itermax, int *iters,
+template <typename S>
+static int refine_cg(pastix_gpu_t &C, VecOps<S> &V, const S *b, S *x, double eps, int itermax, int *iters,
                      double *resid) {
-    const int n = C.n;
-    double *r = C.d_r.p, *z = C.d_z.p, *p = C.d_p.p, *ap = C.d_ap.p;
+    typedef typename HostScalar<S>::type HS;
+    S *r = reinterpret_cast<S *>(C.d_r.p), *z = reinterpret_cast<S *>(C.d_z.p);
+    S *p = reinterpret_cast<S *>(C.d_p.p), *ap = reinterpret_cast<S *>(C.d_ap.p);
     double normb = V.norm(b);
     if (normb == 0.) normb = 1;
     const double normx = V.norm(x);
@@ -966,12 +1073,11 @@ static int refine_cg(pastix_gpu_t &C, VecOps &V, const double *b, double *x, dou
     if (rc) return rc;
     V.copy(z, p);
     int it = 0;
-    (void)n;
     while (resid_b > eps && it < itermax) {
         it++;
         V.spmv(1.0, p, 0.0, ap);
-        double beta = V.dot(r, z);
-        double alpha = V.dot(ap, p);
+        HS beta = V.dot(r, z);
+        HS alpha = V.dot(ap, p);
         alpha = beta / alpha;
         V.axpy(alpha, p, x);
         V.axpy(-alpha, ap, r);
@@ -989,25 +1095,59 @@ static int refine_cg(pastix_gpu_t &C, VecOps &V, const double *b, double *x, dou
     return PASTIX_GPU_SUCCESS;
 }
 
+// Givens rotation that zeroes b under a (z_refine_gmres.c:257-272 for real
+// data).  For complex data the unitary rotation [c s; -conj(s) c] with c real
+// (LAPACK zlartg's convention): the reference's complex form takes a complex
+// cosine and omits the conjugations, which is not unitary.
+static inline void givens(double a, double b, double eps, double &c, double &s) {
+    double t = std::sqrt(a * a + b * b);
+    if (std::fabs(t) <= eps) t = eps;
+    c = a / t;
+    s = b / t;
+}
+static inline void givens(std::complex<double> a, std::complex<double> b, double eps, double &c,
+                          std::complex<double> &s) {
+    const double aa = std::abs(a), ab = std::abs(b);
+    double t = std::sqrt(aa * aa + ab * ab);
+    if (t <= eps) t = eps;
+    if (aa == 0.0) {
+        c = 0.0;
+        s = (ab > 0.0) ? std::conj(b) / ab : std::complex<double>(1.0);
+        return;
+    }
+    c = aa / t;
+    s = (a / aa) * std::conj(b) / t;
+}
+static inline double conj_h(double v) { return v; }
+static inline std::complex<double> conj_h(const std::complex<double> &v) { return std::conj(v); }
+
 // --------------------------------------------------------------------------
 // GMRES(im), right preconditioned (refinement/z_refine_gmres.c:49
 // z_gmres_smp, Saad Alg. 9.5): V holds the Krylov basis, W = M^{-1} V so the
 // solution update needs no extra solve; modified Gram-Schmidt with the
-// projections h_{j,i} kept in device memory (one host round trip per inner
-// iteration, for the Givens rotations on the small Hessenberg matrix).
+// projections h_{j,i} = <v_j, w> kept in device memory (one host round trip
+// per inner iteration, for the Givens rotations on the small Hessenberg
+// matrix).
 // --------------------------------------------------------------------------
-static int refine_gmres(pastix_gpu_t &C, VecOps &V, const double *b, double *x, double eps, int itermax, int im,
+template <typename S>
+static int refine_gmres(pastix_gpu_t &C, VecOps<S> &V, const S *b, S *x, double eps, int itermax, int im,
                         int *iters_out, double *resid_out) {
+    typedef typename HostScalar<S>::type HS;
     const int64_t n = C.n;
     const int im1 = im + 1;
-    if (C.d_gmV.n < (size_t)n * im1) {
-        PGPU_CHECK(C.d_gmV.alloc((size_t)n * im1));
-        PGPU_CHECK(C.d_gmW.alloc((size_t)n * im));
+    const size_t comp = sizeof(S) / sizeof(double);
+    if (C.d_gmV.n < (size_t)n * im1 * comp) {
+        PGPU_CHECK(C.d_gmV.alloc((size_t)n * im1 * comp));
+        PGPU_CHECK(C.d_gmW.alloc((size_t)n * im * comp));
     }
-    if (C.d_gmh.n < (size_t)2 * im1) PGPU_CHECK(C.d_gmh.alloc((size_t)2 * im1));
+    if (C.d_gmh.n < (size_t)2 * im1 * comp) PGPU_CHECK(C.d_gmh.alloc((size_t)2 * im1 * comp));
     cudaStream_t s = C.stream;
-    double *gV = C.d_gmV.p, *gW = C.d_gmW.p, *dh = C.d_gmh.p;
-    std::vector<double> H((size_t)im * im1, 0.0), cs(im, 0.0), sn(im, 0.0), G(im1, 0.0), hcol(im1, 0.0);
+    S *gV = reinterpret_cast<S *>(C.d_gmV.p), *gW = reinterpret_cast<S *>(C.d_gmW.p);
+    S *dh = reinterpret_cast<S *>(C.d_gmh.p);
+    S *part = V.partial();
+    std::vector<HS> H((size_t)im * im1, HS(0.0)), sn(im, HS(0.0)), G(im1, HS(0.0));
+    std::vector<double> cs(im, 0.0);
+    std::vector<S> hcol(im1);
     double normb = V.norm(b);
     if (normb == 0.) normb = 1;
     const double normx = V.norm(x);
@@ -1021,50 +1161,43 @@ static int refine_gmres(pastix_gpu_t &C, VecOps &V, const double *b, double *x, 
         double resid = V.norm(gV);
         resid_b = resid / normb;
         if (resid_b <= eps) break;
-        k_scal<<<1024, 256, 0, s>>>(n, 1.0 / resid, gV);
-        V.launches++;
-        std::fill(G.begin(), G.end(), 0.0);
-        G[0] = resid;
+        V.scal(1.0 / resid, gV);
+        std::fill(G.begin(), G.end(), HS(0.0));
+        G[0] = HS(resid);
         int i = -1;
         bool inflag = true;
         while (inflag) {
             i++;
-            double *vi = gV + (int64_t)i * n, *wi = gW + (int64_t)i * n, *vn = gV + (int64_t)(i + 1) * n;
+            S *vi = gV + (int64_t)i * n, *wi = gW + (int64_t)i * n, *vn = gV + (int64_t)(i + 1) * n;
             V.copy(vi, wi);
             int rc = V.spsv(wi);                       // w_i = M^{-1} v_i
             if (rc) return rc;
             V.spmv(1.0, wi, 0.0, vn);                  // v_{i+1} = A w_i
             for (int j = 0; j <= i; j++) {             // modified Gram-Schmidt
-                k_dot_partial<<<256, RED_THREADS, 0, s>>>(n, vn, gV + (int64_t)j * n, C.d_partial.p);
-                k_dot_final<<<1, RED_THREADS, 0, s>>>(256, C.d_partial.p, dh + j, 0);
-                k_axpy_dev<<<1024, 256, 0, s>>>(n, dh + j, -1.0, gV + (int64_t)j * n, vn);
+                k_dot_partial<S><<<256, RED_THREADS, 0, s>>>(n, gV + (int64_t)j * n, vn, part);
+                k_dot_final<S><<<1, RED_THREADS, 0, s>>>(256, part, dh + j, 0);
+                k_axpy_dev<S><<<1024, 256, 0, s>>>(n, dh + j, -1.0, gV + (int64_t)j * n, vn);
                 V.launches += 3;
             }
-            k_dot_partial<<<256, RED_THREADS, 0, s>>>(n, vn, nullptr, C.d_partial.p);
-            k_dot_final<<<1, RED_THREADS, 0, s>>>(256, C.d_partial.p, dh + i + 1, 1);
+            k_dot_partial<S><<<256, RED_THREADS, 0, s>>>(n, vn, nullptr, part);
+            k_dot_final<S><<<1, RED_THREADS, 0, s>>>(256, part, dh + i + 1, 1);
             V.launches += 2;
-            PGPU_CHECK(cudaMemcpyAsync(hcol.data(), dh, (i + 2) * sizeof(double), cudaMemcpyDeviceToHost, s));
+            PGPU_CHECK(cudaMemcpyAsync(hcol.data(), dh, (i + 2) * sizeof(S), cudaMemcpyDeviceToHost, s));
             PGPU_CHECK(cudaStreamSynchronize(s));
-            const double norm = hcol[i + 1];
-            if (norm > 1e-50) {
-                k_scal<<<1024, 256, 0, s>>>(n, 1.0 / norm, vn);
-                V.launches++;
-            }
-            double *Hi = H.data() + (size_t)i * im1;
-            for (int j = 0; j <= i + 1; j++) Hi[j] = hcol[j];
+            const double norm = std::real(to_host(hcol[i + 1]));
+            if (norm > 1e-50) V.scal(1.0 / norm, vn);
+            HS *Hi = H.data() + (size_t)i * im1;
+            for (int j = 0; j <= i + 1; j++) Hi[j] = to_host(hcol[j]);
             for (int j = 0; j < i; j++) {              // previous Givens rotations
-                const double tmp = Hi[j];
+                const HS tmp = Hi[j];
                 Hi[j] = cs[j] * tmp + sn[j] * Hi[j + 1];
-                Hi[j + 1] = cs[j] * Hi[j + 1] - sn[j] * tmp;
+                Hi[j + 1] = cs[j] * Hi[j + 1] - conj_h(sn[j]) * tmp;
             }
-            double t = std::sqrt(Hi[i] * Hi[i] + Hi[i + 1] * Hi[i + 1]);
-            if (std::fabs(t) <= eps) t = eps;
-            cs[i] = Hi[i] / t;
-            sn[i] = Hi[i + 1] / t;
-            G[i + 1] = -sn[i] * G[i];
+            givens(Hi[i], Hi[i + 1], eps, cs[i], sn[i]);
+            G[i + 1] = -conj_h(sn[i]) * G[i];
             G[i] = cs[i] * G[i];
             Hi[i] = cs[i] * Hi[i] + sn[i] * Hi[i + 1];
-            resid = std::fabs(G[i + 1]);
+            resid = std::abs(G[i + 1]);
             resid_b = resid / normb;
             iters++;
             if (i + 1 >= im || resid_b <= eps || iters >= itermax) inflag = false;
@@ -1072,12 +1205,13 @@ static int refine_gmres(pastix_gpu_t &C, VecOps &V, const double *b, double *x, 
         // y = H^{-1} g (upper triangular, size i+1), x += W y
         const int k = i + 1;
         for (int r = k - 1; r >= 0; r--) {
-            double sum = G[r];
+            HS sum = G[r];
             for (int j = r + 1; j < k; j++) sum -= H[(size_t)j * im1 + r] * G[j];
             G[r] = sum / H[(size_t)r * im1 + r];
         }
-        PGPU_CHECK(cudaMemcpyAsync(dh, G.data(), k * sizeof(double), cudaMemcpyHostToDevice, s));
-        k_gemv_acc<<<1024, 256, 0, s>>>(n, k, gW, n, dh, x);
+        for (int j = 0; j < k; j++) hcol[j] = to_dev(G[j]);
+        PGPU_CHECK(cudaMemcpyAsync(dh, hcol.data(), k * sizeof(S), cudaMemcpyHostToDevice, s));
+        k_gemv_acc<S><<<1024, 256, 0, s>>>(n, k, gW, n, dh, x);
         V.launches++;
         PGPU_CHECK(cudaStreamSynchronize(s));
         if (iters >= itermax) outflag = false;
@@ -1088,56 +1222,68 @@ static int refine_gmres(pastix_gpu_t &C, VecOps &V, const double *b, double *x, 
 }
 
 static int ensure_refine_vectors(pastix_gpu_t &C) {
-    const size_t n = C.n;
-    if (C.d_r.n < n) {
-        PGPU_CHECK(C.d_r.alloc(n));
-        PGPU_CHECK(C.d_z.alloc(n));
-        PGPU_CHECK(C.d_p.alloc(n));
-        PGPU_CHECK(C.d_ap.alloc(n));
-        PGPU_CHECK(C.d_x.alloc(n));
-        PGPU_CHECK(C.d_gm.alloc(2 * n));
+    const size_t n2 = (size_t)C.n * 2;   // room for complex vectors
+    if (C.d_r.n < n2) {
+        PGPU_CHECK(C.d_r.alloc(n2));
+        PGPU_CHECK(C.d_z.alloc(n2));
+        PGPU_CHECK(C.d_p.alloc(n2));
+        PGPU_CHECK(C.d_ap.alloc(n2));
+        PGPU_CHECK(C.d_x.alloc(n2));
+        PGPU_CHECK(C.d_gm.alloc(2 * n2));
     }
     return ensure_work(C);
 }
 
-static int refine_impl(pastix_gpu_t &C, int64_t nrhs, const void *B, int64_t ldb, void *X, int64_t ldx) {
-    int rc = ensure_refine_vectors(C);
-    if (rc) return rc;
+template <typename S>
+static int refine_t(pastix_gpu_t &C, int64_t nrhs, const void *B, int64_t ldb, void *X, int64_t ldx, int *maxit,
+                    double *maxres, int *launches) {
     cudaStream_t s = C.stream;
     double eps = C.dparm[PGPU_DPARM_EPSILON_REFINEMENT];
     if (eps < 0.) eps = 1e-12;   // refinement/pastix_task_refine.c:131-140 (double input)
     const int itermax = (int)C.iparm[PGPU_IPARM_ITERMAX];
     const int method = (int)C.iparm[PGPU_IPARM_REFINEMENT];
-    if (method != PGPU_REFINE_CG && method != PGPU_REFINE_GMRES) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
     const int im = std::max<int>(1, (int)C.iparm[PGPU_IPARM_GMRES_IM]);
     const bool bdev = is_device_ptr(B), xdev = is_device_ptr(X);
-    VecOps V{C};
-    int maxit = 0;
-    double maxres = 0;
-    PGPU_CHECK(cudaEventRecord(C.ev[4], s));
+    VecOps<S> V{C};
     for (int64_t r = 0; r < nrhs; r++) {
-        const double *bcol = reinterpret_cast<const double *>(B) + r * ldb;
-        double *xcol = reinterpret_cast<double *>(X) + r * ldx;
-        double *db = C.d_rhs.p, *dx = C.d_x.p;
-        PGPU_CHECK(cudaMemcpyAsync(db, bcol, C.n * sizeof(double),
-                                   bdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
-        PGPU_CHECK(cudaMemcpyAsync(dx, xcol, C.n * sizeof(double),
-                                   xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+        const S *bcol = reinterpret_cast<const S *>(B) + r * ldb;
+        S *xcol = reinterpret_cast<S *>(X) + r * ldx;
+        S *db = reinterpret_cast<S *>(C.d_rhs.p), *dx = reinterpret_cast<S *>(C.d_x.p);
+        PGPU_CHECK(cudaMemcpyAsync(db, bcol, C.n * sizeof(S), bdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                   s));
+        PGPU_CHECK(cudaMemcpyAsync(dx, xcol, C.n * sizeof(S), xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                   s));
         int it = 0;
         double res = 0;
-        rc = (method == PGPU_REFINE_CG) ? refine_cg(C, V, db, dx, eps, itermax, &it, &res)
-                                        : refine_gmres(C, V, db, dx, eps, itermax, im, &it, &res);
+        int rc = (method == PGPU_REFINE_CG) ? refine_cg<S>(C, V, db, dx, eps, itermax, &it, &res)
+                                            : refine_gmres<S>(C, V, db, dx, eps, itermax, im, &it, &res);
         if (rc) return rc;
-        PGPU_CHECK(cudaMemcpyAsync(xcol, dx, C.n * sizeof(double),
-                                   xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
-        maxit = std::max(maxit, it);
-        maxres = std::max(maxres, res);
+        PGPU_CHECK(cudaMemcpyAsync(xcol, dx, C.n * sizeof(S), xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                   s));
+        *maxit = std::max(*maxit, it);
+        *maxres = std::max(*maxres, res);
     }
+    *launches = V.launches;
+    return PASTIX_GPU_SUCCESS;
+}
+
+static int refine_impl(pastix_gpu_t &C, int64_t nrhs, const void *B, int64_t ldb, void *X, int64_t ldx) {
+    int rc = ensure_refine_vectors(C);
+    if (rc) return rc;
+    const int method = (int)C.iparm[PGPU_IPARM_REFINEMENT];
+    if (method != PGPU_REFINE_CG && method != PGPU_REFINE_GMRES) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    cudaStream_t s = C.stream;
+    int maxit = 0, launches = 0;
+    double maxres = 0;
+    PGPU_CHECK(cudaEventRecord(C.ev[4], s));
+    rc = (C.flttype == PGPU_COMPLEX64) ? refine_t<cdouble>(C, nrhs, B, ldb, X, ldx, &maxit, &maxres, &launches)
+                                       : refine_t<double>(C, nrhs, B, ldb, X, ldx, &maxit, &maxres, &launches);
+    if (rc) return rc;
     PGPU_CHECK(cudaEventRecord(C.ev[5], s));
     PGPU_CHECK(cudaStreamSynchronize(s));
     float ms = 0;
     PGPU_CHECK(cudaEventElapsedTime(&ms, C.ev[4], C.ev[5]));
-    C.stats[2] = V.launches;
+    C.stats[2] = launches;
     C.stats[5] = ms;
     C.iparm[PGPU_IPARM_NBITER] = maxit;
     C.dparm[PGPU_DPARM_RELATIVE_ERROR] = maxres;
@@ -1160,28 +1306,29 @@ extern "C" int pastix_gpu_solve_and_refine(pastix_gpu_t *ctx, int64_t nrhs, cons
     if (C.fact_done < 0) return PASTIX_GPU_ERR_BADPARAMETER;
     PGPU_CHECK(cudaSetDevice(C.device));
     const bool bdev = is_device_ptr(B), xdev = is_device_ptr(X);
+    const size_t es = rhs_esz(C);
     if (bdev && xdev) {
         // X := B, solve in place, then refine -- all on the device
-        PGPU_CHECK(cudaMemcpy2DAsync(X, ldx * sizeof(double), B, ldb * sizeof(double), C.n * sizeof(double), nrhs,
-                                     cudaMemcpyDeviceToDevice, C.stream));
+        PGPU_CHECK(cudaMemcpy2DAsync(X, ldx * es, B, ldb * es, C.n * es, nrhs, cudaMemcpyDeviceToDevice, C.stream));
         int rc = pastix_gpu_solve(ctx, nrhs, X, ldx);
         if (rc) return rc;
         return refine_impl(C, nrhs, B, ldb, X, ldx);
     }
     // host buffers: B crosses once, X comes back once
-    if (C.d_sr_b.n < (size_t)C.n * nrhs) {
-        PGPU_CHECK(C.d_sr_b.alloc((size_t)C.n * nrhs));
-        PGPU_CHECK(C.d_sr_x.alloc((size_t)C.n * nrhs));
+    const size_t words = (size_t)C.n * nrhs * (es / 8);
+    if (C.d_sr_b.n < words) {
+        PGPU_CHECK(C.d_sr_b.alloc(words));
+        PGPU_CHECK(C.d_sr_x.alloc(words));
     }
     double *db = C.d_sr_b.p, *dx = C.d_sr_x.p;
-    PGPU_CHECK(cudaMemcpy2DAsync(db, C.n * sizeof(double), B, ldb * sizeof(double), C.n * sizeof(double), nrhs,
+    PGPU_CHECK(cudaMemcpy2DAsync(db, C.n * es, B, ldb * es, C.n * es, nrhs,
                                  bdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, C.stream));
-    PGPU_CHECK(cudaMemcpyAsync(dx, db, (size_t)C.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, C.stream));
+    PGPU_CHECK(cudaMemcpyAsync(dx, db, words * 8, cudaMemcpyDeviceToDevice, C.stream));
     int rc = pastix_gpu_solve(ctx, nrhs, dx, C.n);
     if (rc) return rc;
     rc = refine_impl(C, nrhs, db, C.n, dx, C.n);
     if (rc) return rc;
-    PGPU_CHECK(cudaMemcpy2DAsync(X, ldx * sizeof(double), dx, C.n * sizeof(double), C.n * sizeof(double), nrhs,
+    PGPU_CHECK(cudaMemcpy2DAsync(X, ldx * es, dx, C.n * es, C.n * es, nrhs,
                                  xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, C.stream));
     PGPU_CHECK(cudaStreamSynchronize(C.stream));
     return PASTIX_GPU_SUCCESS;
@@ -1223,22 +1370,23 @@ static void host_relayout(const pastix_gpu_t &C, const std::vector<T> &dev, T *L
     }
 }
 
+template <typename T>
+static int coeftab_t(pastix_gpu_t &C, void *L, void *U, bool lu) {
+    const size_t ncoef = (size_t)C.coefnbr * (lu ? 2 : 1);
+    std::vector<T> h(ncoef);
+    PGPU_CHECK(cudaMemcpy(h.data(), C.d_coef.p, ncoef * sizeof(T), cudaMemcpyDeviceToHost));
+    host_relayout<T>(C, h, (T *)L, (T *)U, lu);
+    return PASTIX_GPU_SUCCESS;
+}
+
 extern "C" int pastix_gpu_coeftab(pastix_gpu_t *ctx, void *L, void *U) {
     if (!ctx || ctx->fact_done < 0) return PASTIX_GPU_ERR_BADPARAMETER;
     auto &C = *ctx;
     PGPU_CHECK(cudaSetDevice(C.device));
-    const bool lu = (C.fact_done == PGPU_FACT_GETRF);
-    const size_t ncoef = (size_t)C.coefnbr * (lu ? 2 : 1);
-    if (C.coef_float) {
-        std::vector<float> h(ncoef);
-        PGPU_CHECK(cudaMemcpy(h.data(), C.d_coef.p, ncoef * sizeof(float), cudaMemcpyDeviceToHost));
-        host_relayout<float>(C, h, (float *)L, (float *)U, lu);
-    } else {
-        std::vector<double> h(ncoef);
-        PGPU_CHECK(cudaMemcpy(h.data(), C.d_coef.p, ncoef * sizeof(double), cudaMemcpyDeviceToHost));
-        host_relayout<double>(C, h, (double *)L, (double *)U, lu);
-    }
-    return PASTIX_GPU_SUCCESS;
+    const bool lu = (C.fact_mode == FM_GETRF);
+    if (C.flttype == PGPU_COMPLEX64)
+        return C.coef_float ? coeftab_t<cfloat>(C, L, U, lu) : coeftab_t<cdouble>(C, L, U, lu);
+    return C.coef_float ? coeftab_t<float>(C, L, U, lu) : coeftab_t<double>(C, L, U, lu);
 }
 
 extern "C" int pastix_gpu_stats(pastix_gpu_t *ctx, double *stats) {

@@ -35,6 +35,13 @@ struct Meta {
     const int *bfcblk;     // [bloknbr] facing cblk
 };
 
+// Factorization forms of the kernels (pastix_factotype_t: POTRF = LL^h,
+// GETRF = LU, SYTRF = LDL^t, HETRF = LDL^h).  The Hermitian forms (POTRF,
+// HETRF) conjugate the transposed operand; for real scalars that is a no-op.
+enum FactMode { FM_POTRF = 0, FM_GETRF = 1, FM_SYTRF = 2, FM_HETRF = 3 };
+__host__ __device__ constexpr bool fm_conj(int mode) { return mode == FM_POTRF || mode == FM_HETRF; }
+__host__ __device__ constexpr bool fm_ldl(int mode) { return mode == FM_SYTRF || mode == FM_HETRF; }
+
 // Error/status word written by kernels (never traps): bit flags + counters.
 struct Status {
     int nbpivots;      // static pivots applied
@@ -44,18 +51,92 @@ struct Status {
     int timeout;       // a bounded wait inside a kernel gave up (tile skipped)
 };
 
-template <typename T> struct ScalarOps;
-template <> struct ScalarOps<double> {
-    static __device__ __forceinline__ double absval(double a) { return fabs(a); }
-    static __device__ __forceinline__ double sqrtv(double a) { return sqrt(a); }
+// Complex scalar (interleaved re, im: the layout of pastix_complex64_t /
+// pastix_complex32_t and of C99 double/float _Complex).
+template <typename R>
+struct cplx {
+    R re, im;
+    cplx() = default;
+    __host__ __device__ constexpr cplx(R r, R i = R(0)) : re(r), im(i) {}
+    template <typename S>
+    __host__ __device__ explicit cplx(const cplx<S> &o) : re(R(o.re)), im(R(o.im)) {}
+    __host__ __device__ cplx &operator+=(const cplx &o) { re += o.re; im += o.im; return *this; }
+    __host__ __device__ cplx &operator-=(const cplx &o) { re -= o.re; im -= o.im; return *this; }
+    __host__ __device__ cplx &operator*=(const cplx &o) {
+        const R r = re * o.re - im * o.im;
+        im = re * o.im + im * o.re;
+        re = r;
+        return *this;
+    }
 };
-template <> struct ScalarOps<float> {
-    static __device__ __forceinline__ float absval(float a) { return fabsf(a); }
-    static __device__ __forceinline__ float sqrtv(float a) { return sqrtf(a); }
-};
+template <typename R> __host__ __device__ inline cplx<R> operator+(cplx<R> a, const cplx<R> &b) { return a += b; }
+template <typename R> __host__ __device__ inline cplx<R> operator-(cplx<R> a, const cplx<R> &b) { return a -= b; }
+template <typename R> __host__ __device__ inline cplx<R> operator*(cplx<R> a, const cplx<R> &b) { return a *= b; }
+template <typename R> __host__ __device__ inline cplx<R> operator-(const cplx<R> &a) { return cplx<R>(-a.re, -a.im); }
+template <typename R> __host__ __device__ inline cplx<R> operator*(R a, const cplx<R> &b) { return cplx<R>(a * b.re, a * b.im); }
+// Smith's algorithm for the quotient (scaled by the larger part of b).
+template <typename R> __host__ __device__ inline cplx<R> operator/(const cplx<R> &a, const cplx<R> &b) {
+    if (fabs(b.re) >= fabs(b.im)) {
+        const R r = b.im / b.re, d = b.re + b.im * r;
+        return cplx<R>((a.re + a.im * r) / d, (a.im - a.re * r) / d);
+    }
+    const R r = b.re / b.im, d = b.im + b.re * r;
+    return cplx<R>((a.re * r + a.im) / d, (a.im * r - a.re) / d);
+}
+typedef cplx<float> cfloat;
+typedef cplx<double> cdouble;
+
+template <typename T> struct is_cplx { static constexpr bool value = false; };
+template <typename R> struct is_cplx<cplx<R>> { static constexpr bool value = true; };
+
+// Real type of a scalar, and the helpers every kernel uses on T.
+template <typename T> struct real_of { typedef T type; };
+template <typename R> struct real_of<cplx<R>> { typedef R type; };
+
+__host__ __device__ inline float conj_v(float a) { return a; }
+__host__ __device__ inline double conj_v(double a) { return a; }
+template <typename R> __host__ __device__ inline cplx<R> conj_v(const cplx<R> &a) { return cplx<R>(a.re, -a.im); }
+// conjugate when C (Hermitian forms), identity otherwise
+template <bool C, typename T> __host__ __device__ inline T cj(const T &a) { return C ? conj_v(a) : a; }
+
+__host__ __device__ inline float real_v(float a) { return a; }
+__host__ __device__ inline double real_v(double a) { return a; }
+template <typename R> __host__ __device__ inline R real_v(const cplx<R> &a) { return a.re; }
+
+__device__ inline float abs_v(float a) { return fabsf(a); }
+__device__ inline double abs_v(double a) { return fabs(a); }
+template <typename R> __device__ inline R abs_v(const cplx<R> &a) { return hypot(a.re, a.im); }
+
+__device__ inline float abs2_v(float a) { return a * a; }
+__device__ inline double abs2_v(double a) { return a * a; }
+template <typename R> __device__ inline R abs2_v(const cplx<R> &a) { return a.re * a.re + a.im * a.im; }
+
+__device__ inline bool finite_v(float a) { return isfinite(a); }
+__device__ inline bool finite_v(double a) { return isfinite(a); }
+template <typename R> __device__ inline bool finite_v(const cplx<R> &a) { return isfinite(a.re) && isfinite(a.im); }
+
+__device__ inline float sqrt_v(float a) { return sqrtf(a); }
+__device__ inline double sqrt_v(double a) { return sqrt(a); }
+// Cholesky pivots of a Hermitian matrix are real: the square root of the real part
+template <typename R> __device__ inline cplx<R> sqrt_v(const cplx<R> &a) { return cplx<R>(sqrt(a.re), R(0)); }
+
+__device__ __forceinline__ float shfl_v(float v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ double shfl_v(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <typename R> __device__ __forceinline__ cplx<R> shfl_v(const cplx<R> &v, int src) {
+    return cplx<R>(__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src));
+}
+__device__ __forceinline__ float shfl_xor_v(float v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+__device__ __forceinline__ double shfl_xor_v(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+template <typename R> __device__ __forceinline__ cplx<R> shfl_xor_v(const cplx<R> &v, int m) {
+    return cplx<R>(__shfl_xor_sync(0xffffffffu, v.re, m), __shfl_xor_sync(0xffffffffu, v.im, m));
+}
 
 __device__ __forceinline__ void atomic_sub(double *p, double v) { atomicAdd(p, -v); }
 __device__ __forceinline__ void atomic_sub(float *p, float v) { atomicAdd(p, -v); }
+template <typename R> __device__ __forceinline__ void atomic_sub(cplx<R> *p, const cplx<R> &v) {
+    atomicAdd(&p->re, -v.re);
+    atomicAdd(&p->im, -v.im);
+}
 
 // Panel row of global row r inside cblk f: binary search over f's blocks
 // (sorted by frownum, blend/solver.h:497-514 is_block_inside_fblock walks

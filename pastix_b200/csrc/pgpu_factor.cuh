@@ -14,16 +14,25 @@ namespace pgpu {
 // coeftab was zeroed before.  A value that does not fit the factor type
 // (single precision) is flagged, as cpucblk_zccheck_overflow does.
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void k_fillin(int64_t nnz, const double *__restrict__ vals,
+// dst[k] >= 0: coef[dst[k]] = v; dst[k] < 0: coef[~dst[k]] = conj(v) (a
+// Hermitian entry stored in the other triangle after the permutation, the
+// conjugation bcsc/bcsc_zinit.c applies through __fct_conj).
+template <typename T, typename Tin>
+__global__ void k_fillin(int64_t nnz, const Tin *__restrict__ vals,
                          const int64_t *__restrict__ dst, T *__restrict__ coef,
                          Status *st) {
+    typedef typename real_of<T>::type R;
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; k < nnz; k += stride) {
-        double v = vals[k];
-        if (sizeof(T) == 4 && fabs(v) > 3.4028234663852886e38) atomicAdd(&st->overflow, 1);
-        coef[dst[k]] = (T)v;
+        Tin v = vals[k];
+        int64_t d = dst[k];
+        if (d < 0) {
+            d = ~d;
+            v = conj_v(v);
+        }
+        if (sizeof(R) == 4 && !(abs_v(v) <= 3.4028234663852886e38)) atomicAdd(&st->overflow, 1);
+        coef[d] = T(v);
     }
 }
 
@@ -38,7 +47,9 @@ __global__ void k_fillin(int64_t nnz, const double *__restrict__ vals,
 // One CTA computes one GEMM_TM x GEMM_TN tile with a 4x4 register block per
 // thread.  tile = {task, tile_m, tile_n, 0};
 // task = {c, b, f, arow0, M, flags} with flags: 1 A from U, 2 B from U,
-// 4 target U, 8 lower-triangle-only target (symmetric diagonal block).
+// 4 target U, 8 lower-triangle-only target (symmetric diagonal block),
+// 16 scale by the pivots of c (LDL: C -= A D op(B)^t, core_zgemdm),
+// 32 conjugate B (Hermitian forms: op = conj).
 // ---------------------------------------------------------------------------
 constexpr int GEMM_TM = 64, GEMM_TN = 64, GEMM_TK = 16;
 
@@ -52,6 +63,7 @@ __global__ void __launch_bounds__(256) k_gemm_scatter(Meta m, const int4 *__rest
                                                       T *__restrict__ coefL, T *__restrict__ coefU) {
     __shared__ T As[GEMM_TK][GEMM_TM + 4];
     __shared__ T Bs[GEMM_TK][GEMM_TN + 4];
+    __shared__ T Ds[GEMM_TK];
     __shared__ int trow_s[GEMM_TM];
     const int4 tl = tiles[blockIdx.x];
     const GemmTask t = tasks[tl.x];
@@ -80,14 +92,24 @@ __global__ void __launch_bounds__(256) k_gemm_scatter(Meta m, const int4 *__rest
 #pragma unroll
         for (int q = 0; q < 4; q++) acc[a][q] = T(0);
 
+    const bool scale_d = (t.flags & 16) != 0, conj_b = (t.flags & 32) != 0;
+    const T *Dg = coefL + m.coefoff[c];
     for (int k0 = 0; k0 < K; k0 += GEMM_TK) {
+        if (scale_d) {
+            if (tid < GEMM_TK) Ds[tid] = (k0 + tid < K) ? Dg[(int64_t)(k0 + tid) * ld + k0 + tid] : T(0);
+            __syncthreads();
+        }
 #pragma unroll
         for (int s = 0; s < 4; s++) {
             int e = tid + s * 256;
             int r = e >> 4, kk = e & 15;
             int kg = k0 + kk;
-            As[kk][r] = (r < mrows && kg < K) ? A[(int64_t)r * ld + kg] : T(0);
-            Bs[kk][r] = (r < ncols && kg < K) ? B[(int64_t)r * ld + kg] : T(0);
+            T av = (r < mrows && kg < K) ? A[(int64_t)r * ld + kg] : T(0);
+            T bv = (r < ncols && kg < K) ? B[(int64_t)r * ld + kg] : T(0);
+            if (scale_d) av = av * Ds[kk];
+            if (conj_b) bv = conj_v(bv);
+            As[kk][r] = av;
+            Bs[kk][r] = bv;
         }
         __syncthreads();
 #pragma unroll

@@ -1,8 +1,9 @@
 // Blocked panel factorization of a cblk: diagonal block factorization with
 // static pivoting (kernels/core_zpotrfsp.c:68,144 core_zpotf2sp/core_zpotrfsp;
-// kernels/core_zgetrfsp.c:64,138 core_zgetf2sp/core_zgetrfsp) and the panel
-// TRSM of its off-diagonal rows (kernels/core_ztrsmsp.c:71), by column blocks
-// of PB = 32:
+// kernels/core_zgetrfsp.c:64,138 core_zgetf2sp/core_zgetrfsp;
+// kernels/core_zsytrfsp.c:63,141 and kernels/core_zhetrfsp.c:63,144 for
+// LDL^t / LDL^h) and the panel TRSM of its off-diagonal rows
+// (kernels/core_ztrsmsp.c:71), by column blocks of PB = 32:
 //   1. one warp factorizes the PB x PB diagonal tile in shared memory;
 //   2. every row below (and for LU every column to the right) is solved
 //      against the tile, one thread per row;
@@ -19,12 +20,13 @@ namespace pgpu {
 constexpr int PB = 32;
 constexpr int PBL = PB + 1;   // padded shared-memory row length
 
-// C[i][j] -= sum_{l<K} A[i][l] * B[j][l] for i < M, j < N; when lower >= 0
-// only entries with j <= i + lower are touched.  A, B in shared memory (row
-// strides lda, ldb); C anywhere (row stride ldc).
-template <typename T>
+// C[i][j] -= sum_{l<K} A[i][l] * op(B[j][l] s_l) for i < M, j < N (op =
+// conj when CB; s_l = bscale[l] when SC, else 1); when lower >= 0 only
+// entries with j <= i + lower are touched.
+// A, B in shared memory (row strides lda, ldb); C anywhere (row stride ldc).
+template <typename T, bool CB, bool SC = false>
 __device__ __forceinline__ void tile_update(T *C, int64_t ldc, const T *A, int lda, const T *B, int ldb, int M,
-                                            int N, int K, int lower) {
+                                            int N, int K, int lower, const T *bscale = nullptr) {
     const int tm = (M + 3) >> 2, tn = (N + 3) >> 2;
     for (int t = threadIdx.x; t < tm * tn; t += blockDim.x) {
         const int ti = t / tn, tj = t - ti * tn;
@@ -40,7 +42,12 @@ __device__ __forceinline__ void tile_update(T *C, int64_t ldc, const T *A, int l
 #pragma unroll
             for (int p = 0; p < 4; p++) a[p] = (i0 + p < M) ? A[(i0 + p) * lda + l] : T(0);
 #pragma unroll
-            for (int q = 0; q < 4; q++) b[q] = (j0 + q < N) ? B[(j0 + q) * ldb + l] : T(0);
+            for (int q = 0; q < 4; q++) b[q] = (j0 + q < N) ? cj<CB>(B[(j0 + q) * ldb + l]) : T(0);
+            if (SC) {
+                const T sl = cj<CB>(bscale[l]);
+#pragma unroll
+                for (int q = 0; q < 4; q++) b[q] = b[q] * sl;
+            }
 #pragma unroll
             for (int p = 0; p < 4; p++)
 #pragma unroll
@@ -60,36 +67,55 @@ __device__ __forceinline__ void tile_update(T *C, int64_t ldc, const T *A, int l
     }
 }
 
+// Static pivot (sopalin: |a_kk| < crit -> crit, or -crit for a diagonal of
+// negative real part in the LU / LDL forms).
+template <typename T, int MODE>
+__device__ __forceinline__ T static_pivot(T a, typename real_of<T>::type crit, int &npiv) {
+    typedef typename real_of<T>::type R;
+    if (abs_v(a) < crit) {
+        npiv++;
+        return T((MODE != FM_POTRF && real_v(a) < R(0)) ? -crit : crit);
+    }
+    return a;
+}
+
 // Warp-synchronous factorization of the nb x nb tile (row-major, ld PBL).
-// POTRF: lower Cholesky; GETRF: LU without row pivoting.  Static pivoting as
-// in the reference: |a_kk| < crit -> crit (POTRF) or +-crit (GETRF).
-template <typename T, bool LU>
-__device__ __forceinline__ void warp_factor_tile(T *tile, int nb, T crit, int &npiv, int &nneg, int &nbad) {
+//   POTRF: lower Cholesky L L^h (diagonal real and positive);
+//   GETRF: LU without row pivoting (unit L below, U on and above);
+//   SYTRF/HETRF: unit L below, D on the diagonal (L D L^t / L D L^h).
+template <typename T, int MODE>
+__device__ __forceinline__ void warp_factor_tile(T *tile, int nb, typename real_of<T>::type crit, int &npiv,
+                                                 int &nneg, int &nbad) {
+    typedef typename real_of<T>::type R;
+    constexpr bool CJ = fm_conj(MODE);
     const int lane = threadIdx.x & 31;
     for (int k = 0; k < nb; k++) {
         if (lane == 0) {
             T a = tile[k * PBL + k];
-            if (!isfinite(a)) nbad++;
-            if (ScalarOps<T>::absval(a) < crit) {
-                a = (LU && a < T(0)) ? -crit : crit;
-                npiv++;
-            }
-            if (!LU) {
-                if (a < T(0)) nneg++;
-                a = ScalarOps<T>::sqrtv(a);
+            if (!finite_v(a)) nbad++;
+            a = static_pivot<T, MODE>(a, crit, npiv);
+            if (MODE == FM_POTRF) {
+                if (real_v(a) < R(0)) nneg++;
+                a = sqrt_v(a);
             }
             tile[k * PBL + k] = a;
         }
         __syncwarp();
-        const T inv = T(1) / tile[k * PBL + k];
-        if (lane > k && lane < nb) tile[lane * PBL + k] *= inv;
+        const T dk = tile[k * PBL + k];
+        const T inv = T(1) / (MODE == FM_POTRF ? cj<CJ>(dk) : dk);
+        if (lane > k && lane < nb) tile[lane * PBL + k] = tile[lane * PBL + k] * inv;
         __syncwarp();
         if (lane > k && lane < nb) {
             const T lik = tile[lane * PBL + k];
-            if (LU) {
+            if (MODE == FM_GETRF) {
                 for (int j = k + 1; j < nb; j++) tile[lane * PBL + j] -= lik * tile[k * PBL + j];
+            } else if (MODE == FM_POTRF) {
+                for (int j = k + 1; j <= lane; j++) tile[lane * PBL + j] -= lik * cj<CJ>(tile[j * PBL + k]);
             } else {
-                for (int j = k + 1; j <= lane; j++) tile[lane * PBL + j] -= lik * tile[j * PBL + k];
+                // a_ij -= l_ik d_k op(l_jk); LDL^h takes the real part of d_k (zher)
+                const T ld = lik * (MODE == FM_HETRF ? T(real_v(dk)) : dk);
+                for (int j = k + 1; j <= lane; j++) tile[lane * PBL + j] -= ld * cj<CJ>(tile[j * PBL + k]);
+                if (MODE == FM_HETRF) tile[lane * PBL + lane] = T(real_v(tile[lane * PBL + lane]));
             }
         }
         __syncwarp();
@@ -97,14 +123,15 @@ __device__ __forceinline__ void warp_factor_tile(T *tile, int nb, T crit, int &n
 }
 
 // Row solves against the factorized tile (x: nb values of one row, in place).
-//   POTRF rows / LU U^T rows:  x L^T = a  (L = lower of tile; unit for LU)
-//   LU L rows:                 x U   = a  (U = upper of tile, non-unit)
-template <typename T>
+//   lower_t: x op(L)^t = a, L = lower of the tile (unit when `unit`), op =
+//            conj when CJ -- POTRF rows, LU U^t rows, LDL rows (unit);
+//   upper:   x U = a, U = upper of the tile (non-unit) -- LU L rows.
+template <typename T, bool CJ>
 __device__ __forceinline__ void row_solve_lower_t(T *x, const T *tile, int nb, bool unit) {
     for (int j = 0; j < nb; j++) {
         T s = x[j];
-        for (int l = 0; l < j; l++) s -= x[l] * tile[j * PBL + l];
-        x[j] = unit ? s : s * (T(1) / tile[j * PBL + j]);
+        for (int l = 0; l < j; l++) s -= x[l] * cj<CJ>(tile[j * PBL + l]);
+        x[j] = unit ? s : s * (T(1) / cj<CJ>(tile[j * PBL + j]));
     }
 }
 template <typename T>
@@ -119,17 +146,24 @@ __device__ __forceinline__ void row_solve_upper(T *x, const T *tile, int nb) {
 // ---------------------------------------------------------------------------
 // One CTA per cblk of the level.  rows_fused(c) = h_c when h_c <= fuse_rows
 // (the off-diagonal rows are solved here too), else w_c (they go to
-// k_trsm_rows).  Shared memory: tile[PB][PBL] + PL[rows][PBL] (solved
-// column block of L) + for LU PU[w][PBL] (solved row block of U, stored by
-// column) and PO[rows][PBL] (solved column block of the U^T rows).
+// k_trsm_rows).  Shared memory: tile[PB][PBL] + dinv[PB] + PL[rows][PBL]
+// (solved column block) + for GETRF PU[w][PBL] (solved row block of U,
+// stored by column) and PO[rows - w][PBL] (solved column block of the U^t
+// rows).  For LDL, PL holds y = x D (rows times the pivots) and the trailing
+// update takes its right operand as y D^{-1} = x through dinv.
 // ---------------------------------------------------------------------------
-template <typename T, bool LU>
+template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restrict__ cblks, T *__restrict__ coefL,
                                                       T *__restrict__ coefU, double critd, int fuse_rows,
                                                       int pl_rows, int pu_rows, Status *st) {
+    typedef typename real_of<T>::type R;
+    constexpr bool LU = (MODE == FM_GETRF);
+    constexpr bool LDL = fm_ldl(MODE);
+    constexpr bool CJ = fm_conj(MODE);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *tile = reinterpret_cast<T *>(smem_raw);
-    T *PL = tile + PB * PBL;                 // [pl_rows][PBL]: rows r1.. of the panel
+    T *dinv = tile + PB * PBL;               // [PB] inverse pivots (LDL)
+    T *PL = dinv + PB;                       // [pl_rows][PBL]: rows r1.. of the panel
     T *PU = PL + (size_t)pl_rows * PBL;      // [pu_rows][PBL]: columns r1..w (LU only)
     T *PO = PU + (size_t)pu_rows * PBL;      // [rows - w][PBL]: fused U^T rows (LU only)
     const int c = cblks[blockIdx.x];
@@ -137,7 +171,7 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
     const int rows = (h <= fuse_rows) ? h : w;
     T *A = coefL + m.coefoff[c];
     T *AU = coefU + m.coefoff[c];
-    const T crit = T(critd);
+    const R crit = R(critd);
     const int tid = threadIdx.x, nt = blockDim.x;
     int npiv = 0, nneg = 0, nbad = 0;
     for (int jb = 0; jb < w; jb += PB) {
@@ -150,11 +184,12 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
                 tile[i * PBL + j] = A[(int64_t)(jb + i) * ld + jb + j];
             }
             __syncwarp();
-            warp_factor_tile<T, LU>(tile, nb, crit, npiv, nneg, nbad);
+            warp_factor_tile<T, MODE>(tile, nb, crit, npiv, nneg, nbad);
             for (int e = tid; e < nb * nb; e += 32) {
                 const int i = e / nb, j = e - i * nb;
                 if (LU || j <= i) A[(int64_t)(jb + i) * ld + jb + j] = tile[i * PBL + j];
             }
+            if (LDL && tid < nb) dinv[tid] = T(1) / tile[tid * PBL + tid];
         }
         __syncthreads();
         // 2. rows below the tile (diagonal-block rows and fused off-diagonal rows)
@@ -164,12 +199,12 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
 #pragma unroll
             for (int j = 0; j < PB; j++) x[j] = (j < nb) ? row[j] : T(0);
             if (LU) row_solve_upper<T>(x, tile, nb);
-            else row_solve_lower_t<T>(x, tile, nb, false);
+            else row_solve_lower_t<T, CJ>(x, tile, nb, LDL);
 #pragma unroll
             for (int j = 0; j < PB; j++)
                 if (j < nb) {
-                    row[j] = x[j];
-                    PL[(r - r1) * PBL + j] = x[j];
+                    PL[(r - r1) * PBL + j] = x[j];            // LDL: y = x D
+                    row[j] = LDL ? x[j] * dinv[j] : x[j];
                 }
         }
         if (LU) {
@@ -196,7 +231,7 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
                 T *row = AU + (int64_t)r * ld + jb;
 #pragma unroll
                 for (int j = 0; j < PB; j++) x[j] = (j < nb) ? row[j] : T(0);
-                row_solve_lower_t<T>(x, tile, nb, true);
+                row_solve_lower_t<T, false>(x, tile, nb, true);
 #pragma unroll
                 for (int j = 0; j < PB; j++)
                     if (j < nb) {
@@ -211,16 +246,18 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
         if (ncol > 0) {
             if (LU) {
                 // L rows (diagonal block + fused off-diagonal): A[r][c] -= L[r][jb:] U[jb:][c]
-                tile_update<T>(A + (int64_t)r1 * ld + r1, ld, PL, PBL, PU, PBL, rows - r1, ncol, nb, -1);
+                tile_update<T, false>(A + (int64_t)r1 * ld + r1, ld, PL, PBL, PU, PBL, rows - r1, ncol, nb, -1);
                 // fused U^T rows: AU[r][c] -= X[r][jb:] L[c][jb:]
                 if (rows > w)
-                    tile_update<T>(AU + (int64_t)w * ld + r1, ld, PO, PBL, PL, PBL, rows - w, ncol, nb, -1);
+                    tile_update<T, false>(AU + (int64_t)w * ld + r1, ld, PO, PBL, PL, PBL, rows - w, ncol, nb, -1);
             } else {
-                // diagonal block (lower triangle) and fused off-diagonal rows
-                tile_update<T>(A + (int64_t)r1 * ld + r1, ld, PL, PBL, PL, PBL, w - r1, ncol, nb, 0);
+                // diagonal block (lower triangle) and fused off-diagonal rows:
+                // A[r][c] -= Y[r][jb:] op(X[c][jb:]) (Cholesky: Y = X = L;
+                // LDL: Y = L D, X = Y D^{-1})
+                tile_update<T, CJ, LDL>(A + (int64_t)r1 * ld + r1, ld, PL, PBL, PL, PBL, w - r1, ncol, nb, 0, dinv);
                 if (rows > w)
-                    tile_update<T>(A + (int64_t)w * ld + r1, ld, PL + (size_t)(w - r1) * PBL, PBL, PL, PBL,
-                                   rows - w, ncol, nb, -1);
+                    tile_update<T, CJ, LDL>(A + (int64_t)w * ld + r1, ld, PL + (size_t)(w - r1) * PBL, PBL, PL, PBL,
+                                            rows - w, ncol, nb, -1, dinv);
             }
         }
         __syncthreads();
@@ -236,13 +273,19 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
 // Panel TRSM of the off-diagonal rows of large cblks (not fused above):
 // TR rows per CTA kept in shared memory, blocked by PB columns against the
 // factorized diagonal block.  chunk = {cblk, first panel row, panel select
-// (0 L / 1 U), mode} with mode 0 POTRF (x L^T = a), 1 GETRF L side
-// (x U = a), 2 GETRF U side (x L^T = a, unit).
-// Shared memory: X[TR][w+1] + tile[PB][PBL] + P[w][PBL].
+// (0 L / 1 U), mode} with mode
+//   0 POTRF        x op(L)^t = a          (op = conj when CJ)
+//   1 GETRF L side x U = a
+//   2 GETRF U side x L^t = a, unit
+//   3 LDL          x D op(L)^t = a: y op(L)^t = a (unit), then x = y D^{-1}
+//                  (kernels/core_zsytrfsp.c:427-460 / core_zhetrfsp.c with
+//                  D op(L)^t kept in the upper triangle)
+// Shared memory: X[TR][w+1] + tile[PB][PBL] + P[pch][PBL]; the trailing
+// update coefficients go through P in chunks of pch columns.
 // ---------------------------------------------------------------------------
-template <typename T, int TR>
+template <typename T, int TR, bool CJ>
 __global__ void __launch_bounds__(256) k_trsm_rows(Meta m, const int4 *__restrict__ chunks, T *__restrict__ coefL,
-                                                   T *__restrict__ coefU, int maxw) {
+                                                   T *__restrict__ coefU, int maxw, int pch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int4 ch = chunks[blockIdx.x];
     const int c = ch.x, r0 = ch.y, mode = ch.w;
@@ -251,10 +294,11 @@ __global__ void __launch_bounds__(256) k_trsm_rows(Meta m, const int4 *__restric
     const int xl = maxw + 1;
     T *X = reinterpret_cast<T *>(smem_raw);                   // [TR][xl]
     T *tile = X + TR * xl;                                      // [PB][PBL]
-    T *P = tile + PB * PBL;                                     // [maxw][PBL]
+    T *P = tile + PB * PBL;                                     // [pch][PBL]
     const T *D = coefL + m.coefoff[c];
     T *Pan = (ch.z ? coefU : coefL) + m.coefoff[c] + (int64_t)r0 * ld;
     const int tid = threadIdx.x, nt = blockDim.x;
+    const bool cjl = CJ && mode != 2;      // conjugate the L coefficients
     for (int e = tid; e < nrows * w; e += nt) {
         const int i = e / w, j = e - i * w;
         X[i * xl + j] = Pan[(int64_t)i * ld + j];
@@ -265,30 +309,42 @@ __global__ void __launch_bounds__(256) k_trsm_rows(Meta m, const int4 *__restric
             const int i = e / nb, j = e - i * nb;
             tile[i * PBL + j] = D[(int64_t)(jb + i) * ld + jb + j];
         }
-        // coefficients of the trailing update, P[col - r1][l]
-        for (int e = tid; e < ncol * nb; e += nt) {
-            const int cc = e / nb, l = e - cc * nb;
-            P[cc * PBL + l] = (mode == 1) ? D[(int64_t)(jb + l) * ld + r1 + cc]      // U[jb+l][col]
-                                          : D[(int64_t)(r1 + cc) * ld + jb + l];     // L[col][jb+l]
-        }
         __syncthreads();
         for (int i = tid; i < nrows; i += nt) {
             T x[PB];
 #pragma unroll
             for (int j = 0; j < PB; j++) x[j] = (j < nb) ? X[i * xl + jb + j] : T(0);
             if (mode == 1) row_solve_upper<T>(x, tile, nb);
-            else row_solve_lower_t<T>(x, tile, nb, mode == 2);
+            else if (cjl) row_solve_lower_t<T, CJ>(x, tile, nb, mode != 0);
+            else row_solve_lower_t<T, false>(x, tile, nb, mode != 0);
 #pragma unroll
             for (int j = 0; j < PB; j++)
                 if (j < nb) X[i * xl + jb + j] = x[j];
         }
         __syncthreads();
-        if (ncol > 0) tile_update<T>(X + r1, xl, X + jb, xl, P, PBL, nrows, ncol, nb, -1);
-        __syncthreads();
+        for (int cc0 = 0; cc0 < ncol; cc0 += pch) {
+            const int nc2 = min(pch, ncol - cc0);
+            // coefficients of the trailing update, P[col - r1 - cc0][l]
+            for (int e = tid; e < nc2 * nb; e += nt) {
+                const int cc = e / nb, l = e - cc * nb;
+                const int col = r1 + cc0 + cc;
+                if (mode == 1) {
+                    P[cc * PBL + l] = D[(int64_t)(jb + l) * ld + col];      // U[jb+l][col]
+                } else {
+                    const T v = D[(int64_t)col * ld + jb + l];             // L[col][jb+l]
+                    P[cc * PBL + l] = cjl ? conj_v(v) : v;
+                }
+            }
+            __syncthreads();
+            tile_update<T, false>(X + r1 + cc0, xl, X + jb, xl, P, PBL, nrows, nc2, nb, -1);
+            __syncthreads();
+        }
     }
     for (int e = tid; e < nrows * w; e += nt) {
         const int i = e / w, j = e - i * w;
-        Pan[(int64_t)i * ld + j] = X[i * xl + j];
+        T v = X[i * xl + j];
+        if (mode == 3) v = v * (T(1) / D[(int64_t)j * ld + j]);
+        Pan[(int64_t)i * ld + j] = v;
     }
 }
 

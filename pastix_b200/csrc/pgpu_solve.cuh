@@ -46,7 +46,7 @@ __global__ void k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
                 T v = (lane < nb) ? y[(jb + lane) * nrhs + r] : T(0);
                 for (int j = 0; j < nb; j++) {
                     if (!unit && lane == j) v *= dinv;
-                    const T xj = __shfl_sync(0xffffffffu, v, j);
+                    const T xj = shfl_v(v, j);
                     if (lane > j && lane < nb) v -= tile[lane * 33 + j] * xj;
                 }
                 if (lane < nb) y[(jb + lane) * nrhs + r] = v;
@@ -100,7 +100,7 @@ __global__ void k_fwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
             T s = T(0);
             for (int j = lane; j < w; j += 32) s += row[j] * y[r * w + j];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            for (int o = 16; o > 0; o >>= 1) s += shfl_xor_v(s, o);
             if (lane == 0) atomic_sub(&B[(int64_t)r * ldb + grow], s);
         }
     }
@@ -108,14 +108,14 @@ __global__ void k_fwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
 
 // ---------------------------------------------------------------------------
 // Backward, off-diagonal gather (kernels/solve_ztrsmsp.c:450
-// solve_cblk_ztrsmsp_backward walks browtab): B[fcol+j, :] -= sum_i P[i, j]
-// B[row_i, :] over panel rows i >= w of cblk c (P = L for POTRF, U^T for
-// GETRF).  Threads along j (coalesced in the row-major panel); a chunk of
+// solve_cblk_ztrsmsp_backward walks browtab): B[fcol+j, :] -= sum_i op(P[i, j])
+// B[row_i, :] over panel rows i >= w of cblk c (P = L for POTRF / LDL, U^T
+// for GETRF; op = conj for the Hermitian forms when cjp).  Threads along j (coalesced in the row-major panel); a chunk of
 // rows per CTA, partial sums combined atomically.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_bwd_off(Meta m, const int2 *__restrict__ chunks, const T *__restrict__ coef,
-                          T *__restrict__ B, int ldb, int nrhs, int rows_per_chunk) {
+                          T *__restrict__ B, int ldb, int nrhs, int rows_per_chunk, int cjp) {
     const int2 ch = chunks[blockIdx.x];
     const int c = ch.x, r0 = ch.y;
     const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c], h = m.height[c];
@@ -125,7 +125,7 @@ __global__ void k_bwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
         T s[SOLVE_MAXRHS];
         for (int r = 0; r < nrhs; r++) s[r] = T(0);
         for (int i = r0; i < rend; i++) {
-            const T pij = P[(int64_t)i * ld + j];
+            const T pij = cjp ? conj_v(P[(int64_t)i * ld + j]) : P[(int64_t)i * ld + j];
             const int grow = m.rowidx[m.rowbase[c] + i];
             for (int r = 0; r < nrhs; r++) s[r] += pij * B[(int64_t)r * ldb + grow];
         }
@@ -135,14 +135,16 @@ __global__ void k_bwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
 
 // ---------------------------------------------------------------------------
 // Backward, diagonal part: B[fcol:fcol+w, :] := D^{-1} B[...] with
-// D = L_kk^T (POTRF, Left, Lower, ConjTrans/Trans, NonUnit) or the upper
-// triangle U_kk of the LU diagonal block (Left, Upper, NoTrans, NonUnit).
-// Blocked by 32 columns from the last block up: warp 0 substitutes through
-// the tile, then all threads update the rows above.
+// D = op(L_kk)^t (POTRF: Left, Lower, ConjTrans, NonUnit; LDL: the unit
+// lower part, Left, Lower, ConjTrans/Trans, Unit, after k_diag_scale) or the
+// upper triangle U_kk of the LU diagonal block (Left, Upper, NoTrans,
+// NonUnit).  op = conj when cjp.  Blocked by 32 columns from the last block
+// up: warp 0 substitutes through the tile, then all threads update the rows
+// above.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
-                           T *__restrict__ B, int ldb, int nrhs, int upper) {
+                           T *__restrict__ B, int ldb, int nrhs, int upper, int unit, int cjp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *x = reinterpret_cast<T *>(smem_raw);   // [w][nrhs]
     const int c = cblks[blockIdx.x];
@@ -154,24 +156,25 @@ __global__ void k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
         x[e] = B[(int64_t)r * ldb + fc + j];
     }
     __syncthreads();
-    T *tile = x + w * nrhs;                   // [32][33] diagonal tile
+    T *tile = x + w * nrhs;                   // [32][33] diagonal tile (op applied)
     const int nblk = (w + 31) / 32;
     for (int bi = nblk - 1; bi >= 0; bi--) {
         const int jb = bi * 32, nb = min(32, w - jb);
         for (int e = tid; e < nb * nb; e += nt) {
             const int i = e / nb, j = e - i * nb;
-            tile[i * 33 + j] = D[(int64_t)(jb + i) * ld + jb + j];
+            const T v = D[(int64_t)(jb + i) * ld + jb + j];
+            tile[i * 33 + j] = cjp ? conj_v(v) : v;
         }
         __syncthreads();
         if (tid < 32) {
-            const T dinv = (lane < nb) ? T(1) / tile[lane * 33 + lane] : T(1);
+            const T dinv = (lane < nb && !unit) ? T(1) / tile[lane * 33 + lane] : T(1);
             for (int r = 0; r < nrhs; r++) {
                 T v = (lane < nb) ? x[(jb + lane) * nrhs + r] : T(0);
                 for (int j = nb - 1; j >= 0; j--) {
-                    if (lane == j) v *= dinv;
-                    const T xj = __shfl_sync(0xffffffffu, v, j);
+                    if (lane == j) v = v * dinv;
+                    const T xj = shfl_v(v, j);
                     if (lane < j) {
-                        // upper: U[l][j]; Cholesky: L^T[l][j] = L[j][l]
+                        // upper: U[l][j]; Cholesky / LDL: op(L)^t[l][j] = op(L[j][l])
                         const T dlj = upper ? tile[lane * 33 + j] : tile[j * 33 + lane];
                         v -= dlj * xj;
                     }
@@ -188,7 +191,10 @@ __global__ void k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
                 const T *row = D + (int64_t)i * ld + jb;
                 for (int l = 0; l < nb; l++) s += row[l] * x[(jb + l) * nrhs + r];
             } else {
-                for (int l = 0; l < nb; l++) s += D[(int64_t)(jb + l) * ld + i] * x[(jb + l) * nrhs + r];
+                for (int l = 0; l < nb; l++) {
+                    const T v = D[(int64_t)(jb + l) * ld + i];
+                    s += (cjp ? conj_v(v) : v) * x[(jb + l) * nrhs + r];
+                }
             }
             x[i * nrhs + r] -= s;
         }
@@ -197,6 +203,23 @@ __global__ void k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
     for (int e = tid; e < w * nrhs; e += nt) {
         int j = e / nrhs, r = e - j * nrhs;
         B[(int64_t)r * ldb + fc + j] = x[e];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal solve of the LDL forms (kernels/solve_ztrsmsp.c:630
+// solve_cblk_zdiag): B[fcol + j, :] /= D_jj, one CTA per cblk (grid-strided).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_diag_scale(Meta m, const T *__restrict__ coefL, T *__restrict__ B, int ldb, int nrhs) {
+    for (int c = blockIdx.x; c < m.cblknbr; c += gridDim.x) {
+        const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c];
+        const T *D = coefL + m.coefoff[c];
+        for (int e = threadIdx.x; e < w * nrhs; e += blockDim.x) {
+            const int j = e % w, r = e / w;
+            T &v = B[(int64_t)r * ldb + fc + j];
+            v = v * (T(1) / D[(int64_t)j * ld + j]);
+        }
     }
 }
 
@@ -225,68 +248,74 @@ __global__ void k_convert(int64_t n, const Tin *__restrict__ x, Tout *__restrict
 }
 
 // ---------------------------------------------------------------------------
-// Refinement vector kernels, FP64 (bcsc/bcsc_zspmv.c:629 bcsc_zspmv on the
-// permuted matrix held as CSR, one warp per row; bvec_z{dotc,nrm2,axpy,scal,
-// copy}, bcsc/bvec_zcompute.c).  Reductions go through per-CTA partials
-// finished by one CTA, so results are deterministic.
+// Refinement vector kernels, FP64 real (S = double) or complex (S = cdouble)
+// (bcsc/bcsc_zspmv.c:629 bcsc_zspmv on the permuted matrix held as CSR, one
+// warp per row; bvec_z{dotc,nrm2,axpy,scal,copy,gemv}, bcsc/bvec_zcompute.c).
+// Reductions go through per-CTA partials finished by one CTA, so results are
+// deterministic.
 // ---------------------------------------------------------------------------
+template <typename S>
 __global__ void k_spmv(int n, const int64_t *__restrict__ rowptr, const int *__restrict__ col,
-                       const double *__restrict__ val, double alpha, const double *__restrict__ x,
-                       double beta, double *__restrict__ y) {
+                       const S *__restrict__ val, double alpha, const S *__restrict__ x,
+                       double beta, S *__restrict__ y) {
     const int lane = threadIdx.x & 31;
     int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (; row < n; row += nwarps) {
-        double s = 0.0;
+        S s = S(0.0);
         for (int64_t k = rowptr[row] + lane; k < rowptr[row + 1]; k += 32) s += val[k] * x[col[k]];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) y[row] = alpha * s + (beta == 0.0 ? 0.0 : beta * y[row]);
+        for (int o = 16; o > 0; o >>= 1) s += shfl_xor_v(s, o);
+        if (lane == 0) y[row] = alpha * s + (beta == 0.0 ? S(0.0) : beta * y[row]);
     }
 }
 
 constexpr int RED_THREADS = 256;
 
-__device__ __forceinline__ double block_sum(double v, double *sh) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+template <typename S>
+__device__ __forceinline__ S block_sum(S v, S *sh) {
+    for (int o = 16; o > 0; o >>= 1) v += shfl_xor_v(v, o);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) sh[warp] = v;
     __syncthreads();
-    v = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+    v = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : S(0.0);
     if (warp == 0)
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        for (int o = 16; o > 0; o >>= 1) v += shfl_xor_v(v, o);
     return v;
 }
 
-// partial[blockIdx] = sum x*y  (or sum x*x when y == nullptr)
-__global__ void k_dot_partial(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
-                              double *__restrict__ partial) {
-    __shared__ double sh[32];
-    double s = 0.0;
+// partial[blockIdx] = sum conj(x) y (bvec_zdotc), or sum |x|^2 when y == nullptr
+template <typename S>
+__global__ void k_dot_partial(int64_t n, const S *__restrict__ x, const S *__restrict__ y, S *__restrict__ partial) {
+    __shared__ S sh[32];
+    S s = S(0.0);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
-        s += x[i] * (y ? y[i] : x[i]);
+        s += y ? conj_v(x[i]) * y[i] : S(abs2_v(x[i]));
     s = block_sum(s, sh);
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
-__global__ void k_dot_final(int np, const double *__restrict__ partial, double *__restrict__ out,
-                            int do_sqrt) {
-    __shared__ double sh[32];
-    double s = 0.0;
+// *out = sum of the partials (do_sqrt: sqrt of its real part, for norms)
+template <typename S>
+__global__ void k_dot_final(int np, const S *__restrict__ partial, S *__restrict__ out, int do_sqrt) {
+    __shared__ S sh[32];
+    S s = S(0.0);
     for (int i = threadIdx.x; i < np; i += blockDim.x) s += partial[i];
     s = block_sum(s, sh);
-    if (threadIdx.x == 0) *out = do_sqrt ? sqrt(s) : s;
+    if (threadIdx.x == 0) *out = do_sqrt ? S(sqrt(real_v(s))) : s;
 }
 
-__global__ void k_axpy(int64_t n, double alpha, const double *__restrict__ x, double *__restrict__ y) {
+template <typename S>
+__global__ void k_axpy(int64_t n, S alpha, const S *__restrict__ x, S *__restrict__ y) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
         y[i] += alpha * x[i];
 }
 
 // p = z + beta * p
-__global__ void k_xpby(int64_t n, const double *__restrict__ z, double beta, double *__restrict__ p) {
+template <typename S>
+__global__ void k_xpby(int64_t n, const S *__restrict__ z, S beta, S *__restrict__ p) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
         p[i] = z[i] + beta * p[i];
@@ -294,48 +323,56 @@ __global__ void k_xpby(int64_t n, const double *__restrict__ z, double beta, dou
 
 // y += sign * (*alpha) * x with the scalar read from device memory (GMRES
 // orthogonalization without a host round trip per projection).
-__global__ void k_axpy_dev(int64_t n, const double *__restrict__ alpha, double sign, const double *__restrict__ x,
-                           double *__restrict__ y) {
-    const double a = sign * (*alpha);
+template <typename S>
+__global__ void k_axpy_dev(int64_t n, const S *__restrict__ alpha, double sign, const S *__restrict__ x,
+                           S *__restrict__ y) {
+    const S a = sign * (*alpha);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
         y[i] += a * x[i];
 }
 
-__global__ void k_scal(int64_t n, double a, double *__restrict__ x) {
+template <typename S>
+__global__ void k_scal(int64_t n, double a, S *__restrict__ x) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
-        x[i] *= a;
+        x[i] = a * x[i];
 }
 
 // x += W(:, 0:k) y  (bvec_zgemv, bcsc/bvec_zcompute.c; W column-major, ld ldw)
-__global__ void k_gemv_acc(int64_t n, int k, const double *__restrict__ W, int64_t ldw,
-                           const double *__restrict__ y, double *__restrict__ x) {
+template <typename S>
+__global__ void k_gemv_acc(int64_t n, int k, const S *__restrict__ W, int64_t ldw, const S *__restrict__ y,
+                           S *__restrict__ x) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        double s = 0.0;
+        S s = S(0.0);
         for (int j = 0; j < k; j++) s += W[i + j * ldw] * y[j];
         x[i] += s;
     }
 }
 
-// Gather the permuted-matrix values from the user's values.
-__global__ void k_gather_vals(int64_t nnz, const int64_t *__restrict__ src, const double *__restrict__ vals,
-                              double *__restrict__ out) {
+// Gather the permuted-matrix values from the user's values; src < 0 marks
+// the mirrored entry of a Hermitian matrix (conj(vals[~src])).
+template <typename S>
+__global__ void k_gather_vals(int64_t nnz, const int64_t *__restrict__ src, const S *__restrict__ vals,
+                              S *__restrict__ out) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnz;
-         i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = vals[src[i]];
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = src[i];
+        out[i] = (k < 0) ? conj_v(vals[~k]) : vals[k];
+    }
 }
 
 // Weighted sum of squares for the Frobenius norm (off-diagonal entries of a
 // one-triangle symmetric matrix count twice).
-__global__ void k_sumsq_partial(int64_t nnz, const double *__restrict__ v, const int8_t *__restrict__ wgt,
+template <typename S>
+__global__ void k_sumsq_partial(int64_t nnz, const S *__restrict__ v, const int8_t *__restrict__ wgt,
                                 double *__restrict__ partial) {
     __shared__ double sh[32];
     double s = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnz;
          i += (int64_t)gridDim.x * blockDim.x)
-        s += (double)wgt[i] * v[i] * v[i];
+        s += (double)wgt[i] * abs2_v(v[i]);
     s = block_sum(s, sh);
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }

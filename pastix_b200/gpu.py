@@ -110,6 +110,7 @@ class Solver:
         self._h = C.c_void_p()
         _check("pastix_gpu_init", L.pastix_gpu_init(C.byref(self._h), device, _p(ip), _p(dp)))
         self.n = None
+        self.dtype = np.float64      # right-hand-side / solution type (complex128 for complex matrices)
 
     # -- parameters --------------------------------------------------------
     def set_iparm(self, idx, v):
@@ -150,6 +151,7 @@ class Solver:
         rc = load().pastix_gpu_spm(self._h, system.mtxtype, system.flttype, system.n,
                                    _p(self._colptr), _p(self._rowptr))
         _check("pastix_gpu_spm", rc)
+        self.dtype = np.complex128 if np.iscomplexobj(system.values) else np.float64
 
     # -- numerical tasks ---------------------------------------------------
     def numfact(self, values):
@@ -158,7 +160,7 @@ class Solver:
 
     def solve(self, b):
         """Returns x with A x = b (b: n or n x nrhs, host numpy, Fortran order)."""
-        x = np.array(b, dtype=np.float64, order="F", copy=True)
+        x = np.array(b, dtype=self.dtype, order="F", copy=True)
         nrhs = 1 if x.ndim == 1 else x.shape[1]
         _check("pastix_gpu_solve", load().pastix_gpu_solve(self._h, nrhs, _p(x), self.n))
         return x
@@ -168,14 +170,14 @@ class Solver:
         _check("pastix_gpu_solve", load().pastix_gpu_solve(self._h, nrhs, _p(B), ldb))
 
     def refine(self, b, x):
-        b = np.array(b, dtype=np.float64, order="F")
-        x = np.array(x, dtype=np.float64, order="F", copy=True)
+        b = np.array(b, dtype=self.dtype, order="F")
+        x = np.array(x, dtype=self.dtype, order="F", copy=True)
         nrhs = 1 if x.ndim == 1 else x.shape[1]
         _check("pastix_gpu_refine", load().pastix_gpu_refine(self._h, nrhs, _p(b), self.n, _p(x), self.n))
         return x
 
     def solve_and_refine(self, b):
-        b = np.array(b, dtype=np.float64, order="F")
+        b = np.array(b, dtype=self.dtype, order="F")
         x = np.zeros_like(b, order="F")
         nrhs = 1 if x.ndim == 1 else x.shape[1]
         rc = load().pastix_gpu_solve_and_refine(self._h, nrhs, _p(b), self.n, _p(x), self.n)
@@ -195,7 +197,10 @@ class Solver:
             total += h * w
         ip, _ = self.params()
         mixed = ip[IPARM_MIXED] != 0
-        dt = np.float32 if mixed else np.float64
+        if self.dtype == np.complex128:
+            dt = np.complex64 if mixed else np.complex128
+        else:
+            dt = np.float32 if mixed else np.float64
         Lc = np.zeros(total, dt)
         Uc = np.zeros(total, dt) if ip[IPARM_FACTORIZATION] == FACT["getrf"] else None
         _check("pastix_gpu_coeftab", load().pastix_gpu_coeftab(self._h, _p(Lc), _p(Uc)))

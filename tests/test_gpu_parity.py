@@ -167,3 +167,104 @@ def test_mixed_lu_factor_matches_reference_mixed(name, make, fp32_gemm):
     Lg, Ug = s.coeftab()
     assert np.abs(Lg.astype(np.float64) - Lr).max() <= 5e-5 * np.abs(Lr).max()
     assert np.abs(Ug.astype(np.float64) - Ur).max() <= 5e-5 * np.abs(Ur).max()
+
+
+# --- LDL^t / LDL^h and complex data ------------------------------------------
+def _complex_symmetric(A):
+    A.mtxtype = M.PastixSymmetric
+    return A
+
+
+def _real_hermitian(A):
+    A.values = A.values.real.astype(np.complex128)
+    return A
+
+
+def _complex_general(A):
+    """Full storage of the magnetic Laplacian with the lower triangle scaled
+    by (1 + 0.5i): a complex unsymmetric matrix with a symmetric pattern."""
+    import scipy.sparse as sp
+    F = A.to_scipy_full().tocoo()
+    v = np.where(F.row > F.col, F.data * (1 + 0.5j), F.data)
+    G = sp.csc_matrix((v, (F.row, F.col)), shape=F.shape)
+    G.sort_indices()
+    return M.SparseSystem(n=A.n, colptr=G.indptr.astype(np.int64), rowptr=G.indices.astype(np.int64),
+                          values=G.data.copy(), mtxtype=M.PastixGeneral, grid=A.grid, name=A.name + "_gen",
+                          meta={})
+
+
+LDL_CASES = [
+    ("sytrf", lambda: M.diffusion_lognormal(20, 19, 18, 1.0, np.random.default_rng(5)), None),
+    ("sytrf", lambda: _complex_symmetric(M.magnetic_laplacian(14, 13, 12, 0.5, np.random.default_rng(6))), None),
+    ("potrf", lambda: M.magnetic_laplacian(14, 13, 12, -0.5, np.random.default_rng(7)), None),
+    ("hetrf", lambda: _real_hermitian(M.magnetic_laplacian(14, 13, 12, 0.5, np.random.default_rng(8))), None),
+    ("hetrf", lambda: M.magnetic_laplacian(14, 13, 12, 0.5, np.random.default_rng(8)), "hefix"),
+    ("getrf", lambda: _complex_general(M.magnetic_laplacian(9, 8, 7, 0.5, np.random.default_rng(9))), None),
+]
+LDL_IDS = ["sytrf_d", "sytrf_z", "potrf_z", "hetrf_zreal", "hetrf_z", "getrf_z"]
+
+
+@pytest.mark.parametrize("fact,make,variant", LDL_CASES, ids=LDL_IDS)
+def test_ldl_and_complex_factor_solve_match_reference(fact, make, variant):
+    """FP64 / complex128 factors to 1e-12 of the reference's own factors
+    (LDL^h on complex data: the reference with its one-increment fix, see
+    oracle/refbuild/build_ref.py), and the solve to 1e-11 of its solve."""
+    A = make()
+    ref, st = U.run_reference(A, fact, variant=variant)
+    g = U.gpu_structure(A, st)
+    lay = U.layout_of(g)
+    Lr, Ur = U.ref_coeftab_1d(ref, st, lay)
+    s = _gpu_solver(A, st, fact)
+    s.numfact(A.values)
+    Lg, Ug = s.coeftab()
+    mask = np.ones(lay.off[-1], bool) if fact == "getrf" else U.lower_mask(lay)
+    assert np.abs(Lg - Lr)[mask].max() <= 1e-12 * np.abs(Lr).max()
+    if fact == "getrf":
+        assert np.abs(Ug - Ur).max() <= 1e-12 * np.abs(Ur).max()
+    ip, dp = s.params()
+    assert ip[45] == ref.iparm("STATIC_PIVOTING")
+    assert abs(dp[12] - ref.dparm("FACT_THFLOPS")) <= 1e-9 * ref.dparm("FACT_THFLOPS")
+    x, b = M.rhs_from_xtrue(A, 3, np.random.default_rng(17))
+    xg = s.solve(b)
+    xr = ref.solve(b)
+    assert np.abs(xg - xr).max() <= 1e-11 * np.abs(xr).max()
+    assert np.abs(xg - x).max() <= 1e-9
+    s.close()
+
+
+@pytest.mark.parametrize("fact,make,variant", [LDL_CASES[0], LDL_CASES[1], LDL_CASES[4]],
+                         ids=["sytrf_d", "sytrf_z", "hetrf_z"])
+def test_ldl_mixed_factor_matches_reference_mixed(fact, make, variant):
+    A = make()
+    ref, st = U.run_reference(A, fact, mixed=True, variant=variant)
+    g = U.gpu_structure(A, st)
+    lay = U.layout_of(g)
+    Lr, _ = U.ref_coeftab_1d(ref, st, lay)
+    s = _gpu_solver(A, st, fact, mixed=True)
+    s.numfact(A.values)
+    Lg, _ = s.coeftab()
+    assert Lg.dtype == Lr.dtype
+    mask = U.lower_mask(lay)
+    assert np.abs(Lg.astype(np.complex128) - Lr)[mask].max() <= 5e-5 * np.abs(Lr).max()
+    s.close()
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_hetrf_gmres_refinement_reaches_1e12(mixed):
+    """C5's path at a small size: LDL^h of the shifted magnetic Laplacian
+    (complex Hermitian indefinite), complex GMRES(30) to ||r||/||b|| <= 1e-12."""
+    A = M.magnetic_laplacian(16, 15, 14, 0.5, np.random.default_rng(10))
+    ref, st = U.run_reference(A, "hetrf", numfact=False)
+    s = _gpu_solver(A, st, "hetrf", mixed=mixed, refine="gmres")
+    from pastix_b200 import gpu as G
+    s.set_iparm(G.IPARM_GMRES_IM, 30)
+    s.numfact(A.values)
+    x, b = M.rhs_from_xtrue(A, 4, np.random.default_rng(11))
+    xs = s.solve_and_refine(b)
+    Af = A.to_scipy_full()
+    r = b - Af @ xs
+    assert (np.linalg.norm(r, axis=0) / np.linalg.norm(b, axis=0)).max() <= 1e-12
+    assert np.abs(xs - x).max() <= 1e-9
+    ip, _ = s.params()
+    assert ip[52] <= (10 if mixed else 2)
+    s.close()

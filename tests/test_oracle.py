@@ -41,24 +41,75 @@ def test_restatement_matches_golden(name):
     assert np.abs(xp[perm] - g["x"]).max() <= 1e-12 * np.abs(g["x"]).max()
 
 
+def _complex_symmetric(A):
+    """The magnetic Laplacian's lower triangle taken as a complex symmetric
+    (not Hermitian) matrix: the LDL^t of complex data."""
+    A.mtxtype = M.PastixSymmetric
+    return A
+
+
+def _real_hermitian(A):
+    """A Hermitian matrix with real values: the reference's LDL^h kernel is
+    exact on it (its conjugation slip acts on real numbers)."""
+    A.values = A.values.real.astype(np.complex128)
+    return A
+
+
+ORACLE_CASES = [
+    ("potrf", lambda: M.diffusion_lognormal(12, 11, 10, 1.0, np.random.default_rng(2)), None),
+    ("getrf", lambda: M.convdiff_upwind(12, 10, 9, 10.0), None),
+    ("potrf", lambda: M.laplacian_7pt(24), None),
+    ("sytrf", lambda: M.diffusion_lognormal(11, 10, 9, 1.0, np.random.default_rng(5)), None),
+    ("sytrf", lambda: _complex_symmetric(M.magnetic_laplacian(10, 9, 8, 0.5, np.random.default_rng(6))), None),
+    ("potrf", lambda: M.magnetic_laplacian(10, 9, 8, -0.5, np.random.default_rng(7)), None),
+    ("hetrf", lambda: _real_hermitian(M.magnetic_laplacian(10, 9, 8, 0.5, np.random.default_rng(8))), None),
+    ("hetrf", lambda: M.magnetic_laplacian(10, 9, 8, 0.5, np.random.default_rng(8)), "hefix"),
+]
+
+
 @pytest.mark.skipif(not U.ref_available(), reason="reference oracle not built")
-@pytest.mark.parametrize("fact,make", [
-    ("potrf", lambda: M.diffusion_lognormal(12, 11, 10, 1.0, np.random.default_rng(2))),
-    ("getrf", lambda: M.convdiff_upwind(12, 10, 9, 10.0)),
-    ("potrf", lambda: M.laplacian_7pt(24)),
-])
-def test_restatement_matches_reference(fact, make):
+@pytest.mark.parametrize("fact,make,variant", ORACLE_CASES,
+                         ids=["potrf", "getrf", "potrf24", "sytrf", "sytrf_z", "potrf_z", "hetrf_zreal",
+                              "hetrf_z_fixed"])
+def test_restatement_matches_reference(fact, make, variant):
     A = make()
-    ref, st = U.run_reference(A, fact)
+    ref, st = U.run_reference(A, fact, variant=variant)
     g = U.gpu_structure(A, st)
     lay = U.layout_of(g)
     Lr, Ur = U.ref_coeftab_1d(ref, st, lay)
     L, Uc = NP.fillin(lay, A, g["permtab"], lu=(fact == "getrf"))
-    NP.factorize(lay, L, Uc, fact, 2.0 ** -53 * ref.dparm("A_NORM"))
-    mask = U.lower_mask(lay) if fact == "potrf" else np.ones(lay.off[-1], bool)
+    npiv = NP.factorize(lay, L, Uc, fact, 2.0 ** -53 * ref.dparm("A_NORM"))
+    assert npiv == ref.iparm("STATIC_PIVOTING")
+    mask = np.ones(lay.off[-1], bool) if fact == "getrf" else U.lower_mask(lay)
     assert np.abs(L - Lr)[mask].max() <= 1e-13 * np.abs(Lr).max()
     if fact == "getrf":
         assert np.abs(Uc - Ur).max() <= 1e-13 * np.abs(Ur).max()
+    # the solve of the restatement against the reference's own solve
+    x, b = M.rhs_from_xtrue(A, 2, np.random.default_rng(4))
+    xr = ref.solve(b)
+    perm = g["permtab"]
+    bp = np.zeros_like(b)
+    bp[perm] = b
+    xp = np.stack([NP.solve(lay, L, Uc, fact, bp[:, r]) for r in range(2)], axis=1)
+    assert np.abs(xp[perm] - xr).max() <= 1e-11 * np.abs(xr).max()
+    assert np.abs(xp[perm] - x).max() <= 1e-9
+
+
+@pytest.mark.skipif(not U.ref_available(), reason="reference oracle not built")
+def test_reference_ldlh_conjugation_slip_on_complex_data():
+    """Records the reference's LDL^h behaviour on genuinely complex Hermitian
+    data (kernels/core_zhetrfsp.c:92 conjugates with increment 1 a row of
+    stride lda): its factors differ from those of A and its direct solve does
+    not solve A x = b, while the one-increment fix (the "hefix" build) and the
+    restatement agree and solve it."""
+    A = M.magnetic_laplacian(8, 7, 6, 0.5, np.random.default_rng(1))
+    x, b = M.rhs_from_xtrue(A, 1, np.random.default_rng(2))
+    Af = A.to_scipy_full()
+    for variant, bad in ((None, True), ("hefix", False)):
+        ref, st = U.run_reference(A, "hetrf", variant=variant)
+        xr = ref.solve(b)
+        rel = np.abs(b - Af @ xr).max() / np.abs(b).max()
+        assert (rel > 1e-2) if bad else (rel < 1e-13), (variant, rel)
 
 
 def test_golden_files_present():
