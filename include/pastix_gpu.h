@@ -179,6 +179,17 @@ PASTIX_GPU_API int pastix_gpu_refine( pastix_gpu_t *ctx, int64_t nrhs, const voi
 PASTIX_GPU_API int pastix_gpu_solve_and_refine( pastix_gpu_t *ctx, int64_t nrhs, const void *B,
                                  int64_t ldb, void *X, int64_t ldx );
 
+/*
+ * Independent systems merged into one block-diagonal structure (a batch):
+ * segptr[0..nseg] are the first user-numbered unknowns of each system
+ * (segptr[0] = 0, segptr[nseg] = n).  CG refinement then stops when every
+ * system meets its own test ||r_s||_2 / ||b_s||_2 <= eps (the reference runs
+ * each system's refinement separately, refinement/z_refine_grad.c:49), and
+ * DPARM_RELATIVE_ERROR reports the largest of them.  nseg = 0 clears it.
+ * No reference counterpart: the reference has no batched entry point.
+ */
+PASTIX_GPU_API int pastix_gpu_set_segments( pastix_gpu_t *ctx, int64_t nseg, const int64_t *segptr );
+
 /* Copy the output parameters (iparm/dparm, reference indices) out. */
 PASTIX_GPU_API int pastix_gpu_get_params( pastix_gpu_t *ctx, int64_t *iparm, double *dparm );
 /* Change one parameter between calls (e.g. IPARM_MIXED, IPARM_REFINEMENT). */
@@ -206,7 +217,8 @@ PASTIX_GPU_API int pastix_gpu_coeftab( pastix_gpu_t *ctx, void *L, void *U );
  *   stats[11] ms of the tensor-core (tcgen05) update-GEMM launches (part of stats[6])
  *   stats[12] algorithmic flops of the GEMM tasks that ran on the tensor cores
  *   stats[13] tensor-core tiles whose bounded MMA wait timed out (0 when healthy)
- *   stats[14..15] reserved
+ *   stats[14] 1 when the factorization replayed a captured CUDA graph
+ *   stats[15] reserved
  * (16 doubles)
  * The single-precision (mixed) factorization runs its large update GEMMs on
  * the tensor cores with TF32 operands; environment PASTIX_GPU_MIXED_GEMM=fp32

@@ -128,6 +128,9 @@ struct pastix_gpu_s {
     DArr<double> d_rhs, d_x, d_r, d_z, d_p, d_ap, d_gm;   // refinement vectors
     DArr<double> d_sr_b, d_sr_x;   // solve_and_refine staging of host B / X
     DArr<double> d_gmV, d_gmW, d_gmh;   // GMRES basis, preconditioned basis, projections
+    std::vector<int64_t> seg;           // batch: first unknown of each system (+ n), empty if none
+    DArr<int64_t> d_seg;
+    DArr<double> d_segss;               // per-system sums of squares
     std::vector<cudaEvent_t> evpool;   // per-launch timing events
     double plan_gemm_flops = 0;        // update-GEMM flops of the current plan
     double stats[16] = {0};
@@ -641,7 +644,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, double crit, int *launches, La
             const size_t fixed = ((size_t)TRSM_TR * (mw + 1) + PB * PBL) * sizeof(T);
             const int pch = (int)std::min<size_t>(mw, (SMEM_LIMIT - std::min<size_t>(fixed, SMEM_LIMIT)) /
                                                           (PBL * sizeof(T)));
-            if (pch < PB) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+            if (pch < std::min(PB, mw)) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
             const size_t tsm = fixed + (size_t)pch * PBL * sizeof(T);
             PGPU_CHECK(tm.mark(PH_TRSM));
             ktrsm<<<ntr, 256, tsm, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], coefL, coefU, mw, pch);
@@ -1053,7 +1056,30 @@ struct VecOps {
         launches += 3 + (beta != 0.0);
     }
     int spsv(S *z) { return solve_device_block(C, z, C.n, 1, C.d_work.p, &launches); }
+    // per-system 2-norms of x (batch segments)
+    void seg_norms(const S *x, std::vector<double> &out) {
+        const int ns = (int)C.seg.size() - 1;
+        k_seg_sumsq<S><<<std::min(ns, 4096), RED_THREADS, 0, C.stream>>>(ns, C.d_seg.p, x, C.d_segss.p);
+        launches++;
+        out.resize(ns);
+        cudaMemcpyAsync(out.data(), C.d_segss.p, ns * sizeof(double), cudaMemcpyDeviceToHost, C.stream);
+        cudaStreamSynchronize(C.stream);
+        for (auto &v : out) v = std::sqrt(v);
+    }
 };
+
+// Stopping measure of the refinement: ||r||/||b||, or with batch segments the
+// largest per-system ||r_s||/||b_s|| (each system's own test).
+template <typename S>
+static double resid_measure(pastix_gpu_t &C, VecOps<S> &V, const S *r, double normr, double normb,
+                            const std::vector<double> &segb) {
+    if (C.seg.size() < 3) return normr / normb;
+    std::vector<double> sr;
+    V.seg_norms(r, sr);
+    double m = 0;
+    for (size_t i = 0; i < sr.size(); i++) m = std::max(m, sr[i] / (segb[i] > 0 ? segb[i] : 1.0));
+    return m;
+}
 
 template <typename S>
 static int refine_cg(pastix_gpu_t &C, VecOps<S> &V, const S *b, S *x, double eps, int itermax, int *iters,
@@ -1064,10 +1090,12 @@ static int refine_cg(pastix_gpu_t &C, VecOps<S> &V, const S *b, S *x, double eps
     double normb = V.norm(b);
     if (normb == 0.) normb = 1;
     const double normx = V.norm(x);
+    std::vector<double> segb;
+    if (C.seg.size() >= 3) V.seg_norms(b, segb);
     V.copy(b, r);
     if (normx > 0.) V.spmv(-1.0, x, 1.0, r);
     double normr = V.norm(r);
-    double resid_b = normr / normb;
+    double resid_b = resid_measure(C, V, r, normr, normb, segb);
     V.copy(r, z);
     int rc = V.spsv(z);
     if (rc) return rc;
@@ -1088,7 +1116,7 @@ static int refine_cg(pastix_gpu_t &C, VecOps<S> &V, const S *b, S *x, double eps
         beta = alpha / beta;
         V.xpby(z, beta, p);
         normr = V.norm(r);
-        resid_b = normr / normb;
+        resid_b = resid_measure(C, V, r, normr, normb, segb);
     }
     *iters = it;
     *resid = resid_b;
@@ -1330,6 +1358,24 @@ extern "C" int pastix_gpu_solve_and_refine(pastix_gpu_t *ctx, int64_t nrhs, cons
     if (rc) return rc;
     PGPU_CHECK(cudaMemcpy2DAsync(X, ldx * es, dx, C.n * es, C.n * es, nrhs,
                                  xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, C.stream));
+    PGPU_CHECK(cudaStreamSynchronize(C.stream));
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_set_segments(pastix_gpu_t *ctx, int64_t nseg, const int64_t *segptr) {
+    if (!ctx || nseg < 0 || (nseg > 0 && !segptr)) return PASTIX_GPU_ERR_BADPARAMETER;
+    auto &C = *ctx;
+    if (nseg == 0) {
+        C.seg.clear();
+        return PASTIX_GPU_SUCCESS;
+    }
+    if (segptr[0] != 0 || segptr[nseg] != C.n) return PASTIX_GPU_ERR_BADPARAMETER;
+    for (int64_t i = 0; i < nseg; i++)
+        if (segptr[i + 1] < segptr[i]) return PASTIX_GPU_ERR_BADPARAMETER;
+    PGPU_CHECK(cudaSetDevice(C.device));
+    C.seg.assign(segptr, segptr + nseg + 1);
+    PGPU_CHECK(C.d_seg.upload(C.seg, C.stream));
+    PGPU_CHECK(C.d_segss.alloc(nseg));
     PGPU_CHECK(cudaStreamSynchronize(C.stream));
     return PASTIX_GPU_SUCCESS;
 }

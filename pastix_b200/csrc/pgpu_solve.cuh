@@ -363,6 +363,20 @@ __global__ void k_gather_vals(int64_t nnz, const int64_t *__restrict__ src, cons
     }
 }
 
+// Per-segment sum of squares: out[s] = sum |x_i|^2 over [seg[s], seg[s+1]).
+template <typename S>
+__global__ void k_seg_sumsq(int nseg, const int64_t *__restrict__ seg, const S *__restrict__ x,
+                            double *__restrict__ out) {
+    __shared__ double sh[32];
+    for (int sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
+        double v = 0.0;
+        for (int64_t i = seg[sg] + threadIdx.x; i < seg[sg + 1]; i += blockDim.x) v += abs2_v(x[i]);
+        v = block_sum(v, sh);
+        if (threadIdx.x == 0) out[sg] = v;
+        __syncthreads();
+    }
+}
+
 // Weighted sum of squares for the Frobenius norm (off-diagonal entries of a
 // one-triangle symmetric matrix count twice).
 template <typename S>

@@ -63,6 +63,7 @@ def load():
         L.pastix_gpu_set_dparm.argtypes = [P, I, D]
         L.pastix_gpu_coeftab.argtypes = [P, P, P]
         L.pastix_gpu_stats.argtypes = [P, P]
+        L.pastix_gpu_set_segments.argtypes = [P, I64, P]
         L.pastix_gpu_finalize.argtypes = [C.POINTER(P)]
         L.pastix_gpu_finalize.restype = None
         _lib = L
@@ -152,6 +153,13 @@ class Solver:
                                    _p(self._colptr), _p(self._rowptr))
         _check("pastix_gpu_spm", rc)
         self.dtype = np.complex128 if np.iscomplexobj(system.values) else np.float64
+
+    def set_segments(self, offsets):
+        """Batch of independent systems: offsets[i] = first unknown of system i
+        (offsets[-1] = n); refinement then applies each system's own test."""
+        self._seg = np.ascontiguousarray(offsets, np.int64)
+        rc = load().pastix_gpu_set_segments(self._h, len(self._seg) - 1, _p(self._seg))
+        _check("pastix_gpu_set_segments", rc)
 
     # -- numerical tasks ---------------------------------------------------
     def numfact(self, values):
