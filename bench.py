@@ -179,8 +179,10 @@ def fma_peaks():
 
 
 # ---------------------------------------------------------------------------
-def run_arm(A, st, b, mixed, steps, warmup, fact, refine):
-    """One arm (mixed or FP64): device-resident timing, then e2e timing."""
+def run_arm(A, st, b, mixed, steps, warmup, fact, refine, segments=None):
+    """One arm (mixed or FP64): device-resident timing, then e2e timing.
+    segments: batch of independent systems merged into A (per-system
+    refinement test)."""
     import torch
     from pastix_b200 import gpu as G
     s = G.Solver(device=torch.cuda.current_device())
@@ -190,6 +192,8 @@ def run_arm(A, st, b, mixed, steps, warmup, fact, refine):
     s.set_dparm(G.DPARM_EPSILON_REFINEMENT, REFINE_EPS)
     s.set_structure(st)
     s.set_spm(A)
+    if segments is not None:
+        s.set_segments(segments)
     dev = torch.device("cuda", torch.cuda.current_device())
     d_vals = torch.from_numpy(np.ascontiguousarray(A.values)).to(dev)
     d_b = torch.from_numpy(np.asfortranarray(b).reshape(-1, order="F").copy()).to(dev)
@@ -247,6 +251,44 @@ def run_arm(A, st, b, mixed, steps, warmup, fact, refine):
     }
 
 
+def errors_batch(systems, offs, b, x, xtrue):
+    """Largest per-system errors of a batch (each system's own norms)."""
+    out = {}
+    for i, A in enumerate(systems):
+        sl = slice(int(offs[i]), int(offs[i + 1]))
+        e = errors(A, b[sl], x[sl], xtrue[sl])
+        for k, v in e.items():
+            out[k] = max(out.get(k, 0.0), v)
+    return out
+
+
+def cpu_reference_batch(systems, nrhs, fact, refine, mixed, nthreads, budget_s, total_flops):
+    """Reference CPU path on the batch, one system after the other (the
+    reference has no batched entry point), on the leading systems until
+    budget_s of CPU time; scaled to the whole batch by factorization flops."""
+    from oracle import pastix_ref as R
+    t_sum = f_sum = 0.0
+    worst = {}
+    k = 0
+    for A in systems:
+        xs, bs = M.rhs_from_xtrue(A, nrhs, np.random.default_rng(1))
+        r = R.RefSolver(A, fact=fact, nthreads=nthreads, mixed=mixed, refine=refine, eps_refine=REFINE_EPS)
+        r.analyze()
+        t = time.perf_counter()
+        r.numfact()
+        x0 = r.solve(bs)
+        x1 = r.refine(bs, x0)
+        t_sum += time.perf_counter() - t
+        f_sum += r.dparm("FACT_THFLOPS")
+        for kk, v in errors(A, bs, x1, xs).items():
+            worst[kk] = max(worst.get(kk, 0.0), v)
+        r.close()
+        k += 1
+        if t_sum >= budget_s:
+            break
+    return t_sum * total_flops / f_sum, k, t_sum, worst
+
+
 def cpu_reference_sample(cfg, scale, sample_scale, fact, refine, mixed, steps, warmup, nthreads):
     """Reference CPU path on the same problem at `sample_scale` of the grid,
     scaled to the full problem by the factorization-flop ratio."""
@@ -279,20 +321,59 @@ def main():
     fact = {1: "potrf", 2: "potrf", 3: "getrf", 4: "potrf", 5: "hetrf"}[cfg]
     refine = {1: "cg", 2: "cg", 3: "gmres", 4: "cg", 5: "gmres"}[cfg]
     systems, meta = M.config(cfg, scale=args.scale, seed=0)
-    A = systems[0]
-    rng = np.random.default_rng(1)
-    xtrue, b = M.rhs_from_xtrue(A, meta["nrhs"] if cfg != 2 else 1, rng)
+    nrhs = meta["nrhs"] if cfg != 2 else 1
+    batch = (cfg == 4)
+    segments = None
+    if batch:
+        # 512 independent systems: this rank's longest-processing-time shard
+        # (flop-count cost), merged into one block-diagonal forest
+        from pastix_b200 import analysis, batch as B
+        all_structs = [analysis.analyze(a) for a in systems]
+        costs = [B.system_flops(t) for t in all_structs]
+        parts, load = B.shard(costs, world)
+        mine = parts[rank]
+        bsys = [systems[i] for i in mine]
+        bstructs = [all_structs[i] for i in mine]
+        st_batch, segments = B.merge_structures(bstructs)
+        A = B.merge_systems(bsys)
+        xs_l, bs_l = zip(*[M.rhs_from_xtrue(a, nrhs, np.random.default_rng(1000 + int(i)))
+                           for a, i in zip(bsys, mine)])
+        xtrue, b = np.asfortranarray(np.vstack(xs_l)), np.asfortranarray(np.vstack(bs_l))
+        total_flops = float(sum(costs))
+    else:
+        A = systems[0]
+        rng = np.random.default_rng(1)
+        xtrue, b = M.rhs_from_xtrue(A, nrhs, rng)
     config = {"workload": CONFIG_DESC[cfg] + ("" if args.scale == 1.0 else " scaled %.2f" % args.scale),
-              "grid": list(A.grid), "n": A.n, "nnz": A.nnz, "nrhs": int(b.shape[1]),
+              "grid": list(A.grid) if not batch else "512 2D grids, sides %d..%d" % (
+                  min(a.grid[0] for a in systems), max(a.grid[0] for a in systems)),
+              "n": A.n, "nnz": A.nnz, "nrhs": int(b.shape[1]),
               "ordering": "reference grid nested dissection (pastixOrderGrid; Scotch unavailable)",
               "l2": "inputs larger than L2 (coeftab > 126 MB), no flush",
               "refine": "%s, stop at ||r||_2/||b||_2 <= %g" % (refine.upper(), REFINE_EPS),
-              "parallelism": "replicas" if world > 1 else "1 GPU"}
+              "parallelism": ("systems sharded over %d GPUs (LPT on flops)" % world if batch else "replicas")
+              if world > 1 else "1 GPU"}
+    if batch:
+        config["systems_this_rank"] = len(mine)
+        config["batch"] = "all systems of a rank merged into one forest: one launch per elimination-tree level"
 
     if args.impl == "reference":
         if rank != 0:
             return
         nth = os.cpu_count() or 1
+        if batch:
+            value, k, t_s, err = cpu_reference_batch(systems, nrhs, fact, refine, True, nth, 20.0, total_flops)
+            line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "s", "n_gpus": world,
+                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
+                    "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+                    "dtype": "f32 factor + f64 refine", "data": "synthetic (seeded)", "config": config,
+                    "cpu_baseline": {"value": value, "unit": "s", "cores": nth, "kind": "reference",
+                                     "sample": "reference CPU mixed path, system after system: %d of %d systems "
+                                               "took %.2f s, scaled to all by factorization flops" % (
+                                                   k, len(systems), t_s), "errors": err},
+                    "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line))
+            return
         t, thf_s, grid_s, err = cpu_reference_sample(cfg, args.scale, args.cpu_sample_scale, fact, refine, True,
                                                      args.steps, args.warmup, nth)
         value, how = t, "measured on the full problem"
@@ -323,22 +404,27 @@ def main():
     torch.cuda.set_device(local)
     from pastix_b200 import analysis
     t_an = time.perf_counter()
-    st = analysis.analyze(A)
+    st = st_batch if batch else analysis.analyze(A)
     t_an = time.perf_counter() - t_an
     peaks = fma_peaks() if rank == 0 else {}
     barrier(pg)
     with ClockSampler(local) as clk:
-        mixed = run_arm(A, st, b, True, args.steps, args.warmup, fact, refine)
-        fp64 = run_arm(A, st, b, False, args.steps, args.warmup, fact, refine)
+        mixed = run_arm(A, st, b, True, args.steps, args.warmup, fact, refine, segments)
+        fp64 = run_arm(A, st, b, False, args.steps, args.warmup, fact, refine, segments)
     barrier(pg)
     value = reduce_max(pg, mixed["device_s"], local)
     e2e_v = reduce_max(pg, mixed["e2e_s"], local)
     fp64_v = reduce_max(pg, fp64["device_s"], local)
     if rank != 0:
         return
-    err_m = errors(A, b, mixed["x"], xtrue)
-    err_d = errors(A, b, fp64["x"], xtrue)
-    err_e = errors(A, b, mixed["x_e2e"], xtrue)
+    if batch:
+        err_m = errors_batch(bsys, segments, b, mixed["x"], xtrue)
+        err_d = errors_batch(bsys, segments, b, fp64["x"], xtrue)
+        err_e = errors_batch(bsys, segments, b, mixed["x_e2e"], xtrue)
+    else:
+        err_m = errors(A, b, mixed["x"], xtrue)
+        err_d = errors(A, b, fp64["x"], xtrue)
+        err_e = errors(A, b, mixed["x_e2e"], xtrue)
     g_ach = mixed["gemm_flops_per_step"] / (mixed["gemm_ms_per_step"] * 1e-3) / 1e12
     tc_ach = (mixed["tc_flops_per_step"] / (mixed["tc_ms_per_step"] * 1e-3) / 1e12
               if mixed["tc_ms_per_step"] > 0 else None)
@@ -353,7 +439,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 factor + f64 refine", "data": "synthetic (seeded)",
+        "scaling": "strong" if batch else "weak", "vs_baseline": None, "dtype": "f32 factor + f64 refine", "data": "synthetic (seeded)",
         "config": config,
         "fp64": {"value": fp64_v, "unit": "s", "e2e_s": fp64["e2e_s"], "factor_ms": fp64["factor_ms"],
                  "solve_ms": fp64["solve_ms"], "refine_ms": fp64["refine_ms"], "refine_iters": fp64["refine_iters"],
@@ -383,7 +469,14 @@ def main():
         "analysis_s": t_an, "peaks": peaks,
     }
     line["clocks"] = clk.summary()
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline and batch:
+        nth = os.cpu_count() or 1
+        v, k, t_s, err = cpu_reference_batch(systems, nrhs, fact, refine, True, nth, 20.0, total_flops)
+        line["cpu_baseline"] = {"value": v, "unit": "s", "cores": nth, "kind": "reference",
+                                "sample": "reference CPU mixed path, system after system: %d of %d systems took "
+                                          "%.2f s, scaled to all by factorization flops" % (k, len(systems), t_s),
+                                "errors": err}
+    elif world == 1 and not args.no_cpu_baseline:
         try:
             nth = os.cpu_count() or 1
             t, thf_s, grid_s, err = cpu_reference_sample(cfg, args.scale, args.cpu_sample_scale, fact, refine,
