@@ -190,6 +190,27 @@ PASTIX_GPU_API int pastix_gpu_solve_and_refine( pastix_gpu_t *ctx, int64_t nrhs,
  */
 PASTIX_GPU_API int pastix_gpu_set_segments( pastix_gpu_t *ctx, int64_t nseg, const int64_t *segptr );
 
+/*
+ * Learned cost model hooks (the reference's cost models, common/models.c,
+ * have no GPU counterpart: these are new entry points).
+ * pastix_gpu_record_tasks(ctx, 1): the following numfact calls record the
+ * device time of every task (one CTA each: a cblk's panel factorization, a
+ * TRSM row chunk, an update-GEMM tile).  pastix_gpu_task_records: with info
+ * or ns NULL, *count receives the number of records; else up to *count
+ * records are written, info[8 r .. 8 r + 7] = {kind (0 panel, 1 TRSM chunk,
+ * 2 FMA GEMM tile, 3 tensor-core GEMM tile), cblk, a, b, c, d, element
+ * bytes, form (0 LL^t, 1 LU, 2 LDL^t, 3 LDL^h)} with (a, b, c, d) =
+ * (w, h, rows solved in the panel kernel, blocks) for a panel,
+ * (w, rows, mode, panel) for a TRSM chunk, (K, M, N, flags) for a GEMM tile,
+ * and ns[r] its duration in nanoseconds.
+ * pastix_gpu_set_cblk_priority: predicted cost per cblk; inside each level
+ * the panels, TRSM chunks and GEMM tiles of costlier cblks launch first
+ * (longest-processing-time order).  NULL restores the cblk order.
+ */
+PASTIX_GPU_API int pastix_gpu_record_tasks( pastix_gpu_t *ctx, int on );
+PASTIX_GPU_API int pastix_gpu_task_records( pastix_gpu_t *ctx, int64_t *count, int64_t *info, double *ns );
+PASTIX_GPU_API int pastix_gpu_set_cblk_priority( pastix_gpu_t *ctx, const double *prio );
+
 /* Copy the output parameters (iparm/dparm, reference indices) out. */
 PASTIX_GPU_API int pastix_gpu_get_params( pastix_gpu_t *ctx, int64_t *iparm, double *dparm );
 /* Change one parameter between calls (e.g. IPARM_MIXED, IPARM_REFINEMENT). */
@@ -248,6 +269,26 @@ PASTIX_GPU_API int pastix_gpu_analysis_export( const pastix_gpu_analysis_t *an, 
                                                int64_t *bloktab, int64_t *browtab, int64_t *permtab,
                                                int64_t *peritab, int64_t *rangtab, int64_t *treetab );
 PASTIX_GPU_API void pastix_gpu_analysis_free( pastix_gpu_analysis_t **an );
+
+/*
+ * The learned cost model's network: an MLP nfeat -> hidden -> hidden -> 1
+ * (ReLU) in FP64, trained and evaluated on the GPU by the library's own
+ * kernels (forward, backward, Adam).  Parameters packed as W1[hidden][nfeat],
+ * b1[hidden], W2[hidden][hidden], b2[hidden], W3[hidden], b3.  X is row-major
+ * n x nfeat (host), targets t and outputs y have n entries; the loss is the
+ * mean squared error.  Replaces the offline-fitted polynomial models of
+ * common/models.c (no C-ABI counterpart in the reference).
+ */
+typedef struct pastix_gpu_mlp_s pastix_gpu_mlp_t;
+PASTIX_GPU_API int pastix_gpu_mlp_init( pastix_gpu_mlp_t **m, int device, int nfeat, int hidden, uint64_t seed );
+PASTIX_GPU_API int pastix_gpu_mlp_params( pastix_gpu_mlp_t *m, double *params, int64_t *count );
+PASTIX_GPU_API int pastix_gpu_mlp_set_params( pastix_gpu_mlp_t *m, const double *params );
+PASTIX_GPU_API int pastix_gpu_mlp_forward( pastix_gpu_mlp_t *m, int64_t n, const double *X, double *y );
+PASTIX_GPU_API int pastix_gpu_mlp_gradient( pastix_gpu_mlp_t *m, int64_t n, const double *X, const double *t,
+                                            double *grad, double *loss );
+PASTIX_GPU_API int pastix_gpu_mlp_train( pastix_gpu_mlp_t *m, int64_t n, const double *X, const double *t,
+                                         int steps, double lr, double *loss );
+PASTIX_GPU_API void pastix_gpu_mlp_free( pastix_gpu_mlp_t **m );
 
 /* Release the device memory and the context (pastixFinalize, common/api.c:914). */
 PASTIX_GPU_API void pastix_gpu_finalize( pastix_gpu_t **ctx );

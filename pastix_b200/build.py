@@ -17,7 +17,7 @@ LIB = os.path.join(LIBDIR, "libpastix_gpu.so")
 PEAKLIB = os.path.join(LIBDIR, "libpgpu_peak.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["pastix_gpu.cu", "pgpu_analysis.cpp"]
+SOURCES = ["pastix_gpu.cu", "pgpu_mlp.cu", "pgpu_analysis.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=hidden"]

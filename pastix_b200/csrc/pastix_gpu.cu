@@ -132,6 +132,13 @@ struct pastix_gpu_s {
     DArr<int64_t> d_seg;
     DArr<double> d_segss;               // per-system sums of squares
     std::vector<cudaEvent_t> evpool;   // per-launch timing events
+    DArr<double> d_fact_scal;          // [0] ||A||_F, [1] static-pivot threshold (device-side, no host trip)
+    // per-task timings of the last numfact (learned cost model), when record
+    bool record = false;
+    DArr<int64_t> d_prof[4];           // panel CTAs, TRSM chunks, FMA GEMM tiles, tensor-core tiles
+    std::vector<int4> h_tiles, h_tctiles, h_trsm;   // host copies of the plan's launch lists
+    std::vector<GemmTask> h_tasks;
+    int plan_fuse = 0, plan_esz = 0, plan_fmode = -1;
     double plan_gemm_flops = 0;        // update-GEMM flops of the current plan
     double stats[16] = {0};
 };
@@ -170,6 +177,7 @@ extern "C" int pastix_gpu_init(pastix_gpu_t **pctx, int device, const int64_t *i
     PGPU_CHECK(ctx->d_status.alloc(1));
     PGPU_CHECK(ctx->d_partial.alloc(1024));
     PGPU_CHECK(ctx->d_scalar.alloc(16));
+    PGPU_CHECK(ctx->d_fact_scal.alloc(4));
     *pctx = ctx;
     return PASTIX_GPU_SUCCESS;
 }
@@ -554,6 +562,13 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     PGPU_CHECK(C.d_trsm.upload(trsm, s));
     PGPU_CHECK(C.d_tasks.upload(tasks, s));
     PGPU_CHECK(cudaStreamSynchronize(s));
+    C.h_tiles.swap(tiles);
+    C.h_tctiles.swap(tctiles);
+    C.h_trsm.swap(trsm);
+    C.h_tasks.swap(tasks);
+    C.plan_fuse = fuse;
+    C.plan_esz = (int)esz;
+    C.plan_fmode = fmode;
     C.plan_fact = key;
     C.plan_gemm_flops = gflops;
     C.tc_flops = tcflops;
@@ -593,7 +608,7 @@ struct LaunchTimer {
 enum { PH_DIAG = 0, PH_TRSM = 1, PH_GEMM = 2, PH_TC = 3, PH_END = 4 };
 
 template <typename T>
-using PanelKernel = void (*)(Meta, const int *, T *, T *, double, int, int, int, Status *);
+using PanelKernel = void (*)(Meta, const int *, T *, T *, const double *, int, int, int, Status *, int64_t *);
 
 template <typename T>
 static PanelKernel<T> panel_kernel(int fmode) {
@@ -608,7 +623,7 @@ static PanelKernel<T> panel_kernel(int fmode) {
 }
 
 template <typename T>
-static int run_factor(pastix_gpu_t &C, int fmode, double crit, int *launches, LaunchTimer &tm) {
+static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm) {
     const bool lu = (fmode == FM_GETRF);
     T *coefL = reinterpret_cast<T *>(C.d_coef.p);
     T *coefU = lu ? coefL + C.coefnbr : coefL;
@@ -628,6 +643,17 @@ static int run_factor(pastix_gpu_t &C, int fmode, double crit, int *launches, La
         PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         tc_smem_bytes<true>()));
     }
+    int64_t *prof[4] = {nullptr, nullptr, nullptr, nullptr};
+    if (C.record) {
+        const size_t cnt[4] = {(size_t)C.cblknbr, (size_t)C.trsm_ptr[C.nlevels], (size_t)C.tile_ptr[C.nlevels],
+                               (size_t)C.tctile_ptr[C.nlevels]};
+        for (int k = 0; k < 4; k++) {
+            if (C.d_prof[k].n < 2 * cnt[k]) PGPU_CHECK(C.d_prof[k].alloc(2 * cnt[k]));
+            prof[k] = cnt[k] ? C.d_prof[k].p : nullptr;
+        }
+    }
+    auto at = [](int64_t *p, int off) { return p ? p + 2 * (int64_t)off : nullptr; };
+    const double *critp = C.d_fact_scal.p + 1;
     int nl = 0, ngemm = 0;
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
@@ -636,8 +662,8 @@ static int run_factor(pastix_gpu_t &C, int fmode, double crit, int *launches, La
         const size_t psm = (size_t)(PB * PBL + PB + (size_t)(pl + pu + po) * PBL) * sizeof(T);
         if (psm > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
         PGPU_CHECK(tm.mark(PH_DIAG));
-        kpanel<<<ncb, 256, psm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, coefU, crit, fuse, pl, pu,
-                                     C.d_status.p);
+        kpanel<<<ncb, 256, psm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, coefU, critp, fuse, pl, pu,
+                                     C.d_status.p, at(prof[0], C.lvl_ptr[l]));
         nl++;
         const int ntr = C.trsm_ptr[l + 1] - C.trsm_ptr[l];
         if (ntr) {
@@ -647,13 +673,15 @@ static int run_factor(pastix_gpu_t &C, int fmode, double crit, int *launches, La
             if (pch < std::min(PB, mw)) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
             const size_t tsm = fixed + (size_t)pch * PBL * sizeof(T);
             PGPU_CHECK(tm.mark(PH_TRSM));
-            ktrsm<<<ntr, 256, tsm, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], coefL, coefU, mw, pch);
+            ktrsm<<<ntr, 256, tsm, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], coefL, coefU, mw, pch,
+                                        at(prof[1], C.trsm_ptr[l]));
             nl++;
         }
         const int nti = C.tile_ptr[l + 1] - C.tile_ptr[l];
         if (nti) {
             PGPU_CHECK(tm.mark(PH_GEMM));
-            k_gemm_scatter<T><<<nti, 256, 0, s>>>(C.meta, C.d_tiles.p + C.tile_ptr[l], C.d_tasks.p, coefL, coefU);
+            k_gemm_scatter<T><<<nti, 256, 0, s>>>(C.meta, C.d_tiles.p + C.tile_ptr[l], C.d_tasks.p, coefL, coefU,
+                                                  at(prof[2], C.tile_ptr[l]));
             nl++;
             ngemm++;
         }
@@ -663,10 +691,12 @@ static int run_factor(pastix_gpu_t &C, int fmode, double crit, int *launches, La
                 PGPU_CHECK(tm.mark(PH_TC));
                 if (split)
                     k_gemm_scatter_tc<true><<<ntc, TC_THREADS, tc_smem_bytes<true>(), s>>>(
-                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p);
+                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p,
+                        at(prof[3], C.tctile_ptr[l]));
                 else
                     k_gemm_scatter_tc<false><<<ntc, TC_THREADS, tc_smem_bytes<false>(), s>>>(
-                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p);
+                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p,
+                        at(prof[3], C.tctile_ptr[l]));
                 nl++;
                 ngemm++;
             }
@@ -679,25 +709,26 @@ static int run_factor(pastix_gpu_t &C, int fmode, double crit, int *launches, La
     return PASTIX_GPU_SUCCESS;
 }
 
+// ||A||_F into d_fact_scal[0] and the static-pivot threshold into
+// d_fact_scal[1], on the device (sopalin/pastix_task_sopalin.c:461-485; the
+// bcsc stays double, so eps = dlamch('e') also for the mixed factors).
 template <typename S>
-static int dev_norm_frob(pastix_gpu_t &C, double *out) {
+static void dev_norm_and_crit(pastix_gpu_t &C, double magn) {
     cudaStream_t s = C.stream;
     const int nb = 512;
     k_sumsq_partial<S><<<nb, RED_THREADS, 0, s>>>(C.nnz, reinterpret_cast<const S *>(C.d_vals.p), C.d_wgt.p,
                                                   C.d_partial.p);
-    k_dot_final<double><<<1, RED_THREADS, 0, s>>>(nb, C.d_partial.p, C.d_scalar.p, 1);
-    PGPU_CHECK(cudaMemcpyAsync(out, C.d_scalar.p, sizeof(double), cudaMemcpyDeviceToHost, s));
-    PGPU_CHECK(cudaStreamSynchronize(s));
-    return PASTIX_GPU_SUCCESS;
+    k_dot_final<double><<<1, RED_THREADS, 0, s>>>(nb, C.d_partial.p, C.d_fact_scal.p, 1);
+    k_static_pivot_threshold<<<1, 1, 0, s>>>(C.d_fact_scal.p, magn, 1.1102230246251565e-16);
 }
 
 // bcsc -> coeftab in the factor precision, then the level loop
 template <typename T, typename S>
-static int fill_and_factor(pastix_gpu_t &C, int fmode, double crit, int *nl, LaunchTimer &tm) {
+static int fill_and_factor(pastix_gpu_t &C, int fmode, int *nl, LaunchTimer &tm) {
     cudaStream_t s = C.stream;
     k_fillin<T, S><<<2048, 256, 0, s>>>(C.nnz, reinterpret_cast<const S *>(C.d_vals.p), C.d_fill_dst.p,
                                         reinterpret_cast<T *>(C.d_coef.p), C.d_status.p);
-    return run_factor<T>(C, fmode, crit, nl, tm);
+    return run_factor<T>(C, fmode, nl, tm);
 }
 
 extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
@@ -725,17 +756,8 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     // values in (pastix_subtask_spm2bcsc), norm, bcsc -> coeftab
     PGPU_CHECK(cudaMemcpyAsync(C.d_vals.p, values, C.nnz * vsz,
                                is_device_ptr(values) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
-    double anorm = 0;
-    rc = zc ? dev_norm_frob<cdouble>(C, &anorm) : dev_norm_frob<double>(C, &anorm);
-    if (rc) return rc;
-    C.dparm[PGPU_DPARM_A_NORM] = anorm;
-    // static pivoting threshold, sopalin/pastix_task_sopalin.c:461-485 (the
-    // bcsc stays double, so eps = dlamch('e') also for the mixed factors)
-    const double magn = C.dparm[PGPU_DPARM_EPSILON_MAGN_CTRL];
-    double crit;
-    if (magn < 0.) crit = -magn;
-    else if (magn == 0.) crit = 1.1102230246251565e-16 * anorm;
-    else crit = magn * anorm;
+    if (zc) dev_norm_and_crit<cdouble>(C, C.dparm[PGPU_DPARM_EPSILON_MAGN_CTRL]);
+    else dev_norm_and_crit<double>(C, C.dparm[PGPU_DPARM_EPSILON_MAGN_CTRL]);
     if (zc)
         k_gather_vals<cdouble><<<1024, 256, 0, s>>>(C.csr_nnz, C.d_csr_src.p, (const cdouble *)C.d_vals.p,
                                                     (cdouble *)C.d_csr_val.p);
@@ -747,16 +769,19 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     int nl = 0;
     LaunchTimer tm(C);
     if (zc)
-        rc = mixed ? fill_and_factor<cfloat, cdouble>(C, fmode, crit, &nl, tm)
-                   : fill_and_factor<cdouble, cdouble>(C, fmode, crit, &nl, tm);
+        rc = mixed ? fill_and_factor<cfloat, cdouble>(C, fmode, &nl, tm)
+                   : fill_and_factor<cdouble, cdouble>(C, fmode, &nl, tm);
     else
-        rc = mixed ? fill_and_factor<float, double>(C, fmode, crit, &nl, tm)
-                   : fill_and_factor<double, double>(C, fmode, crit, &nl, tm);
+        rc = mixed ? fill_and_factor<float, double>(C, fmode, &nl, tm)
+                   : fill_and_factor<double, double>(C, fmode, &nl, tm);
     if (rc) return rc;
     PGPU_CHECK(cudaEventRecord(C.ev[1], s));
     Status st;
+    double fscal[2];
     PGPU_CHECK(cudaMemcpyAsync(&st, C.d_status.p, sizeof(Status), cudaMemcpyDeviceToHost, s));
+    PGPU_CHECK(cudaMemcpyAsync(fscal, C.d_fact_scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     PGPU_CHECK(cudaStreamSynchronize(s));
+    C.dparm[PGPU_DPARM_A_NORM] = fscal[0];
     float ms = 0;
     PGPU_CHECK(cudaEventElapsedTime(&ms, C.ev[0], C.ev[1]));
     C.stats[0] = launches + nl;
@@ -1377,6 +1402,82 @@ extern "C" int pastix_gpu_set_segments(pastix_gpu_t *ctx, int64_t nseg, const in
     PGPU_CHECK(C.d_seg.upload(C.seg, C.stream));
     PGPU_CHECK(C.d_segss.alloc(nseg));
     PGPU_CHECK(cudaStreamSynchronize(C.stream));
+    return PASTIX_GPU_SUCCESS;
+}
+
+// --------------------------------------------------------------------------
+// Learned cost model hooks: per-task timings recorded by the factorization
+// itself, and a per-cblk cost that orders the work inside each level launch.
+// --------------------------------------------------------------------------
+extern "C" int pastix_gpu_record_tasks(pastix_gpu_t *ctx, int on) {
+    if (!ctx) return PASTIX_GPU_ERR_BADPARAMETER;
+    ctx->record = (on != 0);
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_task_records(pastix_gpu_t *ctx, int64_t *count, int64_t *info, double *ns) {
+    if (!ctx || !count) return PASTIX_GPU_ERR_BADPARAMETER;
+    auto &C = *ctx;
+    if (C.fact_done < 0 || !C.record || C.plan_fact < 0) return PASTIX_GPU_ERR_BADPARAMETER;
+    const int64_t cnt[4] = {C.cblknbr, (int64_t)C.h_trsm.size(), (int64_t)C.h_tiles.size(),
+                            (int64_t)C.h_tctiles.size()};
+    const int64_t total = cnt[0] + cnt[1] + cnt[2] + cnt[3];
+    if (!info || !ns) {
+        *count = total;
+        return PASTIX_GPU_SUCCESS;
+    }
+    if (*count < total) return PASTIX_GPU_ERR_BADPARAMETER;
+    PGPU_CHECK(cudaSetDevice(C.device));
+    std::vector<int64_t> t[4];
+    for (int k = 0; k < 4; k++) {
+        t[k].resize(2 * cnt[k]);
+        if (cnt[k]) PGPU_CHECK(cudaMemcpy(t[k].data(), C.d_prof[k].p, 2 * cnt[k] * sizeof(int64_t),
+                                          cudaMemcpyDeviceToHost));
+    }
+    int64_t r = 0;
+    auto put = [&](int kind, int64_t c, int64_t a, int64_t b, int64_t cc, int64_t d, const int64_t *tt) {
+        int64_t *o = info + 8 * r;
+        o[0] = kind; o[1] = c; o[2] = a; o[3] = b; o[4] = cc; o[5] = d; o[6] = C.plan_esz; o[7] = C.plan_fmode;
+        ns[r] = (double)(tt[1] - tt[0]);
+        r++;
+    };
+    for (int q = 0; q < C.cblknbr; q++) {   // panel CTAs, in launch order (lvl_cblks)
+        const int c = C.lvl_cblks[q];
+        const int h = C.height[c], w = C.width[c];
+        put(0, c, w, h, h <= C.plan_fuse ? h : w, C.fblok[c + 1] - C.fblok[c], &t[0][2 * q]);
+    }
+    for (int64_t i = 0; i < cnt[1]; i++) {
+        const int4 ch = C.h_trsm[i];
+        put(1, ch.x, C.width[ch.x], std::min(32, C.height[ch.x] - ch.y), ch.w, ch.z, &t[1][2 * i]);
+    }
+    for (int k = 2; k < 4; k++) {
+        const auto &tl = (k == 2) ? C.h_tiles : C.h_tctiles;
+        const int bm = (k == 2) ? GEMM_TM : TC_BM, bn = (k == 2) ? GEMM_TN : TC_BN;
+        for (int64_t i = 0; i < cnt[k]; i++) {
+            const GemmTask &g = C.h_tasks[tl[i].x];
+            const int N = C.blrow[g.b] - C.bfrow[g.b] + 1;
+            put(k, g.c, C.width[g.c], std::min(bm, g.M - tl[i].y * bm), std::min(bn, N - tl[i].z * bn), g.flags,
+                &t[k][2 * i]);
+        }
+    }
+    *count = total;
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_set_cblk_priority(pastix_gpu_t *ctx, const double *prio) {
+    if (!ctx || ctx->cblknbr == 0) return PASTIX_GPU_ERR_BADPARAMETER;
+    auto &C = *ctx;
+    PGPU_CHECK(cudaSetDevice(C.device));
+    for (int l = 0; l < C.nlevels; l++) {
+        auto b = C.lvl_cblks.begin() + C.lvl_ptr[l], e = C.lvl_cblks.begin() + C.lvl_ptr[l + 1];
+        if (prio)
+            std::stable_sort(b, e, [prio](int x, int y) { return prio[x] > prio[y]; });
+        else
+            std::sort(b, e);
+    }
+    PGPU_CHECK(C.d_lvl_cblks.upload(C.lvl_cblks, C.stream));
+    PGPU_CHECK(cudaStreamSynchronize(C.stream));
+    C.plan_fact = -1;   // launch lists follow the new order
     return PASTIX_GPU_SUCCESS;
 }
 

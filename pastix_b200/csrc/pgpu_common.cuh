@@ -138,6 +138,15 @@ template <typename R> __device__ __forceinline__ void atomic_sub(cplx<R> *p, con
     atomicAdd(&p->im, -v.im);
 }
 
+// Task timing for the learned cost model: when prof != nullptr, thread 0 of
+// each CTA stores the global timer (ns) at the CTA's start and end in
+// prof[2 * blockIdx.x + {0, 1}].
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // Panel row of global row r inside cblk f: binary search over f's blocks
 // (sorted by frownum, blend/solver.h:497-514 is_block_inside_fblock walks
 // them linearly).  Returns -1 if r is not a row of f.

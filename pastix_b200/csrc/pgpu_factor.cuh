@@ -60,7 +60,9 @@ struct GemmTask {
 template <typename T>
 __global__ void __launch_bounds__(256) k_gemm_scatter(Meta m, const int4 *__restrict__ tiles,
                                                       const GemmTask *__restrict__ tasks,
-                                                      T *__restrict__ coefL, T *__restrict__ coefU) {
+                                                      T *__restrict__ coefL, T *__restrict__ coefU,
+                                                      int64_t *prof) {
+    const uint64_t t_start = prof ? global_ns() : 0;
     __shared__ T As[GEMM_TK][GEMM_TM + 4];
     __shared__ T Bs[GEMM_TK][GEMM_TN + 4];
     __shared__ T Ds[GEMM_TK];
@@ -146,6 +148,13 @@ __global__ void __launch_bounds__(256) k_gemm_scatter(Meta m, const int4 *__rest
             int tc = tcol0 + j;
             if (lower_only && tr < wf && tc > tr) continue;
             atomic_sub(&C[(int64_t)tr * ldf + tc], acc[p][q]);
+        }
+    }
+    if (prof) {
+        __syncthreads();
+        if (tid == 0) {
+            prof[2 * blockIdx.x] = (int64_t)t_start;
+            prof[2 * blockIdx.x + 1] = (int64_t)global_ns();
         }
     }
 }

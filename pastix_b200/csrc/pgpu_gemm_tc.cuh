@@ -148,7 +148,8 @@ template <bool SPLIT>
 __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const int4 *__restrict__ tiles,
                                                                 const GemmTask *__restrict__ tasks,
                                                                 float *__restrict__ coefL,
-                                                                float *__restrict__ coefU, Status *st) {
+                                                                float *__restrict__ coefU, Status *st,
+                                                                int64_t *prof) {
     constexpr int S = TcCfg<SPLIT>::STAGES, NT = TcCfg<SPLIT>::TILES;
     extern __shared__ __align__(16) unsigned char tc_smem_raw[];
     __shared__ __align__(8) uint64_t mbar[S];
@@ -162,6 +163,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
     unsigned char *sbase = tc_smem_raw + (base - raw);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint64_t t_start = prof ? global_ns() : 0;
     const int4 tl = tiles[blockIdx.x];
     const GemmTask t = tasks[tl.x];
     const int c = t.c, b = t.b, f = t.f;
@@ -363,6 +365,10 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS)
                      : "memory");
+    }
+    if (prof && tid == 0) {
+        prof[2 * blockIdx.x] = (int64_t)t_start;
+        prof[2 * blockIdx.x + 1] = (int64_t)global_ns();
     }
 }
 

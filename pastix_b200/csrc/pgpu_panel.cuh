@@ -154,8 +154,8 @@ __device__ __forceinline__ void row_solve_upper(T *x, const T *tile, int nb) {
 // ---------------------------------------------------------------------------
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restrict__ cblks, T *__restrict__ coefL,
-                                                      T *__restrict__ coefU, double critd, int fuse_rows,
-                                                      int pl_rows, int pu_rows, Status *st) {
+                                                      T *__restrict__ coefU, const double *critp, int fuse_rows,
+                                                      int pl_rows, int pu_rows, Status *st, int64_t *prof) {
     typedef typename real_of<T>::type R;
     constexpr bool LU = (MODE == FM_GETRF);
     constexpr bool LDL = fm_ldl(MODE);
@@ -171,8 +171,9 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
     const int rows = (h <= fuse_rows) ? h : w;
     T *A = coefL + m.coefoff[c];
     T *AU = coefU + m.coefoff[c];
-    const R crit = R(critd);
+    const R crit = R(*critp);
     const int tid = threadIdx.x, nt = blockDim.x;
+    const uint64_t t_start = prof ? global_ns() : 0;
     int npiv = 0, nneg = 0, nbad = 0;
     for (int jb = 0; jb < w; jb += PB) {
         const int nb = min(PB, w - jb);
@@ -266,6 +267,10 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
         if (npiv) atomicAdd(&st->nbpivots, npiv);
         if (nneg) atomicAdd(&st->negpivots, nneg);
         if (nbad) atomicAdd(&st->nonfinite, nbad);
+        if (prof) {
+            prof[2 * blockIdx.x] = (int64_t)t_start;
+            prof[2 * blockIdx.x + 1] = (int64_t)global_ns();
+        }
     }
 }
 
@@ -285,7 +290,7 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
 // ---------------------------------------------------------------------------
 template <typename T, int TR, bool CJ>
 __global__ void __launch_bounds__(256) k_trsm_rows(Meta m, const int4 *__restrict__ chunks, T *__restrict__ coefL,
-                                                   T *__restrict__ coefU, int maxw, int pch) {
+                                                   T *__restrict__ coefU, int maxw, int pch, int64_t *prof) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int4 ch = chunks[blockIdx.x];
     const int c = ch.x, r0 = ch.y, mode = ch.w;
@@ -299,6 +304,7 @@ __global__ void __launch_bounds__(256) k_trsm_rows(Meta m, const int4 *__restric
     T *Pan = (ch.z ? coefU : coefL) + m.coefoff[c] + (int64_t)r0 * ld;
     const int tid = threadIdx.x, nt = blockDim.x;
     const bool cjl = CJ && mode != 2;      // conjugate the L coefficients
+    const uint64_t t_start = prof ? global_ns() : 0;
     for (int e = tid; e < nrows * w; e += nt) {
         const int i = e / w, j = e - i * w;
         X[i * xl + j] = Pan[(int64_t)i * ld + j];
@@ -345,6 +351,13 @@ __global__ void __launch_bounds__(256) k_trsm_rows(Meta m, const int4 *__restric
         T v = X[i * xl + j];
         if (mode == 3) v = v * (T(1) / D[(int64_t)j * ld + j]);
         Pan[(int64_t)i * ld + j] = v;
+    }
+    if (prof) {
+        __syncthreads();
+        if (tid == 0) {
+            prof[2 * blockIdx.x] = (int64_t)t_start;
+            prof[2 * blockIdx.x + 1] = (int64_t)global_ns();
+        }
     }
 }
 

@@ -363,6 +363,14 @@ __global__ void k_gather_vals(int64_t nnz, const int64_t *__restrict__ src, cons
     }
 }
 
+// Static pivoting threshold from the matrix norm (sopalin/pastix_task_sopalin.c:
+// 461-485): s[1] = -magn if magn < 0, eps * s[0] if magn == 0, magn * s[0]
+// otherwise, with s[0] = ||A||_F.
+__global__ void k_static_pivot_threshold(double *s, double magn, double eps) {
+    const double anorm = s[0];
+    s[1] = (magn < 0.) ? -magn : ((magn == 0.) ? eps * anorm : magn * anorm);
+}
+
 // Per-segment sum of squares: out[s] = sum |x_i|^2 over [seg[s], seg[s+1]).
 template <typename S>
 __global__ void k_seg_sumsq(int nseg, const int64_t *__restrict__ seg, const S *__restrict__ x,

@@ -1,0 +1,132 @@
+"""Learned cost model: the CPU restatement of the network pinned by finite
+differences, the GPU forward/backward/Adam kernels against it, the task
+records against the plan, and what the trained network gains over the
+flop-count model on held-out tasks."""
+import numpy as np
+import pytest
+
+from oracle import mlp_np as O
+from pastix_b200 import analysis
+from pastix_b200 import batch as B
+from pastix_b200 import costmodel as CM
+from pastix_b200 import matrices as M
+
+F, H = CM.NFEAT, 16
+
+
+def _data(n=200, seed=0):
+    rng = np.random.default_rng(seed)
+    p = rng.normal(0, 0.3, O.count(F, H))
+    X = rng.normal(0, 1, (n, F))
+    t = rng.normal(0, 1, n)
+    return p, X, t
+
+
+def test_oracle_gradient_matches_finite_differences():
+    p, X, t = _data(40)
+    _, g = O.loss_and_grad(p, X, t, F, H)
+    rng = np.random.default_rng(1)
+    for k in rng.choice(len(p), 25, replace=False):
+        e = np.zeros_like(p)
+        e[k] = 1e-6
+        fd = (O.loss_and_grad(p + e, X, t, F, H)[0] - O.loss_and_grad(p - e, X, t, F, H)[0]) / 2e-6
+        assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(g[k])), k
+
+
+def test_plan_tasks_covers_every_cblk():
+    A = M.diffusion_lognormal(12, 11, 10, 1.0, np.random.default_rng(1))
+    st = analysis.analyze(A)
+    info = CM.plan_tasks(st, "potrf", 8)
+    nc = st["cblktab"].shape[0] - 1
+    assert np.array_equal(np.sort(info[info[:, 0] == 0, 1]), np.arange(nc))
+    assert (CM.task_flops(info) > 0).all()
+    X = CM.features(info)
+    assert X.shape == (info.shape[0], CM.NFEAT) and np.isfinite(X).all()
+    fl = CM.FlopModel().predict(info)
+    assert np.allclose(fl, CM.task_flops(info))
+
+
+@pytest.mark.gpu
+def test_mlp_forward_and_gradient_match_oracle():
+    p, X, t = _data(300, seed=3)
+    m = CM.MLPCostModel(hidden=H, seed=1)
+    m.set_params(p)
+    loss, g = m.gradient(X, t)
+    lr, gr = O.loss_and_grad(p, X, t, F, H)
+    assert abs(loss - lr) <= 1e-12 * abs(lr)
+    assert np.abs(g - gr).max() <= 1e-11 * np.abs(gr).max()
+    m.close()
+
+
+@pytest.mark.gpu
+def test_mlp_adam_training_matches_oracle():
+    p, X, t = _data(120, seed=4)
+    m = CM.MLPCostModel(hidden=H, seed=1)
+    m.set_params(p)
+    import ctypes as C
+    from pastix_b200 import gpu as G
+    loss = np.zeros(1)
+    Xc, tc = np.ascontiguousarray(X), np.ascontiguousarray(t)
+    G._check("train", CM._lib().pastix_gpu_mlp_train(m.h, X.shape[0], G._p(Xc), G._p(tc), 25, 1e-2, G._p(loss)))
+    q, mo, vo = p.copy(), np.zeros_like(p), np.zeros_like(p)
+    for step in range(1, 26):
+        _, g = O.loss_and_grad(q, X, t, F, H)
+        q, mo, vo = O.adam_step(q, g, mo, vo, step, 1e-2)
+    assert np.abs(m.params() - q).max() <= 1e-9 * np.abs(q).max()
+    assert abs(loss[0] - O.loss_and_grad(q, X, t, F, H)[0]) <= 1e-9
+    m.close()
+
+
+def _record(systems, fact="potrf", mixed=False):
+    from pastix_b200 import gpu as G
+    bs = B.BatchSolver(systems, fact=fact, mixed=mixed)
+    CM.record_tasks(bs.solver)
+    bs.solver.numfact(bs.values())     # warm-up
+    bs.solver.numfact(bs.values())
+    info, ns = CM.task_records(bs.solver)
+    return bs, info, ns
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fact,mixed", [("potrf", False), ("potrf", True), ("getrf", False)])
+def test_task_records_match_plan(fact, mixed):
+    if fact == "getrf":
+        systems = [M.convdiff_upwind(14, 13, 12, 10.0)]
+    else:
+        systems = [M.diffusion_lognormal(26, 25, 24, 1.0, np.random.default_rng(2))]
+    bs, info, ns = _record(systems, fact, mixed)
+    assert (ns > 0).all()
+    plan = CM.plan_tasks(bs.struct, fact, 4 if mixed else 8, use_tc=mixed)
+    key = lambda a: a[np.lexsort(a.T[::-1])]
+    assert np.array_equal(key(info), key(plan))
+    bs.close()
+
+
+@pytest.mark.gpu
+def test_learned_model_beats_flop_model_on_held_out_systems():
+    """Trained on the task timings of one batch of 2D systems, evaluated on
+    the tasks of another batch: the network's median |log(pred/measured)|
+    is below the per-kind log-linear flop model's."""
+    rng = np.random.default_rng(7)
+    train = [M.diffusion_lognormal(int(q), int(q), 1, 0.5, rng) for q in rng.integers(32, 200, 24)]
+    test = [M.diffusion_lognormal(int(q), int(q), 1, 0.5, rng) for q in rng.integers(32, 200, 12)]
+    test += [M.diffusion_lognormal(18, 17, 16, 1.0, rng)]
+    bs1, i1, n1 = _record(train + [M.diffusion_lognormal(20, 19, 18, 1.0, rng)])
+    bs2, i2, n2 = _record(test)
+    mlp = CM.MLPCostModel(hidden=32, seed=3)
+    mlp.fit(i1, n1, steps=3000, lr=3e-3)
+    flop = CM.FlopModel().fit(i1, n1)
+    e_mlp = CM.log_error(mlp.predict(i2), n2)
+    e_flop = CM.log_error(flop.predict(i2), n2)
+    print("held-out median |log err|: mlp %.3f flop %.3f" % (e_mlp, e_flop))
+    assert e_mlp < e_flop
+    # its per-cblk costs order the level launches; the factors do not change
+    from pastix_b200 import gpu as G
+    L0, _ = bs2.solver.coeftab()
+    CM.set_cblk_priority(bs2.solver, CM.cblk_costs(i2, mlp.predict(i2), bs2.struct["cblktab"].shape[0] - 1))
+    bs2.solver.numfact(bs2.values())
+    L1, _ = bs2.solver.coeftab()
+    assert np.abs(L1 - L0).max() <= 1e-12 * np.abs(L0).max()
+    for b_ in (bs1, bs2):
+        b_.close()
+    mlp.close()
