@@ -842,20 +842,27 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
     PGPU_CHECK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(k_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(k_fwd_off<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
+    // PASTIX_GPU_SOLVE_PROFILE=1: device time per solve phase on stderr (diagnostics)
+    static const bool prof = getenv("PASTIX_GPU_SOLVE_PROFILE") != nullptr;
+    LaunchTimer tm(C);
+    auto mark = [&](int k) { return prof ? tm.mark(k) : cudaSuccess; };
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
+        PGPU_CHECK(mark(0));
         k_fwd_diag<T><<<ncb, 128, ((size_t)mw * nrhs + 32 * 33) * sizeof(T), s>>>(
             C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs, (lu || ldl) ? 1 : 0);
         nl++;
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
+            PGPU_CHECK(mark(1));
             k_fwd_off<T><<<nch, 256, (size_t)mw * nrhs * sizeof(T), s>>>(
                 C.meta, C.d_solve_chunks.p + C.solve_ptr[l], coefL, W, ldb, nrhs, SOLVE_ROWS_PER_CHUNK);
             nl++;
         }
     }
     if (ldl) {
+        PGPU_CHECK(mark(2));
         k_diag_scale<T><<<std::min(C.cblknbr, 4096), 128, 0, s>>>(C.meta, coefL, W, ldb, nrhs);
         nl++;
     }
@@ -864,15 +871,25 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         const int mw = C.lvl_maxw[l];
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
+            PGPU_CHECK(mark(3));
             k_bwd_off<T><<<nch, 128, 0, s>>>(C.meta, C.d_solve_chunks.p + C.solve_ptr[l], coefU, W, ldb, nrhs,
                                               SOLVE_ROWS_PER_CHUNK, lu ? 0 : cjp);
             nl++;
         }
+        PGPU_CHECK(mark(4));
         k_bwd_diag<T><<<ncb, 128, ((size_t)mw * nrhs + 32 * 33) * sizeof(T), s>>>(
             C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs, lu ? 1 : 0, ldl ? 1 : 0, lu ? 0 : cjp);
         nl++;
     }
     PGPU_CHECK(cudaGetLastError());
+    if (prof) {
+        PGPU_CHECK(mark(5));
+        PGPU_CHECK(cudaStreamSynchronize(s));
+        double ms[5];
+        tm.collect(ms, 5);
+        fprintf(stderr, "pastix_gpu solve profile (nrhs %d, %d levels): fwd_diag %.3f fwd_off %.3f diag %.3f "
+                        "bwd_off %.3f bwd_diag %.3f ms\n", nrhs, C.nlevels, ms[0], ms[1], ms[2], ms[3], ms[4]);
+    }
     *launches += nl;
     return PASTIX_GPU_SUCCESS;
 }

@@ -85,33 +85,52 @@ __global__ void k_mlp_delta(int64_t n, Layout L, const double *__restrict__ P, c
     }
 }
 
-// one thread per parameter, summing over the samples in order (deterministic)
-__global__ void k_mlp_grad(int64_t n, Layout L, const double *__restrict__ X, const double *__restrict__ A1,
-                           const double *__restrict__ A2, const double *__restrict__ DY,
-                           const double *__restrict__ D2, const double *__restrict__ D1, double *__restrict__ G) {
+// Gradient, in two deterministic passes: chunk c of MLP_CHUNK samples gives
+// partial[c][p] (one thread per parameter p, samples in order), then the
+// chunks are summed in order.
+constexpr int MLP_CHUNK = 1024;
+
+__global__ void k_mlp_grad_partial(int64_t n, Layout L, const double *__restrict__ X, const double *__restrict__ A1,
+                                   const double *__restrict__ A2, const double *__restrict__ DY,
+                                   const double *__restrict__ D2, const double *__restrict__ D1,
+                                   double *__restrict__ part) {
     const int F = L.F, H = L.H;
+    const int64_t s0 = (int64_t)blockIdx.y * MLP_CHUNK, s1 = min(n, s0 + MLP_CHUNK);
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < L.count();
          p += (int64_t)gridDim.x * blockDim.x) {
         double g = 0.0;
         if (p < L.b1()) {                          // W1[j][i]: sum d1_j x_i
             const int j = (int)(p / F), i = (int)(p % F);
-            for (int64_t s = 0; s < n; s++) g += D1[s * H + j] * X[s * F + i];
+#pragma unroll 8
+            for (int64_t s = s0; s < s1; s++) g += D1[s * H + j] * X[s * F + i];
         } else if (p < L.w2()) {                   // b1[j]
             const int j = (int)(p - L.b1());
-            for (int64_t s = 0; s < n; s++) g += D1[s * H + j];
+#pragma unroll 8
+            for (int64_t s = s0; s < s1; s++) g += D1[s * H + j];
         } else if (p < L.b2()) {                   // W2[k][j]: sum d2_k a1_j
             const int64_t q = p - L.w2();
             const int k = (int)(q / H), j = (int)(q % H);
-            for (int64_t s = 0; s < n; s++) g += D2[s * H + k] * A1[s * H + j];
+#pragma unroll 8
+            for (int64_t s = s0; s < s1; s++) g += D2[s * H + k] * A1[s * H + j];
         } else if (p < L.w3()) {                   // b2[k]
             const int k = (int)(p - L.b2());
-            for (int64_t s = 0; s < n; s++) g += D2[s * H + k];
+#pragma unroll 8
+            for (int64_t s = s0; s < s1; s++) g += D2[s * H + k];
         } else if (p < L.b3()) {                   // W3[k]: sum dy a2_k
             const int k = (int)(p - L.w3());
-            for (int64_t s = 0; s < n; s++) g += DY[s] * A2[s * H + k];
+#pragma unroll 8
+            for (int64_t s = s0; s < s1; s++) g += DY[s] * A2[s * H + k];
         } else {                                   // b3
-            for (int64_t s = 0; s < n; s++) g += DY[s];
+            for (int64_t s = s0; s < s1; s++) g += DY[s];
         }
+        part[(int64_t)blockIdx.y * L.count() + p] = g;
+    }
+}
+
+__global__ void k_mlp_grad_sum(int nchunk, int64_t np, const double *__restrict__ part, double *__restrict__ G) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < np; p += (int64_t)gridDim.x * blockDim.x) {
+        double g = 0.0;
+        for (int c = 0; c < nchunk; c++) g += part[(int64_t)c * np + p];
         G[p] = g;
     }
 }
@@ -173,7 +192,7 @@ struct pastix_gpu_mlp_s {
     int device = 0;
     Layout L{0, 0};
     cudaStream_t stream = nullptr;
-    Buf<double> P, G, M, V, X, T, Y, A1, A2, DY, D2, D1, loss;
+    Buf<double> P, G, M, V, X, T, Y, A1, A2, DY, D2, D1, loss, part;
     int64_t step = 0;
 };
 
@@ -252,6 +271,7 @@ static int mlp_upload(pastix_gpu_mlp_t *m, int64_t n, const double *X, const dou
         MLP_CHECK(m->DY.need(n));
         MLP_CHECK(m->D2.need((size_t)n * H));
         MLP_CHECK(m->D1.need((size_t)n * H));
+        MLP_CHECK(m->part.need((size_t)((n + MLP_CHUNK - 1) / MLP_CHUNK) * m->L.count()));
         MLP_CHECK(cudaMemcpyAsync(m->T.p, T, n * sizeof(double), cudaMemcpyHostToDevice, m->stream));
     }
     return PASTIX_GPU_SUCCESS;
@@ -263,8 +283,10 @@ static void mlp_fwd_bwd(pastix_gpu_mlp_t *m, int64_t n) {
     k_mlp_forward<<<g, 128, 0, m->stream>>>(n, m->L, m->X.p, m->P.p, m->A1.p, m->A2.p, m->Y.p);
     k_mlp_delta<<<g, 128, 0, m->stream>>>(n, m->L, m->P.p, m->A1.p, m->A2.p, m->Y.p, m->T.p, m->DY.p, m->D2.p,
                                          m->D1.p);
-    k_mlp_grad<<<grid_for(m->L.count()), 128, 0, m->stream>>>(n, m->L, m->X.p, m->A1.p, m->A2.p, m->DY.p, m->D2.p,
-                                                             m->D1.p, m->G.p);
+    const int nchunk = (int)((n + MLP_CHUNK - 1) / MLP_CHUNK);
+    k_mlp_grad_partial<<<dim3((unsigned)((m->L.count() + 127) / 128), nchunk), 128, 0, m->stream>>>(
+        n, m->L, m->X.p, m->A1.p, m->A2.p, m->DY.p, m->D2.p, m->D1.p, m->part.p);
+    k_mlp_grad_sum<<<grid_for(m->L.count()), 128, 0, m->stream>>>(nchunk, m->L.count(), m->part.p, m->G.p);
     k_mlp_sqerr<<<1, 256, 0, m->stream>>>(n, m->Y.p, m->T.p, m->loss.p);
 }
 

@@ -114,7 +114,7 @@ def test_learned_model_beats_flop_model_on_held_out_systems():
     bs1, i1, n1 = _record(train + [M.diffusion_lognormal(20, 19, 18, 1.0, rng)])
     bs2, i2, n2 = _record(test)
     mlp = CM.MLPCostModel(hidden=32, seed=3)
-    mlp.fit(i1, n1, steps=3000, lr=3e-3)
+    mlp.fit(i1, n1, steps=2000, lr=3e-3)
     flop = CM.FlopModel().fit(i1, n1)
     e_mlp = CM.log_error(mlp.predict(i2), n2)
     e_flop = CM.log_error(flop.predict(i2), n2)
