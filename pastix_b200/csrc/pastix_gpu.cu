@@ -474,6 +474,12 @@ static int mixed_gemm_mode() {
     return MG_3XTF32;
 }
 static bool tc_enabled() { return mixed_gemm_mode() != MG_FP32; }
+// PASTIX_GPU_TC_KERNEL=tile selects the one-tile-per-CTA tensor-core kernel
+// instead of the persistent warp-specialized one.
+static bool tc_persistent() {
+    const char *e = getenv("PASTIX_GPU_TC_KERNEL");
+    return !(e && std::strcmp(e, "tile") == 0);
+}
 static bool tc_task(int M, int N, int K) { return K >= 32 && M >= 64 && N >= 32 && (int64_t)M * N >= 128 * 64; }
 
 // Kernel form of a factorization request (pastix_factotype_t on a real or
@@ -637,11 +643,18 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     PGPU_CHECK(cudaFuncSetAttribute(kpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(ktrsm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     const bool split = (mixed_gemm_mode() == MG_3XTF32);
+    const bool persist = tc_persistent() && !C.record;   // task timings need one tile per CTA
+    int nsm = 148;
     if constexpr (std::is_same<T, float>::value) {
         PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         tc_smem_bytes<false>()));
         PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         tc_smem_bytes<true>()));
+        PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc_persistent<false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, tcp_smem_bytes<false>()));
+        PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc_persistent<true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, tcp_smem_bytes<true>()));
+        PGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, C.device));
     }
     int64_t *prof[4] = {nullptr, nullptr, nullptr, nullptr};
     if (C.record) {
@@ -687,7 +700,18 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
         }
         if constexpr (std::is_same<T, float>::value) {
             const int ntc = C.tctile_ptr[l + 1] - C.tctile_ptr[l];
-            if (ntc) {
+            if (ntc && persist) {
+                PGPU_CHECK(tm.mark(PH_TC));
+                const int g = std::min(ntc, nsm);
+                if (split)
+                    k_gemm_scatter_tc_persistent<true><<<g, TCP_THREADS, tcp_smem_bytes<true>(), s>>>(
+                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p);
+                else
+                    k_gemm_scatter_tc_persistent<false><<<g, TCP_THREADS, tcp_smem_bytes<false>(), s>>>(
+                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p);
+                nl++;
+                ngemm++;
+            } else if (ntc) {
                 PGPU_CHECK(tm.mark(PH_TC));
                 if (split)
                     k_gemm_scatter_tc<true><<<ntc, TC_THREADS, tc_smem_bytes<true>(), s>>>(
@@ -846,12 +870,22 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
     static const bool prof = getenv("PASTIX_GPU_SOLVE_PROFILE") != nullptr;
     LaunchTimer tm(C);
     auto mark = [&](int k) { return prof ? tm.mark(k) : cudaSuccess; };
+    // staged-panel rows of the diagonal kernels that fit next to the RHS block
+    auto diag_smem = [&](int mw, int *pch) {
+        const size_t fixed = ((size_t)mw * nrhs + 32 * 33) * sizeof(T);
+        const size_t room = fixed < (size_t)SMEM_LIMIT ? (SMEM_LIMIT - fixed) / (33 * sizeof(T)) : 0;
+        *pch = (int)std::min<size_t>(std::max(mw, 1), room);
+        return fixed + (size_t)(*pch) * 33 * sizeof(T);
+    };
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
+        int pch = 0;
+        const size_t dsm = diag_smem(mw, &pch);
+        if (pch < std::min(32, mw)) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
         PGPU_CHECK(mark(0));
-        k_fwd_diag<T><<<ncb, 128, ((size_t)mw * nrhs + 32 * 33) * sizeof(T), s>>>(
-            C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs, (lu || ldl) ? 1 : 0);
+        k_fwd_diag<T><<<ncb, 256, dsm, s>>>(
+            C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs, (lu || ldl) ? 1 : 0, pch);
         nl++;
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
@@ -872,13 +906,16 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
             PGPU_CHECK(mark(3));
-            k_bwd_off<T><<<nch, 128, 0, s>>>(C.meta, C.d_solve_chunks.p + C.solve_ptr[l], coefU, W, ldb, nrhs,
-                                              SOLVE_ROWS_PER_CHUNK, lu ? 0 : cjp);
+            k_bwd_off<T><<<nch, 128, (size_t)SOLVE_ROWS_PER_CHUNK * nrhs * sizeof(T), s>>>(
+                C.meta, C.d_solve_chunks.p + C.solve_ptr[l], coefU, W, ldb, nrhs, SOLVE_ROWS_PER_CHUNK,
+                lu ? 0 : cjp);
             nl++;
         }
+        int pch = 0;
+        const size_t dsm = diag_smem(mw, &pch);
         PGPU_CHECK(mark(4));
-        k_bwd_diag<T><<<ncb, 128, ((size_t)mw * nrhs + 32 * 33) * sizeof(T), s>>>(
-            C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs, lu ? 1 : 0, ldl ? 1 : 0, lu ? 0 : cjp);
+        k_bwd_diag<T><<<ncb, 256, dsm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs,
+                                            lu ? 1 : 0, ldl ? 1 : 0, lu ? 0 : cjp, pch);
         nl++;
     }
     PGPU_CHECK(cudaGetLastError());

@@ -373,3 +373,272 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
 }
 
 }  // namespace pgpu
+
+namespace pgpu {
+
+// ---------------------------------------------------------------------------
+// Persistent, warp-specialized form of the same update GEMM: one CTA per SM
+// walks the level's tiles (tile = blockIdx.x + i * gridDim.x) with three
+// roles running concurrently, so the loads of tile i+1, its MMAs and the
+// scatter-add epilogue of tile i overlap:
+//   warps 0-3 (128 threads): epilogue -- warp w reads TMEM lanes 32w..32w+31
+//                            of the finished accumulator, transposes through
+//                            shared memory and scatter-adds into the target;
+//   warps 4-7 (128 threads): producers -- global -> registers -> (3xTF32:
+//                            hi/lo split) -> SWIZZLE_128B shared-memory ring of
+//                            TCP_STAGES stages, then mbarrier arrive (full);
+//   warp 8, lane 0:          MMA issuer -- waits for a full stage, issues the
+//                            tcgen05.mma of the k-block into one of two TMEM
+//                            accumulators (2 x 128 columns), commits the stage
+//                            back to the producers (empty) and the finished
+//                            tile to the epilogue (acc_full); the epilogue
+//                            hands the accumulator back (acc_empty).
+// Every wait is bounded (mbar_wait): on time-out a role stops, records
+// Status::timeout, and the others run out on their own bounded waits; TMEM is
+// freed after all roles met at the final barrier.
+// ---------------------------------------------------------------------------
+constexpr int TCP_THREADS = 288;
+template <bool SPLIT> struct TcpCfg;
+template <> struct TcpCfg<false> { static constexpr int STAGES = 6, TILES = 2; };
+template <> struct TcpCfg<true> { static constexpr int STAGES = 3, TILES = 4; };
+constexpr int TCP_EPI_BYTES = 4 * 32 * 33 * 4;
+template <bool SPLIT>
+constexpr int tcp_smem_bytes() {
+    return TcpCfg<SPLIT>::STAGES * TcpCfg<SPLIT>::TILES * TC_TILE_BYTES + TCP_EPI_BYTES + 1024;
+}
+constexpr int TCP_TMEM_COLS = 256;
+
+__device__ __forceinline__ void mbar_arrive(uint32_t addr) {
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
+}
+
+struct TcTileView {
+    const float *A, *B;
+    int mrows, ncols, K, nk, flags, c, b, f, arow, j0;
+};
+
+__device__ __forceinline__ TcTileView tc_tile_view(const Meta &m, const int4 tl, const GemmTask *tasks,
+                                                   const float *coefL, const float *coefU) {
+    const GemmTask t = tasks[tl.x];
+    TcTileView v;
+    v.c = t.c;
+    v.b = t.b;
+    v.f = t.f;
+    v.flags = t.flags;
+    v.K = m.width[t.c];
+    const int ld = m.ld[t.c];
+    const int N = m.blrow[t.b] - m.bfrow[t.b] + 1;
+    const int i0 = tl.y * TC_BM;
+    v.j0 = tl.z * TC_BN;
+    v.arow = t.arow0 + i0;
+    v.A = ((t.flags & 1) ? coefU : coefL) + m.coefoff[t.c] + (int64_t)(t.arow0 + i0) * ld;
+    v.B = ((t.flags & 2) ? coefU : coefL) + m.coefoff[t.c] + (int64_t)(m.browoff[t.b] + v.j0) * ld;
+    v.mrows = min(TC_BM, t.M - i0);
+    v.ncols = min(TC_BN, N - v.j0);
+    v.nk = (v.K + TC_BK - 1) / TC_BK;
+    return v;
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(TCP_THREADS, 1)
+    k_gemm_scatter_tc_persistent(Meta m, const int4 *__restrict__ tiles, int ntiles,
+                                 const GemmTask *__restrict__ tasks, float *__restrict__ coefL,
+                                 float *__restrict__ coefU, Status *st) {
+    constexpr int S = TcpCfg<SPLIT>::STAGES, NT = TcpCfg<SPLIT>::TILES;
+    extern __shared__ __align__(16) unsigned char tc_smem_raw[];
+    __shared__ __align__(8) uint64_t full[S], empty[S], accf[2], acce[2], drained;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ int fail_s;
+    __shared__ int trow_s[TC_BM];
+
+    const uint32_t raw = smem_u32(tc_smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char *sbase = tc_smem_raw + (base - raw);
+    float *epi = reinterpret_cast<float *>(sbase + S * NT * TC_TILE_BYTES);   // [4][32][33]
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 8) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                     "r"(TCP_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) {
+            mbar_init(smem_u32(&full[s]), 128);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&accf[b]), 1);
+            mbar_init(smem_u32(&acce[b]), 128);
+        }
+        mbar_init(smem_u32(&drained), 1);
+        fail_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_s;
+    auto tile_addr = [&](int s, int q) { return base + (uint32_t)(s * NT + q) * TC_TILE_BYTES; };
+    auto failed = [&]() { return *(volatile int *)&fail_s != 0; };
+
+    if (warp >= 4 && warp < 8) {
+        // ---------------- producers ----------------
+        const int ptid = tid - 128;
+        constexpr int CH = (TC_BM * 8) / 128;          // 8 chunks of 16 B per operand per thread
+        int it = 0;
+        for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x) {
+            const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU);
+            const int ld = m.ld[v.c];
+            for (int kb = 0; kb < v.nk; kb++, it++) {
+                const int s = it % S;
+                const int k0 = kb * TC_BK;
+                float4 ra[CH], rb[CH];
+#pragma unroll
+                for (int q = 0; q < CH; q++) {
+                    const int e = ptid + q * 128;
+                    const int r = e >> 3, kc = k0 + (e & 7) * 4;
+                    ra[q] = ((r < v.mrows) && (kc < v.K))
+                                ? __ldg(reinterpret_cast<const float4 *>(v.A + (int64_t)r * ld + kc))
+                                : make_float4(0.f, 0.f, 0.f, 0.f);
+                    rb[q] = ((r < v.ncols) && (kc < v.K))
+                                ? __ldg(reinterpret_cast<const float4 *>(v.B + (int64_t)r * ld + kc))
+                                : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                if (it >= S && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((it / S - 1) & 1))) {
+                    atomicExch(&fail_s, 1);
+                    break;
+                }
+#pragma unroll
+                for (int q = 0; q < CH; q++) {
+                    const int e = ptid + q * 128;
+                    const int r = e >> 3, ch = e & 7;
+                    const uint32_t soff = (uint32_t)(r * 128 + ((ch ^ (r & 7)) << 4));
+                    if (SPLIT) {
+                        float4 h, l;
+                        h.x = tf32_hi(ra[q].x); h.y = tf32_hi(ra[q].y); h.z = tf32_hi(ra[q].z); h.w = tf32_hi(ra[q].w);
+                        l.x = ra[q].x - h.x; l.y = ra[q].y - h.y; l.z = ra[q].z - h.z; l.w = ra[q].w - h.w;
+                        sts128(tile_addr(s, 0) + soff, h);
+                        sts128(tile_addr(s, 1) + soff, l);
+                        h.x = tf32_hi(rb[q].x); h.y = tf32_hi(rb[q].y); h.z = tf32_hi(rb[q].z); h.w = tf32_hi(rb[q].w);
+                        l.x = rb[q].x - h.x; l.y = rb[q].y - h.y; l.z = rb[q].z - h.z; l.w = rb[q].w - h.w;
+                        sts128(tile_addr(s, 2) + soff, h);
+                        sts128(tile_addr(s, 3) + soff, l);
+                    } else {
+                        sts128(tile_addr(s, 0) + soff, ra[q]);
+                        sts128(tile_addr(s, 1) + soff, rb[q]);
+                    }
+                }
+                tc_fence_async_smem();
+                mbar_arrive(smem_u32(&full[s]));
+            }
+        }
+    } else if (warp == 8) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            const uint32_t idesc = tc_idesc();
+            int it = 0, tl = 0;
+            for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x, tl++) {
+                const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU);
+                const int ab = tl & 1;
+                const uint32_t acc = tmem + (uint32_t)(ab * 128);
+                if (tl >= 2 && !mbar_wait(smem_u32(&acce[ab]), (uint32_t)((tl / 2 - 1) & 1))) {
+                    atomicExch(&fail_s, 1);
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                bool ok = true;
+                for (int kb = 0; kb < v.nk; kb++, it++) {
+                    const int s = it % S;
+                    if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((it / S) & 1))) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+                    for (int kk = 0; kk < TC_BK / 8; kk++) {
+                        const uint32_t first = (kb > 0 || kk > 0) ? 1u : 0u;
+                        if (SPLIT) {
+                            const uint64_t ah = tc_sdesc(tile_addr(s, 0) + kk * 32),
+                                           al = tc_sdesc(tile_addr(s, 1) + kk * 32);
+                            const uint64_t bh = tc_sdesc(tile_addr(s, 2) + kk * 32),
+                                           bl = tc_sdesc(tile_addr(s, 3) + kk * 32);
+                            tc_mma(acc, al, bh, idesc, first);
+                            tc_mma(acc, ah, bl, idesc, 1u);
+                            tc_mma(acc, ah, bh, idesc, 1u);
+                        } else {
+                            tc_mma(acc, tc_sdesc(tile_addr(s, 0) + kk * 32), tc_sdesc(tile_addr(s, 1) + kk * 32),
+                                   idesc, first);
+                        }
+                    }
+                    tc_commit(smem_u32(&empty[s]));
+                }
+                if (!ok) {
+                    atomicExch(&fail_s, 1);
+                    break;
+                }
+                tc_commit(smem_u32(&accf[ab]));
+            }
+            // every MMA this thread issued has completed before TMEM is freed
+            tc_commit(smem_u32(&drained));
+            if (!mbar_wait(smem_u32(&drained), 0u)) atomicExch(&fail_s, 1);
+        }
+    } else {
+        // ---------------- epilogue (warps 0-3) ----------------
+        float *E = epi + warp * 32 * 33;
+        int tl = 0;
+        for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x, tl++) {
+            const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU);
+            const int ab = tl & 1;
+            // target panel row of my accumulator row (binary search in f's blocks)
+            const int myrow = warp * 32 + lane;
+            int tr = -1;
+            if (myrow < v.mrows) tr = panel_row_of(m, v.f, m.rowidx[m.rowbase[v.c] + v.arow + myrow]);
+            if (!mbar_wait(smem_u32(&accf[ab]), (uint32_t)((tl / 2) & 1))) {
+                atomicExch(&fail_s, 1);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            trow_s[myrow] = tr;
+            __syncwarp();
+            float *C = ((v.flags & 4) ? coefU : coefL) + m.coefoff[v.f];
+            const int ldf = m.ld[v.f], wf = m.width[v.f];
+            const int tcol0 = m.bfrow[v.b] + v.j0 - m.fcol[v.f];
+            const bool lower_only = (v.flags & 8) != 0;
+            for (int cb = 0; cb < TC_BN; cb += 32) {
+                uint32_t r[32];
+                tc_ld32(tmem + (uint32_t)(ab * 128) + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, r);
+                __syncwarp();
+#pragma unroll
+                for (int q = 0; q < 32; q++) E[lane * 33 + q] = __uint_as_float(r[q]);
+                __syncwarp();
+                const int j = cb + lane;
+                if (j < v.ncols) {
+                    const int tc = tcol0 + j;
+                    for (int rr = 0; rr < 32; rr++) {
+                        const int i = warp * 32 + rr;
+                        if (i >= v.mrows) break;
+                        const int t2 = trow_s[i];
+                        if (t2 < 0) continue;
+                        if (lower_only && t2 < wf && tc > t2) continue;
+                        atomicAdd(&C[(int64_t)t2 * ldf + tc], -E[rr * 33 + lane]);
+                    }
+                }
+                __syncwarp();
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(smem_u32(&acce[ab]));
+        }
+    }
+    if (tid == 0 && failed()) atomicAdd(&st->timeout, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 8) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCP_TMEM_COLS)
+                     : "memory");
+    }
+}
+
+}  // namespace pgpu

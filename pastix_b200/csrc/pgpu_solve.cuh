@@ -13,14 +13,16 @@ constexpr int SOLVE_MAXRHS = 16;
 // ---------------------------------------------------------------------------
 // Forward, diagonal part (kernels/solve_ztrsmsp.c:75 solve_blok_ztrsm with
 // Left, Lower, NoTrans): B[fcol:fcol+w, :] := D^{-1} B[...], D = L_kk
-// (POTRF, non-unit) or the unit lower part of the LU diagonal block.  One CTA
-// per cblk of the level, blocked by 32 columns: warp 0 substitutes through
-// the 32x32 tile (shuffles, no block barrier), then all threads update the
-// rows below inside the diagonal block.
+// (POTRF, non-unit) or the unit lower part of the LU / LDL diagonal block.
+// One CTA per cblk of the level, blocked by 32 columns: warp 0 substitutes
+// through the 32x32 tile (shuffles, no block barrier), then all threads
+// update the rows below from the tile's column panel, which is first staged
+// in shared memory with coalesced loads, pch rows at a time (one round of
+// loads per chunk instead of a serial chain of global loads per thread).
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
-                           T *__restrict__ B, int ldb, int nrhs, int unit) {
+__global__ void __launch_bounds__(256) k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
+                                                  T *__restrict__ B, int ldb, int nrhs, int unit, int pch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *y = reinterpret_cast<T *>(smem_raw);   // [w][nrhs]
     const int c = cblks[blockIdx.x];
@@ -31,8 +33,8 @@ __global__ void k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
         int j = e / nrhs, r = e - j * nrhs;
         y[e] = B[(int64_t)r * ldb + fc + j];
     }
-    __syncthreads();
     T *tile = y + w * nrhs;                   // [32][33] diagonal tile
+    T *P = tile + 32 * 33;                    // [pch][33] column panel below the tile
     for (int jb = 0; jb < w; jb += 32) {
         const int nb = min(32, w - jb);
         for (int e = tid; e < nb * nb; e += nt) {
@@ -53,15 +55,22 @@ __global__ void k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
             }
         }
         __syncthreads();
-        const int rem = (w - jb - nb) * nrhs;
-        for (int e = tid; e < rem; e += nt) {
-            const int i = jb + nb + e / nrhs, r = e % nrhs;
-            const T *row = D + (int64_t)i * ld + jb;
-            T s = T(0);
-            for (int l = 0; l < nb; l++) s += row[l] * y[(jb + l) * nrhs + r];
-            y[i * nrhs + r] -= s;
+        for (int r0 = jb + nb; r0 < w; r0 += pch) {
+            const int nr = min(pch, w - r0);
+            for (int e = tid; e < nr * nb; e += nt) {
+                const int i = e / nb, l = e - i * nb;
+                P[i * 33 + l] = D[(int64_t)(r0 + i) * ld + jb + l];
+            }
+            __syncthreads();
+            for (int e = tid; e < nr * nrhs; e += nt) {
+                const int i = e / nrhs, r = e - i * nrhs;
+                T s = T(0);
+#pragma unroll 8
+                for (int l = 0; l < nb; l++) s += P[i * 33 + l] * y[(jb + l) * nrhs + r];
+                y[(r0 + i) * nrhs + r] -= s;
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
     for (int e = tid; e < w * nrhs; e += nt) {
         int j = e / nrhs, r = e - j * nrhs;
@@ -98,6 +107,7 @@ __global__ void k_fwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
         const int grow = m.rowidx[m.rowbase[c] + i];
         for (int r = 0; r < nrhs; r++) {
             T s = T(0);
+#pragma unroll 4
             for (int j = lane; j < w; j += 32) s += row[j] * y[r * w + j];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += shfl_xor_v(s, o);
@@ -116,18 +126,26 @@ __global__ void k_fwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
 template <typename T>
 __global__ void k_bwd_off(Meta m, const int2 *__restrict__ chunks, const T *__restrict__ coef,
                           T *__restrict__ B, int ldb, int nrhs, int rows_per_chunk, int cjp) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *xr = reinterpret_cast<T *>(smem_raw);   // [rows][nrhs]: the solution at the chunk's rows
     const int2 ch = chunks[blockIdx.x];
     const int c = ch.x, r0 = ch.y;
     const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c], h = m.height[c];
     const T *P = coef + m.coefoff[c];
-    const int rend = min(h, r0 + rows_per_chunk);
+    const int rend = min(h, r0 + rows_per_chunk), nr = rend - r0;
+    for (int e = threadIdx.x; e < nr * nrhs; e += blockDim.x) {
+        const int i = e / nrhs, r = e - i * nrhs;
+        xr[e] = B[(int64_t)r * ldb + m.rowidx[m.rowbase[c] + r0 + i]];
+    }
+    __syncthreads();
     for (int j = threadIdx.x; j < w; j += blockDim.x) {
         T s[SOLVE_MAXRHS];
         for (int r = 0; r < nrhs; r++) s[r] = T(0);
-        for (int i = r0; i < rend; i++) {
-            const T pij = cjp ? conj_v(P[(int64_t)i * ld + j]) : P[(int64_t)i * ld + j];
-            const int grow = m.rowidx[m.rowbase[c] + i];
-            for (int r = 0; r < nrhs; r++) s[r] += pij * B[(int64_t)r * ldb + grow];
+#pragma unroll 4
+        for (int i = 0; i < nr; i++) {
+            const T v = P[(int64_t)(r0 + i) * ld + j];
+            const T pij = cjp ? conj_v(v) : v;
+            for (int r = 0; r < nrhs; r++) s[r] += pij * xr[i * nrhs + r];
         }
         for (int r = 0; r < nrhs; r++) atomic_sub(&B[(int64_t)r * ldb + fc + j], s[r]);
     }
@@ -140,11 +158,12 @@ __global__ void k_bwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
 // upper triangle U_kk of the LU diagonal block (Left, Upper, NoTrans,
 // NonUnit).  op = conj when cjp.  Blocked by 32 columns from the last block
 // up: warp 0 substitutes through the tile, then all threads update the rows
-// above.
+// above from the tile's panel staged in shared memory (pch rows at a time).
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
-                           T *__restrict__ B, int ldb, int nrhs, int upper, int unit, int cjp) {
+__global__ void __launch_bounds__(256) k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
+                                                  T *__restrict__ B, int ldb, int nrhs, int upper, int unit, int cjp,
+                                                  int pch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *x = reinterpret_cast<T *>(smem_raw);   // [w][nrhs]
     const int c = cblks[blockIdx.x];
@@ -155,8 +174,8 @@ __global__ void k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
         int j = e / nrhs, r = e - j * nrhs;
         x[e] = B[(int64_t)r * ldb + fc + j];
     }
-    __syncthreads();
     T *tile = x + w * nrhs;                   // [32][33] diagonal tile (op applied)
+    T *P = tile + 32 * 33;                    // [pch][33]: coefficients of the rows above
     const int nblk = (w + 31) / 32;
     for (int bi = nblk - 1; bi >= 0; bi--) {
         const int jb = bi * 32, nb = min(32, w - jb);
@@ -183,22 +202,31 @@ __global__ void k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__res
             }
         }
         __syncthreads();
-        const int rem = jb * nrhs;
-        for (int e = tid; e < rem; e += nt) {
-            const int i = e / nrhs, r = e % nrhs;
-            T s = T(0);
+        for (int r0 = 0; r0 < jb; r0 += pch) {
+            const int nr = min(pch, jb - r0);
+            // P[i][l] = coefficient of x[jb + l] in row r0 + i
             if (upper) {
-                const T *row = D + (int64_t)i * ld + jb;
-                for (int l = 0; l < nb; l++) s += row[l] * x[(jb + l) * nrhs + r];
+                for (int e = tid; e < nr * nb; e += nt) {
+                    const int i = e / nb, l = e - i * nb;
+                    P[i * 33 + l] = D[(int64_t)(r0 + i) * ld + jb + l];
+                }
             } else {
-                for (int l = 0; l < nb; l++) {
-                    const T v = D[(int64_t)(jb + l) * ld + i];
-                    s += (cjp ? conj_v(v) : v) * x[(jb + l) * nrhs + r];
+                for (int e = tid; e < nr * nb; e += nt) {
+                    const int l = e / nr, i = e - l * nr;
+                    const T v = D[(int64_t)(jb + l) * ld + r0 + i];
+                    P[i * 33 + l] = cjp ? conj_v(v) : v;
                 }
             }
-            x[i * nrhs + r] -= s;
+            __syncthreads();
+            for (int e = tid; e < nr * nrhs; e += nt) {
+                const int i = e / nrhs, r = e - i * nrhs;
+                T s = T(0);
+#pragma unroll 8
+                for (int l = 0; l < nb; l++) s += P[i * 33 + l] * x[(jb + l) * nrhs + r];
+                x[(r0 + i) * nrhs + r] -= s;
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
     for (int e = tid; e < w * nrhs; e += nt) {
         int j = e / nrhs, r = e - j * nrhs;
