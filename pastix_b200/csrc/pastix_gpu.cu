@@ -136,6 +136,14 @@ struct pastix_gpu_s {
     // per-task timings of the last numfact (learned cost model), when record
     bool record = false;
     DArr<int64_t> d_prof[4];           // panel CTAs, TRSM chunks, FMA GEMM tiles, tensor-core tiles
+    // panel TRSM as a GEMM against the inverse of the diagonal block (big panels of LL^t / LDL)
+    bool trsm_gemm = false;
+    std::vector<int64_t> invoff, scroff;
+    DArr<int64_t> d_invoff, d_scroff;
+    DArr<unsigned char> d_inv, d_scr;    // inverse workspace (zeroed), per-level TRSM output
+    std::vector<int> inv_ptr, ttile_ptr, tttile_ptr;   // per level: inverse jobs, TRSM FMA / TC tiles
+    DArr<int2> d_invjobs;
+    DArr<int4> d_ttiles, d_tttiles;
     std::vector<int4> h_tiles, h_tctiles, h_trsm;   // host copies of the plan's launch lists
     std::vector<GemmTask> h_tasks;
     int plan_fuse = 0, plan_esz = 0, plan_fmode = -1;
@@ -319,9 +327,11 @@ extern "C" int pastix_gpu_structure(pastix_gpu_t *ctx, int64_t n, int64_t cblknb
     PGPU_CHECK(C.d_bfcblk.upload(C.bfcblk, s));
     PGPU_CHECK(C.d_lvl_cblks.upload(C.lvl_cblks, s));
     PGPU_CHECK(C.d_peritab.upload(C.peritab, s));
+    C.invoff.assign(nc, -1);
+    PGPU_CHECK(C.d_invoff.upload(C.invoff, s));
     C.meta = Meta{C.n, nc, nb, C.d_fcol.p, C.d_width.p, C.d_height.p, C.d_ld.p, C.d_coefoff.p,
                   C.d_fblok.p, C.d_rowbase.p, C.d_rowidx.p, C.d_bfrow.p, C.d_blrow.p, C.d_browoff.p,
-                  C.d_bfcblk.p};
+                  C.d_bfcblk.p, C.d_invoff.p};
 
     // solve chunks (independent of the factorization type)
     std::vector<int2> sch;
@@ -496,13 +506,33 @@ static int fact_mode_of(int fact, bool zc) {
     }
 }
 
+// Panels of LL^t / LDL taller than this many rows get the TRSM-as-GEMM path
+// (inverse of the diagonal block, off-diagonal rows times it on the tensor
+// cores for single precision); PASTIX_GPU_TRSM=rows keeps the row-solve
+// kernel for every panel.
+static const int TRSM_GEMM_ROWS = 256;
+static bool trsm_gemm_enabled() {
+    const char *e = getenv("PASTIX_GPU_TRSM");
+    return !(e && std::strcmp(e, "rows") == 0);
+}
+
 static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     const bool use_tc = fp32 && !zc && tc_enabled() && (fmode == FM_POTRF || fmode == FM_GETRF);
-    const int key = ((fmode * 2 + (fp32 ? 1 : 0)) * 2 + (use_tc ? 1 : 0)) * 2 + (zc ? 1 : 0);
-    if (C.plan_fact == key) return PASTIX_GPU_SUCCESS;
     const bool lu = (fmode == FM_GETRF), ldl = fm_ldl(fmode);
+    const bool tgemm = !lu && !C.record && trsm_gemm_enabled();
+    const int key = ((((fmode * 2 + (fp32 ? 1 : 0)) * 2 + (use_tc ? 1 : 0)) * 2 + (zc ? 1 : 0)) * 2 + (tgemm ? 1 : 0));
+    if (C.plan_fact == key) return PASTIX_GPU_SUCCESS;
     const size_t esz = (fp32 ? 4 : 8) * (zc ? 2 : 1);
-    const int fuse = fuse_rows_for(lu, esz);
+    const int fuse = tgemm ? TRSM_GEMM_ROWS : fuse_rows_for(lu, esz);
+    const bool tc_trsm = tgemm && fp32 && !zc && tc_enabled();
+    std::vector<int2> invjobs;
+    std::vector<int4> ttiles, tttiles;
+    int64_t inv_elems = 0, scr_max = 0;
+    C.inv_ptr.assign(C.nlevels + 1, 0);
+    C.ttile_ptr.assign(C.nlevels + 1, 0);
+    C.tttile_ptr.assign(C.nlevels + 1, 0);
+    C.invoff.assign(C.cblknbr, -1);
+    C.scroff.assign(C.cblknbr, 0);
     const int sym_flags = 8 | (ldl ? 16 : 0) | ((zc && fm_conj(fmode)) ? 32 : 0);
     const double fma_flops = zc ? 8.0 : 2.0;
     std::vector<int4> tiles, trsm, tctiles;
@@ -514,6 +544,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     C.lvl_plrows.assign(C.nlevels, 0);
     C.lvl_porows.assign(C.nlevels, 0);
     for (int l = 0; l < C.nlevels; l++) {
+        int64_t scr_lvl = 0;
         for (int q = C.lvl_ptr[l]; q < C.lvl_ptr[l + 1]; q++) {
             const int c = C.lvl_cblks[q];
             const int w = C.width[c], h = C.height[c];
@@ -525,6 +556,22 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
                     trsm.push_back(make_int4(c, r0, 0, lu ? 1 : (ldl ? 3 : 0)));
                     if (lu) trsm.push_back(make_int4(c, r0, 1, 2));
                 }
+            if (h > fuse && tgemm) {
+                // inverse of the diagonal block, then X = A_off B^t into the scratch
+                C.invoff[c] = inv_elems;
+                inv_elems += round_up((int64_t)w * C.ld[c], 32);
+                for (int jb = 0; jb < w; jb += PB) invjobs.push_back(make_int2(c, jb));
+                C.scroff[c] = scr_lvl;
+                scr_lvl += round_up((int64_t)(h - w) * C.ld[c], 32);
+                const int id = (int)tasks.size();
+                GemmTask g{c, C.fblok[c], c, w, h - w, 64, 0};
+                g.out = C.scroff[c];
+                tasks.push_back(g);
+                const int bm = tc_trsm ? TC_BM : GEMM_TM, bn = tc_trsm ? TC_BN : GEMM_TN;
+                for (int tm = 0; tm < cdiv(h - w, bm); tm++)
+                    for (int tn = 0; tn < cdiv(w, bn); tn++)
+                        (tc_trsm ? tttiles : ttiles).push_back(make_int4(id, tm, tn, 0));
+            }
             const int b1 = C.fblok[c + 1];
             for (int b = C.fblok[c] + 1; b < b1; b++) {
                 const int f = C.bfcblk[b];
@@ -561,7 +608,29 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
         C.tile_ptr[l + 1] = (int)tiles.size();
         C.tctile_ptr[l + 1] = (int)tctiles.size();
         C.trsm_ptr[l + 1] = (int)trsm.size();
+        C.inv_ptr[l + 1] = (int)invjobs.size();
+        C.ttile_ptr[l + 1] = (int)ttiles.size();
+        C.tttile_ptr[l + 1] = (int)tttiles.size();
+        scr_max = std::max(scr_max, scr_lvl);
     }
+    if (tgemm) {
+        PGPU_CHECK(C.d_invjobs.upload(invjobs, C.stream));
+        PGPU_CHECK(C.d_ttiles.upload(ttiles, C.stream));
+        PGPU_CHECK(C.d_tttiles.upload(tttiles, C.stream));
+        PGPU_CHECK(C.d_scroff.upload(C.scroff, C.stream));
+        if (C.d_inv.n < (size_t)inv_elems * esz) {
+            C.d_inv.release();
+            PGPU_CHECK(C.d_inv.alloc((size_t)inv_elems * esz));
+        }
+        if (inv_elems) PGPU_CHECK(cudaMemsetAsync(C.d_inv.p, 0, (size_t)inv_elems * esz, C.stream));
+        if (C.d_scr.n < (size_t)scr_max * esz) {
+            C.d_scr.release();
+            PGPU_CHECK(C.d_scr.alloc((size_t)scr_max * esz));
+        }
+    }
+    PGPU_CHECK(C.d_invoff.upload(C.invoff, C.stream));
+    C.meta.invoff = C.d_invoff.p;
+    C.trsm_gemm = tgemm;
     cudaStream_t s = C.stream;
     PGPU_CHECK(C.d_tiles.upload(tiles, s));
     PGPU_CHECK(C.d_tctiles.upload(tctiles, s));
@@ -634,7 +703,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     T *coefL = reinterpret_cast<T *>(C.d_coef.p);
     T *coefU = lu ? coefL + C.coefnbr : coefL;
     cudaStream_t s = C.stream;
-    const int fuse = fuse_rows_for(lu, sizeof(T));
+    const int fuse = C.plan_fuse;   // rows the panel kernel solves itself (the plan's choice)
     PanelKernel<T> kpanel = panel_kernel<T>(fmode);
     if (!kpanel) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
     // the Hermitian forms conjugate the L coefficients in the row solves
@@ -642,6 +711,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     auto ktrsm = (CPX && fm_conj(fmode)) ? k_trsm_rows<T, TRSM_TR, CPX> : k_trsm_rows<T, TRSM_TR, false>;
     PGPU_CHECK(cudaFuncSetAttribute(kpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(ktrsm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
+    PGPU_CHECK(cudaFuncSetAttribute(k_tri_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     const bool split = (mixed_gemm_mode() == MG_3XTF32);
     const bool persist = tc_persistent() && !C.record;   // task timings need one tile per CTA
     int nsm = 148;
@@ -679,7 +749,41 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                                      C.d_status.p, at(prof[0], C.lvl_ptr[l]));
         nl++;
         const int ntr = C.trsm_ptr[l + 1] - C.trsm_ptr[l];
-        if (ntr) {
+        if (ntr && C.trsm_gemm) {
+            T *inv = reinterpret_cast<T *>(C.d_inv.p);
+            T *scr = reinterpret_cast<T *>(C.d_scr.p);
+            const int nij = C.inv_ptr[l + 1] - C.inv_ptr[l];
+            const size_t ism = ((size_t)mw * PBL + PB * PBL) * sizeof(T);
+            if (ism > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+            PGPU_CHECK(tm.mark(PH_TRSM));
+            k_tri_inverse<T><<<nij, 256, ism, s>>>(C.meta, C.d_invjobs.p + C.inv_ptr[l], coefL, inv,
+                                                   fm_ldl(fmode) ? 1 : 0, (CPX && fm_conj(fmode)) ? 1 : 0,
+                                                   fm_ldl(fmode) ? 1 : 0);
+            nl++;
+            const int ntt = C.ttile_ptr[l + 1] - C.ttile_ptr[l];
+            if (ntt) {
+                k_gemm_scatter<T><<<ntt, 256, 0, s>>>(C.meta, C.d_ttiles.p + C.ttile_ptr[l], C.d_tasks.p, coefL, coefU,
+                                                      inv, scr, nullptr);
+                nl++;
+            }
+            if constexpr (std::is_same<T, float>::value) {
+                const int ntc = C.tttile_ptr[l + 1] - C.tttile_ptr[l];
+                if (ntc) {
+                    const int g = std::min(ntc, nsm);
+                    if (split)
+                        k_gemm_scatter_tc_persistent<true><<<g, TCP_THREADS, tcp_smem_bytes<true>(), s>>>(
+                            C.meta, C.d_tttiles.p + C.tttile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
+                            inv, scr);
+                    else
+                        k_gemm_scatter_tc_persistent<false><<<g, TCP_THREADS, tcp_smem_bytes<false>(), s>>>(
+                            C.meta, C.d_tttiles.p + C.tttile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
+                            inv, scr);
+                    nl++;
+                }
+            }
+            k_trsm_copyback<T><<<ntr, 256, 0, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], C.d_scroff.p, scr, coefL);
+            nl++;
+        } else if (ntr) {
             const size_t fixed = ((size_t)TRSM_TR * (mw + 1) + PB * PBL) * sizeof(T);
             const int pch = (int)std::min<size_t>(mw, (SMEM_LIMIT - std::min<size_t>(fixed, SMEM_LIMIT)) /
                                                           (PBL * sizeof(T)));
@@ -694,7 +798,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
         if (nti) {
             PGPU_CHECK(tm.mark(PH_GEMM));
             k_gemm_scatter<T><<<nti, 256, 0, s>>>(C.meta, C.d_tiles.p + C.tile_ptr[l], C.d_tasks.p, coefL, coefU,
-                                                  at(prof[2], C.tile_ptr[l]));
+                                                  nullptr, nullptr, at(prof[2], C.tile_ptr[l]));
             nl++;
             ngemm++;
         }
@@ -705,22 +809,24 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                 const int g = std::min(ntc, nsm);
                 if (split)
                     k_gemm_scatter_tc_persistent<true><<<g, TCP_THREADS, tcp_smem_bytes<true>(), s>>>(
-                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p);
+                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
+                        nullptr, nullptr);
                 else
                     k_gemm_scatter_tc_persistent<false><<<g, TCP_THREADS, tcp_smem_bytes<false>(), s>>>(
-                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p);
+                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
+                        nullptr, nullptr);
                 nl++;
                 ngemm++;
             } else if (ntc) {
                 PGPU_CHECK(tm.mark(PH_TC));
                 if (split)
                     k_gemm_scatter_tc<true><<<ntc, TC_THREADS, tc_smem_bytes<true>(), s>>>(
-                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p,
-                        at(prof[3], C.tctile_ptr[l]));
+                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr,
+                        nullptr, at(prof[3], C.tctile_ptr[l]));
                 else
                     k_gemm_scatter_tc<false><<<ntc, TC_THREADS, tc_smem_bytes<false>(), s>>>(
-                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p,
-                        at(prof[3], C.tctile_ptr[l]));
+                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr,
+                        nullptr, at(prof[3], C.tctile_ptr[l]));
                 nl++;
                 ngemm++;
             }

@@ -33,6 +33,7 @@ struct Meta {
     const int *blrow;      // [bloknbr] lrownum
     const int *browoff;    // [bloknbr] first panel row of the block
     const int *bfcblk;     // [bloknbr] facing cblk
+    const int64_t *invoff; // [cblknbr] offset of the cblk's diagonal-block inverse (TRSM as GEMM), -1 if none
 };
 
 // Factorization forms of the kernels (pastix_factotype_t: POTRF = LL^h,

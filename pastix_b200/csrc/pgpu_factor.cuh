@@ -49,18 +49,24 @@ __global__ void k_fillin(int64_t nnz, const Tin *__restrict__ vals,
 // task = {c, b, f, arow0, M, flags} with flags: 1 A from U, 2 B from U,
 // 4 target U, 8 lower-triangle-only target (symmetric diagonal block),
 // 16 scale by the pivots of c (LDL: C -= A D op(B)^t, core_zgemdm),
-// 32 conjugate B (Hermitian forms: op = conj).
+// 32 conjugate B (Hermitian forms: op = conj),
+// 64 panel TRSM as a GEMM: X = A B^t with A the off-diagonal rows of c
+//    (arow0 = w_c, M = h_c - w_c), B the inverse of its diagonal block
+//    (inv + invoff[c], N = K = w_c), X stored (not accumulated) at scr + out
+//    with row stride ld_c.
 // ---------------------------------------------------------------------------
 constexpr int GEMM_TM = 64, GEMM_TN = 64, GEMM_TK = 16;
 
 struct GemmTask {
     int c, b, f, arow0, M, flags;
+    int64_t out;   // flags & 64 (panel TRSM as GEMM): element offset of X in the level's scratch
 };
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_gemm_scatter(Meta m, const int4 *__restrict__ tiles,
                                                       const GemmTask *__restrict__ tasks,
                                                       T *__restrict__ coefL, T *__restrict__ coefU,
+                                                      const T *__restrict__ inv, T *__restrict__ scr,
                                                       int64_t *prof) {
     const uint64_t t_start = prof ? global_ns() : 0;
     __shared__ T As[GEMM_TK][GEMM_TM + 4];
@@ -71,15 +77,17 @@ __global__ void __launch_bounds__(256) k_gemm_scatter(Meta m, const int4 *__rest
     const GemmTask t = tasks[tl.x];
     const int c = t.c, b = t.b, f = t.f;
     const int K = m.width[c], ld = m.ld[c];
-    const int N = m.blrow[b] - m.bfrow[b] + 1;
+    const bool trsm = (t.flags & 64) != 0;
+    const int N = trsm ? K : m.blrow[b] - m.bfrow[b] + 1;
     const int i0 = tl.y * GEMM_TM, j0 = tl.z * GEMM_TN;
     const T *A = ((t.flags & 1) ? coefU : coefL) + m.coefoff[c] + (int64_t)(t.arow0 + i0) * ld;
-    const T *B = ((t.flags & 2) ? coefU : coefL) + m.coefoff[c] + (int64_t)(m.browoff[b] + j0) * ld;
+    const T *B = trsm ? inv + m.invoff[c] + (int64_t)j0 * ld
+                      : ((t.flags & 2) ? coefU : coefL) + m.coefoff[c] + (int64_t)(m.browoff[b] + j0) * ld;
     const int mrows = min(GEMM_TM, t.M - i0), ncols = min(GEMM_TN, N - j0);
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
 
     // target panel row of each tile row (binary search in f's blocks)
-    if (tid < GEMM_TM) {
+    if (tid < GEMM_TM && !trsm) {
         int tr = -1;
         if (tid < mrows) {
             int grow = m.rowidx[m.rowbase[c] + t.arow0 + i0 + tid];
@@ -130,6 +138,27 @@ __global__ void __launch_bounds__(256) k_gemm_scatter(Meta m, const int4 *__rest
         __syncthreads();
     }
 
+    if (trsm) {
+        T *O = scr + t.out + (int64_t)i0 * ld + j0;
+#pragma unroll
+        for (int p = 0; p < 4; p++) {
+            const int i = ty * 4 + p;
+            if (i >= mrows) continue;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int j = tx * 4 + q;
+                if (j < ncols) O[(int64_t)i * ld + j] = acc[p][q];
+            }
+        }
+        if (prof) {
+            __syncthreads();
+            if (tid == 0) {
+                prof[2 * blockIdx.x] = (int64_t)t_start;
+                prof[2 * blockIdx.x + 1] = (int64_t)global_ns();
+            }
+        }
+        return;
+    }
     T *C = ((t.flags & 4) ? coefU : coefL) + m.coefoff[f];
     const int ldf = m.ld[f];
     const int tcol0 = m.bfrow[b] + j0 - m.fcol[f];

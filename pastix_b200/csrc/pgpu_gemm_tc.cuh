@@ -149,7 +149,8 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
                                                                 const GemmTask *__restrict__ tasks,
                                                                 float *__restrict__ coefL,
                                                                 float *__restrict__ coefU, Status *st,
-                                                                int64_t *prof) {
+                                                                const float *__restrict__ inv,
+                                                                float *__restrict__ scr, int64_t *prof) {
     constexpr int S = TcCfg<SPLIT>::STAGES, NT = TcCfg<SPLIT>::TILES;
     extern __shared__ __align__(16) unsigned char tc_smem_raw[];
     __shared__ __align__(8) uint64_t mbar[S];
@@ -168,10 +169,12 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
     const GemmTask t = tasks[tl.x];
     const int c = t.c, b = t.b, f = t.f;
     const int K = m.width[c], ld = m.ld[c];
-    const int N = m.blrow[b] - m.bfrow[b] + 1;
+    const bool trsm = (t.flags & 64) != 0;
+    const int N = trsm ? K : m.blrow[b] - m.bfrow[b] + 1;
     const int i0 = tl.y * TC_BM, j0 = tl.z * TC_BN;
     const float *A = ((t.flags & 1) ? coefU : coefL) + m.coefoff[c] + (int64_t)(t.arow0 + i0) * ld;
-    const float *B = ((t.flags & 2) ? coefU : coefL) + m.coefoff[c] + (int64_t)(m.browoff[b] + j0) * ld;
+    const float *B = trsm ? inv + m.invoff[c] + (int64_t)j0 * ld
+                          : ((t.flags & 2) ? coefU : coefL) + m.coefoff[c] + (int64_t)(m.browoff[b] + j0) * ld;
     const int mrows = min(TC_BM, t.M - i0), ncols = min(TC_BN, N - j0);
     const int nk = (K + TC_BK - 1) / TC_BK;
 
@@ -188,7 +191,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
     }
     {
         int tr = -1;
-        if (tid < mrows) tr = panel_row_of(m, f, m.rowidx[m.rowbase[c] + t.arow0 + i0 + tid]);
+        if (tid < mrows && !trsm) tr = panel_row_of(m, f, m.rowidx[m.rowbase[c] + t.arow0 + i0 + tid]);
         trow_s[tid] = tr;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -331,6 +334,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
     if (!fail_s) {
         // epilogue: TMEM -> registers -> transpose in shared memory -> atomics
         float *E = reinterpret_cast<float *>(sbase) + warp * 32 * 33;
+        float *O = trsm ? scr + t.out + (int64_t)i0 * ld + j0 : nullptr;
         float *C = ((t.flags & 4) ? coefU : coefL) + m.coefoff[f];
         const int ldf = m.ld[f], wf = m.width[f];
         const int tcol0 = m.bfrow[b] + j0 - m.fcol[f];
@@ -343,7 +347,13 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
             for (int q = 0; q < 32; q++) E[lane * 33 + q] = __uint_as_float(v[q]);
             __syncwarp();
             const int j = cb + lane;
-            if (j < ncols) {
+            if (j < ncols && trsm) {
+                for (int rr = 0; rr < 32; rr++) {
+                    const int i = warp * 32 + rr;
+                    if (i >= mrows) break;
+                    O[(int64_t)i * ld + j] = E[rr * 33 + lane];
+                }
+            } else if (j < ncols) {
                 const int tc = tcol0 + j;
                 for (int rr = 0; rr < 32; rr++) {
                     const int i = warp * 32 + rr;
@@ -414,25 +424,30 @@ __device__ __forceinline__ void mbar_arrive(uint32_t addr) {
 
 struct TcTileView {
     const float *A, *B;
-    int mrows, ncols, K, nk, flags, c, b, f, arow, j0;
+    int mrows, ncols, K, nk, flags, c, b, f, arow, j0, i0;
+    int64_t out;
 };
 
 __device__ __forceinline__ TcTileView tc_tile_view(const Meta &m, const int4 tl, const GemmTask *tasks,
-                                                   const float *coefL, const float *coefU) {
+                                                   const float *coefL, const float *coefU, const float *inv) {
     const GemmTask t = tasks[tl.x];
     TcTileView v;
     v.c = t.c;
     v.b = t.b;
     v.f = t.f;
     v.flags = t.flags;
+    v.out = t.out;
     v.K = m.width[t.c];
     const int ld = m.ld[t.c];
-    const int N = m.blrow[t.b] - m.bfrow[t.b] + 1;
+    const bool trsm = (t.flags & 64) != 0;
+    const int N = trsm ? v.K : m.blrow[t.b] - m.bfrow[t.b] + 1;
     const int i0 = tl.y * TC_BM;
+    v.i0 = i0;
     v.j0 = tl.z * TC_BN;
     v.arow = t.arow0 + i0;
     v.A = ((t.flags & 1) ? coefU : coefL) + m.coefoff[t.c] + (int64_t)(t.arow0 + i0) * ld;
-    v.B = ((t.flags & 2) ? coefU : coefL) + m.coefoff[t.c] + (int64_t)(m.browoff[t.b] + v.j0) * ld;
+    v.B = trsm ? inv + m.invoff[t.c] + (int64_t)v.j0 * ld
+               : ((t.flags & 2) ? coefU : coefL) + m.coefoff[t.c] + (int64_t)(m.browoff[t.b] + v.j0) * ld;
     v.mrows = min(TC_BM, t.M - i0);
     v.ncols = min(TC_BN, N - v.j0);
     v.nk = (v.K + TC_BK - 1) / TC_BK;
@@ -443,7 +458,8 @@ template <bool SPLIT>
 __global__ void __launch_bounds__(TCP_THREADS, 1)
     k_gemm_scatter_tc_persistent(Meta m, const int4 *__restrict__ tiles, int ntiles,
                                  const GemmTask *__restrict__ tasks, float *__restrict__ coefL,
-                                 float *__restrict__ coefU, Status *st) {
+                                 float *__restrict__ coefU, Status *st, const float *__restrict__ inv,
+                                 float *__restrict__ scr) {
     constexpr int S = TcpCfg<SPLIT>::STAGES, NT = TcpCfg<SPLIT>::TILES;
     extern __shared__ __align__(16) unsigned char tc_smem_raw[];
     __shared__ __align__(8) uint64_t full[S], empty[S], accf[2], acce[2], drained;
@@ -489,7 +505,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
         constexpr int CH = (TC_BM * 8) / 128;          // 8 chunks of 16 B per operand per thread
         int it = 0;
         for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x) {
-            const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU);
+            const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU, inv);
             const int ld = m.ld[v.c];
             for (int kb = 0; kb < v.nk; kb++, it++) {
                 const int s = it % S;
@@ -540,7 +556,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
             const uint32_t idesc = tc_idesc();
             int it = 0, tl = 0;
             for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x, tl++) {
-                const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU);
+                const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU, inv);
                 const int ab = tl & 1;
                 const uint32_t acc = tmem + (uint32_t)(ab * 128);
                 if (tl >= 2 && !mbar_wait(smem_u32(&acce[ab]), (uint32_t)((tl / 2 - 1) & 1))) {
@@ -589,12 +605,13 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
         float *E = epi + warp * 32 * 33;
         int tl = 0;
         for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x, tl++) {
-            const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU);
+            const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU, inv);
             const int ab = tl & 1;
             // target panel row of my accumulator row (binary search in f's blocks)
             const int myrow = warp * 32 + lane;
+            const bool trsm = (v.flags & 64) != 0;
             int tr = -1;
-            if (myrow < v.mrows) tr = panel_row_of(m, v.f, m.rowidx[m.rowbase[v.c] + v.arow + myrow]);
+            if (myrow < v.mrows && !trsm) tr = panel_row_of(m, v.f, m.rowidx[m.rowbase[v.c] + v.arow + myrow]);
             if (!mbar_wait(smem_u32(&accf[ab]), (uint32_t)((tl / 2) & 1))) {
                 atomicExch(&fail_s, 1);
                 break;
@@ -614,7 +631,15 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
                 for (int q = 0; q < 32; q++) E[lane * 33 + q] = __uint_as_float(r[q]);
                 __syncwarp();
                 const int j = cb + lane;
-                if (j < v.ncols) {
+                if (j < v.ncols && trsm) {
+                    const int ldc = m.ld[v.c];
+                    float *O = scr + v.out + (int64_t)v.i0 * ldc + v.j0;
+                    for (int rr = 0; rr < 32; rr++) {
+                        const int i = warp * 32 + rr;
+                        if (i >= v.mrows) break;
+                        O[(int64_t)i * ldc + j] = E[rr * 33 + lane];
+                    }
+                } else if (j < v.ncols) {
                     const int tc = tcol0 + j;
                     for (int rr = 0; rr < 32; rr++) {
                         const int i = warp * 32 + rr;

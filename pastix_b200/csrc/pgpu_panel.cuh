@@ -362,3 +362,99 @@ __global__ void __launch_bounds__(256) k_trsm_rows(Meta m, const int4 *__restric
 }
 
 }  // namespace pgpu
+
+namespace pgpu {
+
+// ---------------------------------------------------------------------------
+// Inverse of the factorized diagonal block, for the panel TRSM done as a
+// GEMM (X = A_off B^t with B the inverse below, on the tensor cores for the
+// single-precision factors).  B = op(L_kk)^{-1} row-major in the inverse
+// workspace (inv + invoff[c], row stride ld_c), op = conj when cjp; for LDL
+// (unit L) each row n is divided by d_n, so that X = A (D op(L)^t)^{-1}.
+// The strict upper part of B is left untouched (zero from the allocation).
+// One CTA per (cblk, 32-column block jb): columns [jb, jb+32) of the
+// inverse by blocked forward substitution over the 32-row tiles below jb.
+// Shared memory: X[w - jb][33] + Lb[32][33].
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restrict__ jobs,
+                                                     const T *__restrict__ coefL, T *__restrict__ inv,
+                                                     int unit, int cjp, int scale_d) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int2 jbv = jobs[blockIdx.x];
+    const int c = jbv.x, jb = jbv.y;
+    const int w = m.width[c], ld = m.ld[c];
+    const int nb = min(PB, w - jb), nrow = w - jb;
+    const T *D = coefL + m.coefoff[c];
+    T *Inv = inv + m.invoff[c];
+    T *X = reinterpret_cast<T *>(smem_raw);   // [nrow][PBL]
+    T *Lb = X + (size_t)nrow * PBL;           // [PB][PBL]
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < nrow * PB; e += nt) {
+        const int i = e / PB, q = e - i * PB;
+        X[i * PBL + q] = (i == q && q < nb) ? T(1) : T(0);
+    }
+    __syncthreads();
+    for (int ib = jb; ib < w; ib += PB) {
+        const int nbi = min(PB, w - ib);
+        // (1) X[ib..] -= L[ib.., jb..ib) X[jb..ib)
+        for (int kb = jb; kb < ib; kb += PB) {
+            for (int e = tid; e < nbi * PB; e += nt) {
+                const int r = e / PB, k = e - r * PB;
+                const T v = D[(int64_t)(ib + r) * ld + kb + k];
+                Lb[r * PBL + k] = cjp ? conj_v(v) : v;
+            }
+            __syncthreads();
+            for (int e = tid; e < nbi * nb; e += nt) {
+                const int r = e / nb, q = e - r * nb;
+                T s = T(0);
+#pragma unroll 8
+                for (int k = 0; k < PB; k++) s += Lb[r * PBL + k] * X[(kb - jb + k) * PBL + q];
+                X[(ib - jb + r) * PBL + q] -= s;
+            }
+            __syncthreads();
+        }
+        // (2) X[ib..ib+nbi) = L_tile^{-1} X[ib..ib+nbi), one lane per column
+        for (int e = tid; e < nbi * nbi; e += nt) {
+            const int r = e / nbi, k = e - r * nbi;
+            const T v = D[(int64_t)(ib + r) * ld + ib + k];
+            Lb[r * PBL + k] = cjp ? conj_v(v) : v;
+        }
+        __syncthreads();
+        if (tid < nb) {
+            const int q = tid;
+            for (int r = 0; r < nbi; r++) {
+                T s = X[(ib - jb + r) * PBL + q];
+                for (int k = 0; k < r; k++) s -= Lb[r * PBL + k] * X[(ib - jb + k) * PBL + q];
+                X[(ib - jb + r) * PBL + q] = unit ? s : s * (T(1) / Lb[r * PBL + r]);
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < nrow * nb; e += nt) {
+        const int i = e / nb, q = e - i * nb;
+        T v = X[i * PBL + q];
+        if (scale_d) v = v * (T(1) / D[(int64_t)(jb + i) * ld + jb + i]);
+        Inv[(int64_t)(jb + i) * ld + jb + q] = v;
+    }
+}
+
+// Copy the TRSM result (X of the GEMM, in the level's scratch at scroff[c],
+// row stride ld_c) back into the off-diagonal rows of the panel.  One CTA per
+// TRSM chunk {cblk, first row, panel, mode} of 32 rows.
+template <typename T>
+__global__ void k_trsm_copyback(Meta m, const int4 *__restrict__ chunks, const int64_t *__restrict__ scroff,
+                                const T *__restrict__ scr, T *__restrict__ coefL) {
+    const int4 ch = chunks[blockIdx.x];
+    const int c = ch.x, r0 = ch.y;
+    const int w = m.width[c], h = m.height[c], ld = m.ld[c];
+    const int nr = min(32, h - r0);
+    const T *src = scr + scroff[c] + (int64_t)(r0 - w) * ld;
+    T *dst = coefL + m.coefoff[c] + (int64_t)r0 * ld;
+    for (int e = threadIdx.x; e < nr * w; e += blockDim.x) {
+        const int i = e / w, j = e - i * w;
+        dst[(int64_t)i * ld + j] = src[(int64_t)i * ld + j];
+    }
+}
+
+}  // namespace pgpu
