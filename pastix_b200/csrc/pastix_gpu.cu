@@ -519,11 +519,11 @@ static bool trsm_gemm_enabled() {
 static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     const bool use_tc = fp32 && !zc && tc_enabled() && (fmode == FM_POTRF || fmode == FM_GETRF);
     const bool lu = (fmode == FM_GETRF), ldl = fm_ldl(fmode);
-    const bool tgemm = !lu && !C.record && trsm_gemm_enabled();
+    const bool tgemm = !C.record && trsm_gemm_enabled();
     const int key = ((((fmode * 2 + (fp32 ? 1 : 0)) * 2 + (use_tc ? 1 : 0)) * 2 + (zc ? 1 : 0)) * 2 + (tgemm ? 1 : 0));
     if (C.plan_fact == key) return PASTIX_GPU_SUCCESS;
     const size_t esz = (fp32 ? 4 : 8) * (zc ? 2 : 1);
-    const int fuse = tgemm ? TRSM_GEMM_ROWS : fuse_rows_for(lu, esz);
+    const int fuse = tgemm ? std::min(TRSM_GEMM_ROWS, fuse_rows_for(lu, esz)) : fuse_rows_for(lu, esz);
     const bool tc_trsm = tgemm && fp32 && !zc && tc_enabled();
     std::vector<int2> invjobs;
     std::vector<int4> ttiles, tttiles;
@@ -556,21 +556,26 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
                     trsm.push_back(make_int4(c, r0, 0, lu ? 1 : (ldl ? 3 : 0)));
                     if (lu) trsm.push_back(make_int4(c, r0, 1, 2));
                 }
-            if (h > fuse && tgemm) {
+            if (h > fuse && h > w && tgemm) {
                 // inverse of the diagonal block, then X = A_off B^t into the scratch
+                // (LU: two inverses and two outputs, the L and the U^t side)
+                const int sides = lu ? 2 : 1;
                 C.invoff[c] = inv_elems;
-                inv_elems += round_up((int64_t)w * C.ld[c], 32);
-                for (int jb = 0; jb < w; jb += PB) invjobs.push_back(make_int2(c, jb));
+                inv_elems += sides * inv_span(w, C.ld[c]);
+                for (int kind = 0; kind < sides; kind++)
+                    for (int jb = 0; jb < w; jb += PB) invjobs.push_back(make_int2(c, jb + (kind << 20)));
                 C.scroff[c] = scr_lvl;
-                scr_lvl += round_up((int64_t)(h - w) * C.ld[c], 32);
-                const int id = (int)tasks.size();
-                GemmTask g{c, C.fblok[c], c, w, h - w, 64, 0};
-                g.out = C.scroff[c];
-                tasks.push_back(g);
-                const int bm = tc_trsm ? TC_BM : GEMM_TM, bn = tc_trsm ? TC_BN : GEMM_TN;
-                for (int tm = 0; tm < cdiv(h - w, bm); tm++)
-                    for (int tn = 0; tn < cdiv(w, bn); tn++)
-                        (tc_trsm ? tttiles : ttiles).push_back(make_int4(id, tm, tn, 0));
+                scr_lvl += sides * inv_span(h - w, C.ld[c]);
+                for (int side = 0; side < sides; side++) {
+                    const int id = (int)tasks.size();
+                    GemmTask g{c, C.fblok[c], c, w, h - w, side ? (64 | 128 | 1) : 64, 0};
+                    g.out = C.scroff[c] + (side ? inv_span(h - w, C.ld[c]) : 0);
+                    tasks.push_back(g);
+                    const int bm = tc_trsm ? TC_BM : GEMM_TM, bn = tc_trsm ? TC_BN : GEMM_TN;
+                    for (int tm = 0; tm < cdiv(h - w, bm); tm++)
+                        for (int tn = 0; tn < cdiv(w, bn); tn++)
+                            (tc_trsm ? tttiles : ttiles).push_back(make_int4(id, tm, tn, 0));
+                }
             }
             const int b1 = C.fblok[c + 1];
             for (int b = C.fblok[c] + 1; b < b1; b++) {
@@ -758,7 +763,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             PGPU_CHECK(tm.mark(PH_TRSM));
             k_tri_inverse<T><<<nij, 256, ism, s>>>(C.meta, C.d_invjobs.p + C.inv_ptr[l], coefL, inv,
                                                    fm_ldl(fmode) ? 1 : 0, (CPX && fm_conj(fmode)) ? 1 : 0,
-                                                   fm_ldl(fmode) ? 1 : 0);
+                                                   fm_ldl(fmode) ? 1 : 0, lu ? 1 : 0);
             nl++;
             const int ntt = C.ttile_ptr[l + 1] - C.ttile_ptr[l];
             if (ntt) {
@@ -781,7 +786,8 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                     nl++;
                 }
             }
-            k_trsm_copyback<T><<<ntr, 256, 0, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], C.d_scroff.p, scr, coefL);
+            k_trsm_copyback<T><<<ntr, 256, 0, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], C.d_scroff.p, scr, coefL,
+                                                   coefU);
             nl++;
         } else if (ntr) {
             const size_t fixed = ((size_t)TRSM_TR * (mw + 1) + PB * PBL) * sizeof(T);
@@ -977,21 +983,37 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
     LaunchTimer tm(C);
     auto mark = [&](int k) { return prof ? tm.mark(k) : cudaSuccess; };
     // staged-panel rows of the diagonal kernels that fit next to the RHS block
-    auto diag_smem = [&](int mw, int *pch) {
-        const size_t fixed = ((size_t)mw * nrhs + 32 * 33) * sizeof(T);
-        const size_t room = fixed < (size_t)SMEM_LIMIT ? (SMEM_LIMIT - fixed) / (33 * sizeof(T)) : 0;
-        *pch = (int)std::min<size_t>(std::max(mw, 1), room);
-        return fixed + (size_t)(*pch) * 33 * sizeof(T);
+    // and, on levels with diagonal-block inverses (panel TRSM done as a GEMM),
+    // the rows of the inverse staged per chunk (ipch rows x w)
+    static const bool inv_solve = !(getenv("PASTIX_GPU_SOLVE_INV") && std::strcmp(getenv("PASTIX_GPU_SOLVE_INV"), "0") == 0);
+    const T *inv = (C.trsm_gemm && inv_solve) ? reinterpret_cast<const T *>(C.d_inv.p) : nullptr;
+    auto diag_smem = [&](int l, int mw, int *pch, int *ipch) {
+        const size_t es = sizeof(T);
+        const size_t fixed = ((size_t)mw * nrhs + 32 * 33) * es;
+        size_t dsm;
+        *ipch = 0;
+        if (inv && C.inv_ptr[l + 1] > C.inv_ptr[l]) {
+            const size_t fixed_i = (size_t)2 * mw * nrhs * es;
+            dsm = std::min<size_t>(SMEM_LIMIT, std::max(fixed_i + (size_t)64 * mw * es, fixed + (size_t)mw * 33 * es));
+            *ipch = dsm > fixed_i ? (int)std::min<size_t>(mw, (dsm - fixed_i) / ((size_t)mw * es)) : 0;
+        } else {
+            dsm = std::min<size_t>(SMEM_LIMIT, fixed + (size_t)std::max(mw, 1) * 33 * es);
+        }
+        *pch = dsm > fixed ? (int)std::min<size_t>(std::max(mw, 1), (dsm - fixed) / (33 * es)) : 0;
+        return dsm;
     };
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
         int pch = 0;
-        const size_t dsm = diag_smem(mw, &pch);
-        if (pch < std::min(32, mw)) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+        int ipch = 0;
+        const size_t dsm = diag_smem(l, mw, &pch, &ipch);
+        if (pch < std::min(32, mw) || (inv && C.inv_ptr[l + 1] > C.inv_ptr[l] && ipch < 1))
+            return PASTIX_GPU_ERR_NOTIMPLEMENTED;
         PGPU_CHECK(mark(0));
         k_fwd_diag<T><<<ncb, 256, dsm, s>>>(
-            C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs, (lu || ldl) ? 1 : 0, pch);
+            C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs, (lu || ldl) ? 1 : 0, pch, inv,
+            ldl ? 1 : 0, cjp, ipch);
         nl++;
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
@@ -1018,10 +1040,11 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
             nl++;
         }
         int pch = 0;
-        const size_t dsm = diag_smem(mw, &pch);
+        int ipch = 0;
+        const size_t dsm = diag_smem(l, mw, &pch, &ipch);
         PGPU_CHECK(mark(4));
         k_bwd_diag<T><<<ncb, 256, dsm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs,
-                                            lu ? 1 : 0, ldl ? 1 : 0, lu ? 0 : cjp, pch);
+                                            lu ? 1 : 0, ldl ? 1 : 0, lu ? 0 : cjp, pch, inv, ldl ? 1 : 0, ipch);
         nl++;
     }
     PGPU_CHECK(cudaGetLastError());

@@ -43,6 +43,10 @@ enum FactMode { FM_POTRF = 0, FM_GETRF = 1, FM_SYTRF = 2, FM_HETRF = 3 };
 __host__ __device__ constexpr bool fm_conj(int mode) { return mode == FM_POTRF || mode == FM_HETRF; }
 __host__ __device__ constexpr bool fm_ldl(int mode) { return mode == FM_SYTRF || mode == FM_HETRF; }
 
+// Elements between the two diagonal-block inverses of an LU cblk (and
+// between its L- and U-side TRSM outputs in the scratch): w x ld rounded to 32.
+__host__ __device__ inline int64_t inv_span(int64_t rows, int64_t ld) { return (rows * ld + 31) / 32 * 32; }
+
 // Error/status word written by kernels (never traps): bit flags + counters.
 struct Status {
     int nbpivots;      // static pivots applied
@@ -146,6 +150,27 @@ __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+// Block-cooperative copy of `total` elements, element e read by src(e) and
+// written by dst(e, v), U loads in flight per thread: the loads of a batch
+// are issued before any of their stores, so a global -> shared staging loop
+// costs one memory latency per U elements instead of one per element.
+template <int U = 8, typename Src, typename Dst>
+__device__ __forceinline__ void batched_copy(int total, int tid, int nt, Src src, Dst dst) {
+    for (int e0 = tid; e0 < total; e0 += nt * U) {
+        decltype(src(0)) r[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int e = e0 + u * nt;
+            if (e < total) r[u] = src(e);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int e = e0 + u * nt;
+            if (e < total) dst(e, r[u]);
+        }
+    }
 }
 
 // Panel row of global row r inside cblk f: binary search over f's blocks

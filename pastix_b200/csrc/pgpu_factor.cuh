@@ -53,7 +53,7 @@ __global__ void k_fillin(int64_t nnz, const Tin *__restrict__ vals,
 // 64 panel TRSM as a GEMM: X = A B^t with A the off-diagonal rows of c
 //    (arow0 = w_c, M = h_c - w_c), B the inverse of its diagonal block
 //    (inv + invoff[c], N = K = w_c), X stored (not accumulated) at scr + out
-//    with row stride ld_c.
+//    with row stride ld_c; 128: B is the cblk's second inverse (LU U^t side).
 // ---------------------------------------------------------------------------
 constexpr int GEMM_TM = 64, GEMM_TN = 64, GEMM_TK = 16;
 
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256) k_gemm_scatter(Meta m, const int4 *__rest
     const int N = trsm ? K : m.blrow[b] - m.bfrow[b] + 1;
     const int i0 = tl.y * GEMM_TM, j0 = tl.z * GEMM_TN;
     const T *A = ((t.flags & 1) ? coefU : coefL) + m.coefoff[c] + (int64_t)(t.arow0 + i0) * ld;
-    const T *B = trsm ? inv + m.invoff[c] + (int64_t)j0 * ld
+    const T *B = trsm ? inv + m.invoff[c] + ((t.flags & 128) ? inv_span(K, ld) : 0) + (int64_t)j0 * ld
                       : ((t.flags & 2) ? coefU : coefL) + m.coefoff[c] + (int64_t)(m.browoff[b] + j0) * ld;
     const int mrows = min(GEMM_TM, t.M - i0), ncols = min(GEMM_TN, N - j0);
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;

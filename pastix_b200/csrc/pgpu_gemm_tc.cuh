@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
     const int N = trsm ? K : m.blrow[b] - m.bfrow[b] + 1;
     const int i0 = tl.y * TC_BM, j0 = tl.z * TC_BN;
     const float *A = ((t.flags & 1) ? coefU : coefL) + m.coefoff[c] + (int64_t)(t.arow0 + i0) * ld;
-    const float *B = trsm ? inv + m.invoff[c] + (int64_t)j0 * ld
+    const float *B = trsm ? inv + m.invoff[c] + ((t.flags & 128) ? inv_span(K, ld) : 0) + (int64_t)j0 * ld
                           : ((t.flags & 2) ? coefU : coefL) + m.coefoff[c] + (int64_t)(m.browoff[b] + j0) * ld;
     const int mrows = min(TC_BM, t.M - i0), ncols = min(TC_BN, N - j0);
     const int nk = (K + TC_BK - 1) / TC_BK;
@@ -446,7 +446,7 @@ __device__ __forceinline__ TcTileView tc_tile_view(const Meta &m, const int4 tl,
     v.j0 = tl.z * TC_BN;
     v.arow = t.arow0 + i0;
     v.A = ((t.flags & 1) ? coefU : coefL) + m.coefoff[t.c] + (int64_t)(t.arow0 + i0) * ld;
-    v.B = trsm ? inv + m.invoff[t.c] + (int64_t)v.j0 * ld
+    v.B = trsm ? inv + m.invoff[t.c] + ((t.flags & 128) ? inv_span(v.K, ld) : 0) + (int64_t)v.j0 * ld
                : ((t.flags & 2) ? coefU : coefL) + m.coefoff[t.c] + (int64_t)(m.browoff[t.b] + v.j0) * ld;
     v.mrows = min(TC_BM, t.M - i0);
     v.ncols = min(TC_BN, N - v.j0);

@@ -178,13 +178,12 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
     for (int jb = 0; jb < w; jb += PB) {
         const int nb = min(PB, w - jb);
         const int r1 = jb + nb;              // first row / column after the tile
-        // 1. diagonal tile
+        // 1. diagonal tile (loaded by the whole CTA, factorized by warp 0)
+        batched_copy(
+            nb * nb, tid, nt, [&](int e) { const int i = e / nb, j = e - i * nb; return A[(int64_t)(jb + i) * ld + jb + j]; },
+            [&](int e, T v) { const int i = e / nb, j = e - i * nb; tile[i * PBL + j] = v; });
+        __syncthreads();
         if (tid < 32) {
-            for (int e = tid; e < nb * nb; e += 32) {
-                const int i = e / nb, j = e - i * nb;
-                tile[i * PBL + j] = A[(int64_t)(jb + i) * ld + jb + j];
-            }
-            __syncwarp();
             warp_factor_tile<T, MODE>(tile, nb, crit, npiv, nneg, nbad);
             for (int e = tid; e < nb * nb; e += 32) {
                 const int i = e / nb, j = e - i * nb;
@@ -305,16 +304,14 @@ __global__ void __launch_bounds__(256) k_trsm_rows(Meta m, const int4 *__restric
     const int tid = threadIdx.x, nt = blockDim.x;
     const bool cjl = CJ && mode != 2;      // conjugate the L coefficients
     const uint64_t t_start = prof ? global_ns() : 0;
-    for (int e = tid; e < nrows * w; e += nt) {
-        const int i = e / w, j = e - i * w;
-        X[i * xl + j] = Pan[(int64_t)i * ld + j];
-    }
+    batched_copy(
+        nrows * w, tid, nt, [&](int e) { const int i = e / w, j = e - i * w; return Pan[(int64_t)i * ld + j]; },
+        [&](int e, T v) { const int i = e / w, j = e - i * w; X[i * xl + j] = v; });
     for (int jb = 0; jb < w; jb += PB) {
         const int nb = min(PB, w - jb), r1 = jb + nb, ncol = w - r1;
-        for (int e = tid; e < nb * nb; e += nt) {
-            const int i = e / nb, j = e - i * nb;
-            tile[i * PBL + j] = D[(int64_t)(jb + i) * ld + jb + j];
-        }
+        batched_copy(
+            nb * nb, tid, nt, [&](int e) { const int i = e / nb, j = e - i * nb; return D[(int64_t)(jb + i) * ld + jb + j]; },
+            [&](int e, T v) { const int i = e / nb, j = e - i * nb; tile[i * PBL + j] = v; });
         __syncthreads();
         for (int i = tid; i < nrows; i += nt) {
             T x[PB];
@@ -331,16 +328,16 @@ __global__ void __launch_bounds__(256) k_trsm_rows(Meta m, const int4 *__restric
         for (int cc0 = 0; cc0 < ncol; cc0 += pch) {
             const int nc2 = min(pch, ncol - cc0);
             // coefficients of the trailing update, P[col - r1 - cc0][l]
-            for (int e = tid; e < nc2 * nb; e += nt) {
-                const int cc = e / nb, l = e - cc * nb;
-                const int col = r1 + cc0 + cc;
-                if (mode == 1) {
-                    P[cc * PBL + l] = D[(int64_t)(jb + l) * ld + col];      // U[jb+l][col]
-                } else {
+            batched_copy(
+                nc2 * nb, tid, nt,
+                [&](int e) {
+                    const int cc = e / nb, l = e - cc * nb;
+                    const int col = r1 + cc0 + cc;
+                    if (mode == 1) return D[(int64_t)(jb + l) * ld + col];  // U[jb+l][col]
                     const T v = D[(int64_t)col * ld + jb + l];             // L[col][jb+l]
-                    P[cc * PBL + l] = cjl ? conj_v(v) : v;
-                }
-            }
+                    return cjl ? conj_v(v) : v;
+                },
+                [&](int e, T v) { const int cc = e / nb, l = e - cc * nb; P[cc * PBL + l] = v; });
             __syncthreads();
             tile_update<T, false>(X + r1 + cc0, xl, X + jb, xl, P, PBL, nrows, nc2, nb, -1);
             __syncthreads();
@@ -376,17 +373,23 @@ namespace pgpu {
 // inverse by blocked forward substitution over the 32-row tiles below jb.
 // Shared memory: X[w - jb][33] + Lb[32][33].
 // ---------------------------------------------------------------------------
+// LU (lu != 0): job.y = jb + (kind << 20); kind 0 inverts U^t (the upper
+// triangle of the diagonal block read transposed, non-unit) into the first
+// slot -- B of the L-side TRSM, X = A U^{-1} -- and kind 1 the unit lower L
+// into the second slot (inv_span further) -- B of the U^t-side TRSM.
 template <typename T>
 __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restrict__ jobs,
                                                      const T *__restrict__ coefL, T *__restrict__ inv,
-                                                     int unit, int cjp, int scale_d) {
+                                                     int unit, int cjp, int scale_d, int lu) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int2 jbv = jobs[blockIdx.x];
-    const int c = jbv.x, jb = jbv.y;
+    const int c = jbv.x, jb = jbv.y & 0xFFFFF, kind = jbv.y >> 20;
     const int w = m.width[c], ld = m.ld[c];
     const int nb = min(PB, w - jb), nrow = w - jb;
     const T *D = coefL + m.coefoff[c];
-    T *Inv = inv + m.invoff[c];
+    T *Inv = inv + m.invoff[c] + (kind ? inv_span(w, ld) : 0);
+    const bool tr = lu && kind == 0;      // U^t: element (r, k) read at D[k][r]
+    if (lu) unit = kind;
     T *X = reinterpret_cast<T *>(smem_raw);   // [nrow][PBL]
     T *Lb = X + (size_t)nrow * PBL;           // [PB][PBL]
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -399,11 +402,14 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
         const int nbi = min(PB, w - ib);
         // (1) X[ib..] -= L[ib.., jb..ib) X[jb..ib)
         for (int kb = jb; kb < ib; kb += PB) {
-            for (int e = tid; e < nbi * PB; e += nt) {
-                const int r = e / PB, k = e - r * PB;
-                const T v = D[(int64_t)(ib + r) * ld + kb + k];
-                Lb[r * PBL + k] = cjp ? conj_v(v) : v;
-            }
+            batched_copy(
+                nbi * PB, tid, nt,
+                [&](int e) {
+                    const int r = e / PB, k = e - r * PB;
+                    const T v = tr ? D[(int64_t)(kb + k) * ld + ib + r] : D[(int64_t)(ib + r) * ld + kb + k];
+                    return cjp ? conj_v(v) : v;
+                },
+                [&](int e, T v) { const int r = e / PB, k = e - r * PB; Lb[r * PBL + k] = v; });
             __syncthreads();
             for (int e = tid; e < nbi * nb; e += nt) {
                 const int r = e / nb, q = e - r * nb;
@@ -415,11 +421,14 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
             __syncthreads();
         }
         // (2) X[ib..ib+nbi) = L_tile^{-1} X[ib..ib+nbi), one lane per column
-        for (int e = tid; e < nbi * nbi; e += nt) {
-            const int r = e / nbi, k = e - r * nbi;
-            const T v = D[(int64_t)(ib + r) * ld + ib + k];
-            Lb[r * PBL + k] = cjp ? conj_v(v) : v;
-        }
+        batched_copy(
+            nbi * nbi, tid, nt,
+            [&](int e) {
+                const int r = e / nbi, k = e - r * nbi;
+                const T v = tr ? D[(int64_t)(ib + k) * ld + ib + r] : D[(int64_t)(ib + r) * ld + ib + k];
+                return cjp ? conj_v(v) : v;
+            },
+            [&](int e, T v) { const int r = e / nbi, k = e - r * nbi; Lb[r * PBL + k] = v; });
         __syncthreads();
         if (tid < nb) {
             const int q = tid;
@@ -442,19 +451,20 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
 // Copy the TRSM result (X of the GEMM, in the level's scratch at scroff[c],
 // row stride ld_c) back into the off-diagonal rows of the panel.  One CTA per
 // TRSM chunk {cblk, first row, panel, mode} of 32 rows.
+// For LU the U^t rows (panel 1) come from the second half of the cblk's
+// scratch (inv_span(h - w, ld) further) and go to the U coeftab.
 template <typename T>
 __global__ void k_trsm_copyback(Meta m, const int4 *__restrict__ chunks, const int64_t *__restrict__ scroff,
-                                const T *__restrict__ scr, T *__restrict__ coefL) {
+                                const T *__restrict__ scr, T *__restrict__ coefL, T *__restrict__ coefU) {
     const int4 ch = chunks[blockIdx.x];
     const int c = ch.x, r0 = ch.y;
     const int w = m.width[c], h = m.height[c], ld = m.ld[c];
     const int nr = min(32, h - r0);
-    const T *src = scr + scroff[c] + (int64_t)(r0 - w) * ld;
-    T *dst = coefL + m.coefoff[c] + (int64_t)r0 * ld;
-    for (int e = threadIdx.x; e < nr * w; e += blockDim.x) {
-        const int i = e / w, j = e - i * w;
-        dst[(int64_t)i * ld + j] = src[(int64_t)i * ld + j];
-    }
+    const T *src = scr + scroff[c] + (ch.z ? inv_span(h - w, ld) : 0) + (int64_t)(r0 - w) * ld;
+    T *dst = (ch.z ? coefU : coefL) + m.coefoff[c] + (int64_t)r0 * ld;
+    batched_copy(
+        nr * w, threadIdx.x, blockDim.x, [&](int e) { const int i = e / w, j = e - i * w; return src[(int64_t)i * ld + j]; },
+        [&](int e, T v) { const int i = e / w, j = e - i * w; dst[(int64_t)i * ld + j] = v; });
 }
 
 }  // namespace pgpu

@@ -20,27 +20,89 @@ constexpr int SOLVE_MAXRHS = 16;
 // in shared memory with coalesced loads, pch rows at a time (one round of
 // loads per chunk instead of a serial chain of global loads per thread).
 // ---------------------------------------------------------------------------
+// Diagonal solve of a cblk whose factorization left the inverse of its
+// diagonal block (the panel TRSM done as a GEMM): Binv = op(L)^{-1}, each row
+// n divided by d_n for LDL.  Forward: y = L^{-1} b, y_n = sum_k
+// op(Binv[n][k] s_n) b_k (s_n = d_n for LDL, else 1); backward: x = op(L)^{-t} z,
+// x_k = sum_n Binv[n][k] s_n z_n.  The rows of Binv are staged in shared
+// memory pch rows at a time (coalesced), the dot products run from there:
+// one burst of loads per chunk instead of a chain per 32-column tile.
+template <typename T>
+__device__ void diag_solve_inverse(const T *__restrict__ Bi, const T *__restrict__ D, int w, int ld, int nrhs,
+                                   bool backward, bool ldl, bool cjp, T *__restrict__ v, T *__restrict__ outp,
+                                   T *__restrict__ P, int pch, T *__restrict__ Bg, int64_t ldb, int fc) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    // v: [w][nrhs] right-hand side in shared memory; outp: [w][nrhs] accumulators (backward)
+    if (backward)
+        for (int e = tid; e < w * nrhs; e += nt) outp[e] = T(0);
+    for (int n0 = 0; n0 < w; n0 += pch) {
+        const int nr = min(pch, w - n0), kmax = n0 + nr;     // rows n0..n0+nr, columns 0..kmax
+        __syncthreads();
+        batched_copy(
+            nr * kmax, tid, nt,
+            [&](int e) {
+                const int i = e / kmax, k = e - i * kmax;
+                T b = (k <= n0 + i) ? Bi[(int64_t)(n0 + i) * ld + k] : T(0);
+                if (ldl) b = b * D[(int64_t)(n0 + i) * ld + n0 + i];
+                return b;
+            },
+            [&](int e, T v) { P[e] = v; });
+        __syncthreads();
+        if (!backward) {
+            for (int e = tid; e < nr * nrhs; e += nt) {
+                const int i = e / nrhs, r = e - i * nrhs;
+                T s = T(0);
+                const T *row = P + (int64_t)i * kmax;
+#pragma unroll 4
+                for (int k = 0; k <= n0 + i; k++) s += (cjp ? conj_v(row[k]) : row[k]) * v[k * nrhs + r];
+                Bg[(int64_t)r * ldb + fc + n0 + i] = s;
+            }
+        } else {
+            for (int e = tid; e < kmax * nrhs; e += nt) {
+                const int k = e / nrhs, r = e - k * nrhs;
+                T s = T(0);
+#pragma unroll 4
+                for (int i = max(0, k - n0); i < nr; i++) s += P[(int64_t)i * kmax + k] * v[(n0 + i) * nrhs + r];
+                outp[e] += s;
+            }
+        }
+    }
+    if (backward) {
+        __syncthreads();
+        for (int e = tid; e < w * nrhs; e += nt) {
+            const int j = e / nrhs, r = e - j * nrhs;
+            Bg[(int64_t)r * ldb + fc + j] = outp[e];
+        }
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
-                                                  T *__restrict__ B, int ldb, int nrhs, int unit, int pch) {
+                                                  T *__restrict__ B, int ldb, int nrhs, int unit, int pch,
+                                                  const T *__restrict__ inv, int ldl, int cjp, int ipch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *y = reinterpret_cast<T *>(smem_raw);   // [w][nrhs]
     const int c = cblks[blockIdx.x];
     const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c];
     const T *D = coefL + m.coefoff[c];
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
-    for (int e = tid; e < w * nrhs; e += nt) {
-        int j = e / nrhs, r = e - j * nrhs;
-        y[e] = B[(int64_t)r * ldb + fc + j];
+    batched_copy(
+        w * nrhs, tid, nt, [&](int e) { const int j = e / nrhs, r = e - j * nrhs; return B[(int64_t)r * ldb + fc + j]; },
+        [&](int e, T v) { y[e] = v; });
+    if (inv && m.invoff[c] >= 0) {
+        // LU: the unit-lower inverse is the cblk's second one
+        __syncthreads();
+        diag_solve_inverse<T>(inv + m.invoff[c] + (unit && !ldl ? inv_span(w, ld) : 0), D, w, ld, nrhs, false,
+                              ldl != 0, cjp != 0, y, nullptr, y + (size_t)w * nrhs, ipch, B, ldb, fc);
+        return;
     }
     T *tile = y + w * nrhs;                   // [32][33] diagonal tile
     T *P = tile + 32 * 33;                    // [pch][33] column panel below the tile
     for (int jb = 0; jb < w; jb += 32) {
         const int nb = min(32, w - jb);
-        for (int e = tid; e < nb * nb; e += nt) {
-            const int i = e / nb, j = e - i * nb;
-            tile[i * 33 + j] = D[(int64_t)(jb + i) * ld + jb + j];
-        }
+        batched_copy(
+            nb * nb, tid, nt, [&](int e) { const int i = e / nb, j = e - i * nb; return D[(int64_t)(jb + i) * ld + jb + j]; },
+            [&](int e, T v) { const int i = e / nb, j = e - i * nb; tile[i * 33 + j] = v; });
         __syncthreads();
         if (tid < 32) {
             const T dinv = (lane < nb) ? T(1) / tile[lane * 33 + lane] : T(1);
@@ -57,10 +119,9 @@ __global__ void __launch_bounds__(256) k_fwd_diag(Meta m, const int *__restrict_
         __syncthreads();
         for (int r0 = jb + nb; r0 < w; r0 += pch) {
             const int nr = min(pch, w - r0);
-            for (int e = tid; e < nr * nb; e += nt) {
-                const int i = e / nb, l = e - i * nb;
-                P[i * 33 + l] = D[(int64_t)(r0 + i) * ld + jb + l];
-            }
+            batched_copy(
+                nr * nb, tid, nt, [&](int e) { const int i = e / nb, l = e - i * nb; return D[(int64_t)(r0 + i) * ld + jb + l]; },
+                [&](int e, T v) { const int i = e / nb, l = e - i * nb; P[i * 33 + l] = v; });
             __syncthreads();
             for (int e = tid; e < nr * nrhs; e += nt) {
                 const int i = e / nrhs, r = e - i * nrhs;
@@ -94,10 +155,9 @@ __global__ void k_fwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
     const int c = ch.x, r0 = ch.y;
     const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c], h = m.height[c];
     const int tid = threadIdx.x, nt = blockDim.x;
-    for (int e = tid; e < w * nrhs; e += nt) {
-        int r = e / w, j = e - r * w;
-        y[e] = B[(int64_t)r * ldb + fc + j];
-    }
+    batched_copy(
+        w * nrhs, tid, nt, [&](int e) { const int r = e / w, j = e - r * w; return B[(int64_t)r * ldb + fc + j]; },
+        [&](int e, T v) { y[e] = v; });
     __syncthreads();
     const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     const T *P = coef + m.coefoff[c];
@@ -163,27 +223,35 @@ __global__ void k_bwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
 template <typename T>
 __global__ void __launch_bounds__(256) k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
                                                   T *__restrict__ B, int ldb, int nrhs, int upper, int unit, int cjp,
-                                                  int pch) {
+                                                  int pch, const T *__restrict__ inv, int ldl, int ipch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *x = reinterpret_cast<T *>(smem_raw);   // [w][nrhs]
     const int c = cblks[blockIdx.x];
     const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c];
     const T *D = coefL + m.coefoff[c];
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
-    for (int e = tid; e < w * nrhs; e += nt) {
-        int j = e / nrhs, r = e - j * nrhs;
-        x[e] = B[(int64_t)r * ldb + fc + j];
+    batched_copy(
+        w * nrhs, tid, nt, [&](int e) { const int j = e / nrhs, r = e - j * nrhs; return B[(int64_t)r * ldb + fc + j]; },
+        [&](int e, T v) { x[e] = v; });
+    if (inv && m.invoff[c] >= 0) {
+        __syncthreads();
+        diag_solve_inverse<T>(inv + m.invoff[c], D, w, ld, nrhs, true, ldl != 0, false, x, x + (size_t)w * nrhs,
+                              x + (size_t)2 * w * nrhs, ipch, B, ldb, fc);
+        return;
     }
     T *tile = x + w * nrhs;                   // [32][33] diagonal tile (op applied)
     T *P = tile + 32 * 33;                    // [pch][33]: coefficients of the rows above
     const int nblk = (w + 31) / 32;
     for (int bi = nblk - 1; bi >= 0; bi--) {
         const int jb = bi * 32, nb = min(32, w - jb);
-        for (int e = tid; e < nb * nb; e += nt) {
-            const int i = e / nb, j = e - i * nb;
-            const T v = D[(int64_t)(jb + i) * ld + jb + j];
-            tile[i * 33 + j] = cjp ? conj_v(v) : v;
-        }
+        batched_copy(
+            nb * nb, tid, nt,
+            [&](int e) {
+                const int i = e / nb, j = e - i * nb;
+                const T v = D[(int64_t)(jb + i) * ld + jb + j];
+                return cjp ? conj_v(v) : v;
+            },
+            [&](int e, T v) { const int i = e / nb, j = e - i * nb; tile[i * 33 + j] = v; });
         __syncthreads();
         if (tid < 32) {
             const T dinv = (lane < nb && !unit) ? T(1) / tile[lane * 33 + lane] : T(1);
@@ -206,16 +274,18 @@ __global__ void __launch_bounds__(256) k_bwd_diag(Meta m, const int *__restrict_
             const int nr = min(pch, jb - r0);
             // P[i][l] = coefficient of x[jb + l] in row r0 + i
             if (upper) {
-                for (int e = tid; e < nr * nb; e += nt) {
-                    const int i = e / nb, l = e - i * nb;
-                    P[i * 33 + l] = D[(int64_t)(r0 + i) * ld + jb + l];
-                }
+                batched_copy(
+                    nr * nb, tid, nt, [&](int e) { const int i = e / nb, l = e - i * nb; return D[(int64_t)(r0 + i) * ld + jb + l]; },
+                    [&](int e, T v) { const int i = e / nb, l = e - i * nb; P[i * 33 + l] = v; });
             } else {
-                for (int e = tid; e < nr * nb; e += nt) {
-                    const int l = e / nr, i = e - l * nr;
-                    const T v = D[(int64_t)(jb + l) * ld + r0 + i];
-                    P[i * 33 + l] = cjp ? conj_v(v) : v;
-                }
+                batched_copy(
+                    nr * nb, tid, nt,
+                    [&](int e) {
+                        const int l = e / nr, i = e - l * nr;
+                        const T v = D[(int64_t)(jb + l) * ld + r0 + i];
+                        return cjp ? conj_v(v) : v;
+                    },
+                    [&](int e, T v) { const int l = e / nr, i = e - l * nr; P[i * 33 + l] = v; });
             }
             __syncthreads();
             for (int e = tid; e < nr * nrhs; e += nt) {

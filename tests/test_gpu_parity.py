@@ -16,6 +16,8 @@ CASES = [
     ("lap20", lambda: M.laplacian_7pt(20), "potrf"),
     ("diff14", lambda: M.diffusion_lognormal(14, 14, 14, 1.0, np.random.default_rng(3)), "potrf"),
     ("diff2d", lambda: M.diffusion_lognormal(40, 33, 1, 0.5, np.random.default_rng(4)), "potrf"),
+    # tall panels (TRSM as a GEMM, diagonal-block inverses in the solve) and a root wider than 256
+    ("diff26", lambda: M.diffusion_lognormal(26, 25, 24, 1.0, np.random.default_rng(12)), "potrf"),
     ("cd10", lambda: M.convdiff_upwind(10, 10, 10, 10.0), "getrf"),
     ("cd9x7x5", lambda: M.convdiff_upwind(9, 7, 5, 10.0), "getrf"),
 ]
