@@ -89,7 +89,14 @@ struct pastix_gpu_s {
     int64_t coefnbr = 0;      // elements of one (L or U) coeftab incl. padding
     int maxw = 0;
     int nlevels = 0;
-    std::vector<int> lvl_ptr, lvl_cblks, lvl_maxw;
+    std::vector<int> lvl_ptr, lvl_cblks, lvl_maxw, cblk_level;
+    // lookahead: the update tiles of a level that target the next level run
+    // on the main stream, the others on stream2, overlapping the panels of
+    // the levels that follow
+    cudaStream_t stream2 = nullptr;
+    std::vector<cudaEvent_t> la_events;
+    std::vector<int> tile_crit, tctile_crit;   // per level: critical (next-level) tiles first
+    double side_ms[4] = {0};                   // stream2 GEMM time of the last numfact, per phase
     double thflops[2][3] = {{0}};   // [complex][POTRF, GETRF, LDL] algorithmic flops
 
     // ---- device structure ----
@@ -131,7 +138,7 @@ struct pastix_gpu_s {
     std::vector<int64_t> seg;           // batch: first unknown of each system (+ n), empty if none
     DArr<int64_t> d_seg;
     DArr<double> d_segss;               // per-system sums of squares
-    std::vector<cudaEvent_t> evpool;   // per-launch timing events
+    std::vector<cudaEvent_t> evpool, evpool2;   // per-launch timing events (main, stream2)
     DArr<double> d_fact_scal;          // [0] ||A||_F, [1] static-pivot threshold (device-side, no host trip)
     // per-task timings of the last numfact (learned cost model), when record
     bool record = false;
@@ -180,7 +187,10 @@ extern "C" int pastix_gpu_init(pastix_gpu_t **pctx, int device, const int64_t *i
     default_params(ctx->iparm, ctx->dparm);
     if (iparm) std::memcpy(ctx->iparm, iparm, sizeof(ctx->iparm));
     if (dparm) std::memcpy(ctx->dparm, dparm, sizeof(ctx->dparm));
-    PGPU_CHECK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    int prio_lo = 0, prio_hi = 0;
+    PGPU_CHECK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    PGPU_CHECK(cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_hi));
+    PGPU_CHECK(cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking, prio_lo));
     for (auto &e : ctx->ev) PGPU_CHECK(cudaEventCreate(&e));
     PGPU_CHECK(ctx->d_status.alloc(1));
     PGPU_CHECK(ctx->d_partial.alloc(1024));
@@ -298,6 +308,7 @@ extern "C" int pastix_gpu_structure(pastix_gpu_t *ctx, int64_t n, int64_t cblknb
     }
     C.nlevels = 0;
     for (int c = 0; c < nc; c++) C.nlevels = std::max(C.nlevels, level[c] + 1);
+    C.cblk_level = level;
     C.lvl_ptr.assign(C.nlevels + 1, 0);
     for (int c = 0; c < nc; c++) C.lvl_ptr[level[c] + 1]++;
     for (int l = 0; l < C.nlevels; l++) C.lvl_ptr[l + 1] += C.lvl_ptr[l];
@@ -490,6 +501,13 @@ static bool tc_persistent() {
     const char *e = getenv("PASTIX_GPU_TC_KERNEL");
     return !(e && std::strcmp(e, "tile") == 0);
 }
+// PASTIX_GPU_LOOKAHEAD=0 runs every update GEMM of a level on the main
+// stream before the next level's panels.
+static bool lookahead_enabled() {
+    const char *e = getenv("PASTIX_GPU_LOOKAHEAD");
+    return !(e && std::strcmp(e, "0") == 0);
+}
+static const int LA_RESERVED_SMS = 16;   // left free by stream2's persistent GEMMs for the critical path
 static bool tc_task(int M, int N, int K) { return K >= 32 && M >= 64 && N >= 32 && (int64_t)M * N >= 128 * 64; }
 
 // Kernel form of a factorization request (pastix_factotype_t on a real or
@@ -543,8 +561,15 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     C.trsm_ptr.assign(C.nlevels + 1, 0);
     C.lvl_plrows.assign(C.nlevels, 0);
     C.lvl_porows.assign(C.nlevels, 0);
+    C.tile_crit.assign(C.nlevels, 0);
+    C.tctile_crit.assign(C.nlevels, 0);
+    std::vector<int4> lt[2], ltc[2];   // this level's FMA / tensor-core tiles: [0] next-level targets, [1] others
     for (int l = 0; l < C.nlevels; l++) {
         int64_t scr_lvl = 0;
+        for (int k = 0; k < 2; k++) {
+            lt[k].clear();
+            ltc[k].clear();
+        }
         for (int q = C.lvl_ptr[l]; q < C.lvl_ptr[l + 1]; q++) {
             const int c = C.lvl_cblks[q];
             const int w = C.width[c], h = C.height[c];
@@ -581,6 +606,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
             for (int b = C.fblok[c] + 1; b < b1; b++) {
                 const int f = C.bfcblk[b];
                 const int N = C.blrow[b] - C.bfrow[b] + 1;
+                const int crit = (C.cblk_level[f] == l + 1) ? 0 : 1;
                 auto add = [&](int arow0, int flags) {
                     const int M = h - arow0;
                     if (M <= 0) return;
@@ -592,14 +618,14 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
                         for (int tm = 0; tm < cdiv(M, TC_BM); tm++)
                             for (int tn = 0; tn < cdiv(N, TC_BN); tn++) {
                                 if ((flags & 8) && tm < tn) continue;
-                                tctiles.push_back(make_int4(id, tm, tn, 0));
+                                ltc[crit].push_back(make_int4(id, tm, tn, 0));
                             }
                         return;
                     }
                     for (int tm = 0; tm < cdiv(M, GEMM_TM); tm++)
                         for (int tn = 0; tn < cdiv(N, GEMM_TN); tn++) {
                             if ((flags & 8) && tm < tn) continue;   // strictly upper tiles of the diagonal block
-                            tiles.push_back(make_int4(id, tm, tn, 0));
+                            lt[crit].push_back(make_int4(id, tm, tn, 0));
                         }
                 };
                 if (!lu) {
@@ -609,6 +635,12 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
                     if (b + 1 < b1) add(C.browoff[b + 1], 1 | 4);  // U side: A = U^T, B = L rows of b
                 }
             }
+        }
+        C.tile_crit[l] = (int)lt[0].size();
+        C.tctile_crit[l] = (int)ltc[0].size();
+        for (int k = 0; k < 2; k++) {
+            tiles.insert(tiles.end(), lt[k].begin(), lt[k].end());
+            tctiles.insert(tctiles.end(), ltc[k].begin(), ltc[k].end());
         }
         C.tile_ptr[l + 1] = (int)tiles.size();
         C.tctile_ptr[l + 1] = (int)tctiles.size();
@@ -661,25 +693,29 @@ static const int SMEM_LIMIT = 227 * 1024;
 // the last), so launch i took ev[i+1] - ev[i]; kinds[i] says which phase.
 struct LaunchTimer {
     pastix_gpu_t &C;
+    cudaStream_t st;
+    std::vector<cudaEvent_t> &pool;
     std::vector<int> kinds;
     int used = 0;
-    explicit LaunchTimer(pastix_gpu_t &c) : C(c) {}
+    explicit LaunchTimer(pastix_gpu_t &c) : C(c), st(c.stream), pool(c.evpool) {}
+    LaunchTimer(pastix_gpu_t &c, cudaStream_t s, std::vector<cudaEvent_t> &p) : C(c), st(s), pool(p) {}
     cudaError_t mark(int kind) {
-        if (used >= (int)C.evpool.size()) {
+        if (used >= (int)pool.size()) {
             cudaEvent_t e;
             cudaError_t r = cudaEventCreate(&e);
             if (r != cudaSuccess) return r;
-            C.evpool.push_back(e);
+            pool.push_back(e);
         }
         kinds.push_back(kind);
-        return cudaEventRecord(C.evpool[used++], C.stream);
+        return cudaEventRecord(pool[used++], st);
     }
-    // after the stream was synchronized: accumulate ms per kind
+    // after the stream was synchronized: accumulate ms per kind (a mark of
+    // kind -1 closes an interval without opening a timed one)
     void collect(double *ms, int nkind) {
         for (int k = 0; k < nkind; k++) ms[k] = 0;
         for (int i = 0; i + 1 < used; i++) {
             float t = 0;
-            if (kinds[i] >= 0 && kinds[i] < nkind && cudaEventElapsedTime(&t, C.evpool[i], C.evpool[i + 1]) == cudaSuccess)
+            if (kinds[i] >= 0 && kinds[i] < nkind && cudaEventElapsedTime(&t, pool[i], pool[i + 1]) == cudaSuccess)
                 ms[kinds[i]] += t;
         }
     }
@@ -743,8 +779,64 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     auto at = [](int64_t *p, int off) { return p ? p + 2 * (int64_t)off : nullptr; };
     const double *critp = C.d_fact_scal.p + 1;
     int nl = 0, ngemm = 0;
+    // lookahead over two streams (off while recording task timings)
+    const bool la = lookahead_enabled() && !C.record;
+    LaunchTimer tm2(C, C.stream2, C.evpool2);
+    if (la) {
+        while ((int)C.la_events.size() < 2 * C.nlevels) {
+            cudaEvent_t e;
+            PGPU_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            C.la_events.push_back(e);
+        }
+        // stream2 starts after the fill-in (recorded by the caller on the main stream)
+        PGPU_CHECK(cudaEventRecord(C.ev[1], s));
+        PGPU_CHECK(cudaStreamWaitEvent(C.stream2, C.ev[1], 0));
+    }
+    auto launch_gemms = [&](cudaStream_t st, LaunchTimer &lt, int t0, int nt, int c0, int ntc, int gcap) -> int {
+        if (nt) {
+            PGPU_CHECK(lt.mark(PH_GEMM));
+            k_gemm_scatter<T><<<nt, 256, 0, st>>>(C.meta, C.d_tiles.p + t0, C.d_tasks.p, coefL, coefU, nullptr,
+                                                  nullptr, at(prof[2], t0));
+            if (la) PGPU_CHECK(lt.mark(PH_END));
+            nl++;
+            ngemm++;
+        }
+        if constexpr (std::is_same<T, float>::value) {
+            if (ntc) {
+                PGPU_CHECK(lt.mark(PH_TC));
+                if (persist) {
+                    const int g = std::min(ntc, gcap);
+                    if (split)
+                        k_gemm_scatter_tc_persistent<true><<<g, TCP_THREADS, tcp_smem_bytes<true>(), st>>>(
+                            C.meta, C.d_tctiles.p + c0, ntc, C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr,
+                            nullptr);
+                    else
+                        k_gemm_scatter_tc_persistent<false><<<g, TCP_THREADS, tcp_smem_bytes<false>(), st>>>(
+                            C.meta, C.d_tctiles.p + c0, ntc, C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr,
+                            nullptr);
+                } else if (split) {
+                    k_gemm_scatter_tc<true><<<ntc, TC_THREADS, tc_smem_bytes<true>(), st>>>(
+                        C.meta, C.d_tctiles.p + c0, C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr, nullptr,
+                        at(prof[3], c0));
+                } else {
+                    k_gemm_scatter_tc<false><<<ntc, TC_THREADS, tc_smem_bytes<false>(), st>>>(
+                        C.meta, C.d_tctiles.p + c0, C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr, nullptr,
+                        at(prof[3], c0));
+                }
+                if (la) PGPU_CHECK(lt.mark(PH_END));
+                nl++;
+                ngemm++;
+            }
+        }
+        return PASTIX_GPU_SUCCESS;
+    };
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
+        // the deferred updates into this level's cblks were issued on stream2 two levels back or earlier
+        if (la && l >= 2) {
+            PGPU_CHECK(tm.mark(PH_END));
+            PGPU_CHECK(cudaStreamWaitEvent(s, C.la_events[2 * (l - 2) + 1], 0));
+        }
         const int mw = C.lvl_maxw[l];
         const int pl = C.lvl_plrows[l], pu = lu ? mw : 0, po = lu ? C.lvl_porows[l] : 0;
         const size_t psm = (size_t)(PB * PBL + PB + (size_t)(pl + pu + po) * PBL) * sizeof(T);
@@ -800,46 +892,36 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                                         at(prof[1], C.trsm_ptr[l]));
             nl++;
         }
-        const int nti = C.tile_ptr[l + 1] - C.tile_ptr[l];
-        if (nti) {
-            PGPU_CHECK(tm.mark(PH_GEMM));
-            k_gemm_scatter<T><<<nti, 256, 0, s>>>(C.meta, C.d_tiles.p + C.tile_ptr[l], C.d_tasks.p, coefL, coefU,
-                                                  nullptr, nullptr, at(prof[2], C.tile_ptr[l]));
-            nl++;
-            ngemm++;
+        // update GEMMs of the level: with lookahead the tiles whose target is
+        // in the next level run here, the rest on stream2 once this level's
+        // panels are final
+        const int nti = C.tile_ptr[l + 1] - C.tile_ptr[l], ntc = C.tctile_ptr[l + 1] - C.tctile_ptr[l];
+        if (la) {
+            PGPU_CHECK(cudaEventRecord(C.la_events[2 * l], s));
+            int rc = launch_gemms(s, tm, C.tile_ptr[l], C.tile_crit[l], C.tctile_ptr[l], C.tctile_crit[l], nsm);
+            if (rc) return rc;
+            PGPU_CHECK(cudaStreamWaitEvent(C.stream2, C.la_events[2 * l], 0));
+            rc = launch_gemms(C.stream2, tm2, C.tile_ptr[l] + C.tile_crit[l], nti - C.tile_crit[l],
+                              C.tctile_ptr[l] + C.tctile_crit[l], ntc - C.tctile_crit[l],
+                              std::max(1, nsm - LA_RESERVED_SMS));
+            if (rc) return rc;
+            PGPU_CHECK(cudaEventRecord(C.la_events[2 * l + 1], C.stream2));
+        } else {
+            const int rc = launch_gemms(s, tm, C.tile_ptr[l], nti, C.tctile_ptr[l], ntc, nsm);
+            if (rc) return rc;
         }
-        if constexpr (std::is_same<T, float>::value) {
-            const int ntc = C.tctile_ptr[l + 1] - C.tctile_ptr[l];
-            if (ntc && persist) {
-                PGPU_CHECK(tm.mark(PH_TC));
-                const int g = std::min(ntc, nsm);
-                if (split)
-                    k_gemm_scatter_tc_persistent<true><<<g, TCP_THREADS, tcp_smem_bytes<true>(), s>>>(
-                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
-                        nullptr, nullptr);
-                else
-                    k_gemm_scatter_tc_persistent<false><<<g, TCP_THREADS, tcp_smem_bytes<false>(), s>>>(
-                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
-                        nullptr, nullptr);
-                nl++;
-                ngemm++;
-            } else if (ntc) {
-                PGPU_CHECK(tm.mark(PH_TC));
-                if (split)
-                    k_gemm_scatter_tc<true><<<ntc, TC_THREADS, tc_smem_bytes<true>(), s>>>(
-                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr,
-                        nullptr, at(prof[3], C.tctile_ptr[l]));
-                else
-                    k_gemm_scatter_tc<false><<<ntc, TC_THREADS, tc_smem_bytes<false>(), s>>>(
-                        C.meta, C.d_tctiles.p + C.tctile_ptr[l], C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr,
-                        nullptr, at(prof[3], C.tctile_ptr[l]));
-                nl++;
-                ngemm++;
-            }
-        }
+    }
+    if (la && C.nlevels > 0) {
+        PGPU_CHECK(tm2.mark(PH_END));
+        PGPU_CHECK(cudaStreamWaitEvent(s, C.la_events[2 * (C.nlevels - 1) + 1], 0));
     }
     PGPU_CHECK(tm.mark(PH_END));
     PGPU_CHECK(cudaGetLastError());
+    std::fill(C.side_ms, C.side_ms + 4, 0.0);
+    if (la) {
+        PGPU_CHECK(cudaStreamSynchronize(C.stream2));
+        tm2.collect(C.side_ms, 4);
+    }
     *launches = nl;
     C.stats[7] = ngemm;
     return PASTIX_GPU_SUCCESS;
@@ -927,9 +1009,9 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
         tm.collect(ph, 4);
         C.stats[8] = ph[PH_DIAG];
         C.stats[9] = ph[PH_TRSM];
-        C.stats[6] = ph[PH_GEMM] + ph[PH_TC];
+        C.stats[6] = ph[PH_GEMM] + ph[PH_TC] + C.side_ms[PH_GEMM] + C.side_ms[PH_TC];
         C.stats[10] = C.plan_gemm_flops;
-        C.stats[11] = ph[PH_TC];
+        C.stats[11] = ph[PH_TC] + C.side_ms[PH_TC];
         C.stats[12] = mixed ? C.tc_flops : 0.0;
         C.stats[13] = st.timeout;
     }
@@ -1458,7 +1540,7 @@ static int refine_gmres(pastix_gpu_t &C, VecOps<S> &V, const S *b, S *x, double 
 }
 
 static int ensure_refine_vectors(pastix_gpu_t &C) {
-    const size_t n2 = (size_t)C.n * 2;   // room for complex vectors
+    const size_t n2 = (size_t)C.n * 2 * MULTI_MAX;   // complex, up to MULTI_MAX columns
     if (C.d_r.n < n2) {
         PGPU_CHECK(C.d_r.alloc(n2));
         PGPU_CHECK(C.d_z.alloc(n2));
@@ -1467,7 +1549,296 @@ static int ensure_refine_vectors(pastix_gpu_t &C) {
         PGPU_CHECK(C.d_x.alloc(n2));
         PGPU_CHECK(C.d_gm.alloc(2 * n2));
     }
+    if (C.d_rhs.n < n2) PGPU_CHECK(C.d_rhs.alloc(n2));
+    if (C.d_partial.n < (size_t)2 * 256 * MULTI_MAX) PGPU_CHECK(C.d_partial.alloc((size_t)2 * 256 * MULTI_MAX));
+    if (C.d_scalar.n < (size_t)4 * MULTI_MAX) PGPU_CHECK(C.d_scalar.alloc((size_t)4 * MULTI_MAX));
     return ensure_work(C);
+}
+
+// --------------------------------------------------------------------------
+// Lockstep refinement of k <= MULTI_MAX right-hand sides: the reference
+// refines one column after the other (refinement/pastix_task_refine.c:120-161);
+// here the k columns share every SpMV and preconditioner solve (one
+// multi-RHS supernodal solve instead of k single ones) while each keeps its
+// own scalars, stopping test and iteration count -- a converged column is
+// frozen (step 0) while the others go on.
+// --------------------------------------------------------------------------
+template <typename S>
+struct BlockOps {
+    typedef typename HostScalar<S>::type HS;
+    pastix_gpu_t &C;
+    int k;
+    int launches = 0;
+    S *partial() { return reinterpret_cast<S *>(C.d_partial.p); }
+    S *scal() { return reinterpret_cast<S *>(C.d_scalar.p); }
+    // per-column conj(x_c) . y_c (or ||x_c||^2), launched only
+    void dot_dev(const S *x, const S *y, S *out, int do_sqrt) {
+        const int nb = 256;
+        k_dot_partial_multi<S><<<dim3(nb, k), RED_THREADS, 0, C.stream>>>(C.n, x, y, partial());
+        k_dot_final_multi<S><<<k, RED_THREADS, 0, C.stream>>>(nb, partial(), out, do_sqrt);
+        launches += 2;
+    }
+    void dot(const S *x, const S *y, std::vector<HS> &out) {
+        dot_dev(x, y, scal(), 0);
+        std::vector<S> h(k);
+        cudaMemcpyAsync(h.data(), scal(), k * sizeof(S), cudaMemcpyDeviceToHost, C.stream);
+        cudaStreamSynchronize(C.stream);
+        out.resize(k);
+        for (int c = 0; c < k; c++) out[c] = to_host(h[c]);
+    }
+    void norm(const S *x, std::vector<double> &out) {
+        std::vector<HS> d;
+        dot(x, nullptr, d);
+        out.resize(k);
+        for (int c = 0; c < k; c++) out[c] = std::sqrt(std::real(d[c]));
+    }
+    void axpy(const std::vector<HS> &a, const S *x, S *y) {
+        Coefs<S> cf;
+        for (int c = 0; c < MULTI_MAX; c++) cf.v[c] = to_dev(c < k ? a[c] : HS(0.0));
+        k_axpy_multi<S><<<1024, 256, 0, C.stream>>>(C.n, k, cf, x, y);
+        launches++;
+    }
+    void xpby(const S *z, const std::vector<HS> &beta, S *p) {
+        Coefs<S> cf;
+        for (int c = 0; c < MULTI_MAX; c++) cf.v[c] = to_dev(c < k ? beta[c] : HS(0.0));
+        k_xpby_multi<S><<<1024, 256, 0, C.stream>>>(C.n, k, z, cf, p);
+        launches++;
+    }
+    void scal(const std::vector<double> &a, S *x) {
+        Coefs<double> cf;
+        for (int c = 0; c < MULTI_MAX; c++) cf.v[c] = c < k ? a[c] : 1.0;
+        k_scal_multi<S><<<1024, 256, 0, C.stream>>>(C.n, k, cf, x);
+        launches++;
+    }
+    void copy(const S *x, S *y) {
+        cudaMemcpyAsync(y, x, (size_t)C.n * k * sizeof(S), cudaMemcpyDeviceToDevice, C.stream);
+    }
+    void spmv(double alpha, const S *x, double beta, S *y) {
+        const int n = C.n;
+        S *xp = reinterpret_cast<S *>(C.d_gm.p), *yp = xp + (size_t)n * k;
+        const S *val = reinterpret_cast<const S *>(C.d_csr_val.p);
+        const int grid = std::min(4096, cdiv((int64_t)n * k, 256));
+        k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, k, C.d_peritab.p, x, n, xp, n, 0);
+        if (beta != 0.0) k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, k, C.d_peritab.p, y, n, yp, n, 0);
+        k_spmv_multi<S><<<cdiv((int64_t)n * 32, 256), 256, 0, C.stream>>>(n, k, C.d_csr_ptr.p, C.d_csr_col.p, val,
+                                                                           alpha, xp, beta, yp);
+        k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, k, C.d_peritab.p, yp, n, y, n, 1);
+        launches += 3 + (beta != 0.0);
+    }
+    int spsv(S *z) { return solve_device_block(C, z, C.n, k, C.d_work.p, &launches); }
+    // per column: ||r_c|| / ||b_c||, or with batch segments the largest
+    // per-system ratio of the column
+    void measure(const S *r, const std::vector<double> &normr, const std::vector<double> &normb,
+                 const std::vector<double> &segb, std::vector<double> &out) {
+        out.resize(k);
+        if (C.seg.size() < 3) {
+            for (int c = 0; c < k; c++) out[c] = normr[c] / normb[c];
+            return;
+        }
+        const int ns = (int)C.seg.size() - 1;
+        std::vector<double> sr((size_t)ns * k);
+        k_seg_sumsq_multi<S><<<dim3(std::min(ns, 4096), k), RED_THREADS, 0, C.stream>>>(ns, C.d_seg.p, C.n, r,
+                                                                                      C.d_segss.p);
+        launches++;
+        cudaMemcpyAsync(sr.data(), C.d_segss.p, sr.size() * sizeof(double), cudaMemcpyDeviceToHost, C.stream);
+        cudaStreamSynchronize(C.stream);
+        for (int c = 0; c < k; c++) {
+            double m = 0;
+            for (int i = 0; i < ns; i++) {
+                const double sb = segb[(size_t)c * ns + i];
+                m = std::max(m, std::sqrt(sr[(size_t)c * ns + i]) / (sb > 0 ? sb : 1.0));
+            }
+            out[c] = m;
+        }
+    }
+    void seg_norms(const S *x, std::vector<double> &out) {
+        if (C.seg.size() < 3) return;
+        const int ns = (int)C.seg.size() - 1;
+        out.resize((size_t)ns * k);
+        k_seg_sumsq_multi<S><<<dim3(std::min(ns, 4096), k), RED_THREADS, 0, C.stream>>>(ns, C.d_seg.p, C.n, x,
+                                                                                      C.d_segss.p);
+        launches++;
+        cudaMemcpyAsync(out.data(), C.d_segss.p, out.size() * sizeof(double), cudaMemcpyDeviceToHost, C.stream);
+        cudaStreamSynchronize(C.stream);
+        for (auto &v : out) v = std::sqrt(v);
+    }
+};
+
+// Preconditioned CG (refinement/z_refine_grad.c:49) on k columns in lockstep.
+template <typename S>
+static int refine_cg_block(pastix_gpu_t &C, BlockOps<S> &V, const S *b, S *x, double eps, int itermax,
+                           std::vector<int> &iters, std::vector<double> &resid) {
+    typedef typename HostScalar<S>::type HS;
+    const int k = V.k;
+    S *r = reinterpret_cast<S *>(C.d_r.p), *z = reinterpret_cast<S *>(C.d_z.p);
+    S *p = reinterpret_cast<S *>(C.d_p.p), *ap = reinterpret_cast<S *>(C.d_ap.p);
+    std::vector<double> normb, normx, normr, segb, res;
+    V.norm(b, normb);
+    for (auto &v : normb)
+        if (v == 0.) v = 1;
+    V.norm(x, normx);
+    V.seg_norms(b, segb);
+    V.copy(b, r);
+    V.spmv(-1.0, x, 1.0, r);
+    V.norm(r, normr);
+    V.measure(r, normr, normb, segb, res);
+    iters.assign(k, 0);
+    std::vector<char> active(k);
+    bool any = false;
+    for (int c = 0; c < k; c++) any |= (active[c] = res[c] > eps && itermax > 0);
+    if (any) {
+        V.copy(r, z);
+        int rc = V.spsv(z);
+        if (rc) return rc;
+        V.copy(z, p);
+    }
+    std::vector<HS> beta, alpha, alpha2, step(k), mstep(k);
+    while (any) {
+        V.spmv(1.0, p, 0.0, ap);
+        V.dot(r, z, beta);
+        V.dot(ap, p, alpha);
+        for (int c = 0; c < k; c++) {
+            step[c] = active[c] ? beta[c] / alpha[c] : HS(0.0);
+            mstep[c] = -step[c];
+        }
+        V.axpy(step, p, x);
+        V.axpy(mstep, ap, r);
+        V.copy(r, z);
+        int rc = V.spsv(z);
+        if (rc) return rc;
+        V.dot(r, z, alpha2);
+        for (int c = 0; c < k; c++) beta[c] = active[c] ? alpha2[c] / beta[c] : HS(0.0);
+        V.xpby(z, beta, p);
+        V.norm(r, normr);
+        V.measure(r, normr, normb, segb, res);
+        any = false;
+        for (int c = 0; c < k; c++) {
+            if (!active[c]) continue;
+            iters[c]++;
+            active[c] = res[c] > eps && iters[c] < itermax;
+            any |= active[c];
+        }
+    }
+    resid = res;
+    return PASTIX_GPU_SUCCESS;
+}
+
+// GMRES(im), right preconditioned (refinement/z_refine_gmres.c:49), on k
+// columns in lockstep: one Krylov basis per column (block j of V holds v_j
+// of every column), per-column Hessenberg matrices and Givens rotations on
+// the host.  A column leaves the inner loop when it converges or fills its
+// basis; the restart cycle ends when every column has left it.
+template <typename S>
+static int refine_gmres_block(pastix_gpu_t &C, BlockOps<S> &V, const S *b, S *x, double eps, int itermax, int im,
+                              std::vector<int> &iters_out, std::vector<double> &resid_out) {
+    typedef typename HostScalar<S>::type HS;
+    const int k = V.k;
+    const int64_t n = C.n, nk = (int64_t)n * k;
+    const int im1 = im + 1;
+    const size_t comp = sizeof(S) / sizeof(double);
+    if (C.d_gmV.n < (size_t)nk * im1 * comp) {
+        PGPU_CHECK(C.d_gmV.alloc((size_t)nk * im1 * comp));
+        PGPU_CHECK(C.d_gmW.alloc((size_t)nk * im * comp));
+    }
+    if (C.d_gmh.n < (size_t)2 * im1 * k * comp) PGPU_CHECK(C.d_gmh.alloc((size_t)2 * im1 * k * comp));
+    cudaStream_t s = C.stream;
+    S *gV = reinterpret_cast<S *>(C.d_gmV.p), *gW = reinterpret_cast<S *>(C.d_gmW.p);
+    S *dh = reinterpret_cast<S *>(C.d_gmh.p);     // [j][c]
+    std::vector<std::vector<HS>> H(k, std::vector<HS>((size_t)im * im1, HS(0.0))), G(k, std::vector<HS>(im1)),
+        sn(k, std::vector<HS>(im));
+    std::vector<std::vector<double>> cs(k, std::vector<double>(im, 0.0));
+    std::vector<S> hcol((size_t)im1 * k);
+    std::vector<double> normb, normx, rr, segb, resid(k, 0.0), resid_b(k, 0.0), scl(k);
+    V.norm(b, normb);
+    for (auto &v : normb)
+        if (v == 0.) v = 1;
+    V.norm(x, normx);
+    V.seg_norms(b, segb);
+    std::vector<int> iters(k, 0), kc(k, 0);
+    std::vector<char> out(k, 1), in(k, 0), cyc(k, 0);
+    while (true) {
+        // r0 = b - A x for every column
+        V.copy(b, gV);
+        V.spmv(-1.0, x, 1.0, gV);
+        V.norm(gV, rr);
+        V.measure(gV, rr, normb, segb, resid_b);
+        bool any = false;
+        for (int c = 0; c < k; c++) {
+            if (out[c] && resid_b[c] <= eps) out[c] = 0;
+            cyc[c] = in[c] = out[c];
+            any |= out[c];
+            scl[c] = out[c] ? 1.0 / rr[c] : 1.0;
+            if (out[c]) {
+                std::fill(G[c].begin(), G[c].end(), HS(0.0));
+                G[c][0] = HS(rr[c]);
+            }
+        }
+        if (!any) break;
+        V.scal(scl, gV);
+        int i = -1;
+        bool inner = true;
+        while (inner) {
+            i++;
+            S *vi = gV + (int64_t)i * nk, *wi = gW + (int64_t)i * nk, *vn = gV + (int64_t)(i + 1) * nk;
+            V.copy(vi, wi);
+            int rc = V.spsv(wi);                      // w_i = M^{-1} v_i
+            if (rc) return rc;
+            V.spmv(1.0, wi, 0.0, vn);                 // v_{i+1} = A w_i
+            for (int j = 0; j <= i; j++) {            // modified Gram-Schmidt, per column
+                V.dot_dev(gV + (int64_t)j * nk, vn, dh + (size_t)j * k, 0);
+                k_axpy_multi_dev<S><<<1024, 256, 0, s>>>(n, k, dh + (size_t)j * k, -1.0, gV + (int64_t)j * nk, vn);
+                V.launches++;
+            }
+            V.dot_dev(vn, nullptr, dh + (size_t)(i + 1) * k, 1);
+            PGPU_CHECK(cudaMemcpyAsync(hcol.data(), dh, (size_t)(i + 2) * k * sizeof(S), cudaMemcpyDeviceToHost, s));
+            PGPU_CHECK(cudaStreamSynchronize(s));
+            inner = false;
+            for (int c = 0; c < k; c++) {
+                const double nrm = std::real(to_host(hcol[(size_t)(i + 1) * k + c]));
+                scl[c] = (in[c] && nrm > 1e-50) ? 1.0 / nrm : 1.0;
+                if (!in[c]) continue;
+                HS *Hi = H[c].data() + (size_t)i * im1;
+                for (int j = 0; j <= i + 1; j++) Hi[j] = to_host(hcol[(size_t)j * k + c]);
+                for (int j = 0; j < i; j++) {          // previous Givens rotations
+                    const HS tmp = Hi[j];
+                    Hi[j] = cs[c][j] * tmp + sn[c][j] * Hi[j + 1];
+                    Hi[j + 1] = cs[c][j] * Hi[j + 1] - conj_h(sn[c][j]) * tmp;
+                }
+                givens(Hi[i], Hi[i + 1], eps, cs[c][i], sn[c][i]);
+                G[c][i + 1] = -conj_h(sn[c][i]) * G[c][i];
+                G[c][i] = cs[c][i] * G[c][i];
+                Hi[i] = cs[c][i] * Hi[i] + sn[c][i] * Hi[i + 1];
+                resid[c] = std::abs(G[c][i + 1]);
+                resid_b[c] = resid[c] / normb[c];
+                iters[c]++;
+                kc[c] = i + 1;
+                if (i + 1 >= im || resid_b[c] <= eps || iters[c] >= itermax) in[c] = 0;
+                inner |= (bool)in[c];
+            }
+            V.scal(scl, vn);
+        }
+        // per column: y = H^{-1} g, x_c += W_c y
+        for (int c = 0; c < k; c++) {
+            if (!cyc[c]) continue;
+            std::vector<HS> &Gc = G[c];
+            const int kk = kc[c];
+            for (int r = kk - 1; r >= 0; r--) {
+                HS sum = Gc[r];
+                for (int j = r + 1; j < kk; j++) sum -= H[c][(size_t)j * im1 + r] * Gc[j];
+                Gc[r] = sum / H[c][(size_t)r * im1 + r];
+            }
+            for (int j = 0; j < kk; j++) hcol[j] = to_dev(Gc[j]);
+            PGPU_CHECK(cudaMemcpyAsync(dh + (size_t)c * im1, hcol.data(), kk * sizeof(S), cudaMemcpyHostToDevice, s));
+            k_gemv_acc<S><<<1024, 256, 0, s>>>(n, kk, gW + (int64_t)c * n, nk, dh + (size_t)c * im1,
+                                               x + (int64_t)c * n);
+            V.launches++;
+            if (iters[c] >= itermax) out[c] = 0;
+        }
+        PGPU_CHECK(cudaStreamSynchronize(s));
+    }
+    iters_out = iters;
+    resid_out = resid_b;
+    return PASTIX_GPU_SUCCESS;
 }
 
 template <typename S>
@@ -1480,26 +1851,30 @@ static int refine_t(pastix_gpu_t &C, int64_t nrhs, const void *B, int64_t ldb, v
     const int method = (int)C.iparm[PGPU_IPARM_REFINEMENT];
     const int im = std::max<int>(1, (int)C.iparm[PGPU_IPARM_GMRES_IM]);
     const bool bdev = is_device_ptr(B), xdev = is_device_ptr(X);
-    VecOps<S> V{C};
-    for (int64_t r = 0; r < nrhs; r++) {
-        const S *bcol = reinterpret_cast<const S *>(B) + r * ldb;
-        S *xcol = reinterpret_cast<S *>(X) + r * ldx;
+    const size_t es = sizeof(S);
+    for (int64_t r0 = 0; r0 < nrhs; r0 += MULTI_MAX) {
+        const int k = (int)std::min<int64_t>(MULTI_MAX, nrhs - r0);
+        BlockOps<S> V{C, k};
+        const S *bcol = reinterpret_cast<const S *>(B) + r0 * ldb;
+        S *xcol = reinterpret_cast<S *>(X) + r0 * ldx;
         S *db = reinterpret_cast<S *>(C.d_rhs.p), *dx = reinterpret_cast<S *>(C.d_x.p);
-        PGPU_CHECK(cudaMemcpyAsync(db, bcol, C.n * sizeof(S), bdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                   s));
-        PGPU_CHECK(cudaMemcpyAsync(dx, xcol, C.n * sizeof(S), xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                   s));
-        int it = 0;
-        double res = 0;
-        int rc = (method == PGPU_REFINE_CG) ? refine_cg<S>(C, V, db, dx, eps, itermax, &it, &res)
-                                            : refine_gmres<S>(C, V, db, dx, eps, itermax, im, &it, &res);
+        PGPU_CHECK(cudaMemcpy2DAsync(db, C.n * es, bcol, ldb * es, C.n * es, k,
+                                     bdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+        PGPU_CHECK(cudaMemcpy2DAsync(dx, C.n * es, xcol, ldx * es, C.n * es, k,
+                                     xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+        std::vector<int> it;
+        std::vector<double> res;
+        int rc = (method == PGPU_REFINE_CG) ? refine_cg_block<S>(C, V, db, dx, eps, itermax, it, res)
+                                            : refine_gmres_block<S>(C, V, db, dx, eps, itermax, im, it, res);
         if (rc) return rc;
-        PGPU_CHECK(cudaMemcpyAsync(xcol, dx, C.n * sizeof(S), xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                                   s));
-        *maxit = std::max(*maxit, it);
-        *maxres = std::max(*maxres, res);
+        PGPU_CHECK(cudaMemcpy2DAsync(xcol, ldx * es, dx, C.n * es, C.n * es, k,
+                                     xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+        for (int c = 0; c < k; c++) {
+            *maxit = std::max(*maxit, it[c]);
+            *maxres = std::max(*maxres, res[c]);
+        }
+        *launches += V.launches;
     }
-    *launches = V.launches;
     return PASTIX_GPU_SUCCESS;
 }
 
@@ -1583,7 +1958,7 @@ extern "C" int pastix_gpu_set_segments(pastix_gpu_t *ctx, int64_t nseg, const in
     PGPU_CHECK(cudaSetDevice(C.device));
     C.seg.assign(segptr, segptr + nseg + 1);
     PGPU_CHECK(C.d_seg.upload(C.seg, C.stream));
-    PGPU_CHECK(C.d_segss.alloc(nseg));
+    PGPU_CHECK(C.d_segss.alloc((size_t)nseg * MULTI_MAX));
     PGPU_CHECK(cudaStreamSynchronize(C.stream));
     return PASTIX_GPU_SUCCESS;
 }
@@ -1732,6 +2107,12 @@ extern "C" void pastix_gpu_finalize(pastix_gpu_t **pctx) {
     if (C->stream) cudaStreamSynchronize(C->stream);
     for (auto &e : C->ev) cudaEventDestroy(e);
     for (auto &e : C->evpool) cudaEventDestroy(e);
+    for (auto &e : C->evpool2) cudaEventDestroy(e);
+    for (auto &e : C->la_events) cudaEventDestroy(e);
+    if (C->stream2) {
+        cudaStreamSynchronize(C->stream2);
+        cudaStreamDestroy(C->stream2);
+    }
     if (C->stream) cudaStreamDestroy(C->stream);
     delete C;   // every DArr member frees its device memory
     *pctx = nullptr;

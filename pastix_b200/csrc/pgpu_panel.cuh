@@ -53,17 +53,25 @@ __device__ __forceinline__ void tile_update(T *C, int64_t ldc, const T *A, int l
 #pragma unroll
                 for (int q = 0; q < 4; q++) acc[p][q] += a[p] * b[q];
         }
+        // read all 16 targets before writing any: one memory latency per
+        // tile instead of a read-write round trip per element (C may be in
+        // global memory, where the compiler cannot reorder them itself)
+        T cv[4][4];
 #pragma unroll
-        for (int p = 0; p < 4; p++) {
-            const int i = i0 + p;
-            if (i >= M) continue;
+        for (int p = 0; p < 4; p++)
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const int j = j0 + q;
-                if (j >= N || (lower >= 0 && j > i + lower)) continue;
-                C[(int64_t)i * ldc + j] -= acc[p][q];
+                const int i = i0 + p, j = j0 + q;
+                const bool ok = i < M && j < N && !(lower >= 0 && j > i + lower);
+                cv[p][q] = ok ? C[(int64_t)i * ldc + j] : T(0);
             }
-        }
+#pragma unroll
+        for (int p = 0; p < 4; p++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int i = i0 + p, j = j0 + q;
+                if (i < M && j < N && !(lower >= 0 && j > i + lower)) C[(int64_t)i * ldc + j] = cv[p][q] - acc[p][q];
+            }
     }
 }
 

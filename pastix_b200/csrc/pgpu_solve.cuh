@@ -449,6 +449,127 @@ __global__ void k_gemv_acc(int64_t n, int k, const S *__restrict__ W, int64_t ld
     }
 }
 
+// ---------------------------------------------------------------------------
+// Multi-right-hand-side forms for the refinement run in lockstep on k <= 16
+// columns (column-major, ld = n): each column keeps its own scalars, and
+// each column's reductions follow exactly the single-column kernels' order,
+// so a column's iterates are those of running it alone (the reference
+// refines one right-hand side after the other, refinement/pastix_task_refine.c).
+// ---------------------------------------------------------------------------
+constexpr int MULTI_MAX = 16;
+template <typename S> struct Coefs { S v[MULTI_MAX]; };
+
+// partial[c * gridDim.x + b] = sum over the block's share of conj(x_c) y_c
+// (|x_c|^2 when y == nullptr); blockIdx.y = column
+template <typename S>
+__global__ void k_dot_partial_multi(int64_t n, const S *__restrict__ x, const S *__restrict__ y,
+                                    S *__restrict__ partial) {
+    __shared__ S sh[32];
+    const int c = blockIdx.y;
+    const S *xc = x + (int64_t)c * n;
+    const S *yc = y ? y + (int64_t)c * n : nullptr;
+    S s = S(0.0);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s += yc ? conj_v(xc[i]) * yc[i] : S(abs2_v(xc[i]));
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) partial[(int64_t)c * gridDim.x + blockIdx.x] = s;
+}
+
+// out[c] = sum of column c's np partials (sqrt of the real part when do_sqrt)
+template <typename S>
+__global__ void k_dot_final_multi(int np, const S *__restrict__ partial, S *__restrict__ out, int do_sqrt) {
+    __shared__ S sh[32];
+    const int c = blockIdx.x;
+    S s = S(0.0);
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partial[(int64_t)c * np + i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) out[c] = do_sqrt ? S(sqrt(real_v(s))) : s;
+}
+
+// y_c += a_c x_c (a from the parameter block)
+template <typename S>
+__global__ void k_axpy_multi(int64_t n, int k, Coefs<S> a, const S *__restrict__ x, S *__restrict__ y) {
+    const int64_t tot = n * k;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x)
+        y[e] += a.v[e / n] * x[e];
+}
+
+// y_c += sign * alpha[c] x_c with alpha in device memory (GMRES projections)
+template <typename S>
+__global__ void k_axpy_multi_dev(int64_t n, int k, const S *__restrict__ alpha, double sign, const S *__restrict__ x,
+                                 S *__restrict__ y) {
+    const int64_t tot = n * k;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x)
+        y[e] += (sign * alpha[e / n]) * x[e];
+}
+
+// p_c = z_c + beta_c p_c
+template <typename S>
+__global__ void k_xpby_multi(int64_t n, int k, const S *__restrict__ z, Coefs<S> beta, S *__restrict__ p) {
+    const int64_t tot = n * k;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x)
+        p[e] = z[e] + beta.v[e / n] * p[e];
+}
+
+// x_c *= a_c
+template <typename S>
+__global__ void k_scal_multi(int64_t n, int k, Coefs<double> a, S *__restrict__ x) {
+    const int64_t tot = n * k;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x)
+        x[e] = a.v[e / n] * x[e];
+}
+
+// y_c = alpha A x_c + beta y_c on the permuted CSR, one warp per row, all
+// columns from one pass over the row (same summation order per column as
+// k_spmv)
+template <typename S>
+__global__ void k_spmv_multi(int n, int k, const int64_t *__restrict__ rowptr, const int *__restrict__ col,
+                             const S *__restrict__ val, double alpha, const S *__restrict__ x, double beta,
+                             S *__restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (; row < n; row += nwarps) {
+        S s[MULTI_MAX];
+#pragma unroll
+        for (int c = 0; c < MULTI_MAX; c++) s[c] = S(0.0);
+        for (int64_t q = rowptr[row] + lane; q < rowptr[row + 1]; q += 32) {
+            const S v = val[q];
+            const int cc = col[q];
+#pragma unroll
+            for (int c = 0; c < MULTI_MAX; c++)
+                if (c < k) s[c] += v * x[(int64_t)c * n + cc];
+        }
+#pragma unroll
+        for (int c = 0; c < MULTI_MAX; c++) {
+            if (c >= k) break;
+            S t = s[c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += shfl_xor_v(t, o);
+            if (lane == 0) {
+                S &yy = y[(int64_t)c * n + row];
+                yy = alpha * t + (beta == 0.0 ? S(0.0) : beta * yy);
+            }
+        }
+    }
+}
+
+// out[c * nseg + s] = sum |x_c|^2 over segment s (blockIdx.y = column)
+template <typename S>
+__global__ void k_seg_sumsq_multi(int nseg, const int64_t *__restrict__ seg, int64_t n, const S *__restrict__ x,
+                                  double *__restrict__ out) {
+    __shared__ double sh[32];
+    const int c = blockIdx.y;
+    const S *xc = x + (int64_t)c * n;
+    for (int sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
+        double v = 0.0;
+        for (int64_t i = seg[sg] + threadIdx.x; i < seg[sg + 1]; i += blockDim.x) v += abs2_v(xc[i]);
+        v = block_sum(v, sh);
+        if (threadIdx.x == 0) out[(int64_t)c * nseg + sg] = v;
+        __syncthreads();
+    }
+}
+
 // Gather the permuted-matrix values from the user's values; src < 0 marks
 // the mirrored entry of a Hermitian matrix (conj(vals[~src])).
 template <typename S>
