@@ -1075,9 +1075,11 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         size_t dsm;
         *ipch = 0;
         if (inv && C.inv_ptr[l + 1] > C.inv_ptr[l]) {
+            // rows of the inverse are staged padded to 16 bytes
+            const size_t rowb = (size_t)round_up(mw, 16 / (int64_t)es) * es;
             const size_t fixed_i = (size_t)2 * mw * nrhs * es;
-            dsm = std::min<size_t>(SMEM_LIMIT, std::max(fixed_i + (size_t)64 * mw * es, fixed + (size_t)mw * 33 * es));
-            *ipch = dsm > fixed_i ? (int)std::min<size_t>(mw, (dsm - fixed_i) / ((size_t)mw * es)) : 0;
+            dsm = std::min<size_t>(SMEM_LIMIT, std::max(fixed_i + (size_t)128 * rowb, fixed + (size_t)mw * 33 * es));
+            *ipch = dsm > fixed_i ? (int)std::min<size_t>(mw, (dsm - fixed_i) / rowb) : 0;
         } else {
             dsm = std::min<size_t>(SMEM_LIMIT, fixed + (size_t)std::max(mw, 1) * 33 * es);
         }
@@ -1093,7 +1095,8 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         if (pch < std::min(32, mw) || (inv && C.inv_ptr[l + 1] > C.inv_ptr[l] && ipch < 1))
             return PASTIX_GPU_ERR_NOTIMPLEMENTED;
         PGPU_CHECK(mark(0));
-        k_fwd_diag<T><<<ncb, 256, dsm, s>>>(
+        const int dthreads = (inv && C.inv_ptr[l + 1] > C.inv_ptr[l]) ? 1024 : 256;
+        k_fwd_diag<T><<<ncb, dthreads, dsm, s>>>(
             C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs, (lu || ldl) ? 1 : 0, pch, inv,
             ldl ? 1 : 0, cjp, ipch);
         nl++;
@@ -1125,7 +1128,8 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         int ipch = 0;
         const size_t dsm = diag_smem(l, mw, &pch, &ipch);
         PGPU_CHECK(mark(4));
-        k_bwd_diag<T><<<ncb, 256, dsm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs,
+        const int dthreads = (inv && C.inv_ptr[l + 1] > C.inv_ptr[l]) ? 1024 : 256;
+        k_bwd_diag<T><<<ncb, dthreads, dsm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, W, ldb, nrhs,
                                             lu ? 1 : 0, ldl ? 1 : 0, lu ? 0 : cjp, pch, inv, ldl ? 1 : 0, ipch);
         nl++;
     }

@@ -32,29 +32,41 @@ __device__ void diag_solve_inverse(const T *__restrict__ Bi, const T *__restrict
                                    bool backward, bool ldl, bool cjp, T *__restrict__ v, T *__restrict__ outp,
                                    T *__restrict__ P, int pch, T *__restrict__ Bg, int64_t ldb, int fc) {
     const int tid = threadIdx.x, nt = blockDim.x;
+    constexpr int VEC = 16 / sizeof(T);       // elements per 16-byte vector (rows of Bi are 16-byte aligned)
     // v: [w][nrhs] right-hand side in shared memory; outp: [w][nrhs] accumulators (backward)
-    if (backward)
+    if (backward) {
         for (int e = tid; e < w * nrhs; e += nt) outp[e] = T(0);
+        if (ldl)   // x_k = sum_n Binv[n][k] (d_n z_n): scale z by D first
+            for (int e = tid; e < w * nrhs; e += nt) v[e] = v[e] * D[(int64_t)(e / nrhs) * ld + e / nrhs];
+    }
     for (int n0 = 0; n0 < w; n0 += pch) {
         const int nr = min(pch, w - n0), kmax = n0 + nr;     // rows n0..n0+nr, columns 0..kmax
+        const int kv = (kmax + VEC - 1) / VEC, kp = kv * VEC;  // 16-byte vectors per row, padded row length
         __syncthreads();
-        batched_copy(
-            nr * kmax, tid, nt,
+        // rows of Binv are zero beyond the diagonal and in the padding (the
+        // workspace is cleared when the plan is built), so whole vectors move
+        batched_copy<4>(
+            nr * kv, tid, nt,
             [&](int e) {
-                const int i = e / kmax, k = e - i * kmax;
-                T b = (k <= n0 + i) ? Bi[(int64_t)(n0 + i) * ld + k] : T(0);
-                if (ldl) b = b * D[(int64_t)(n0 + i) * ld + n0 + i];
-                return b;
+                const int i = e / kv, q = e - i * kv;
+                return reinterpret_cast<const uint4 *>(Bi + (int64_t)(n0 + i) * ld)[q];
             },
-            [&](int e, T v) { P[e] = v; });
+            [&](int e, uint4 x) {
+                const int i = e / kv, q = e - i * kv;
+                reinterpret_cast<uint4 *>(P + (int64_t)i * kp)[q] = x;
+            });
         __syncthreads();
         if (!backward) {
             for (int e = tid; e < nr * nrhs; e += nt) {
                 const int i = e / nrhs, r = e - i * nrhs;
                 T s = T(0);
-                const T *row = P + (int64_t)i * kmax;
+                const T *row = P + (int64_t)i * kp;
 #pragma unroll 4
                 for (int k = 0; k <= n0 + i; k++) s += (cjp ? conj_v(row[k]) : row[k]) * v[k * nrhs + r];
+                if (ldl) {
+                    const T d = D[(int64_t)(n0 + i) * ld + n0 + i];
+                    s = s * (cjp ? conj_v(d) : d);
+                }
                 Bg[(int64_t)r * ldb + fc + n0 + i] = s;
             }
         } else {
@@ -62,7 +74,7 @@ __device__ void diag_solve_inverse(const T *__restrict__ Bi, const T *__restrict
                 const int k = e / nrhs, r = e - k * nrhs;
                 T s = T(0);
 #pragma unroll 4
-                for (int i = max(0, k - n0); i < nr; i++) s += P[(int64_t)i * kmax + k] * v[(n0 + i) * nrhs + r];
+                for (int i = max(0, k - n0); i < nr; i++) s += P[(int64_t)i * kp + k] * v[(n0 + i) * nrhs + r];
                 outp[e] += s;
             }
         }
@@ -77,7 +89,7 @@ __device__ void diag_solve_inverse(const T *__restrict__ Bi, const T *__restrict
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
+__global__ void __launch_bounds__(1024) k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
                                                   T *__restrict__ B, int ldb, int nrhs, int unit, int pch,
                                                   const T *__restrict__ inv, int ldl, int cjp, int ipch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -221,7 +233,7 @@ __global__ void k_bwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
 // above from the tile's panel staged in shared memory (pch rows at a time).
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
+__global__ void __launch_bounds__(1024) k_bwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
                                                   T *__restrict__ B, int ldb, int nrhs, int upper, int unit, int cjp,
                                                   int pch, const T *__restrict__ inv, int ldl, int ipch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
