@@ -97,6 +97,12 @@ struct pastix_gpu_s {
     std::vector<cudaEvent_t> la_events;
     std::vector<int> tile_crit, tctile_crit;   // per level: critical (next-level) tiles first
     double side_ms[4] = {0};                   // stream2 GEMM time of the last numfact, per phase
+    // CUDA graph of the factorization sequence (norm .. last level), replayed
+    // while the plan, the coeftab and the value buffers stay the same
+    bool capturing = false;
+    cudaGraph_t fact_graph = nullptr;
+    cudaGraphExec_t fact_exec = nullptr;
+    int64_t graph_key[4] = {-1, -1, -1, -1};
     double thflops[2][3] = {{0}};   // [complex][POTRF, GETRF, LDL] algorithmic flops
 
     // ---- device structure ----
@@ -700,6 +706,7 @@ struct LaunchTimer {
     explicit LaunchTimer(pastix_gpu_t &c) : C(c), st(c.stream), pool(c.evpool) {}
     LaunchTimer(pastix_gpu_t &c, cudaStream_t s, std::vector<cudaEvent_t> &p) : C(c), st(s), pool(p) {}
     cudaError_t mark(int kind) {
+        if (C.capturing) return cudaSuccess;   // no timing inside a captured graph
         if (used >= (int)pool.size()) {
             cudaEvent_t e;
             cudaError_t r = cudaEventCreate(&e);
@@ -783,14 +790,14 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     const bool la = lookahead_enabled() && !C.record;
     LaunchTimer tm2(C, C.stream2, C.evpool2);
     if (la) {
-        while ((int)C.la_events.size() < 2 * C.nlevels) {
+        while ((int)C.la_events.size() < 2 * C.nlevels + 1) {
             cudaEvent_t e;
             PGPU_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             C.la_events.push_back(e);
         }
-        // stream2 starts after the fill-in (recorded by the caller on the main stream)
-        PGPU_CHECK(cudaEventRecord(C.ev[1], s));
-        PGPU_CHECK(cudaStreamWaitEvent(C.stream2, C.ev[1], 0));
+        // stream2 forks from the main stream after the fill-in
+        PGPU_CHECK(cudaEventRecord(C.la_events[2 * C.nlevels], s));
+        PGPU_CHECK(cudaStreamWaitEvent(C.stream2, C.la_events[2 * C.nlevels], 0));
     }
     auto launch_gemms = [&](cudaStream_t st, LaunchTimer &lt, int t0, int nt, int c0, int ntc, int gcap) -> int {
         if (nt) {
@@ -918,7 +925,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     PGPU_CHECK(tm.mark(PH_END));
     PGPU_CHECK(cudaGetLastError());
     std::fill(C.side_ms, C.side_ms + 4, 0.0);
-    if (la) {
+    if (la && !C.capturing) {
         PGPU_CHECK(cudaStreamSynchronize(C.stream2));
         tm2.collect(C.side_ms, 4);
     }
@@ -974,25 +981,59 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     // values in (pastix_subtask_spm2bcsc), norm, bcsc -> coeftab
     PGPU_CHECK(cudaMemcpyAsync(C.d_vals.p, values, C.nnz * vsz,
                                is_device_ptr(values) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
-    if (zc) dev_norm_and_crit<cdouble>(C, C.dparm[PGPU_DPARM_EPSILON_MAGN_CTRL]);
-    else dev_norm_and_crit<double>(C, C.dparm[PGPU_DPARM_EPSILON_MAGN_CTRL]);
-    if (zc)
-        k_gather_vals<cdouble><<<1024, 256, 0, s>>>(C.csr_nnz, C.d_csr_src.p, (const cdouble *)C.d_vals.p,
-                                                    (cdouble *)C.d_csr_val.p);
-    else
-        k_gather_vals<double><<<1024, 256, 0, s>>>(C.csr_nnz, C.d_csr_src.p, C.d_vals.p, C.d_csr_val.p);
-    PGPU_CHECK(cudaMemsetAsync(C.d_status.p, 0, sizeof(Status), s));
-    PGPU_CHECK(cudaMemsetAsync(C.d_coef.p, 0, ncoef * esz, s));
     int launches = 4;
     int nl = 0;
     LaunchTimer tm(C);
-    if (zc)
-        rc = mixed ? fill_and_factor<cfloat, cdouble>(C, fmode, &nl, tm)
-                   : fill_and_factor<cdouble, cdouble>(C, fmode, &nl, tm);
-    else
-        rc = mixed ? fill_and_factor<float, double>(C, fmode, &nl, tm)
-                   : fill_and_factor<double, double>(C, fmode, &nl, tm);
-    if (rc) return rc;
+    auto enqueue = [&]() -> int {
+        if (zc) dev_norm_and_crit<cdouble>(C, C.dparm[PGPU_DPARM_EPSILON_MAGN_CTRL]);
+        else dev_norm_and_crit<double>(C, C.dparm[PGPU_DPARM_EPSILON_MAGN_CTRL]);
+        if (zc)
+            k_gather_vals<cdouble><<<1024, 256, 0, s>>>(C.csr_nnz, C.d_csr_src.p, (const cdouble *)C.d_vals.p,
+                                                        (cdouble *)C.d_csr_val.p);
+        else
+            k_gather_vals<double><<<1024, 256, 0, s>>>(C.csr_nnz, C.d_csr_src.p, C.d_vals.p, C.d_csr_val.p);
+        PGPU_CHECK(cudaMemsetAsync(C.d_status.p, 0, sizeof(Status), s));
+        PGPU_CHECK(cudaMemsetAsync(C.d_coef.p, 0, ncoef * esz, s));
+        if (zc)
+            return mixed ? fill_and_factor<cfloat, cdouble>(C, fmode, &nl, tm)
+                         : fill_and_factor<cdouble, cdouble>(C, fmode, &nl, tm);
+        return mixed ? fill_and_factor<float, double>(C, fmode, &nl, tm)
+                     : fill_and_factor<double, double>(C, fmode, &nl, tm);
+    };
+    // PASTIX_GPU_GRAPH=1: capture the sequence once per (plan, coeftab,
+    // mode) and replay it; the per-phase timings are then not available
+    const char *ge = getenv("PASTIX_GPU_GRAPH");
+    const bool graph = ge && std::strcmp(ge, "1") == 0 && !C.record;
+    bool replayed = false;
+    if (graph) {
+        const int64_t key[4] = {C.plan_fact, (int64_t)(uintptr_t)C.d_coef.p, mixed * 8 + fmode,
+                                (int64_t)(uintptr_t)C.d_vals.p};
+        if (!C.fact_exec || std::memcmp(key, C.graph_key, sizeof(key)) != 0) {
+            if (C.fact_exec) cudaGraphExecDestroy(C.fact_exec);
+            if (C.fact_graph) cudaGraphDestroy(C.fact_graph);
+            C.fact_exec = nullptr;
+            C.fact_graph = nullptr;
+            PGPU_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            C.capturing = true;
+            rc = enqueue();
+            C.capturing = false;
+            cudaGraph_t g = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(s, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            PGPU_CHECK(ec);
+            C.fact_graph = g;
+            PGPU_CHECK(cudaGraphInstantiate(&C.fact_exec, g, 0));
+            std::memcpy(C.graph_key, key, sizeof(key));
+        }
+        PGPU_CHECK(cudaGraphLaunch(C.fact_exec, s));
+        replayed = true;
+    } else {
+        rc = enqueue();
+        if (rc) return rc;
+    }
     PGPU_CHECK(cudaEventRecord(C.ev[1], s));
     Status st;
     double fscal[2];
@@ -1014,6 +1055,7 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
         C.stats[11] = ph[PH_TC] + C.side_ms[PH_TC];
         C.stats[12] = mixed ? C.tc_flops : 0.0;
         C.stats[13] = st.timeout;
+        C.stats[14] = replayed ? 1.0 : 0.0;
     }
     if (st.timeout) {
         fprintf(stderr, "pastix_gpu: %d tensor-core GEMM tiles timed out waiting for their MMAs\n", st.timeout);
@@ -1077,7 +1119,7 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         if (inv && C.inv_ptr[l + 1] > C.inv_ptr[l]) {
             // rows of the inverse are staged padded to 16 bytes
             const size_t rowb = (size_t)round_up(mw, 16 / (int64_t)es) * es;
-            const size_t fixed_i = (size_t)2 * mw * nrhs * es;
+            const size_t fixed_i = ((size_t)2 * mw * nrhs + 16) * es;   // + alignment of the staged rows
             dsm = std::min<size_t>(SMEM_LIMIT, std::max(fixed_i + (size_t)128 * rowb, fixed + (size_t)mw * 33 * es));
             *ipch = dsm > fixed_i ? (int)std::min<size_t>(mw, (dsm - fixed_i) / rowb) : 0;
         } else {
@@ -2113,6 +2155,8 @@ extern "C" void pastix_gpu_finalize(pastix_gpu_t **pctx) {
     for (auto &e : C->evpool) cudaEventDestroy(e);
     for (auto &e : C->evpool2) cudaEventDestroy(e);
     for (auto &e : C->la_events) cudaEventDestroy(e);
+    if (C->fact_exec) cudaGraphExecDestroy(C->fact_exec);
+    if (C->fact_graph) cudaGraphDestroy(C->fact_graph);
     if (C->stream2) {
         cudaStreamSynchronize(C->stream2);
         cudaStreamDestroy(C->stream2);

@@ -27,6 +27,13 @@ constexpr int SOLVE_MAXRHS = 16;
 // x_k = sum_n Binv[n][k] s_n z_n.  The rows of Binv are staged in shared
 // memory pch rows at a time (coalesced), the dot products run from there:
 // one burst of loads per chunk instead of a chain per 32-column tile.
+// element count rounded up to a whole number of 16-byte vectors
+template <typename T>
+__host__ __device__ inline size_t align16_elems(size_t n) {
+    const size_t v = 16 / sizeof(T) > 0 ? 16 / sizeof(T) : 1;
+    return (n + v - 1) / v * v;
+}
+
 template <typename T>
 __device__ void diag_solve_inverse(const T *__restrict__ Bi, const T *__restrict__ D, int w, int ld, int nrhs,
                                    bool backward, bool ldl, bool cjp, T *__restrict__ v, T *__restrict__ outp,
@@ -102,10 +109,12 @@ __global__ void __launch_bounds__(1024) k_fwd_diag(Meta m, const int *__restrict
         w * nrhs, tid, nt, [&](int e) { const int j = e / nrhs, r = e - j * nrhs; return B[(int64_t)r * ldb + fc + j]; },
         [&](int e, T v) { y[e] = v; });
     if (inv && m.invoff[c] >= 0) {
-        // LU: the unit-lower inverse is the cblk's second one
+        // LU: the unit-lower inverse is the cblk's second one; the staged
+        // rows start on a 16-byte boundary (vector stores)
         __syncthreads();
         diag_solve_inverse<T>(inv + m.invoff[c] + (unit && !ldl ? inv_span(w, ld) : 0), D, w, ld, nrhs, false,
-                              ldl != 0, cjp != 0, y, nullptr, y + (size_t)w * nrhs, ipch, B, ldb, fc);
+                              ldl != 0, cjp != 0, y, nullptr, y + align16_elems<T>((size_t)w * nrhs), ipch, B, ldb,
+                              fc);
         return;
     }
     T *tile = y + w * nrhs;                   // [32][33] diagonal tile
@@ -248,7 +257,7 @@ __global__ void __launch_bounds__(1024) k_bwd_diag(Meta m, const int *__restrict
     if (inv && m.invoff[c] >= 0) {
         __syncthreads();
         diag_solve_inverse<T>(inv + m.invoff[c], D, w, ld, nrhs, true, ldl != 0, false, x, x + (size_t)w * nrhs,
-                              x + (size_t)2 * w * nrhs, ipch, B, ldb, fc);
+                              x + align16_elems<T>((size_t)2 * w * nrhs), ipch, B, ldb, fc);
         return;
     }
     T *tile = x + w * nrhs;                   // [32][33] diagonal tile (op applied)

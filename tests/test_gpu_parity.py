@@ -270,3 +270,31 @@ def test_hetrf_gmres_refinement_reaches_1e12(mixed):
     ip, _ = s.params()
     assert ip[52] <= (10 if mixed else 2)
     s.close()
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_factorization_graph_replay_matches_direct(mixed, monkeypatch):
+    """PASTIX_GPU_GRAPH=1: the factorization sequence (norm, fill-in, every
+    level's panels, TRSMs and update GEMMs on both lookahead streams) is
+    captured once and replayed; its factors equal the directly launched
+    ones and a new set of values reuses the same graph."""
+    A = M.diffusion_lognormal(24, 23, 22, 1.0, np.random.default_rng(21))
+    ref, st = U.run_reference(A, "potrf", numfact=False)
+    s = _gpu_solver(A, st, "potrf", mixed=mixed)
+    s.numfact(A.values)
+    L0, _ = s.coeftab()
+    monkeypatch.setenv("PASTIX_GPU_GRAPH", "1")
+    s.numfact(A.values)                  # capture
+    s.numfact(A.values)                  # replay
+    assert s.stats()["graph_replayed"] == 1.0
+    L1, _ = s.coeftab()
+    tol = 1e-12 if not mixed else 1e-5
+    assert np.abs(L1.astype(np.float64) - L0).max() <= tol * np.abs(L0).max()
+    vals2 = A.values * 2.0               # same pattern, new values: same graph
+    s.numfact(vals2)
+    L2, _ = s.coeftab()
+    assert np.abs(L2.astype(np.float64) - np.sqrt(2.0) * L0).max() <= 10 * tol * np.abs(L0).max()
+    x, b = M.rhs_from_xtrue(A, 2, np.random.default_rng(3))
+    xs = s.solve(2.0 * b)
+    assert np.abs(xs - x).max() <= (1e-9 if not mixed else 1e-3)
+    s.close()
