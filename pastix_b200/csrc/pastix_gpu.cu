@@ -1102,6 +1102,13 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
     PGPU_CHECK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(k_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(k_fwd_off<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
+    PGPU_CHECK(cudaFuncSetAttribute(k_bwd_off<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
+    // off-diagonal kernels: the chunk's rows (padded to 16 bytes) + the RHS values they need
+    auto off_smem = [&](int mw, bool fwd) {
+        const size_t wp = (size_t)round_up(mw, 16 / (int64_t)sizeof(T));
+        const size_t rhs = fwd ? (size_t)nrhs * wp : (size_t)SOLVE_ROWS_PER_CHUNK * nrhs;
+        return (align16_elems<T>(rhs) + (size_t)SOLVE_ROWS_PER_CHUNK * wp) * sizeof(T);
+    };
     // PASTIX_GPU_SOLVE_PROFILE=1: device time per solve phase on stderr (diagnostics)
     static const bool prof = getenv("PASTIX_GPU_SOLVE_PROFILE") != nullptr;
     LaunchTimer tm(C);
@@ -1145,7 +1152,7 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
             PGPU_CHECK(mark(1));
-            k_fwd_off<T><<<nch, 256, (size_t)mw * nrhs * sizeof(T), s>>>(
+            k_fwd_off<T><<<nch, 256, off_smem(mw, true), s>>>(
                 C.meta, C.d_solve_chunks.p + C.solve_ptr[l], coefL, W, ldb, nrhs, SOLVE_ROWS_PER_CHUNK);
             nl++;
         }
@@ -1161,7 +1168,7 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
             PGPU_CHECK(mark(3));
-            k_bwd_off<T><<<nch, 128, (size_t)SOLVE_ROWS_PER_CHUNK * nrhs * sizeof(T), s>>>(
+            k_bwd_off<T><<<nch, 256, off_smem(mw, false), s>>>(
                 C.meta, C.d_solve_chunks.p + C.solve_ptr[l], coefU, W, ldb, nrhs, SOLVE_ROWS_PER_CHUNK,
                 lu ? 0 : cjp);
             nl++;
@@ -1206,6 +1213,12 @@ static int ensure_work(pastix_gpu_t &C) {
 // Permute in (down-casting for single-precision factors), solve, permute out.
 template <typename S, typename T>
 static int solve_block_t(pastix_gpu_t &C, S *dB, int64_t ldb, int nrhs, T *W, int *launches) {
+    // complex128 factors: at most 8 right-hand sides per pass (shared-memory staging of the solve kernels)
+    if (sizeof(T) == 16 && nrhs > 8) {
+        int rc = solve_block_t<S, T>(C, dB, ldb, 8, W, launches);
+        if (rc) return rc;
+        return solve_block_t<S, T>(C, dB + 8 * ldb, ldb, nrhs - 8, W, launches);
+    }
     cudaStream_t s = C.stream;
     const int n = C.n;
     const int grid = std::min(4096, cdiv((int64_t)n * nrhs, 256));

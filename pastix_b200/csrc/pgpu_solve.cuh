@@ -10,6 +10,13 @@ namespace pgpu {
 
 constexpr int SOLVE_MAXRHS = 16;
 
+// element count rounded up to a whole number of 16-byte vectors
+template <typename T>
+__host__ __device__ inline size_t align16_elems(size_t n) {
+    const size_t v = 16 / sizeof(T) > 0 ? 16 / sizeof(T) : 1;
+    return (n + v - 1) / v * v;
+}
+
 // ---------------------------------------------------------------------------
 // Forward, diagonal part (kernels/solve_ztrsmsp.c:75 solve_blok_ztrsm with
 // Left, Lower, NoTrans): B[fcol:fcol+w, :] := D^{-1} B[...], D = L_kk
@@ -27,13 +34,6 @@ constexpr int SOLVE_MAXRHS = 16;
 // x_k = sum_n Binv[n][k] s_n z_n.  The rows of Binv are staged in shared
 // memory pch rows at a time (coalesced), the dot products run from there:
 // one burst of loads per chunk instead of a chain per 32-column tile.
-// element count rounded up to a whole number of 16-byte vectors
-template <typename T>
-__host__ __device__ inline size_t align16_elems(size_t n) {
-    const size_t v = 16 / sizeof(T) > 0 ? 16 / sizeof(T) : 1;
-    return (n + v - 1) / v * v;
-}
-
 template <typename T>
 __device__ void diag_solve_inverse(const T *__restrict__ Bi, const T *__restrict__ D, int w, int ld, int nrhs,
                                    bool backward, bool ldl, bool cjp, T *__restrict__ v, T *__restrict__ outp,
@@ -168,28 +168,36 @@ __global__ void __launch_bounds__(1024) k_fwd_diag(Meta m, const int *__restrict
 // the subtraction is atomic.  chunks[i] = {cblk, first panel row}.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_fwd_off(Meta m, const int2 *__restrict__ chunks, const T *__restrict__ coef,
-                          T *__restrict__ B, int ldb, int nrhs, int rows_per_chunk) {
+__global__ void __launch_bounds__(256) k_fwd_off(Meta m, const int2 *__restrict__ chunks, const T *__restrict__ coef,
+                                                 T *__restrict__ B, int ldb, int nrhs, int rows_per_chunk) {
+    // the chunk's rows are staged in shared memory with 16-byte vector
+    // loads (one burst), then one warp per row reads them from there
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *y = reinterpret_cast<T *>(smem_raw);   // [nrhs][w]
+    constexpr int VEC = 16 / sizeof(T);
     const int2 ch = chunks[blockIdx.x];
     const int c = ch.x, r0 = ch.y;
     const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c], h = m.height[c];
+    const int wv = (w + VEC - 1) / VEC, wp = wv * VEC;
+    const int rend = min(h, r0 + rows_per_chunk), nr = rend - r0;
+    T *y = reinterpret_cast<T *>(smem_raw);            // [nrhs][wp] (zero padded)
+    T *Pr = y + align16_elems<T>((size_t)nrhs * wp);    // [nr][wp]
     const int tid = threadIdx.x, nt = blockDim.x;
+    const T *P = coef + m.coefoff[c] + (int64_t)r0 * ld;
+    batched_copy<4>(
+        nr * wv, tid, nt, [&](int e) { const int i = e / wv, q = e - i * wv; return reinterpret_cast<const uint4 *>(P + (int64_t)i * ld)[q]; },
+        [&](int e, uint4 v) { const int i = e / wv, q = e - i * wv; reinterpret_cast<uint4 *>(Pr + (int64_t)i * wp)[q] = v; });
     batched_copy(
-        w * nrhs, tid, nt, [&](int e) { const int r = e / w, j = e - r * w; return B[(int64_t)r * ldb + fc + j]; },
+        nrhs * wp, tid, nt,
+        [&](int e) { const int r = e / wp, j = e - r * wp; return j < w ? B[(int64_t)r * ldb + fc + j] : T(0); },
         [&](int e, T v) { y[e] = v; });
     __syncthreads();
     const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    const T *P = coef + m.coefoff[c];
-    const int rend = min(h, r0 + rows_per_chunk);
-    for (int i = r0 + warp; i < rend; i += nw) {
-        const T *row = P + (int64_t)i * ld;
-        const int grow = m.rowidx[m.rowbase[c] + i];
+    for (int i = warp; i < nr; i += nw) {
+        const T *row = Pr + (int64_t)i * wp;
+        const int grow = m.rowidx[m.rowbase[c] + r0 + i];
         for (int r = 0; r < nrhs; r++) {
             T s = T(0);
-#pragma unroll 4
-            for (int j = lane; j < w; j += 32) s += row[j] * y[r * w + j];
+            for (int j = lane; j < w; j += 32) s += row[j] * y[r * wp + j];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += shfl_xor_v(s, o);
             if (lane == 0) atomic_sub(&B[(int64_t)r * ldb + grow], s);
@@ -201,34 +209,41 @@ __global__ void k_fwd_off(Meta m, const int2 *__restrict__ chunks, const T *__re
 // Backward, off-diagonal gather (kernels/solve_ztrsmsp.c:450
 // solve_cblk_ztrsmsp_backward walks browtab): B[fcol+j, :] -= sum_i op(P[i, j])
 // B[row_i, :] over panel rows i >= w of cblk c (P = L for POTRF / LDL, U^T
-// for GETRF; op = conj for the Hermitian forms when cjp).  Threads along j (coalesced in the row-major panel); a chunk of
-// rows per CTA, partial sums combined atomically.
+// for GETRF; op = conj for the Hermitian forms when cjp).  The chunk's rows
+// are staged in shared memory (16-byte vector loads), then one thread per
+// column sums them; partial sums of the chunks are combined atomically.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_bwd_off(Meta m, const int2 *__restrict__ chunks, const T *__restrict__ coef,
-                          T *__restrict__ B, int ldb, int nrhs, int rows_per_chunk, int cjp) {
+__global__ void __launch_bounds__(256) k_bwd_off(Meta m, const int2 *__restrict__ chunks, const T *__restrict__ coef,
+                                                 T *__restrict__ B, int ldb, int nrhs, int rows_per_chunk, int cjp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *xr = reinterpret_cast<T *>(smem_raw);   // [rows][nrhs]: the solution at the chunk's rows
+    constexpr int VEC = 16 / sizeof(T);
     const int2 ch = chunks[blockIdx.x];
     const int c = ch.x, r0 = ch.y;
     const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c], h = m.height[c];
-    const T *P = coef + m.coefoff[c];
+    const int wv = (w + VEC - 1) / VEC, wp = wv * VEC;
     const int rend = min(h, r0 + rows_per_chunk), nr = rend - r0;
-    for (int e = threadIdx.x; e < nr * nrhs; e += blockDim.x) {
-        const int i = e / nrhs, r = e - i * nrhs;
-        xr[e] = B[(int64_t)r * ldb + m.rowidx[m.rowbase[c] + r0 + i]];
-    }
+    T *xr = reinterpret_cast<T *>(smem_raw);            // [rows][nrhs]: the solution at the chunk's rows
+    T *Pr = xr + align16_elems<T>((size_t)rows_per_chunk * nrhs);   // [nr][wp]
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const T *P = coef + m.coefoff[c] + (int64_t)r0 * ld;
+    batched_copy<4>(
+        nr * wv, tid, nt, [&](int e) { const int i = e / wv, q = e - i * wv; return reinterpret_cast<const uint4 *>(P + (int64_t)i * ld)[q]; },
+        [&](int e, uint4 v) { const int i = e / wv, q = e - i * wv; reinterpret_cast<uint4 *>(Pr + (int64_t)i * wp)[q] = v; });
+    batched_copy(
+        nr * nrhs, tid, nt,
+        [&](int e) { const int i = e / nrhs, r = e - i * nrhs; return B[(int64_t)r * ldb + m.rowidx[m.rowbase[c] + r0 + i]]; },
+        [&](int e, T v) { xr[e] = v; });
     __syncthreads();
-    for (int j = threadIdx.x; j < w; j += blockDim.x) {
-        T s[SOLVE_MAXRHS];
-        for (int r = 0; r < nrhs; r++) s[r] = T(0);
-#pragma unroll 4
+    for (int e = tid; e < w * nrhs; e += nt) {
+        const int j = e % w, r = e / w;
+        T s = T(0);
+#pragma unroll 8
         for (int i = 0; i < nr; i++) {
-            const T v = P[(int64_t)(r0 + i) * ld + j];
-            const T pij = cjp ? conj_v(v) : v;
-            for (int r = 0; r < nrhs; r++) s[r] += pij * xr[i * nrhs + r];
+            const T v = Pr[(int64_t)i * wp + j];
+            s += (cjp ? conj_v(v) : v) * xr[i * nrhs + r];
         }
-        for (int r = 0; r < nrhs; r++) atomic_sub(&B[(int64_t)r * ldb + fc + j], s[r]);
+        atomic_sub(&B[(int64_t)r * ldb + fc + j], s);
     }
 }
 
