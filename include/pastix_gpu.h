@@ -211,6 +211,29 @@ PASTIX_GPU_API int pastix_gpu_record_tasks( pastix_gpu_t *ctx, int on );
 PASTIX_GPU_API int pastix_gpu_task_records( pastix_gpu_t *ctx, int64_t *count, int64_t *info, double *ns );
 PASTIX_GPU_API int pastix_gpu_set_cblk_priority( pastix_gpu_t *ctx, const double *prio );
 
+/*
+ * Kernel variants and launch shapes (the autotuner's knobs, no reference
+ * counterpart; the reference's equivalents are compile-time block sizes):
+ *   PGPU_TUNE_MIXED_GEMM      0 FP32 FMA, 1 TF32, 2 3xTF32 (default) update GEMMs
+ *   PGPU_TUNE_TC_KERNEL       1 persistent warp-specialized (default), 0 one tile per CTA
+ *   PGPU_TUNE_LOOKAHEAD       1 (default): deferred update GEMMs on a second stream
+ *   PGPU_TUNE_LA_RESERVED_SMS SMs left to the critical path by the second stream (16)
+ *   PGPU_TUNE_TRSM_GEMM       1 (default): tall panels' TRSM as a GEMM against the inverse
+ *   PGPU_TUNE_TRSM_GEMM_ROWS  panel height above which it applies (256)
+ *   PGPU_TUNE_TC_MIN_MN       smallest M x N update sent to the tensor cores (8192)
+ * Setting one invalidates the factorization plan (rebuilt by the next numfact).
+ */
+#define PGPU_TUNE_MIXED_GEMM      0
+#define PGPU_TUNE_TC_KERNEL       1
+#define PGPU_TUNE_LOOKAHEAD       2
+#define PGPU_TUNE_LA_RESERVED_SMS 3
+#define PGPU_TUNE_TRSM_GEMM       4
+#define PGPU_TUNE_TRSM_GEMM_ROWS  5
+#define PGPU_TUNE_TC_MIN_MN       6
+#define PGPU_TUNE_COUNT           7
+PASTIX_GPU_API int pastix_gpu_set_tuning( pastix_gpu_t *ctx, int key, int64_t value );
+PASTIX_GPU_API int pastix_gpu_get_tuning( pastix_gpu_t *ctx, int key, int64_t *value );
+
 /* Copy the output parameters (iparm/dparm, reference indices) out. */
 PASTIX_GPU_API int pastix_gpu_get_params( pastix_gpu_t *ctx, int64_t *iparm, double *dparm );
 /* Change one parameter between calls (e.g. IPARM_MIXED, IPARM_REFINEMENT). */

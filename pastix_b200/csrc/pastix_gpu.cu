@@ -130,6 +130,9 @@ struct pastix_gpu_s {
     DArr<double> d_csr_val, d_vals;
     bool have_spm = false;
 
+    // ---- tuning (pastix_gpu_set_tuning; the autotuner's knobs) ----
+    int64_t tune[PGPU_TUNE_COUNT] = {0};
+
     // ---- numerical state ----
     DArr<unsigned char> d_coef;
     int coef_float = 0;     // factor precision of d_coef
@@ -177,6 +180,8 @@ static void default_params(int64_t *iparm, double *dparm) {
     dparm[PGPU_DPARM_EPSILON_MAGN_CTRL] = 0.0;
 }
 
+static void default_tuning(int64_t *t);
+
 extern "C" int pastix_gpu_init(pastix_gpu_t **pctx, int device, const int64_t *iparm, const double *dparm) {
     if (!pctx) return PASTIX_GPU_ERR_BADPARAMETER;
     *pctx = nullptr;
@@ -191,6 +196,7 @@ extern "C" int pastix_gpu_init(pastix_gpu_t **pctx, int device, const int64_t *i
     pastix_gpu_t *ctx = new pastix_gpu_t();
     ctx->device = device;
     default_params(ctx->iparm, ctx->dparm);
+    default_tuning(ctx->tune);
     if (iparm) std::memcpy(ctx->iparm, iparm, sizeof(ctx->iparm));
     if (dparm) std::memcpy(ctx->dparm, dparm, sizeof(ctx->dparm));
     int prio_lo = 0, prio_hi = 0;
@@ -490,31 +496,36 @@ static int fuse_rows_for(bool lu, size_t esz) {
 static const int TRSM_TR = 32;   // panel rows per k_trsm_rows CTA
 
 // Single-precision update GEMMs large enough for a 128 x 128 tensor-core tile
-// go to k_gemm_scatter_tc.  PASTIX_GPU_MIXED_GEMM selects the operand mode:
-// "3xtf32" (default; split products, about FP32 accuracy), "tf32" (one TF32
-// product) or "fp32" (no tensor cores: FP32 FMA tiles only).
+// go to the tcgen05 kernel.  Tuning PGPU_TUNE_MIXED_GEMM selects the operand
+// mode: 3xTF32 (default; split products, about FP32 accuracy), TF32 (one
+// product) or FP32 (no tensor cores: FMA tiles only); its default comes from
+// PASTIX_GPU_MIXED_GEMM = 3xtf32 | tf32 | fp32.  The other knobs and their
+// environment defaults: PGPU_TUNE_TC_KERNEL (PASTIX_GPU_TC_KERNEL=tile: one
+// tile per CTA instead of the persistent kernel), PGPU_TUNE_LOOKAHEAD
+// (PASTIX_GPU_LOOKAHEAD=0 disables it), PGPU_TUNE_LA_RESERVED_SMS (16),
+// PGPU_TUNE_TRSM_GEMM (PASTIX_GPU_TRSM=rows disables the TRSM-as-GEMM path),
+// PGPU_TUNE_TRSM_GEMM_ROWS (256: panels taller than this take it),
+// PGPU_TUNE_TC_MIN_MN (8192: smallest M x N sent to the tensor cores).
 enum { MG_FP32 = 0, MG_TF32 = 1, MG_3XTF32 = 2 };
-static int mixed_gemm_mode() {
+static void default_tuning(int64_t *t) {
     const char *e = getenv("PASTIX_GPU_MIXED_GEMM");
-    if (e && std::strcmp(e, "fp32") == 0) return MG_FP32;
-    if (e && std::strcmp(e, "tf32") == 0) return MG_TF32;
-    return MG_3XTF32;
+    t[PGPU_TUNE_MIXED_GEMM] = (e && std::strcmp(e, "fp32") == 0) ? MG_FP32
+                              : (e && std::strcmp(e, "tf32") == 0) ? MG_TF32 : MG_3XTF32;
+    e = getenv("PASTIX_GPU_TC_KERNEL");
+    t[PGPU_TUNE_TC_KERNEL] = (e && std::strcmp(e, "tile") == 0) ? 0 : 1;
+    e = getenv("PASTIX_GPU_LOOKAHEAD");
+    t[PGPU_TUNE_LOOKAHEAD] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
+    t[PGPU_TUNE_LA_RESERVED_SMS] = 16;
+    e = getenv("PASTIX_GPU_TRSM");
+    t[PGPU_TUNE_TRSM_GEMM] = (e && std::strcmp(e, "rows") == 0) ? 0 : 1;
+    t[PGPU_TUNE_TRSM_GEMM_ROWS] = 256;
+    t[PGPU_TUNE_TC_MIN_MN] = 128 * 64;
 }
-static bool tc_enabled() { return mixed_gemm_mode() != MG_FP32; }
-// PASTIX_GPU_TC_KERNEL=tile selects the one-tile-per-CTA tensor-core kernel
-// instead of the persistent warp-specialized one.
-static bool tc_persistent() {
-    const char *e = getenv("PASTIX_GPU_TC_KERNEL");
-    return !(e && std::strcmp(e, "tile") == 0);
+static int mixed_gemm_mode(const pastix_gpu_t &C) { return (int)C.tune[PGPU_TUNE_MIXED_GEMM]; }
+static bool tc_enabled(const pastix_gpu_t &C) { return mixed_gemm_mode(C) != MG_FP32; }
+static bool tc_task(const pastix_gpu_t &C, int M, int N, int K) {
+    return K >= 32 && M >= 64 && N >= 32 && (int64_t)M * N >= C.tune[PGPU_TUNE_TC_MIN_MN];
 }
-// PASTIX_GPU_LOOKAHEAD=0 runs every update GEMM of a level on the main
-// stream before the next level's panels.
-static bool lookahead_enabled() {
-    const char *e = getenv("PASTIX_GPU_LOOKAHEAD");
-    return !(e && std::strcmp(e, "0") == 0);
-}
-static const int LA_RESERVED_SMS = 16;   // left free by stream2's persistent GEMMs for the critical path
-static bool tc_task(int M, int N, int K) { return K >= 32 && M >= 64 && N >= 32 && (int64_t)M * N >= 128 * 64; }
 
 // Kernel form of a factorization request (pastix_factotype_t on a real or
 // complex matrix): the real LDL^h is the LDL^t, LL^t of a complex symmetric
@@ -530,25 +541,20 @@ static int fact_mode_of(int fact, bool zc) {
     }
 }
 
-// Panels of LL^t / LDL taller than this many rows get the TRSM-as-GEMM path
-// (inverse of the diagonal block, off-diagonal rows times it on the tensor
-// cores for single precision); PASTIX_GPU_TRSM=rows keeps the row-solve
-// kernel for every panel.
-static const int TRSM_GEMM_ROWS = 256;
-static bool trsm_gemm_enabled() {
-    const char *e = getenv("PASTIX_GPU_TRSM");
-    return !(e && std::strcmp(e, "rows") == 0);
-}
 
 static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
-    const bool use_tc = fp32 && !zc && tc_enabled() && (fmode == FM_POTRF || fmode == FM_GETRF);
+    const bool use_tc = fp32 && !zc && tc_enabled(C) && (fmode == FM_POTRF || fmode == FM_GETRF);
     const bool lu = (fmode == FM_GETRF), ldl = fm_ldl(fmode);
-    const bool tgemm = !C.record && trsm_gemm_enabled();
+    // panels taller than TRSM_GEMM_ROWS: inverse of the diagonal block, then the
+    // off-diagonal rows times it as a GEMM (tensor cores in single precision)
+    const bool tgemm = !C.record && C.tune[PGPU_TUNE_TRSM_GEMM] != 0;
     const int key = ((((fmode * 2 + (fp32 ? 1 : 0)) * 2 + (use_tc ? 1 : 0)) * 2 + (zc ? 1 : 0)) * 2 + (tgemm ? 1 : 0));
+    // (set_tuning invalidates the plan, so the knobs need no place in the key)
     if (C.plan_fact == key) return PASTIX_GPU_SUCCESS;
     const size_t esz = (fp32 ? 4 : 8) * (zc ? 2 : 1);
-    const int fuse = tgemm ? std::min(TRSM_GEMM_ROWS, fuse_rows_for(lu, esz)) : fuse_rows_for(lu, esz);
-    const bool tc_trsm = tgemm && fp32 && !zc && tc_enabled();
+    const int fuse = tgemm ? std::min((int)C.tune[PGPU_TUNE_TRSM_GEMM_ROWS], fuse_rows_for(lu, esz))
+                           : fuse_rows_for(lu, esz);
+    const bool tc_trsm = tgemm && fp32 && !zc && tc_enabled(C);
     std::vector<int2> invjobs;
     std::vector<int4> ttiles, tttiles;
     int64_t inv_elems = 0, scr_max = 0;
@@ -619,7 +625,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
                     const int id = (int)tasks.size();
                     tasks.push_back(GemmTask{c, b, f, arow0, M, flags});
                     gflops += fma_flops * M * N * w;
-                    if (use_tc && tc_task(M, N, w)) {
+                    if (use_tc && tc_task(C, M, N, w)) {
                         tcflops += 2.0 * M * N * w;
                         for (int tm = 0; tm < cdiv(M, TC_BM); tm++)
                             for (int tn = 0; tn < cdiv(N, TC_BN); tn++) {
@@ -760,8 +766,8 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     PGPU_CHECK(cudaFuncSetAttribute(kpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(ktrsm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(k_tri_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
-    const bool split = (mixed_gemm_mode() == MG_3XTF32);
-    const bool persist = tc_persistent() && !C.record;   // task timings need one tile per CTA
+    const bool split = (mixed_gemm_mode(C) == MG_3XTF32);
+    const bool persist = C.tune[PGPU_TUNE_TC_KERNEL] != 0 && !C.record;   // task timings need one tile per CTA
     int nsm = 148;
     if constexpr (std::is_same<T, float>::value) {
         PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -787,7 +793,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     const double *critp = C.d_fact_scal.p + 1;
     int nl = 0, ngemm = 0;
     // lookahead over two streams (off while recording task timings)
-    const bool la = lookahead_enabled() && !C.record;
+    const bool la = C.tune[PGPU_TUNE_LOOKAHEAD] != 0 && !C.record;
     LaunchTimer tm2(C, C.stream2, C.evpool2);
     if (la) {
         while ((int)C.la_events.size() < 2 * C.nlevels + 1) {
@@ -910,7 +916,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             PGPU_CHECK(cudaStreamWaitEvent(C.stream2, C.la_events[2 * l], 0));
             rc = launch_gemms(C.stream2, tm2, C.tile_ptr[l] + C.tile_crit[l], nti - C.tile_crit[l],
                               C.tctile_ptr[l] + C.tctile_crit[l], ntc - C.tctile_crit[l],
-                              std::max(1, nsm - LA_RESERVED_SMS));
+                              std::max(1, nsm - (int)C.tune[PGPU_TUNE_LA_RESERVED_SMS]));
             if (rc) return rc;
             PGPU_CHECK(cudaEventRecord(C.la_events[2 * l + 1], C.stream2));
         } else {
@@ -2095,6 +2101,23 @@ extern "C" int pastix_gpu_set_cblk_priority(pastix_gpu_t *ctx, const double *pri
     PGPU_CHECK(C.d_lvl_cblks.upload(C.lvl_cblks, C.stream));
     PGPU_CHECK(cudaStreamSynchronize(C.stream));
     C.plan_fact = -1;   // launch lists follow the new order
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_set_tuning(pastix_gpu_t *ctx, int key, int64_t value) {
+    if (!ctx || key < 0 || key >= PGPU_TUNE_COUNT) return PASTIX_GPU_ERR_BADPARAMETER;
+    if (key == PGPU_TUNE_MIXED_GEMM && (value < MG_FP32 || value > MG_3XTF32)) return PASTIX_GPU_ERR_BADPARAMETER;
+    if ((key == PGPU_TUNE_TRSM_GEMM_ROWS && value < 32) || (key == PGPU_TUNE_LA_RESERVED_SMS && value < 0) ||
+        (key == PGPU_TUNE_TC_MIN_MN && value < 0))
+        return PASTIX_GPU_ERR_BADPARAMETER;
+    ctx->tune[key] = value;
+    ctx->plan_fact = -1;   // the next numfact rebuilds its launch lists (and graph)
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_get_tuning(pastix_gpu_t *ctx, int key, int64_t *value) {
+    if (!ctx || !value || key < 0 || key >= PGPU_TUNE_COUNT) return PASTIX_GPU_ERR_BADPARAMETER;
+    *value = ctx->tune[key];
     return PASTIX_GPU_SUCCESS;
 }
 
