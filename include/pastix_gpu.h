@@ -203,12 +203,15 @@ PASTIX_GPU_API int pastix_gpu_set_segments( pastix_gpu_t *ctx, int64_t nseg, con
  * (w, h, rows solved in the panel kernel, blocks) for a panel,
  * (w, rows, mode, panel) for a TRSM chunk, (K, M, N, flags) for a GEMM tile,
  * and ns[r] its duration in nanoseconds.
+ * pastix_gpu_task_times: the same records' start and end stamps (device
+ * global timer, ns), times[2 r] and times[2 r + 1], for a timeline.
  * pastix_gpu_set_cblk_priority: predicted cost per cblk; inside each level
  * the panels, TRSM chunks and GEMM tiles of costlier cblks launch first
  * (longest-processing-time order).  NULL restores the cblk order.
  */
 PASTIX_GPU_API int pastix_gpu_record_tasks( pastix_gpu_t *ctx, int on );
 PASTIX_GPU_API int pastix_gpu_task_records( pastix_gpu_t *ctx, int64_t *count, int64_t *info, double *ns );
+PASTIX_GPU_API int pastix_gpu_task_times( pastix_gpu_t *ctx, int64_t *count, int64_t *times );
 PASTIX_GPU_API int pastix_gpu_set_cblk_priority( pastix_gpu_t *ctx, const double *prio );
 
 /*

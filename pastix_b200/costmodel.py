@@ -48,6 +48,7 @@ def _lib():
         P, I64, I, D = C.c_void_p, C.c_int64, C.c_int, C.c_double
         L.pastix_gpu_record_tasks.argtypes = [P, I]
         L.pastix_gpu_task_records.argtypes = [P, P, P, P]
+        L.pastix_gpu_task_times.argtypes = [P, P, P]
         L.pastix_gpu_set_cblk_priority.argtypes = [P, P]
         L.pastix_gpu_mlp_init.argtypes = [C.POINTER(P), I, I, I, C.c_uint64]
         L.pastix_gpu_mlp_params.argtypes = [P, P, P]
@@ -76,6 +77,16 @@ def task_records(solver):
     ns = np.zeros(n, np.float64)
     G._check("pastix_gpu_task_records", L.pastix_gpu_task_records(solver._h, G._p(cnt), G._p(info), G._p(ns)))
     return info, ns
+
+
+def task_times(solver):
+    """(n, 2) int64 start/end device timestamps (ns) of the same records."""
+    L = _lib()
+    cnt = np.zeros(1, np.int64)
+    G._check("pastix_gpu_task_times", L.pastix_gpu_task_times(solver._h, G._p(cnt), None))
+    t = np.zeros((int(cnt[0]), 2), np.int64)
+    G._check("pastix_gpu_task_times", L.pastix_gpu_task_times(solver._h, G._p(cnt), G._p(t)))
+    return t
 
 
 def set_cblk_priority(solver, prio):

@@ -863,12 +863,16 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             T *inv = reinterpret_cast<T *>(C.d_inv.p);
             T *scr = reinterpret_cast<T *>(C.d_scr.p);
             const int nij = C.inv_ptr[l + 1] - C.inv_ptr[l];
-            const size_t ism = ((size_t)mw * PBL + PB * PBL) * sizeof(T);
-            if (ism > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+            // X[w][33] + a 32-row strip of L, kch columns wide (as wide as fits, a multiple of 32)
+            const size_t xs = (size_t)mw * PBL * sizeof(T);
+            if (xs + (size_t)PB * (PB + 1) * sizeof(T) > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+            int kch = (int)std::min<size_t>(round_up(mw, PB), ((SMEM_LIMIT - xs) / ((size_t)PB * sizeof(T)) - 1));
+            kch = std::max(PB, kch / PB * PB);
+            const size_t ism = xs + (size_t)PB * (kch + 1) * sizeof(T);
             PGPU_CHECK(tm.mark(PH_TRSM));
             k_tri_inverse<T><<<nij, 256, ism, s>>>(C.meta, C.d_invjobs.p + C.inv_ptr[l], coefL, inv,
                                                    fm_ldl(fmode) ? 1 : 0, (CPX && fm_conj(fmode)) ? 1 : 0,
-                                                   fm_ldl(fmode) ? 1 : 0, lu ? 1 : 0);
+                                                   fm_ldl(fmode) ? 1 : 0, lu ? 1 : 0, kch);
             nl++;
             const int ntt = C.ttile_ptr[l + 1] - C.ttile_ptr[l];
             if (ntt) {
@@ -2038,7 +2042,21 @@ extern "C" int pastix_gpu_record_tasks(pastix_gpu_t *ctx, int on) {
     return PASTIX_GPU_SUCCESS;
 }
 
+static int task_records_impl(pastix_gpu_t *ctx, int64_t *count, int64_t *info, double *ns, int64_t *times);
+
 extern "C" int pastix_gpu_task_records(pastix_gpu_t *ctx, int64_t *count, int64_t *info, double *ns) {
+    if (!info || !ns) return task_records_impl(ctx, count, nullptr, nullptr, nullptr);
+    return task_records_impl(ctx, count, info, ns, nullptr);
+}
+
+extern "C" int pastix_gpu_task_times(pastix_gpu_t *ctx, int64_t *count, int64_t *times) {
+    if (!times) return task_records_impl(ctx, count, nullptr, nullptr, nullptr);
+    std::vector<int64_t> info(8 * std::max<int64_t>(*count, 0));
+    std::vector<double> ns(std::max<int64_t>(*count, 0));
+    return task_records_impl(ctx, count, info.data(), ns.data(), times);
+}
+
+static int task_records_impl(pastix_gpu_t *ctx, int64_t *count, int64_t *info, double *ns, int64_t *times) {
     if (!ctx || !count) return PASTIX_GPU_ERR_BADPARAMETER;
     auto &C = *ctx;
     if (C.fact_done < 0 || !C.record || C.plan_fact < 0) return PASTIX_GPU_ERR_BADPARAMETER;
@@ -2062,6 +2080,10 @@ extern "C" int pastix_gpu_task_records(pastix_gpu_t *ctx, int64_t *count, int64_
         int64_t *o = info + 8 * r;
         o[0] = kind; o[1] = c; o[2] = a; o[3] = b; o[4] = cc; o[5] = d; o[6] = C.plan_esz; o[7] = C.plan_fmode;
         ns[r] = (double)(tt[1] - tt[0]);
+        if (times) {
+            times[2 * r] = tt[0];
+            times[2 * r + 1] = tt[1];
+        }
         r++;
     };
     for (int q = 0; q < C.cblknbr; q++) {   // panel CTAs, in launch order (lvl_cblks)

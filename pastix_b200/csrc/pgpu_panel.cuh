@@ -379,7 +379,8 @@ namespace pgpu {
 // The strict upper part of B is left untouched (zero from the allocation).
 // One CTA per (cblk, 32-column block jb): columns [jb, jb+32) of the
 // inverse by blocked forward substitution over the 32-row tiles below jb.
-// Shared memory: X[w - jb][33] + Lb[32][33].
+// Shared memory: X[w - jb][33] + Lb[32][kch + 1]: the rows of a 32-row tile
+// left of it are staged kch columns at a time (one burst of loads per chunk).
 // ---------------------------------------------------------------------------
 // LU (lu != 0): job.y = jb + (kind << 20); kind 0 inverts U^t (the upper
 // triangle of the diagonal block read transposed, non-unit) into the first
@@ -388,7 +389,7 @@ namespace pgpu {
 template <typename T>
 __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restrict__ jobs,
                                                      const T *__restrict__ coefL, T *__restrict__ inv,
-                                                     int unit, int cjp, int scale_d, int lu) {
+                                                     int unit, int cjp, int scale_d, int lu, int kch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int2 jbv = jobs[blockIdx.x];
     const int c = jbv.x, jb = jbv.y & 0xFFFFF, kind = jbv.y >> 20;
@@ -399,7 +400,8 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
     const bool tr = lu && kind == 0;      // U^t: element (r, k) read at D[k][r]
     if (lu) unit = kind;
     T *X = reinterpret_cast<T *>(smem_raw);   // [nrow][PBL]
-    T *Lb = X + (size_t)nrow * PBL;           // [PB][PBL]
+    T *Lb = X + (size_t)nrow * PBL;           // [PB][kch + 1]
+    const int lb = kch + 1;
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int e = tid; e < nrow * PB; e += nt) {
         const int i = e / PB, q = e - i * PB;
@@ -408,22 +410,35 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
     __syncthreads();
     for (int ib = jb; ib < w; ib += PB) {
         const int nbi = min(PB, w - ib);
-        // (1) X[ib..] -= L[ib.., jb..ib) X[jb..ib)
-        for (int kb = jb; kb < ib; kb += PB) {
-            batched_copy(
-                nbi * PB, tid, nt,
-                [&](int e) {
-                    const int r = e / PB, k = e - r * PB;
-                    const T v = tr ? D[(int64_t)(kb + k) * ld + ib + r] : D[(int64_t)(ib + r) * ld + kb + k];
-                    return cjp ? conj_v(v) : v;
-                },
-                [&](int e, T v) { const int r = e / PB, k = e - r * PB; Lb[r * PBL + k] = v; });
+        // (1) X[ib..] -= L[ib.., jb..ib) X[jb..ib), kch columns of L at a time
+        for (int kc0 = jb; kc0 < ib; kc0 += kch) {
+            const int kn = min(kch, ib - kc0);
+            if (tr)   // U^t rows are U columns: coalesce along the row index
+                batched_copy(
+                    nbi * kn, tid, nt,
+                    [&](int e) {
+                        const int k = e / nbi, r = e - k * nbi;
+                        const T v = D[(int64_t)(kc0 + k) * ld + ib + r];
+                        return cjp ? conj_v(v) : v;
+                    },
+                    [&](int e, T v) { const int k = e / nbi, r = e - k * nbi; Lb[r * lb + k] = v; });
+            else
+                batched_copy(
+                    nbi * kn, tid, nt,
+                    [&](int e) {
+                        const int r = e / kn, k = e - r * kn;
+                        const T v = D[(int64_t)(ib + r) * ld + kc0 + k];
+                        return cjp ? conj_v(v) : v;
+                    },
+                    [&](int e, T v) { const int r = e / kn, k = e - r * kn; Lb[r * lb + k] = v; });
             __syncthreads();
             for (int e = tid; e < nbi * nb; e += nt) {
                 const int r = e / nb, q = e - r * nb;
                 T s = T(0);
+                const T *Lr = Lb + r * lb;
+                const T *Xc = X + (kc0 - jb) * PBL + q;
 #pragma unroll 8
-                for (int k = 0; k < PB; k++) s += Lb[r * PBL + k] * X[(kb - jb + k) * PBL + q];
+                for (int k = 0; k < kn; k++) s += Lr[k] * Xc[k * PBL];
                 X[(ib - jb + r) * PBL + q] -= s;
             }
             __syncthreads();
@@ -436,14 +451,14 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
                 const T v = tr ? D[(int64_t)(ib + k) * ld + ib + r] : D[(int64_t)(ib + r) * ld + ib + k];
                 return cjp ? conj_v(v) : v;
             },
-            [&](int e, T v) { const int r = e / nbi, k = e - r * nbi; Lb[r * PBL + k] = v; });
+            [&](int e, T v) { const int r = e / nbi, k = e - r * nbi; Lb[r * lb + k] = v; });
         __syncthreads();
         if (tid < nb) {
             const int q = tid;
             for (int r = 0; r < nbi; r++) {
                 T s = X[(ib - jb + r) * PBL + q];
-                for (int k = 0; k < r; k++) s -= Lb[r * PBL + k] * X[(ib - jb + k) * PBL + q];
-                X[(ib - jb + r) * PBL + q] = unit ? s : s * (T(1) / Lb[r * PBL + r]);
+                for (int k = 0; k < r; k++) s -= Lb[r * lb + k] * X[(ib - jb + k) * PBL + q];
+                X[(ib - jb + r) * PBL + q] = unit ? s : s * (T(1) / Lb[r * lb + r]);
             }
         }
         __syncthreads();

@@ -99,6 +99,8 @@ def test_task_records_match_plan(fact, mixed):
     plan = CM.plan_tasks(bs.struct, fact, 4 if mixed else 8, use_tc=mixed)
     key = lambda a: a[np.lexsort(a.T[::-1])]
     assert np.array_equal(key(info), key(plan))
+    tt = CM.task_times(bs.solver)
+    assert tt.shape == (info.shape[0], 2) and np.array_equal(tt[:, 1] - tt[:, 0], ns.astype(np.int64))
     bs.close()
 
 
