@@ -8,6 +8,8 @@ library's CUDA events), by coordinate descent over a small candidate space:
   trsm_gemm_rows   panel height above which the TRSM runs as a GEMM
   tc_min_mn        smallest M x N update sent to the tensor cores
   la_reserved_sms  SMs the lookahead stream leaves to the critical path
+  wide_panel       narrowest diagonal block given to the left-looking
+                   512-thread panel kernel (0: none)
   mixed_gemm       3xTF32 vs one TF32 product (objective "solve": the
                    refinement's extra iterations are part of the cost)
 
@@ -24,7 +26,7 @@ import numpy as np
 from . import gpu as G
 
 KNOBS = {"mixed_gemm": 0, "tc_kernel": 1, "lookahead": 2, "la_reserved_sms": 3, "trsm_gemm": 4,
-         "trsm_gemm_rows": 5, "tc_min_mn": 6}
+         "trsm_gemm_rows": 5, "tc_min_mn": 6, "wide_panel": 7}
 
 DEFAULT_SPACE = {
     "trsm_gemm_rows": [128, 256, 512],

@@ -6,6 +6,7 @@
 #include "pgpu_solve.cuh"
 #include "pgpu_panel.cuh"
 #include "pgpu_gemm_tc.cuh"
+#include "pgpu_panel_wide.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -114,6 +115,11 @@ struct pastix_gpu_s {
     // ---- factorization plan (per factotype) ----
     int plan_fact = -1;
     std::vector<int> tile_ptr, tctile_ptr, trsm_ptr, lvl_plrows, lvl_porows;
+    // panel launches of a level: k_panel_factor over the narrow cblks and
+    // k_panel_wide over the wide diagonal blocks, jobs {cblk, position in
+    // lvl_cblks} (the position indexes the task records)
+    std::vector<int> pn_ptr, pw_ptr, lvl_pmaxw, lvl_wmaxw;
+    DArr<int2> d_pjobs, d_wjobs;
     DArr<int4> d_tiles, d_tctiles, d_trsm;
     double tc_flops = 0;   // update-GEMM flops on the tensor-core path
     DArr<GemmTask> d_tasks;
@@ -481,6 +487,9 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
     return PASTIX_GPU_SUCCESS;
 }
 
+static const int SMEM_LIMIT = 227 * 1024;   // opt-in shared memory per CTA
+static const int WP_SMEM_LIMIT = SMEM_LIMIT - 1024;   // k_panel_wide's dynamic part (it has static arrays)
+
 // --------------------------------------------------------------------------
 // Factorization plan for one factorization type.
 // --------------------------------------------------------------------------
@@ -520,6 +529,8 @@ static void default_tuning(int64_t *t) {
     t[PGPU_TUNE_TRSM_GEMM] = (e && std::strcmp(e, "rows") == 0) ? 0 : 1;
     t[PGPU_TUNE_TRSM_GEMM_ROWS] = 256;
     t[PGPU_TUNE_TC_MIN_MN] = 128 * 64;
+    e = getenv("PASTIX_GPU_WIDE_PANEL");
+    t[PGPU_TUNE_WIDE_PANEL] = e ? std::atoi(e) : 128;
 }
 static int mixed_gemm_mode(const pastix_gpu_t &C) { return (int)C.tune[PGPU_TUNE_MIXED_GEMM]; }
 static bool tc_enabled(const pastix_gpu_t &C) { return mixed_gemm_mode(C) != MG_FP32; }
@@ -541,6 +552,21 @@ static int fact_mode_of(int fact, bool zc) {
     }
 }
 
+
+// Chunk width (bytes per row) of k_panel_wide for width w: the widest of
+// 128 / 64 / 32 bytes whose buffers fit in shared memory, 0 if none does.
+static int wide_kcb(int w, size_t esz, bool lu, bool ldl) {
+    for (int kcb = 128; kcb >= 32; kcb /= 2)
+        if (wp_smem_bytes(w, esz, lu, ldl, kcb) <= (size_t)WP_SMEM_LIMIT) return kcb;
+    return 0;
+}
+// Diagonal blocks at least PGPU_TUNE_WIDE_PANEL columns wide (0: never)
+// are factorized by k_panel_wide, when one CTA covers them (elements of up
+// to 8 bytes).
+static bool wide_panel(const pastix_gpu_t &C, int w, size_t esz, bool lu, bool ldl) {
+    const int64_t wmin = C.tune[PGPU_TUNE_WIDE_PANEL];
+    return wmin > 0 && w >= wmin && esz <= 8 && wp_tiles_fit(w, lu) && wide_kcb(w, esz, lu, ldl) > 0;
+}
 
 static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     const bool use_tc = fp32 && !zc && tc_enabled(C) && (fmode == FM_POTRF || fmode == FM_GETRF);
@@ -573,6 +599,11 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     C.trsm_ptr.assign(C.nlevels + 1, 0);
     C.lvl_plrows.assign(C.nlevels, 0);
     C.lvl_porows.assign(C.nlevels, 0);
+    C.lvl_pmaxw.assign(C.nlevels, 0);
+    C.lvl_wmaxw.assign(C.nlevels, 0);
+    C.pn_ptr.assign(C.nlevels + 1, 0);
+    C.pw_ptr.assign(C.nlevels + 1, 0);
+    std::vector<int2> pjobs, wjobs;
     C.tile_crit.assign(C.nlevels, 0);
     C.tctile_crit.assign(C.nlevels, 0);
     std::vector<int4> lt[2], ltc[2];   // this level's FMA / tensor-core tiles: [0] next-level targets, [1] others
@@ -586,8 +617,15 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
             const int c = C.lvl_cblks[q];
             const int w = C.width[c], h = C.height[c];
             const int rows = (h <= fuse) ? h : w;
-            C.lvl_plrows[l] = std::max(C.lvl_plrows[l], rows);
-            C.lvl_porows[l] = std::max(C.lvl_porows[l], rows - w);
+            if (rows == w && wide_panel(C, w, esz, lu, ldl)) {
+                wjobs.push_back(make_int2(c, q));
+                C.lvl_wmaxw[l] = std::max(C.lvl_wmaxw[l], w);
+            } else {
+                pjobs.push_back(make_int2(c, q));
+                C.lvl_plrows[l] = std::max(C.lvl_plrows[l], rows);
+                C.lvl_porows[l] = std::max(C.lvl_porows[l], rows - w);
+                C.lvl_pmaxw[l] = std::max(C.lvl_pmaxw[l], w);
+            }
             if (h > fuse)
                 for (int r0 = w; r0 < h; r0 += TRSM_TR) {
                     trsm.push_back(make_int4(c, r0, 0, lu ? 1 : (ldl ? 3 : 0)));
@@ -657,6 +695,8 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
         C.tile_ptr[l + 1] = (int)tiles.size();
         C.tctile_ptr[l + 1] = (int)tctiles.size();
         C.trsm_ptr[l + 1] = (int)trsm.size();
+        C.pn_ptr[l + 1] = (int)pjobs.size();
+        C.pw_ptr[l + 1] = (int)wjobs.size();
         C.inv_ptr[l + 1] = (int)invjobs.size();
         C.ttile_ptr[l + 1] = (int)ttiles.size();
         C.tttile_ptr[l + 1] = (int)tttiles.size();
@@ -685,6 +725,8 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     PGPU_CHECK(C.d_tctiles.upload(tctiles, s));
     PGPU_CHECK(C.d_trsm.upload(trsm, s));
     PGPU_CHECK(C.d_tasks.upload(tasks, s));
+    PGPU_CHECK(C.d_pjobs.upload(pjobs, s));
+    PGPU_CHECK(C.d_wjobs.upload(wjobs, s));
     PGPU_CHECK(cudaStreamSynchronize(s));
     C.h_tiles.swap(tiles);
     C.h_tctiles.swap(tctiles);
@@ -698,8 +740,6 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     C.tc_flops = tcflops;
     return PASTIX_GPU_SUCCESS;
 }
-
-static const int SMEM_LIMIT = 227 * 1024;
 
 // Per-launch timing: one event recorded before every launch (and one after
 // the last), so launch i took ev[i+1] - ev[i]; kinds[i] says which phase.
@@ -737,7 +777,25 @@ struct LaunchTimer {
 enum { PH_DIAG = 0, PH_TRSM = 1, PH_GEMM = 2, PH_TC = 3, PH_END = 4 };
 
 template <typename T>
-using PanelKernel = void (*)(Meta, const int *, T *, T *, const double *, int, int, int, Status *, int64_t *);
+using PanelKernel = void (*)(Meta, const int2 *, T *, T *, const double *, int, int, int, Status *, int64_t *);
+template <typename T>
+using WideKernel = void (*)(Meta, const int2 *, T *, const double *, int, Status *, int64_t *);
+
+template <typename T>
+static WideKernel<T> wide_kernel(int fmode) {
+    if constexpr (sizeof(T) > 8) {
+        return nullptr;
+    } else {
+        switch (fmode) {
+        case FM_GETRF: return k_panel_wide<T, FM_GETRF>;
+        case FM_SYTRF: return k_panel_wide<T, FM_SYTRF>;
+        case FM_HETRF:
+            if constexpr (is_cplx<T>::value) return k_panel_wide<T, FM_HETRF>;
+            return nullptr;
+        default: return k_panel_wide<T, FM_POTRF>;
+        }
+    }
+}
 
 template <typename T>
 static PanelKernel<T> panel_kernel(int fmode) {
@@ -760,6 +818,9 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     const int fuse = C.plan_fuse;   // rows the panel kernel solves itself (the plan's choice)
     PanelKernel<T> kpanel = panel_kernel<T>(fmode);
     if (!kpanel) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    WideKernel<T> kwide = wide_kernel<T>(fmode);
+    if (kwide)
+        PGPU_CHECK(cudaFuncSetAttribute(kwide, cudaFuncAttributeMaxDynamicSharedMemorySize, WP_SMEM_LIMIT));
     // the Hermitian forms conjugate the L coefficients in the row solves
     constexpr bool CPX = is_cplx<T>::value;
     auto ktrsm = (CPX && fm_conj(fmode)) ? k_trsm_rows<T, TRSM_TR, CPX> : k_trsm_rows<T, TRSM_TR, false>;
@@ -851,13 +912,26 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             PGPU_CHECK(cudaStreamWaitEvent(s, C.la_events[2 * (l - 2) + 1], 0));
         }
         const int mw = C.lvl_maxw[l];
-        const int pl = C.lvl_plrows[l], pu = lu ? mw : 0, po = lu ? C.lvl_porows[l] : 0;
-        const size_t psm = (size_t)(PB * PBL + PB + (size_t)(pl + pu + po) * PBL) * sizeof(T);
-        if (psm > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
         PGPU_CHECK(tm.mark(PH_DIAG));
-        kpanel<<<ncb, 256, psm, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], coefL, coefU, critp, fuse, pl, pu,
-                                     C.d_status.p, at(prof[0], C.lvl_ptr[l]));
-        nl++;
+        const int npw = C.pw_ptr[l + 1] - C.pw_ptr[l], npn = C.pn_ptr[l + 1] - C.pn_ptr[l];
+        if (npw) {
+            // wide diagonal blocks first: they are the level's longest panels
+            const int wmw = C.lvl_wmaxw[l];
+            const int kcb = wide_kcb(wmw, sizeof(T), lu, fm_ldl(fmode));
+            if (!kwide || kcb == 0) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+            kwide<<<npw, WP_THREADS, wp_smem_bytes(wmw, sizeof(T), lu, fm_ldl(fmode), kcb), s>>>(
+                C.meta, C.d_wjobs.p + C.pw_ptr[l], coefL, critp, kcb / (int)sizeof(T), C.d_status.p, prof[0]);
+            nl++;
+        }
+        if (npn) {
+            const int pmw = C.lvl_pmaxw[l];
+            const int pl = C.lvl_plrows[l], pu = lu ? pmw : 0, po = lu ? C.lvl_porows[l] : 0;
+            const size_t psm = (size_t)(PB * PBL + PB + (size_t)(pl + pu + po) * PBL) * sizeof(T);
+            if (psm > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+            kpanel<<<npn, 256, psm, s>>>(C.meta, C.d_pjobs.p + C.pn_ptr[l], coefL, coefU, critp, fuse, pl, pu,
+                                         C.d_status.p, prof[0]);
+            nl++;
+        }
         const int ntr = C.trsm_ptr[l + 1] - C.trsm_ptr[l];
         if (ntr && C.trsm_gemm) {
             T *inv = reinterpret_cast<T *>(C.d_inv.p);
@@ -2130,7 +2204,7 @@ extern "C" int pastix_gpu_set_tuning(pastix_gpu_t *ctx, int key, int64_t value) 
     if (!ctx || key < 0 || key >= PGPU_TUNE_COUNT) return PASTIX_GPU_ERR_BADPARAMETER;
     if (key == PGPU_TUNE_MIXED_GEMM && (value < MG_FP32 || value > MG_3XTF32)) return PASTIX_GPU_ERR_BADPARAMETER;
     if ((key == PGPU_TUNE_TRSM_GEMM_ROWS && value < 32) || (key == PGPU_TUNE_LA_RESERVED_SMS && value < 0) ||
-        (key == PGPU_TUNE_TC_MIN_MN && value < 0))
+        (key == PGPU_TUNE_TC_MIN_MN && value < 0) || (key == PGPU_TUNE_WIDE_PANEL && value < 0))
         return PASTIX_GPU_ERR_BADPARAMETER;
     ctx->tune[key] = value;
     ctx->plan_fact = -1;   // the next numfact rebuilds its launch lists (and graph)

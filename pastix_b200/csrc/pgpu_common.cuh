@@ -173,6 +173,24 @@ __device__ __forceinline__ void batched_copy(int total, int tid, int nt, Src src
     }
 }
 
+// Shared-memory address and asynchronous global -> shared copies
+// (cp.async: 16 bytes through L2 only, or 4 / 8 / 16 bytes through L1; a
+// commit closes a group, wait<N> leaves at most N groups in flight).
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void *gptr, bool valid) {
+    const int sz = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr), "l"(gptr), "r"(sz) : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_ca(uint32_t saddr, const void *gptr) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(saddr), "l"(gptr), "n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // Panel row of global row r inside cblk f: binary search over f's blocks
 // (sorted by frownum, blend/solver.h:497-514 is_block_inside_fblock walks
 // them linearly).  Returns -1 if r is not a row of f.

@@ -48,9 +48,6 @@ constexpr int tc_smem_bytes() {
 }
 constexpr int TC_TMEM_COLS = 128;
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 
 // Shared-memory matrix descriptor: K-major, SWIZZLE_128B, 8-row groups
 // 1024 B apart (stride byte offset), version 1 (sm_100).
@@ -64,10 +61,13 @@ __device__ __forceinline__ uint64_t tc_sdesc(uint32_t saddr) {
     return d;
 }
 
-// Instruction descriptor: D fp32, A/B tf32, both K-major, M = 128, N = 128.
-__device__ __forceinline__ uint32_t tc_idesc() {
-    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+// Instruction descriptor: D fp32, A/B tf32, both K-major, M = 128, N = n
+// (a multiple of 16 up to 128: a tile with fewer valid columns issues
+// narrower MMAs instead of multiplying zero rows).
+__device__ __forceinline__ uint32_t tc_idesc(int n = TC_BN) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
 }
+__device__ __forceinline__ int tc_mma_n(int ncols) { return min(TC_BN, (ncols + 15) & ~15); }
 
 __device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
@@ -90,13 +90,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
     }
 }
 
-__device__ __forceinline__ void cp_async16(uint32_t saddr, const void *gptr, bool valid) {
-    const int sz = valid ? 16 : 0;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr), "l"(gptr), "r"(sz) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 __device__ __forceinline__ void tc_fence_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -201,7 +194,8 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
 
     // operand tile q (0 A / 1 B for TF32; 0 A hi, 1 A lo, 2 B hi, 3 B lo split) of stage s
     auto tile_addr = [&](int s, int q) { return base + (uint32_t)(s * NT + q) * TC_TILE_BYTES; };
-    const uint32_t idesc = tc_idesc();
+    const int nmma = tc_mma_n(ncols);
+    const uint32_t idesc = tc_idesc(nmma);
     auto issue = [&](int s, int kb) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
@@ -235,8 +229,9 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
                 cp_async16(tile_addr(s, 0) + soff, va ? (const void *)(A + (int64_t)r * ld + kc) : (const void *)A,
                            va);
                 const bool vb = (r < ncols) && (kc < K);
-                cp_async16(tile_addr(s, 1) + soff, vb ? (const void *)(B + (int64_t)r * ld + kc) : (const void *)B,
-                           vb);
+                if (r < nmma)
+                    cp_async16(tile_addr(s, 1) + soff, vb ? (const void *)(B + (int64_t)r * ld + kc) : (const void *)B,
+                               vb);
             }
         };
 #pragma unroll
@@ -281,6 +276,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_scatter_tc(Meta m, const in
                                                   : make_float4(0.f, 0.f, 0.f, 0.f);
             }
         };
+        // (B rows >= nmma are stored too: the tile kernel keeps one code path)
         auto split_store = [&](int s) {
 #pragma unroll
             for (int q = 0; q < CH; q++) {
@@ -522,6 +518,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
                                 ? __ldg(reinterpret_cast<const float4 *>(v.B + (int64_t)r * ld + kc))
                                 : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
+                const int nmma = tc_mma_n(v.ncols);   // B rows the MMAs read
                 if (it >= S && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((it / S - 1) & 1))) {
                     atomicExch(&fail_s, 1);
                     break;
@@ -537,13 +534,15 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
                         l.x = ra[q].x - h.x; l.y = ra[q].y - h.y; l.z = ra[q].z - h.z; l.w = ra[q].w - h.w;
                         sts128(tile_addr(s, 0) + soff, h);
                         sts128(tile_addr(s, 1) + soff, l);
-                        h.x = tf32_hi(rb[q].x); h.y = tf32_hi(rb[q].y); h.z = tf32_hi(rb[q].z); h.w = tf32_hi(rb[q].w);
-                        l.x = rb[q].x - h.x; l.y = rb[q].y - h.y; l.z = rb[q].z - h.z; l.w = rb[q].w - h.w;
-                        sts128(tile_addr(s, 2) + soff, h);
-                        sts128(tile_addr(s, 3) + soff, l);
+                        if (r < nmma) {
+                            h.x = tf32_hi(rb[q].x); h.y = tf32_hi(rb[q].y); h.z = tf32_hi(rb[q].z); h.w = tf32_hi(rb[q].w);
+                            l.x = rb[q].x - h.x; l.y = rb[q].y - h.y; l.z = rb[q].z - h.z; l.w = rb[q].w - h.w;
+                            sts128(tile_addr(s, 2) + soff, h);
+                            sts128(tile_addr(s, 3) + soff, l);
+                        }
                     } else {
                         sts128(tile_addr(s, 0) + soff, ra[q]);
-                        sts128(tile_addr(s, 1) + soff, rb[q]);
+                        if (r < nmma) sts128(tile_addr(s, 1) + soff, rb[q]);
                     }
                 }
                 tc_fence_async_smem();
@@ -553,10 +552,10 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
     } else if (warp == 8) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            const uint32_t idesc = tc_idesc();
             int it = 0, tl = 0;
             for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x, tl++) {
                 const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU, inv);
+                const uint32_t idesc = tc_idesc(tc_mma_n(v.ncols));
                 const int ab = tl & 1;
                 const uint32_t acc = tmem + (uint32_t)(ab * 128);
                 if (tl >= 2 && !mbar_wait(smem_u32(&acce[ab]), (uint32_t)((tl / 2 - 1) & 1))) {

@@ -152,7 +152,7 @@ __device__ __forceinline__ void row_solve_upper(T *x, const T *tile, int nb) {
 }
 
 // ---------------------------------------------------------------------------
-// One CTA per cblk of the level.  rows_fused(c) = h_c when h_c <= fuse_rows
+// One CTA per job {cblk, record slot}.  rows_fused(c) = h_c when h_c <= fuse_rows
 // (the off-diagonal rows are solved here too), else w_c (they go to
 // k_trsm_rows).  Shared memory: tile[PB][PBL] + dinv[PB] + PL[rows][PBL]
 // (solved column block) + for GETRF PU[w][PBL] (solved row block of U,
@@ -161,7 +161,7 @@ __device__ __forceinline__ void row_solve_upper(T *x, const T *tile, int nb) {
 // update takes its right operand as y D^{-1} = x through dinv.
 // ---------------------------------------------------------------------------
 template <typename T, int MODE>
-__global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restrict__ cblks, T *__restrict__ coefL,
+__global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int2 *__restrict__ jobs, T *__restrict__ coefL,
                                                       T *__restrict__ coefU, const double *critp, int fuse_rows,
                                                       int pl_rows, int pu_rows, Status *st, int64_t *prof) {
     typedef typename real_of<T>::type R;
@@ -174,7 +174,8 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
     T *PL = dinv + PB;                       // [pl_rows][PBL]: rows r1.. of the panel
     T *PU = PL + (size_t)pl_rows * PBL;      // [pu_rows][PBL]: columns r1..w (LU only)
     T *PO = PU + (size_t)pu_rows * PBL;      // [rows - w][PBL]: fused U^T rows (LU only)
-    const int c = cblks[blockIdx.x];
+    const int2 job = jobs[blockIdx.x];
+    const int c = job.x;
     const int w = m.width[c], h = m.height[c], ld = m.ld[c];
     const int rows = (h <= fuse_rows) ? h : w;
     T *A = coefL + m.coefoff[c];
@@ -275,8 +276,8 @@ __global__ void __launch_bounds__(256) k_panel_factor(Meta m, const int *__restr
         if (nneg) atomicAdd(&st->negpivots, nneg);
         if (nbad) atomicAdd(&st->nonfinite, nbad);
         if (prof) {
-            prof[2 * blockIdx.x] = (int64_t)t_start;
-            prof[2 * blockIdx.x + 1] = (int64_t)global_ns();
+            prof[2 * job.y] = (int64_t)t_start;
+            prof[2 * job.y + 1] = (int64_t)global_ns();
         }
     }
 }

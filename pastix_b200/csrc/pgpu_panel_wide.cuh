@@ -1,0 +1,305 @@
+// Diagonal-block factorization of wide cblks (w of a few hundred columns, the
+// separators near the root of the elimination tree, whose off-diagonal rows
+// are solved afterwards by the inverse + GEMM path): the same factorization
+// as k_panel_factor with rows = w (kernels/core_zpotrfsp.c:144
+// core_zpotrfsp, kernels/core_zgetrfsp.c:138 core_zgetrfsp,
+// kernels/core_zsytrfsp.c:141 / core_zhetrfsp.c:144), reorganized for one
+// 512-thread CTA per cblk as a left-looking (Crout) sweep over column blocks
+// of PB = 32:
+//
+//   for each column block jb:
+//     1. C = A[jb:w, jb:jb+nb] (and for LU R = A[jb:jb+nb, jb+nb:w]^t) is
+//        copied to shared memory (cp.async, in flight during step 2);
+//     2. C -= L[jb:w, 0:jb] op(L[jb:jb+nb, 0:jb] D)^t       (LL^h, LDL^t/h)
+//        C -= L[jb:w, 0:jb] U[0:jb, jb:jb+nb]               (LU, L side)
+//        R -= U[0:jb, jb+nb:w]^t L[jb:jb+nb, 0:jb]^t        (LU, U side)
+//        with the finished columns streamed through shared memory in
+//        chunks of kc columns (double-buffered cp.async), 4 x 4 register
+//        tiles per thread (rows strided by the row-group count, columns by
+//        8, so that each warp's 16-byte loads hit distinct banks);
+//     3. one warp factorizes the nb x nb tile (static pivoting), the rows
+//        below are solved against it one thread per row (LU: and the
+//        columns of R against its unit lower part);
+//     4. C (and R) are written back.
+//
+// Compared with the right-looking k_panel_factor the trailing matrix is
+// never re-read and re-written through L2 for every column block: each
+// finished column block is read once per later block as a chunk operand.
+#pragma once
+
+#include "pgpu_common.cuh"
+#include "pgpu_panel.cuh"
+
+namespace pgpu {
+
+constexpr int WP_THREADS = 512;
+
+// Tiles a thread owns: C tiles (rows of the block column) plus, for LU, R
+// tiles (columns of the row block); 4 x 4 entries each.
+template <int MODE>
+constexpr int wp_ntt() { return MODE == FM_GETRF ? 3 : 2; }
+
+// Row groups of a tile set over m rows: ceil(m / 4) rounded up to a multiple
+// of 4, so that every warp's 32 tiles are of one kind.
+__host__ __device__ inline int wp_row_groups(int m) { return (((m + 3) >> 2) + 3) & ~3; }
+
+template <typename T>
+__device__ __forceinline__ void wp_lds16(const T *p, T (&v)[16 / sizeof(T)]) {
+    const uint4 u = *reinterpret_cast<const uint4 *>(p);
+    memcpy(v, &u, 16);
+}
+
+// Row solves against the factorized tile with the row in registers (fully
+// unrolled, so x stays out of local memory); rdiag[j] = 1 / op(diagonal j).
+//   lower_t: x op(L)^t = a (unit when UNIT);  upper: x U = a;
+//   unit_lower: L y = a for a column y (LU row block).
+template <typename T, bool CJ, bool UNIT>
+__device__ __forceinline__ void wp_solve_lower_t(T (&x)[PB], const T *tile, const T *rdiag, int nb) {
+#pragma unroll
+    for (int j = 0; j < PB; j++)
+        if (j < nb) {
+            T s = x[j];
+#pragma unroll
+            for (int l = 0; l < j; l++) s -= x[l] * cj<CJ>(tile[j * PBL + l]);
+            x[j] = UNIT ? s : s * rdiag[j];
+        }
+}
+template <typename T>
+__device__ __forceinline__ void wp_solve_upper(T (&x)[PB], const T *tile, const T *rdiag, int nb) {
+#pragma unroll
+    for (int j = 0; j < PB; j++)
+        if (j < nb) {
+            T s = x[j];
+#pragma unroll
+            for (int l = 0; l < j; l++) s -= x[l] * tile[l * PBL + j];
+            x[j] = s * rdiag[j];
+        }
+}
+template <typename T>
+__device__ __forceinline__ void wp_solve_unit_lower(T (&y)[PB], const T *tile, int nb) {
+#pragma unroll
+    for (int j = 0; j < PB; j++)
+        if (j < nb) {
+            T s = y[j];
+#pragma unroll
+            for (int l = 0; l < j; l++) s -= tile[j * PBL + l] * y[l];
+            y[j] = s;
+        }
+}
+
+// Shared memory (elements of T): Ach[2][w + 16][kc + VK] chunk buffers of
+// the left columns, for LU Uch[2][w + 16][kc + VK] (the U rows above,
+// transposed), C[w][PBL], for LU R[w][PBL], for LDL d[w].
+template <typename T, int MODE>
+__global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *__restrict__ jobs,
+                                                           T *__restrict__ coefL, const double *critp, int kc,
+                                                           Status *st, int64_t *prof) {
+    typedef typename real_of<T>::type R;
+    constexpr bool LU = (MODE == FM_GETRF);
+    constexpr bool LDL = fm_ldl(MODE);
+    constexpr bool CJ = fm_conj(MODE);
+    constexpr int VK = 16 / sizeof(T);
+    constexpr int NTT = wp_ntt<MODE>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ T rdiag[PB];                        // 1 / op(tile diagonal); LDL: 1 / d
+    const int2 job = jobs[blockIdx.x];
+    const int c = job.x;
+    const int w = m.width[c], ld = m.ld[c];
+    T *A = coefL + m.coefoff[c];
+    const int S = kc + VK;                         // chunk row stride: 16 bytes of padding
+    const int64_t bufsz = (int64_t)(w + 16) * S;   // w rows + the tiles' overhang
+    T *Ach = reinterpret_cast<T *>(smem_raw);
+    T *Uch = Ach + 2 * bufsz;                      // buffer b of Uch = Ach + (2 + b) * bufsz
+    T *Cb = Uch + (LU ? 2 * bufsz : 0);
+    T *Rb = Cb + (int64_t)w * PBL;
+    T *dsm = Rb + (LU ? (int64_t)w * PBL : 0);
+    const R crit = R(*critp);
+    const int tid = threadIdx.x;
+    const uint64_t t_start = prof ? global_ns() : 0;
+    int npiv = 0, nneg = 0, nbad = 0;
+
+    for (int jb = 0; jb < w; jb += PB) {
+        const int nb = min(PB, w - jb), M = w - jb, MR = LU ? M - nb : 0;
+        // 1. the block column (and the row block right of the tile), in flight during the update
+        for (int e = tid; e < M * nb; e += WP_THREADS) {
+            const int r = e / nb, j = e - r * nb;
+            cp_async_ca<sizeof(T)>(smem_u32(Cb + r * PBL + j), A + (int64_t)(jb + r) * ld + jb + j);
+        }
+        if (LU)
+            for (int e = tid; e < MR * nb; e += WP_THREADS) {
+                const int j = e / MR, i = e - j * MR;
+                cp_async_ca<sizeof(T)>(smem_u32(Rb + i * PBL + j), A + (int64_t)(jb + j) * ld + jb + nb + i);
+            }
+        cp_async_commit();
+        // 2. left-looking update with the finished columns [0, jb)
+        const int RG = wp_row_groups(M), RG2 = LU ? wp_row_groups(MR) : 0;
+        const int ntiles = (RG + RG2) * 8;
+        T acc[NTT][4][4];
+        if (jb > 0) {
+            auto stage = [&](int bf, int k0) {
+                T *dA = Ach + bf * bufsz;
+                const int pieces = kc / VK;
+                for (int e = tid; e < M * pieces; e += WP_THREADS) {
+                    const int r = e / pieces, pc = e - r * pieces;
+                    cp_async16(smem_u32(dA + r * S + pc * VK), A + (int64_t)(jb + r) * ld + k0 + pc * VK, true);
+                }
+                if (LU) {
+                    T *dU = Uch + bf * bufsz;
+                    for (int e = tid; e < kc * M; e += WP_THREADS) {
+                        const int kk = e / M, i = e - kk * M;
+                        cp_async_ca<sizeof(T)>(smem_u32(dU + i * S + kk), A + (int64_t)(k0 + kk) * ld + jb + i);
+                    }
+                }
+            };
+            // operand rows of each owned tile, as element offsets from Ach
+            // (buffer 0): left row p at lo[t] + p * ls[t], right row q at
+            // ro[t] + 8 q S.  Rows past the valid ones (up to M + 15) stay
+            // inside the buffers and only feed entries that are discarded.
+            int lo[NTT], ls[NTT], ro[NTT];
+#pragma unroll
+            for (int t = 0; t < NTT; t++) {
+                const int u = tid + t * WP_THREADS;
+                const bool rt = LU && u >= RG * 8;     // an R tile
+                const int uu = rt ? u - RG * 8 : u;
+                const int ti = uu >> 3, tj = uu & 7;
+                // C tile: left = L rows (Ach), right = L rows (Ach) or U^t rows (Uch)
+                // R tile: left = U^t rows nb.. (Uch), right = L rows (Ach)
+                lo[t] = rt ? (int)(2 * bufsz) + (nb + ti) * S : ti * S;
+                ls[t] = (rt ? RG2 : RG) * S;
+                ro[t] = (LU && !rt) ? (int)(2 * bufsz) + tj * S : tj * S;
+#pragma unroll
+                for (int p = 0; p < 4; p++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[t][p][q] = T(0);
+            }
+            const int nck = jb / kc;
+            stage(0, 0);
+            cp_async_commit();
+            for (int ck = 0; ck < nck; ck++) {
+                if (ck + 1 < nck) stage((ck + 1) & 1, (ck + 1) * kc);
+                cp_async_commit();
+                cp_async_wait<1>();
+                __syncthreads();
+                const T *base = Ach + (ck & 1) * bufsz;
+                const int k0 = ck * kc;
+#pragma unroll
+                for (int t = 0; t < NTT; t++) {
+                    if (tid + t * WP_THREADS >= ntiles) break;     // whole warps (ntiles is a multiple of 32)
+#pragma unroll 2
+                    for (int kk = 0; kk < kc; kk += VK) {
+                        T a[4][VK], b[4][VK];
+#pragma unroll
+                        for (int p = 0; p < 4; p++) wp_lds16<T>(base + lo[t] + p * ls[t] + kk, a[p]);
+#pragma unroll
+                        for (int q = 0; q < 4; q++) wp_lds16<T>(base + ro[t] + q * 8 * S + kk, b[q]);
+#pragma unroll
+                        for (int v = 0; v < VK; v++) {
+                            T dk = T(1);
+                            if (LDL) dk = dsm[k0 + kk + v];
+#pragma unroll
+                            for (int q = 0; q < 4; q++) {
+                                T bq = cj<CJ>(b[q][v]);
+                                if (LDL) bq = bq * dk;
+#pragma unroll
+                                for (int p = 0; p < 4; p++) acc[t][p][q] += a[p][v] * bq;
+                            }
+                        }
+                    }
+                }
+                __syncthreads();                  // the buffer is refilled two chunks later
+            }
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+        if (jb > 0) {
+#pragma unroll
+            for (int t = 0; t < NTT; t++) {
+                const int u = tid + t * WP_THREADS;
+                if (u >= ntiles) break;
+                const bool rt = u >= RG * 8;
+                const int uu = rt ? u - RG * 8 : u;
+                const int ti = uu >> 3, tj = uu & 7;
+                const int rg = rt ? RG2 : RG, rows = rt ? MR : M;
+                T *D = rt ? Rb : Cb;
+#pragma unroll
+                for (int p = 0; p < 4; p++) {
+                    const int r = ti + p * rg;
+                    if (r >= rows) continue;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int j = tj + 8 * q;
+                        if (j < nb) D[r * PBL + j] -= acc[t][p][q];
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // 3. the tile, then the rows below it (and the columns of R)
+        if (tid < 32) {
+            warp_factor_tile<T, MODE>(Cb, nb, crit, npiv, nneg, nbad);
+            if (tid < nb) {
+                const T d = Cb[tid * PBL + tid];
+                if (LDL) dsm[jb + tid] = d;
+                rdiag[tid] = T(1) / (MODE == FM_POTRF ? cj<CJ>(d) : d);
+            }
+        }
+        __syncthreads();
+        for (int r = nb + tid; r < M; r += WP_THREADS) {
+            T x[PB];
+#pragma unroll
+            for (int j = 0; j < PB; j++) x[j] = (j < nb) ? Cb[r * PBL + j] : T(0);
+            if (LU) wp_solve_upper<T>(x, Cb, rdiag, nb);
+            else if (LDL) wp_solve_lower_t<T, CJ, true>(x, Cb, rdiag, nb);
+            else wp_solve_lower_t<T, CJ, false>(x, Cb, rdiag, nb);
+#pragma unroll
+            for (int j = 0; j < PB; j++)
+                if (j < nb) Cb[r * PBL + j] = LDL ? x[j] * rdiag[j] : x[j];
+        }
+        if (LU)
+            for (int i = tid; i < MR; i += WP_THREADS) {
+                T y[PB];
+#pragma unroll
+                for (int j = 0; j < PB; j++) y[j] = (j < nb) ? Rb[i * PBL + j] : T(0);
+                wp_solve_unit_lower<T>(y, Cb, nb);
+#pragma unroll
+                for (int j = 0; j < PB; j++)
+                    if (j < nb) Rb[i * PBL + j] = y[j];
+            }
+        __syncthreads();
+        // 4. write back (the symmetric forms keep the tile's lower triangle only)
+        for (int e = tid; e < M * nb; e += WP_THREADS) {
+            const int r = e / nb, j = e - r * nb;
+            if (LU || r >= nb || j <= r) A[(int64_t)(jb + r) * ld + jb + j] = Cb[r * PBL + j];
+        }
+        if (LU)
+            for (int e = tid; e < MR * nb; e += WP_THREADS) {
+                const int j = e / MR, i = e - j * MR;
+                A[(int64_t)(jb + j) * ld + jb + nb + i] = Rb[i * PBL + j];
+            }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        if (npiv) atomicAdd(&st->nbpivots, npiv);
+        if (nneg) atomicAdd(&st->negpivots, nneg);
+        if (nbad) atomicAdd(&st->nonfinite, nbad);
+        if (prof) {
+            prof[2 * job.y] = (int64_t)t_start;
+            prof[2 * job.y + 1] = (int64_t)global_ns();
+        }
+    }
+}
+
+// Shared memory of k_panel_wide for width w with chunks of kcb bytes per row.
+__host__ inline size_t wp_smem_bytes(int w, size_t esz, bool lu, bool ldl, int kcb) {
+    const size_t chunk_row = (size_t)kcb + 16;
+    return 2 * (size_t)(w + 16) * chunk_row * (lu ? 2 : 1) + (size_t)w * PBL * esz * (lu ? 2 : 1) +
+           (ldl ? (size_t)w * esz : 0);
+}
+
+// Whether one CTA covers width w with its tile budget.
+__host__ inline bool wp_tiles_fit(int w, bool lu) {
+    const int rg = wp_row_groups(w), rg2 = lu ? wp_row_groups(w > PB ? w - PB : 0) : 0;
+    return (rg + rg2) * 8 <= (lu ? 3 : 2) * WP_THREADS;
+}
+
+}  // namespace pgpu

@@ -20,6 +20,8 @@ CASES = [
     ("diff26", lambda: M.diffusion_lognormal(26, 25, 24, 1.0, np.random.default_rng(12)), "potrf"),
     ("cd10", lambda: M.convdiff_upwind(10, 10, 10, 10.0), "getrf"),
     ("cd9x7x5", lambda: M.convdiff_upwind(9, 7, 5, 10.0), "getrf"),
+    # LU with diagonal blocks of 128 and 256 columns (the wide-panel kernel)
+    ("cd16", lambda: M.convdiff_upwind(16, 16, 16, 10.0), "getrf"),
 ]
 
 
@@ -297,4 +299,43 @@ def test_factorization_graph_replay_matches_direct(mixed, monkeypatch):
     x, b = M.rhs_from_xtrue(A, 2, np.random.default_rng(3))
     xs = s.solve(2.0 * b)
     assert np.abs(xs - x).max() <= (1e-9 if not mixed else 1e-3)
+    s.close()
+
+
+WIDE_CASES = [
+    ("potrf", lambda: M.diffusion_lognormal(26, 25, 24, 1.0, np.random.default_rng(12)), False),
+    ("potrf", lambda: M.diffusion_lognormal(26, 25, 24, 1.0, np.random.default_rng(12)), True),
+    ("getrf", lambda: M.convdiff_upwind(16, 16, 16, 10.0), False),
+    ("getrf", lambda: M.convdiff_upwind(16, 16, 16, 10.0), True),
+    ("sytrf", lambda: M.diffusion_lognormal(20, 19, 18, 1.0, np.random.default_rng(5)), False),
+    ("sytrf", lambda: M.diffusion_lognormal(20, 19, 18, 1.0, np.random.default_rng(5)), True),
+    ("hetrf", lambda: M.magnetic_laplacian(14, 13, 12, 0.5, np.random.default_rng(8)), True),
+    ("potrf", lambda: M.magnetic_laplacian(14, 13, 12, -0.5, np.random.default_rng(7)), True),
+]
+
+
+@pytest.mark.parametrize("fact,make,mixed", WIDE_CASES,
+                         ids=["potrf_d", "potrf_s", "getrf_d", "getrf_s", "sytrf_d", "sytrf_s", "hetrf_c", "potrf_c"])
+def test_wide_panel_kernel_matches_narrow(fact, make, mixed):
+    """Diagonal blocks of 128 columns and more go to the left-looking
+    512-thread kernel; with it switched off (PGPU_TUNE_WIDE_PANEL = 0) the
+    right-looking panel kernel factorizes them.  Both factors agree to the
+    rounding of their different summation orders."""
+    from pastix_b200 import autotune as AT
+    A = make()
+    ref, st = U.run_reference(A, fact, numfact=False)
+    s = _gpu_solver(A, st, fact, mixed=mixed)
+    assert AT.get_knob(s, "wide_panel") == 128
+    s.numfact(A.values)
+    L1, U1 = s.coeftab()
+    AT.set_knob(s, "wide_panel", 0)
+    s.numfact(A.values)
+    L0, U0 = s.coeftab()
+    tol = 2e-5 if mixed else 1e-12
+    g = U.gpu_structure(A, st)
+    lay = U.layout_of(g)
+    mask = np.ones(lay.off[-1], bool) if fact == "getrf" else U.lower_mask(lay)
+    assert np.abs(L1 - L0)[mask].max() <= tol * np.abs(L0).max()
+    if fact == "getrf":
+        assert np.abs(U1 - U0).max() <= tol * np.abs(U0).max()
     s.close()
