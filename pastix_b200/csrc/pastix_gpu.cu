@@ -938,11 +938,12 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             T *scr = reinterpret_cast<T *>(C.d_scr.p);
             const int nij = C.inv_ptr[l + 1] - C.inv_ptr[l];
             // X[w][33] + a 32-row strip of L, kch columns wide (as wide as fits, a multiple of 32)
-            const size_t xs = (size_t)mw * PBL * sizeof(T);
-            if (xs + (size_t)PB * (PB + 1) * sizeof(T) > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
-            int kch = (int)std::min<size_t>(round_up(mw, PB), ((SMEM_LIMIT - xs) / ((size_t)PB * sizeof(T)) - 1));
+            const size_t xs = tri_inverse_lb_offset(mw, sizeof(T));
+            const int vk = std::max<int>(1, 16 / (int)sizeof(T));
+            if (xs + (size_t)PB * (PB + vk) * sizeof(T) > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+            int kch = (int)std::min<size_t>(round_up(mw, PB), ((SMEM_LIMIT - xs) / ((size_t)PB * sizeof(T)) - vk));
             kch = std::max(PB, kch / PB * PB);
-            const size_t ism = xs + (size_t)PB * (kch + 1) * sizeof(T);
+            const size_t ism = xs + (size_t)PB * (kch + vk) * sizeof(T);
             PGPU_CHECK(tm.mark(PH_TRSM));
             k_tri_inverse<T><<<nij, 256, ism, s>>>(C.meta, C.d_invjobs.p + C.inv_ptr[l], coefL, inv,
                                                    fm_ldl(fmode) ? 1 : 0, (CPX && fm_conj(fmode)) ? 1 : 0,

@@ -390,10 +390,12 @@ namespace pgpu {
 //   warps 0-3 (128 threads): epilogue -- warp w reads TMEM lanes 32w..32w+31
 //                            of the finished accumulator, transposes through
 //                            shared memory and scatter-adds into the target;
-//   warps 4-7 (128 threads): producers -- global -> registers -> (3xTF32:
+//   warps 4-11 (2 x 128):    producers -- global -> registers -> (3xTF32:
 //                            hi/lo split) -> SWIZZLE_128B shared-memory ring of
 //                            TCP_STAGES stages, then mbarrier arrive (full);
-//   warp 8, lane 0:          MMA issuer -- waits for a full stage, issues the
+//                            the two groups take alternate k-blocks, so two
+//                            stages' loads are in flight at once;
+//   warp 12, lane 0:         MMA issuer -- waits for a full stage, issues the
 //                            tcgen05.mma of the k-block into one of two TMEM
 //                            accumulators (2 x 128 columns), commits the stage
 //                            back to the producers (empty) and the finished
@@ -403,7 +405,9 @@ namespace pgpu {
 // Status::timeout, and the others run out on their own bounded waits; TMEM is
 // freed after all roles met at the final barrier.
 // ---------------------------------------------------------------------------
-constexpr int TCP_THREADS = 288;
+constexpr int TCP_PGROUPS = 2;                              // producer groups of 4 warps
+constexpr int TCP_MMA_WARP = 4 + 4 * TCP_PGROUPS;
+constexpr int TCP_THREADS = 32 * (TCP_MMA_WARP + 1);
 template <bool SPLIT> struct TcpCfg;
 template <> struct TcpCfg<false> { static constexpr int STAGES = 6, TILES = 2; };
 template <> struct TcpCfg<true> { static constexpr int STAGES = 3, TILES = 4; };
@@ -469,7 +473,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
     float *epi = reinterpret_cast<float *>(sbase + S * NT * TC_TILE_BYTES);   // [4][32][33]
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (warp == 8) {
+    if (warp == TCP_MMA_WARP) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
                      "r"(TCP_TMEM_COLS)
                      : "memory");
@@ -495,15 +499,19 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
     auto tile_addr = [&](int s, int q) { return base + (uint32_t)(s * NT + q) * TC_TILE_BYTES; };
     auto failed = [&]() { return *(volatile int *)&fail_s != 0; };
 
-    if (warp >= 4 && warp < 8) {
+    if (warp >= 4 && warp < TCP_MMA_WARP) {
         // ---------------- producers ----------------
-        const int ptid = tid - 128;
+        // group g fills the k-blocks it with it % TCP_PGROUPS == g, so that
+        // the loads of consecutive stages are in flight together
+        const int grp = (warp - 4) >> 2;
+        const int ptid = tid - 128 * (1 + grp);
         constexpr int CH = (TC_BM * 8) / 128;          // 8 chunks of 16 B per operand per thread
         int it = 0;
         for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x) {
             const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU, inv);
             const int ld = m.ld[v.c];
             for (int kb = 0; kb < v.nk; kb++, it++) {
+                if (it % TCP_PGROUPS != grp) continue;
                 const int s = it % S;
                 const int k0 = kb * TC_BK;
                 float4 ra[CH], rb[CH];
@@ -549,7 +557,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
                 mbar_arrive(smem_u32(&full[s]));
             }
         }
-    } else if (warp == 8) {
+    } else if (warp == TCP_MMA_WARP) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             int it = 0, tl = 0;
@@ -658,7 +666,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
     if (tid == 0 && failed()) atomicAdd(&st->timeout, 1);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 8) {
+    if (warp == TCP_MMA_WARP) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCP_TMEM_COLS)
                      : "memory");

@@ -4,7 +4,7 @@
 // kernels/core_zsytrfsp.c:63,141 and kernels/core_zhetrfsp.c:63,144 for
 // LDL^t / LDL^h) and the panel TRSM of its off-diagonal rows
 // (kernels/core_ztrsmsp.c:71), by column blocks of PB = 32:
-//   1. one warp factorizes the PB x PB diagonal tile in shared memory;
+//   1. one warp factorizes the PB x PB diagonal tile (rows in registers);
 //   2. every row below (and for LU every column to the right) is solved
 //      against the tile, one thread per row;
 //   3. the trailing part of the panel is updated with the solved column
@@ -91,9 +91,75 @@ __device__ __forceinline__ T static_pivot(T a, typename real_of<T>::type crit, i
 //   POTRF: lower Cholesky L L^h (diagonal real and positive);
 //   GETRF: LU without row pivoting (unit L below, U on and above);
 //   SYTRF/HETRF: unit L below, D on the diagonal (L D L^t / L D L^h).
+// Lane i keeps row i of the tile in registers; the pivot, the scaled column
+// and (LU) the pivot row reach the other lanes by warp shuffles, so no step
+// waits on a shared-memory round trip.  The pivot is evaluated on every lane
+// alike; lane 0's counters are reported.  The tile is read from and written
+// back to shared memory (row-major, ld PBL).
 template <typename T, int MODE>
 __device__ __forceinline__ void warp_factor_tile(T *tile, int nb, typename real_of<T>::type crit, int &npiv,
-                                                 int &nneg, int &nbad) {
+                                                     int &nneg, int &nbad) {
+    typedef typename real_of<T>::type R;
+    constexpr bool CJ = fm_conj(MODE);
+    const int lane = threadIdx.x & 31;
+    T a[PB];
+#pragma unroll
+    for (int j = 0; j < PB; j++) a[j] = (lane < nb && j < nb) ? tile[lane * PBL + j] : T(0);
+    int piv = 0, neg = 0, bad = 0;
+#pragma unroll
+    for (int k = 0; k < PB; k++) {
+        if (k >= nb) continue;   // (not break: the loop must unroll fully to keep a[] in registers)
+        T dk = shfl_v(a[k], k);
+        if (!finite_v(dk)) bad++;
+        dk = static_pivot<T, MODE>(dk, crit, piv);
+        if (MODE == FM_POTRF) {
+            if (real_v(dk) < R(0)) neg++;
+            dk = sqrt_v(dk);
+        }
+        if (lane == k) a[k] = dk;
+        const T inv = T(1) / (MODE == FM_POTRF ? cj<CJ>(dk) : dk);
+        const bool below = lane > k && lane < nb;
+        if (below) a[k] = a[k] * inv;
+        const T lik = a[k];
+        if (MODE == FM_GETRF) {
+#pragma unroll
+            for (int j = k + 1; j < PB; j++) {
+                const T ukj = shfl_v(a[j], k);
+                if (below) a[j] -= lik * ukj;
+            }
+        } else {
+            // a_ij -= l_ik op(l_jk) (Cholesky); a_ij -= l_ik d_k op(l_jk) (LDL; LDL^h takes the real part of d_k)
+            const T ld = (MODE == FM_POTRF) ? lik : lik * (MODE == FM_HETRF ? T(real_v(dk)) : dk);
+#pragma unroll
+            for (int j = k + 1; j < PB; j++) {
+                const T ljk = shfl_v(a[k], j);
+                if (below && j <= lane) a[j] -= ld * cj<CJ>(ljk);
+            }
+            if (MODE == FM_HETRF) {
+#pragma unroll
+                for (int j = k + 1; j < PB; j++)
+                    if (below && j == lane) a[j] = T(real_v(a[j]));
+            }
+        }
+    }
+    if (lane == 0) {
+        npiv += piv;
+        nneg += neg;
+        nbad += bad;
+    }
+    if (lane < nb) {
+#pragma unroll
+        for (int j = 0; j < PB; j++)
+            if (j < nb) tile[lane * PBL + j] = a[j];
+    }
+}
+
+// Shared-memory form of the same factorization (the tile stays in shared
+// memory, lane 0 evaluates the pivots): for kernels whose register budget
+// cannot hold a row of 8-byte elements next to their other live values.
+template <typename T, int MODE>
+__device__ __forceinline__ void warp_factor_tile_smem(T *tile, int nb, typename real_of<T>::type crit, int &npiv,
+                                                      int &nneg, int &nbad) {
     typedef typename real_of<T>::type R;
     constexpr bool CJ = fm_conj(MODE);
     const int lane = threadIdx.x & 31;
@@ -380,13 +446,21 @@ namespace pgpu {
 // The strict upper part of B is left untouched (zero from the allocation).
 // One CTA per (cblk, 32-column block jb): columns [jb, jb+32) of the
 // inverse by blocked forward substitution over the 32-row tiles below jb.
-// Shared memory: X[w - jb][33] + Lb[32][kch + 1]: the rows of a 32-row tile
-// left of it are staged kch columns at a time (one burst of loads per chunk).
+// Shared memory: X[w - jb][33] + Lb[32][kch + VK]: the rows of a 32-row tile
+// left of it are staged kch columns at a time (one burst of loads per chunk),
+// 16-byte aligned rows read as broadcast vectors; each tile's triangular
+// solve runs on all 8 warps (lane = row, columns split across the warps).
+// Launched with 256 threads.
 // ---------------------------------------------------------------------------
 // LU (lu != 0): job.y = jb + (kind << 20); kind 0 inverts U^t (the upper
 // triangle of the diagonal block read transposed, non-unit) into the first
 // slot -- B of the L-side TRSM, X = A U^{-1} -- and kind 1 the unit lower L
 // into the second slot (inv_span further) -- B of the U^t-side TRSM.
+// Byte offset of the L strip buffer behind X[nrow][PBL] (16-byte aligned).
+__host__ __device__ inline size_t tri_inverse_lb_offset(int nrow, size_t esz) {
+    return ((size_t)nrow * PBL * esz + 15) / 16 * 16;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restrict__ jobs,
                                                      const T *__restrict__ coefL, T *__restrict__ inv,
@@ -400,9 +474,10 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
     T *Inv = inv + m.invoff[c] + (kind ? inv_span(w, ld) : 0);
     const bool tr = lu && kind == 0;      // U^t: element (r, k) read at D[k][r]
     if (lu) unit = kind;
+    constexpr int VK = 16 / sizeof(T) > 0 ? 16 / sizeof(T) : 1;   // k values per 16-byte load
     T *X = reinterpret_cast<T *>(smem_raw);   // [nrow][PBL]
-    T *Lb = X + (size_t)nrow * PBL;           // [PB][kch + 1]
-    const int lb = kch + 1;
+    T *Lb = reinterpret_cast<T *>(smem_raw + tri_inverse_lb_offset(nrow, sizeof(T)));   // [PB][kch + VK]
+    const int lb = kch + VK;                  // 16-byte rows
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int e = tid; e < nrow * PB; e += nt) {
         const int i = e / PB, q = e - i * PB;
@@ -433,14 +508,30 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
                     },
                     [&](int e, T v) { const int r = e / kn, k = e - r * kn; Lb[r * lb + k] = v; });
             __syncthreads();
-            for (int e = tid; e < nbi * nb; e += nt) {
-                const int r = e / nb, q = e - r * nb;
-                T s = T(0);
-                const T *Lr = Lb + r * lb;
+            {
+                // thread: rows r4..r4+3 of the strip, column q; the four L
+                // rows come as 16-byte broadcast loads (one per row and VK k)
+                const int q = tid & 31, r4 = (tid >> 5) * 4;
+                T acc[4] = {T(0), T(0), T(0), T(0)};
                 const T *Xc = X + (kc0 - jb) * PBL + q;
-#pragma unroll 8
-                for (int k = 0; k < kn; k++) s += Lr[k] * Xc[k * PBL];
-                X[(ib - jb + r) * PBL + q] -= s;
+                for (int k = 0; k < kn; k += VK) {
+                    T lv[4][VK];
+#pragma unroll
+                    for (int p = 0; p < 4; p++) {
+                        const uint4 u = *reinterpret_cast<const uint4 *>(Lb + (r4 + p) * lb + k);
+                        memcpy(lv[p], &u, 16);
+                    }
+#pragma unroll
+                    for (int v = 0; v < VK; v++) {
+                        const T xv = Xc[(k + v) * PBL];
+#pragma unroll
+                        for (int p = 0; p < 4; p++) acc[p] += lv[p][v] * xv;
+                    }
+                }
+                if (q < nb)
+#pragma unroll
+                    for (int p = 0; p < 4; p++)
+                        if (r4 + p < nbi) X[(ib - jb + r4 + p) * PBL + q] -= acc[p];
             }
             __syncthreads();
         }
@@ -454,12 +545,32 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
             },
             [&](int e, T v) { const int r = e / nbi, k = e - r * nbi; Lb[r * lb + k] = v; });
         __syncthreads();
-        if (tid < nb) {
-            const int q = tid;
-            for (int r = 0; r < nbi; r++) {
-                T s = X[(ib - jb + r) * PBL + q];
-                for (int k = 0; k < r; k++) s -= Lb[r * lb + k] * X[(ib - jb + k) * PBL + q];
-                X[(ib - jb + r) * PBL + q] = unit ? s : s * (T(1) / Lb[r * lb + r]);
+        {
+            // warp w solves columns w, w + 8, w + 16, w + 24 with lane = row:
+            // x_k = y_k / L_kk on lane k, broadcast, y_r -= L_rk x_k below
+            const int warp = tid >> 5, lane = tid & 31;
+            T y[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int q = warp + 8 * u;
+                y[u] = (lane < nbi && q < nb) ? X[(ib - jb + lane) * PBL + q] : T(0);
+            }
+            const T rinv = (!unit && lane < nbi) ? T(1) / Lb[lane * lb + lane] : T(1);
+#pragma unroll
+            for (int k = 0; k < PB; k++) {
+                if (k >= nbi) break;
+                const T lrk = (lane > k && lane < nbi) ? Lb[lane * lb + k] : T(0);
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (lane == k && !unit) y[u] = y[u] * rinv;
+                    const T xk = shfl_v(y[u], k);
+                    if (lane > k) y[u] -= lrk * xk;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int q = warp + 8 * u;
+                if (lane < nbi && q < nb) X[(ib - jb + lane) * PBL + q] = y[u];
             }
         }
         __syncthreads();

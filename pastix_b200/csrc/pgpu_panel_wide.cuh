@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
             const int r = e / nb, j = e - r * nb;
             cp_async_ca<sizeof(T)>(smem_u32(Cb + r * PBL + j), A + (int64_t)(jb + r) * ld + jb + j);
         }
-        if (LU)
+        if constexpr (LU)
             for (int e = tid; e < MR * nb; e += WP_THREADS) {
                 const int j = e / MR, i = e - j * MR;
                 cp_async_ca<sizeof(T)>(smem_u32(Rb + i * PBL + j), A + (int64_t)(jb + j) * ld + jb + nb + i);
@@ -236,7 +236,8 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
         }
         // 3. the tile, then the rows below it (and the columns of R)
         if (tid < 32) {
-            warp_factor_tile<T, MODE>(Cb, nb, crit, npiv, nneg, nbad);
+            if constexpr (sizeof(T) == 4) warp_factor_tile<T, MODE>(Cb, nb, crit, npiv, nneg, nbad);
+            else warp_factor_tile_smem<T, MODE>(Cb, nb, crit, npiv, nneg, nbad);
             if (tid < nb) {
                 const T d = Cb[tid * PBL + tid];
                 if (LDL) dsm[jb + tid] = d;
@@ -271,7 +272,7 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
             const int r = e / nb, j = e - r * nb;
             if (LU || r >= nb || j <= r) A[(int64_t)(jb + r) * ld + jb + j] = Cb[r * PBL + j];
         }
-        if (LU)
+        if constexpr (LU)
             for (int e = tid; e < MR * nb; e += WP_THREADS) {
                 const int j = e / MR, i = e - j * MR;
                 A[(int64_t)(jb + j) * ld + jb + nb + i] = Rb[i * PBL + j];
