@@ -63,6 +63,7 @@ inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 inline int cdiv(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
 const int SOLVE_ROWS_PER_CHUNK = 32;
+const int SOLVE_SMALL_MAXH = 512;   // tallest cblk of a level solved one warp per cblk
 
 bool is_device_ptr(const void *p) {
     cudaPointerAttributes at;
@@ -90,7 +91,7 @@ struct pastix_gpu_s {
     int64_t coefnbr = 0;      // elements of one (L or U) coeftab incl. padding
     int maxw = 0;
     int nlevels = 0;
-    std::vector<int> lvl_ptr, lvl_cblks, lvl_maxw, cblk_level;
+    std::vector<int> lvl_ptr, lvl_cblks, lvl_maxw, lvl_maxh, cblk_level;
     // lookahead: the update tiles of a level that target the next level run
     // on the main stream, the others on stream2, overlapping the panels of
     // the levels that follow
@@ -332,11 +333,13 @@ extern "C" int pastix_gpu_structure(pastix_gpu_t *ctx, int64_t n, int64_t cblknb
     for (int l = 0; l < C.nlevels; l++) C.lvl_ptr[l + 1] += C.lvl_ptr[l];
     C.lvl_cblks.assign(nc, 0);
     C.lvl_maxw.assign(C.nlevels, 0);
+    C.lvl_maxh.assign(C.nlevels, 0);
     {
         std::vector<int> pos(C.lvl_ptr.begin(), C.lvl_ptr.end() - 1);
         for (int c = 0; c < nc; c++) {
             C.lvl_cblks[pos[level[c]]++] = c;
             C.lvl_maxw[level[c]] = std::max(C.lvl_maxw[level[c]], C.width[c]);
+            C.lvl_maxh[level[c]] = std::max(C.lvl_maxh[level[c]], C.height[c]);
         }
     }
 
@@ -1220,9 +1223,18 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         *pch = dsm > fixed ? (int)std::min<size_t>(std::max(mw, 1), (dsm - fixed) / (33 * es)) : 0;
         return dsm;
     };
+    // levels of narrow, short cblks: one warp per cblk, diagonal and off-diagonal parts in one launch
+    auto small_level = [&](int l) { return C.lvl_maxw[l] <= 32 && C.lvl_maxh[l] <= SOLVE_SMALL_MAXH; };
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
+        if (small_level(l)) {
+            PGPU_CHECK(mark(0));
+            k_fwd_small<T><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], ncb, coefL, W, ldb,
+                                                        nrhs, (lu || ldl) ? 1 : 0);
+            nl++;
+            continue;
+        }
         int pch = 0;
         int ipch = 0;
         const size_t dsm = diag_smem(l, mw, &pch, &ipch);
@@ -1250,6 +1262,13 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
     for (int l = C.nlevels - 1; l >= 0; l--) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
+        if (small_level(l)) {
+            PGPU_CHECK(mark(4));
+            k_bwd_small<T><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], ncb, coefL, coefU, W,
+                                                        ldb, nrhs, lu ? 1 : 0, ldl ? 1 : 0, lu ? 0 : cjp);
+            nl++;
+            continue;
+        }
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
             PGPU_CHECK(mark(3));

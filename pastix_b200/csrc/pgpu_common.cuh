@@ -136,6 +136,12 @@ template <typename R> __device__ __forceinline__ cplx<R> shfl_xor_v(const cplx<R
     return cplx<R>(__shfl_xor_sync(0xffffffffu, v.re, m), __shfl_xor_sync(0xffffffffu, v.im, m));
 }
 
+__device__ __forceinline__ void atomic_add(double *p, double v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v); }
+template <typename R> __device__ __forceinline__ void atomic_add(cplx<R> *p, const cplx<R> &v) {
+    atomicAdd(&p->re, v.re);
+    atomicAdd(&p->im, v.im);
+}
 __device__ __forceinline__ void atomic_sub(double *p, double v) { atomicAdd(p, -v); }
 __device__ __forceinline__ void atomic_sub(float *p, float v) { atomicAdd(p, -v); }
 template <typename R> __device__ __forceinline__ void atomic_sub(cplx<R> *p, const cplx<R> &v) {

@@ -418,6 +418,12 @@ constexpr int tcp_smem_bytes() {
 }
 constexpr int TCP_TMEM_COLS = 256;
 
+// Atomic add of 4 consecutive floats (16-byte aligned address).
+__device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, float d) {
+    asm volatile("red.relaxed.gpu.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive(uint32_t addr) {
     asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
 }
@@ -646,15 +652,27 @@ __global__ void __launch_bounds__(TCP_THREADS, 1)
                         if (i >= v.mrows) break;
                         O[(int64_t)i * ldc + j] = E[rr * 33 + lane];
                     }
-                } else if (j < v.ncols) {
-                    const int tc = tcol0 + j;
-                    for (int rr = 0; rr < 32; rr++) {
-                        const int i = warp * 32 + rr;
-                        if (i >= v.mrows) break;
-                        const int t2 = trow_s[i];
+                } else if (!trsm && cb < v.ncols) {
+                    // scatter-add with 16-byte vector reductions: the block's
+                    // target columns [tcs, tcs + nvalid) lie in 9 groups of 4
+                    // columns aligned in the target row (any alignment of
+                    // tcs); entries outside it, or masked, add zero
+                    const int nvalid = min(32, v.ncols - cb);
+                    const int tcs = tcol0 + cb, a0 = tcs & ~3, o = tcs - a0;
+                    for (int k = lane; k < 32 * 9; k += 32) {
+                        const int rr = k / 9, g = k - rr * 9;
+                        const int t2 = trow_s[warp * 32 + rr];     // -1: no target (or row past the tile)
                         if (t2 < 0) continue;
-                        if (lower_only && t2 < wf && tc > t2) continue;
-                        atomicAdd(&C[(int64_t)t2 * ldf + tc], -E[rr * 33 + lane]);
+                        float a[4];
+                        bool any = false;
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            const int jj = 4 * g + u - o, tc = a0 + 4 * g + u;
+                            const bool ok = jj >= 0 && jj < nvalid && !(lower_only && t2 < wf && tc > t2);
+                            a[u] = ok ? -E[rr * 33 + (ok ? jj : 0)] : 0.f;
+                            any |= ok;
+                        }
+                        if (any) red_add_v4(&C[(int64_t)t2 * ldf + a0 + 4 * g], a[0], a[1], a[2], a[3]);
                     }
                 }
                 __syncwarp();

@@ -49,47 +49,48 @@ __device__ __forceinline__ void wp_lds16(const T *p, T (&v)[16 / sizeof(T)]) {
     memcpy(v, &u, 16);
 }
 
-// Row solves against the factorized tile with the row in registers (fully
-// unrolled, so x stays out of local memory); rdiag[j] = 1 / op(diagonal j).
-//   lower_t: x op(L)^t = a (unit when UNIT);  upper: x U = a;
-//   unit_lower: L y = a for a column y (LU row block).
+// Row solve against the factorized tile with the row in registers (fully
+// unrolled, so x stays out of local memory):
+//   x[j] = (x[j] - sum_{l<j} x[l] op(C[j][l])) * (UNIT ? 1 : rdiag[j])
+// in increasing l, C row-major with 16-byte rows (ldc), read as broadcast
+// vectors.  C = the tile's lower part (LL^h, LDL rows; LU row block, unit),
+// or the transposed upper part (LU rows: x U = a).
 template <typename T, bool CJ, bool UNIT>
-__device__ __forceinline__ void wp_solve_lower_t(T (&x)[PB], const T *tile, const T *rdiag, int nb) {
+__device__ __forceinline__ void wp_solve_rows(T (&x)[PB], const T *C, int ldc, const T *rdiag, int nb) {
+    constexpr int VK = 16 / sizeof(T);
 #pragma unroll
     for (int j = 0; j < PB; j++)
         if (j < nb) {
             T s = x[j];
 #pragma unroll
-            for (int l = 0; l < j; l++) s -= x[l] * cj<CJ>(tile[j * PBL + l]);
+            for (int l0 = 0; l0 < j; l0 += VK) {
+                T c[VK];
+                wp_lds16<T>(C + j * ldc + l0, c);
+#pragma unroll
+                for (int v = 0; v < VK; v++)
+                    if (l0 + v < j) s -= x[l0 + v] * cj<CJ>(c[v]);
+            }
             x[j] = UNIT ? s : s * rdiag[j];
         }
 }
-template <typename T>
-__device__ __forceinline__ void wp_solve_upper(T (&x)[PB], const T *tile, const T *rdiag, int nb) {
-#pragma unroll
-    for (int j = 0; j < PB; j++)
-        if (j < nb) {
-            T s = x[j];
-#pragma unroll
-            for (int l = 0; l < j; l++) s -= x[l] * tile[l * PBL + j];
-            x[j] = s * rdiag[j];
-        }
+
+// Byte offset of the tile operands TA / TB, and the shared memory of
+// k_panel_wide for width w with chunks of kcb bytes per row.
+__host__ __device__ inline size_t wp_tile_offset(int w, size_t esz, bool lu, bool ldl, int kcb) {
+    const size_t chunk_row = (size_t)kcb + 16;
+    const size_t b = 2 * (size_t)(w + 16) * chunk_row * (lu ? 2 : 1) + (size_t)w * PBL * esz * (lu ? 2 : 1) +
+                     (ldl ? (size_t)w * esz : 0);
+    return (b + 15) / 16 * 16;
 }
-template <typename T>
-__device__ __forceinline__ void wp_solve_unit_lower(T (&y)[PB], const T *tile, int nb) {
-#pragma unroll
-    for (int j = 0; j < PB; j++)
-        if (j < nb) {
-            T s = y[j];
-#pragma unroll
-            for (int l = 0; l < j; l++) s -= tile[j * PBL + l] * y[l];
-            y[j] = s;
-        }
+__host__ inline size_t wp_smem_bytes(int w, size_t esz, bool lu, bool ldl, int kcb) {
+    return wp_tile_offset(w, esz, lu, ldl, kcb) + (size_t)(lu ? 2 : 1) * PB * (PB * esz + 16);
 }
 
 // Shared memory (elements of T): Ach[2][w + 16][kc + VK] chunk buffers of
 // the left columns, for LU Uch[2][w + 16][kc + VK] (the U rows above,
-// transposed), C[w][PBL], for LU R[w][PBL], for LDL d[w].
+// transposed), C[w][PBL], for LU R[w][PBL], for LDL d[w], then (16-byte
+// aligned) the factorized tile as row solve operands TA[PB][PB + VK] and
+// for LU TB[PB][PB + VK].
 template <typename T, int MODE>
 __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *__restrict__ jobs,
                                                            T *__restrict__ coefL, const double *critp, int kc,
@@ -113,6 +114,9 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
     T *Cb = Uch + (LU ? 2 * bufsz : 0);
     T *Rb = Cb + (int64_t)w * PBL;
     T *dsm = Rb + (LU ? (int64_t)w * PBL : 0);
+    constexpr int LDT = PB + VK;
+    T *TA = reinterpret_cast<T *>(smem_raw + wp_tile_offset(w, sizeof(T), LU, LDL, kc * (int)sizeof(T)));
+    T *TB = TA + PB * LDT;
     const R crit = R(*critp);
     const int tid = threadIdx.x;
     const uint64_t t_start = prof ? global_ns() : 0;
@@ -243,25 +247,31 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
                 if (LDL) dsm[jb + tid] = d;
                 rdiag[tid] = T(1) / (MODE == FM_POTRF ? cj<CJ>(d) : d);
             }
+            // the tile as 16-byte rows: TA = lower part (LU: U^t), TB = lower part (LU)
+            for (int e = tid; e < nb * nb; e += 32) {
+                const int j = e / nb, l = e - j * nb;
+                TA[j * LDT + l] = LU ? Cb[l * PBL + j] : Cb[j * PBL + l];
+                if (LU) TB[j * LDT + l] = Cb[j * PBL + l];
+            }
         }
         __syncthreads();
         for (int r = nb + tid; r < M; r += WP_THREADS) {
             T x[PB];
 #pragma unroll
             for (int j = 0; j < PB; j++) x[j] = (j < nb) ? Cb[r * PBL + j] : T(0);
-            if (LU) wp_solve_upper<T>(x, Cb, rdiag, nb);
-            else if (LDL) wp_solve_lower_t<T, CJ, true>(x, Cb, rdiag, nb);
-            else wp_solve_lower_t<T, CJ, false>(x, Cb, rdiag, nb);
+            if (LU) wp_solve_rows<T, false, false>(x, TA, LDT, rdiag, nb);
+            else if (LDL) wp_solve_rows<T, CJ, true>(x, TA, LDT, rdiag, nb);
+            else wp_solve_rows<T, CJ, false>(x, TA, LDT, rdiag, nb);
 #pragma unroll
             for (int j = 0; j < PB; j++)
                 if (j < nb) Cb[r * PBL + j] = LDL ? x[j] * rdiag[j] : x[j];
         }
-        if (LU)
+        if constexpr (LU)
             for (int i = tid; i < MR; i += WP_THREADS) {
                 T y[PB];
 #pragma unroll
                 for (int j = 0; j < PB; j++) y[j] = (j < nb) ? Rb[i * PBL + j] : T(0);
-                wp_solve_unit_lower<T>(y, Cb, nb);
+                wp_solve_rows<T, false, true>(y, TB, LDT, rdiag, nb);
 #pragma unroll
                 for (int j = 0; j < PB; j++)
                     if (j < nb) Rb[i * PBL + j] = y[j];
@@ -288,13 +298,6 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
             prof[2 * job.y + 1] = (int64_t)global_ns();
         }
     }
-}
-
-// Shared memory of k_panel_wide for width w with chunks of kcb bytes per row.
-__host__ inline size_t wp_smem_bytes(int w, size_t esz, bool lu, bool ldl, int kcb) {
-    const size_t chunk_row = (size_t)kcb + 16;
-    return 2 * (size_t)(w + 16) * chunk_row * (lu ? 2 : 1) + (size_t)w * PBL * esz * (lu ? 2 : 1) +
-           (ldl ? (size_t)w * esz : 0);
 }
 
 // Whether one CTA covers width w with its tile budget.

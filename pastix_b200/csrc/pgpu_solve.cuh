@@ -95,6 +95,109 @@ __device__ void diag_solve_inverse(const T *__restrict__ Bi, const T *__restrict
     }
 }
 
+// Forward product with the inverse for up to 4 right-hand sides: one warp
+// per row n of Bi, lanes across k in 16-byte vectors read straight from
+// global memory (no staging), the warp's partial sums reduced by shuffles:
+// B[fc + n] = sum_{k <= n} op(Bi[n][k]) v[k] (times d_n for LDL).
+template <typename T, int NR>
+__device__ void diag_solve_inverse_fwd_warp(const T *__restrict__ Bi, const T *__restrict__ D, int w, int ld,
+                                            bool ldl, bool cjp, const T *__restrict__ v, T *__restrict__ Bg,
+                                            int64_t ldb, int fc) {
+    constexpr int VEC = 16 / sizeof(T);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int n = warp; n < w; n += nw) {
+        const T *row = Bi + (int64_t)n * ld;
+        T acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) acc[r] = T(0);
+        for (int k0 = lane * VEC; k0 <= n; k0 += 32 * VEC) {
+            const uint4 u = __ldg(reinterpret_cast<const uint4 *>(row + k0));
+            T e[VEC];
+            memcpy(e, &u, 16);
+#pragma unroll
+            for (int q = 0; q < VEC; q++) {
+                const int k = k0 + q;
+                if (k <= n) {
+                    const T b = cjp ? conj_v(e[q]) : e[q];
+#pragma unroll
+                    for (int r = 0; r < NR; r++) acc[r] += b * v[k * NR + r];
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[r] += shfl_xor_v(acc[r], o);
+        }
+        if (lane == 0) {
+            T d = T(1);
+            if (ldl) {
+                d = D[(int64_t)n * ld + n];
+                if (cjp) d = conj_v(d);
+            }
+#pragma unroll
+            for (int r = 0; r < NR; r++) Bg[(int64_t)r * ldb + fc + n] = ldl ? acc[r] * d : acc[r];
+        }
+    }
+}
+
+// Backward product with the inverse for 1 or 2 right-hand sides:
+// x[k] = sum_{n >= k} Bi[n][k] v'[n] (v' = d v for LDL).  One warp per row
+// n, each lane accumulating its k-vectors (KS of them, w <= 32 KS VEC) in
+// registers; the warps' partial sums meet in shared memory (atomics), then
+// B[fc + k] = x[k].  xacc: [w][NR] shared accumulators.
+template <typename T, int NR, int KS>
+__device__ void diag_solve_inverse_bwd_warp(const T *__restrict__ Bi, const T *__restrict__ D, int w, int ld,
+                                            bool ldl, const T *__restrict__ v, T *__restrict__ xacc,
+                                            T *__restrict__ Bg, int64_t ldb, int fc) {
+    constexpr int VEC = 16 / sizeof(T);
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    for (int e = tid; e < w * NR; e += nt) xacc[e] = T(0);
+    T part[KS][VEC][NR];
+#pragma unroll
+    for (int q = 0; q < KS; q++)
+#pragma unroll
+        for (int u = 0; u < VEC; u++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) part[q][u][r] = T(0);
+    __syncthreads();
+    for (int n = warp; n < w; n += nw) {
+        T vn[NR];
+        const T dn = ldl ? D[(int64_t)n * ld + n] : T(1);
+#pragma unroll
+        for (int r = 0; r < NR; r++) vn[r] = ldl ? v[n * NR + r] * dn : v[n * NR + r];
+        const T *row = Bi + (int64_t)n * ld;
+#pragma unroll
+        for (int q = 0; q < KS; q++) {
+            const int k0 = (lane + 32 * q) * VEC;
+            if (k0 <= n) {
+                const uint4 u4 = __ldg(reinterpret_cast<const uint4 *>(row + k0));
+                T e[VEC];
+                memcpy(e, &u4, 16);
+#pragma unroll
+                for (int u = 0; u < VEC; u++)
+                    if (k0 + u <= n)
+#pragma unroll
+                        for (int r = 0; r < NR; r++) part[q][u][r] += e[u] * vn[r];
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < KS; q++)
+#pragma unroll
+        for (int u = 0; u < VEC; u++) {
+            const int k = (lane + 32 * q) * VEC + u;
+            if (k < w && k <= warp + (w - 1 - warp) / nw * nw)   // this warp saw a row n >= k
+#pragma unroll
+                for (int r = 0; r < NR; r++) atomic_add(&xacc[k * NR + r], part[q][u][r]);
+        }
+    __syncthreads();
+    for (int e = tid; e < w * NR; e += nt) {
+        const int k = e / NR, r = e - k * NR;
+        Bg[(int64_t)r * ldb + fc + k] = xacc[e];
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(1024) k_fwd_diag(Meta m, const int *__restrict__ cblks, const T *__restrict__ coefL,
                                                   T *__restrict__ B, int ldb, int nrhs, int unit, int pch,
@@ -112,9 +215,15 @@ __global__ void __launch_bounds__(1024) k_fwd_diag(Meta m, const int *__restrict
         // LU: the unit-lower inverse is the cblk's second one; the staged
         // rows start on a 16-byte boundary (vector stores)
         __syncthreads();
-        diag_solve_inverse<T>(inv + m.invoff[c] + (unit && !ldl ? inv_span(w, ld) : 0), D, w, ld, nrhs, false,
-                              ldl != 0, cjp != 0, y, nullptr, y + align16_elems<T>((size_t)w * nrhs), ipch, B, ldb,
-                              fc);
+        const T *Bi = inv + m.invoff[c] + (unit && !ldl ? inv_span(w, ld) : 0);
+        switch (nrhs) {
+        case 1: diag_solve_inverse_fwd_warp<T, 1>(Bi, D, w, ld, ldl != 0, cjp != 0, y, B, ldb, fc); return;
+        case 2: diag_solve_inverse_fwd_warp<T, 2>(Bi, D, w, ld, ldl != 0, cjp != 0, y, B, ldb, fc); return;
+        case 4: diag_solve_inverse_fwd_warp<T, 4>(Bi, D, w, ld, ldl != 0, cjp != 0, y, B, ldb, fc); return;
+        default: break;
+        }
+        diag_solve_inverse<T>(Bi, D, w, ld, nrhs, false, ldl != 0, cjp != 0, y, nullptr,
+                              y + align16_elems<T>((size_t)w * nrhs), ipch, B, ldb, fc);
         return;
     }
     T *tile = y + w * nrhs;                   // [32][33] diagonal tile
@@ -248,6 +357,96 @@ __global__ void __launch_bounds__(256) k_bwd_off(Meta m, const int2 *__restrict_
 }
 
 // ---------------------------------------------------------------------------
+// Levels of narrow cblks (w <= 32, no diagonal-block inverse: the leaves of
+// the elimination tree, tens of thousands of them): one warp per cblk does
+// the diagonal solve and its off-diagonal rows in one launch, the solution
+// of the cblk kept in the lanes' registers (lane j holds x_j) and handed
+// to the row products by shuffles.  Same operations as k_fwd_diag +
+// k_fwd_off (forward) and k_bwd_off + k_bwd_diag (backward) for these
+// cblks; the backward gather needs no atomics (one warp owns the cblk).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwd_small(Meta m, const int *__restrict__ cblks, int ncb,
+                                                   const T *__restrict__ coefL, T *__restrict__ B, int ldb, int nrhs,
+                                                   int unit) {
+    const int lane = threadIdx.x & 31;
+    const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (q >= ncb) return;                                  // whole warps
+    const int c = cblks[q];
+    const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c], h = m.height[c];
+    const T *D = coefL + m.coefoff[c];
+    const T dinv = (lane < w && !unit) ? T(1) / D[(int64_t)lane * ld + lane] : T(1);
+    const int *rows = m.rowidx + m.rowbase[c];
+    for (int r = 0; r < nrhs; r++) {
+        T *Br = B + (int64_t)r * ldb;
+        T v = (lane < w) ? Br[fc + lane] : T(0);
+        for (int j = 0; j < w; j++) {
+            if (lane == j) v = v * dinv;
+            const T xj = shfl_v(v, j);
+            if (lane > j && lane < w) v -= D[(int64_t)lane * ld + j] * xj;
+        }
+        if (lane < w) Br[fc + lane] = v;
+        for (int i0 = w; i0 < h; i0 += 32) {
+            const int i = i0 + lane;
+            const T *row = D + (int64_t)i * ld;
+            T s = T(0);
+            for (int j = 0; j < w; j++) {
+                const T xj = shfl_v(v, j);
+                if (i < h) s += row[j] * xj;
+            }
+            if (i < h) atomic_sub(&Br[rows[i]], s);
+        }
+    }
+}
+
+// upper != 0: U of the LU diagonal block (row-major upper part, non-unit),
+// P = the U^t panel (coefP); else op(L)^t with op = conj when cjp, P = L.
+template <typename T>
+__global__ void __launch_bounds__(256) k_bwd_small(Meta m, const int *__restrict__ cblks, int ncb,
+                                                   const T *__restrict__ coefL, const T *__restrict__ coefP,
+                                                   T *__restrict__ B, int ldb, int nrhs, int upper, int unit,
+                                                   int cjp) {
+    const int lane = threadIdx.x & 31;
+    const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (q >= ncb) return;
+    const int c = cblks[q];
+    const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c], h = m.height[c];
+    const T *D = coefL + m.coefoff[c];
+    const T *P = coefP + m.coefoff[c];
+    const int *rows = m.rowidx + m.rowbase[c];
+    T dinv = T(1);
+    if (lane < w && !unit) {
+        const T d = D[(int64_t)lane * ld + lane];
+        dinv = T(1) / (cjp ? conj_v(d) : d);
+    }
+    for (int r = 0; r < nrhs; r++) {
+        T *Br = B + (int64_t)r * ldb;
+        // gather: x_j -= sum_i op(P[i][j]) x[row_i]
+        T s = T(0);
+        if (lane < w)
+            for (int i = w; i < h; i++) {
+                const T pv = P[(int64_t)i * ld + lane];
+                s += (cjp ? conj_v(pv) : pv) * Br[rows[i]];
+            }
+        T v = (lane < w) ? Br[fc + lane] - s : T(0);
+        for (int j = w - 1; j >= 0; j--) {
+            if (lane == j) v = v * dinv;
+            const T xj = shfl_v(v, j);
+            if (lane < j) {
+                T dlj;
+                if (upper) dlj = D[(int64_t)lane * ld + j];
+                else {
+                    dlj = D[(int64_t)j * ld + lane];
+                    if (cjp) dlj = conj_v(dlj);
+                }
+                v -= dlj * xj;
+            }
+        }
+        if (lane < w) Br[fc + lane] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Backward, diagonal part: B[fcol:fcol+w, :] := D^{-1} B[...] with
 // D = op(L_kk)^t (POTRF: Left, Lower, ConjTrans, NonUnit; LDL: the unit
 // lower part, Left, Lower, ConjTrans/Trans, Unit, after k_diag_scale) or the
@@ -271,7 +470,23 @@ __global__ void __launch_bounds__(1024) k_bwd_diag(Meta m, const int *__restrict
         [&](int e, T v) { x[e] = v; });
     if (inv && m.invoff[c] >= 0) {
         __syncthreads();
-        diag_solve_inverse<T>(inv + m.invoff[c], D, w, ld, nrhs, true, ldl != 0, false, x, x + (size_t)w * nrhs,
+        const T *Bi = inv + m.invoff[c];
+        constexpr int VEC = 16 / sizeof(T);
+        T *acc = x + (size_t)w * nrhs;
+        // register budget of the 1024-thread block: KS VEC NR elements of T per lane
+        if (nrhs == 1 && w <= 32 * 4 * VEC) {
+            diag_solve_inverse_bwd_warp<T, 1, 4>(Bi, D, w, ld, ldl != 0, x, acc, B, ldb, fc);
+            return;
+        }
+        if (nrhs == 1 && w <= 32 * 8 * VEC && sizeof(T) * 8 * VEC <= 128) {
+            diag_solve_inverse_bwd_warp<T, 1, 8>(Bi, D, w, ld, ldl != 0, x, acc, B, ldb, fc);
+            return;
+        }
+        if (nrhs == 2 && w <= 32 * 4 * VEC && sizeof(T) * 8 * VEC <= 128) {
+            diag_solve_inverse_bwd_warp<T, 2, 4>(Bi, D, w, ld, ldl != 0, x, acc, B, ldb, fc);
+            return;
+        }
+        diag_solve_inverse<T>(Bi, D, w, ld, nrhs, true, ldl != 0, false, x, acc,
                               x + align16_elems<T>((size_t)2 * w * nrhs), ipch, B, ldb, fc);
         return;
     }
