@@ -226,6 +226,8 @@ PASTIX_GPU_API int pastix_gpu_set_cblk_priority( pastix_gpu_t *ctx, const double
  *   PGPU_TUNE_TC_MIN_MN       smallest M x N update sent to the tensor cores (8192)
  *   PGPU_TUNE_WIDE_PANEL      narrowest diagonal block factorized by the 512-thread
  *                             left-looking kernel (128; 0 disables it)
+ *   PGPU_TUNE_TC_TMA          1 (default): 3xTF32 operands pre-split once per panel and
+ *                             loaded by TMA; 0: split by producer warps per tile
  * Setting one invalidates the factorization plan (rebuilt by the next numfact).
  */
 #define PGPU_TUNE_MIXED_GEMM      0
@@ -236,7 +238,8 @@ PASTIX_GPU_API int pastix_gpu_set_cblk_priority( pastix_gpu_t *ctx, const double
 #define PGPU_TUNE_TRSM_GEMM_ROWS  5
 #define PGPU_TUNE_TC_MIN_MN       6
 #define PGPU_TUNE_WIDE_PANEL      7
-#define PGPU_TUNE_COUNT           8
+#define PGPU_TUNE_TC_TMA          8
+#define PGPU_TUNE_COUNT           9
 PASTIX_GPU_API int pastix_gpu_set_tuning( pastix_gpu_t *ctx, int key, int64_t value );
 PASTIX_GPU_API int pastix_gpu_get_tuning( pastix_gpu_t *ctx, int key, int64_t *value );
 

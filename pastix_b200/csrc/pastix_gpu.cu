@@ -7,6 +7,9 @@
 #include "pgpu_panel.cuh"
 #include "pgpu_gemm_tc.cuh"
 #include "pgpu_panel_wide.cuh"
+#include "pgpu_gemm_tma.cuh"
+
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <chrono>
@@ -164,6 +167,16 @@ struct pastix_gpu_s {
     std::vector<int64_t> invoff, scroff;
     DArr<int64_t> d_invoff, d_scroff;
     DArr<unsigned char> d_inv, d_scr;    // inverse workspace (zeroed), per-level TRSM output
+    // TMA operands of the tensor-core GEMMs: hi/lo mirrors [2][plane] of the
+    // coeftab and of the inverses (3xTF32), one tensor map per (source cblk,
+    // operand kind), split jobs {cblk, row, panel, -} per level
+    bool tma = false;
+    DArr<float> d_hilo, d_ihilo;
+    int64_t hilo_plane = 0, ihilo_plane = 0;
+    DArr<CUtensorMap> d_tmaps;
+    DArr<int> d_mapidx;
+    std::vector<int> split_ptr;
+    DArr<int4> d_split;
     std::vector<int> inv_ptr, ttile_ptr, tttile_ptr;   // per level: inverse jobs, TRSM FMA / TC tiles
     DArr<int2> d_invjobs;
     DArr<int4> d_ttiles, d_tttiles;
@@ -534,8 +547,40 @@ static void default_tuning(int64_t *t) {
     t[PGPU_TUNE_TC_MIN_MN] = 128 * 64;
     e = getenv("PASTIX_GPU_WIDE_PANEL");
     t[PGPU_TUNE_WIDE_PANEL] = e ? std::atoi(e) : 128;
+    e = getenv("PASTIX_GPU_TC_TMA");
+    t[PGPU_TUNE_TC_TMA] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
 }
 static int mixed_gemm_mode(const pastix_gpu_t &C) { return (int)C.tune[PGPU_TUNE_MIXED_GEMM]; }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); nullptr when the driver does not provide it.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 3-D map {K = w, rows, planes} over float rows of stride ld (elements),
+// planes `plane` elements apart, box {32, 128, planes}, SWIZZLE_128B.
+static bool encode_panel_map(CUtensorMap *map, float *base, int w, int rows, int ld, int planes, int64_t plane) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)w, (cuuint64_t)rows, (cuuint64_t)planes};
+    const cuuint64_t strides[2] = {(cuuint64_t)ld * 4, (cuuint64_t)std::max<int64_t>(plane, 1) * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)TC_BK, (cuuint32_t)TC_BM, (cuuint32_t)planes};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 static bool tc_enabled(const pastix_gpu_t &C) { return mixed_gemm_mode(C) != MG_FP32; }
 static bool tc_task(const pastix_gpu_t &C, int M, int N, int K) {
     return K >= 32 && M >= 64 && N >= 32 && (int64_t)M * N >= C.tune[PGPU_TUNE_TC_MIN_MN];
@@ -705,6 +750,58 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
         C.tttile_ptr[l + 1] = (int)tttiles.size();
         scr_max = std::max(scr_max, scr_lvl);
     }
+    // TMA operands (3xTF32, persistent kernel): hi/lo mirrors, tensor maps of
+    // the source cblks, split jobs of their off-diagonal rows per level
+    C.tma = use_tc && mixed_gemm_mode(C) == MG_3XTF32 && C.tune[PGPU_TUNE_TC_KERNEL] != 0 && !C.record &&
+            C.tune[PGPU_TUNE_TC_TMA] != 0 && tensor_map_encoder() != nullptr;
+    C.split_ptr.assign(C.nlevels + 1, 0);
+    if (C.tma) {
+        std::vector<char> src(C.cblknbr, 0);
+        for (const int4 &t : tctiles) src[tasks[t.x].c] = 1;
+        for (const int4 &t : tttiles) src[tasks[t.x].c] = 1;
+        const int64_t ncoef = C.coefnbr * (lu ? 2 : 1);
+        C.hilo_plane = (ncoef + 31) / 32 * 32;
+        C.ihilo_plane = (inv_elems + 31) / 32 * 32;
+        if (C.d_hilo.n < (size_t)(2 * C.hilo_plane)) PGPU_CHECK(C.d_hilo.alloc(2 * C.hilo_plane));
+        if (C.d_ihilo.n < (size_t)(2 * C.ihilo_plane))
+            PGPU_CHECK(C.d_ihilo.alloc(2 * std::max<int64_t>(C.ihilo_plane, 32)));
+        // the inverses' strict upper parts are never written: zero planes
+        PGPU_CHECK(cudaMemsetAsync(C.d_ihilo.p, 0, C.d_ihilo.n * sizeof(float), C.stream));
+        std::vector<int> mapidx(C.cblknbr, -1);
+        std::vector<CUtensorMap> maps;
+        std::vector<int4> split;
+        for (int l = 0; l < C.nlevels && C.tma; l++) {
+            for (int q = C.lvl_ptr[l]; q < C.lvl_ptr[l + 1]; q++) {
+                const int c = C.lvl_cblks[q];
+                if (!src[c]) continue;
+                const int w = C.width[c], h = C.height[c], ld = C.ld[c];
+                mapidx[c] = (int)maps.size();
+                maps.resize(maps.size() + TMAP_KINDS);
+                CUtensorMap *mp = &maps[mapidx[c]];
+                std::memset(mp, 0, TMAP_KINDS * sizeof(CUtensorMap));
+                bool ok = encode_panel_map(mp + TMAP_L, C.d_hilo.p + C.coefoff[c], w, h, ld, 2, C.hilo_plane);
+                if (lu) ok = ok && encode_panel_map(mp + TMAP_U, C.d_hilo.p + C.coefnbr + C.coefoff[c], w, h, ld, 2,
+                                                    C.hilo_plane);
+                if (C.invoff[c] >= 0) {
+                    ok = ok && encode_panel_map(mp + TMAP_I, C.d_ihilo.p + C.invoff[c], w, w, ld, 2, C.ihilo_plane);
+                    if (lu)
+                        ok = ok && encode_panel_map(mp + TMAP_I2, C.d_ihilo.p + C.invoff[c] + inv_span(w, ld), w, w,
+                                                    ld, 2, C.ihilo_plane);
+                }
+                if (!ok) C.tma = false;
+                for (int r0 = w; r0 < h; r0 += 32)
+                    for (int panel = 0; panel < (lu ? 2 : 1); panel++) split.push_back(make_int4(c, r0, panel, 0));
+            }
+            C.split_ptr[l + 1] = (int)split.size();
+        }
+        if (C.tma) {
+            PGPU_CHECK(C.d_tmaps.upload(maps, C.stream));
+            PGPU_CHECK(C.d_mapidx.upload(mapidx, C.stream));
+            PGPU_CHECK(C.d_split.upload(split, C.stream));
+        } else {
+            C.split_ptr.assign(C.nlevels + 1, 0);
+        }
+    }
     if (tgemm) {
         PGPU_CHECK(C.d_invjobs.upload(invjobs, C.stream));
         PGPU_CHECK(C.d_ttiles.upload(ttiles, C.stream));
@@ -812,6 +909,14 @@ static PanelKernel<T> panel_kernel(int fmode) {
     }
 }
 
+// The hi / lo planes as the kernels' element type: only single-precision
+// factors have them.
+template <typename T>
+static T *hilo_of(float *p) {
+    if constexpr (std::is_same<T, float>::value) return p;
+    else return nullptr;
+}
+
 template <typename T>
 static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm) {
     const bool lu = (fmode == FM_GETRF);
@@ -842,6 +947,8 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, tcp_smem_bytes<false>()));
         PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc_persistent<true>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, tcp_smem_bytes<true>()));
+        PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        tma_smem_bytes<true>()));
         PGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, C.device));
     }
     int64_t *prof[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -869,6 +976,17 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
         PGPU_CHECK(cudaEventRecord(C.la_events[2 * C.nlevels], s));
         PGPU_CHECK(cudaStreamWaitEvent(C.stream2, C.la_events[2 * C.nlevels], 0));
     }
+    // hi / lo split of the level's tensor-core source rows (before their first use as TMA operands)
+    auto split_level = [&](int l) {
+        if constexpr (std::is_same<T, float>::value) {
+            const int nsp = C.split_ptr[l + 1] - C.split_ptr[l];
+            if (C.tma && nsp) {
+                k_split_rows<<<nsp, 256, 0, s>>>(C.meta, C.d_split.p + C.split_ptr[l], coefL, coefU, C.d_hilo.p,
+                                                 C.hilo_plane, C.coefnbr);
+                nl++;
+            }
+        }
+    };
     auto launch_gemms = [&](cudaStream_t st, LaunchTimer &lt, int t0, int nt, int c0, int ntc, int gcap) -> int {
         if (nt) {
             PGPU_CHECK(lt.mark(PH_GEMM));
@@ -881,7 +999,12 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
         if constexpr (std::is_same<T, float>::value) {
             if (ntc) {
                 PGPU_CHECK(lt.mark(PH_TC));
-                if (persist) {
+                if (persist && C.tma) {
+                    const int g = std::min(ntc, gcap);
+                    k_gemm_scatter_tc_tma<true><<<g, TMA_THREADS, tma_smem_bytes<true>(), st>>>(
+                        C.meta, C.d_tctiles.p + c0, ntc, C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr,
+                        C.d_tmaps.p, C.d_mapidx.p);
+                } else if (persist) {
                     const int g = std::min(ntc, gcap);
                     if (split)
                         k_gemm_scatter_tc_persistent<true><<<g, TCP_THREADS, tcp_smem_bytes<true>(), st>>>(
@@ -950,8 +1073,10 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             PGPU_CHECK(tm.mark(PH_TRSM));
             k_tri_inverse<T><<<nij, 256, ism, s>>>(C.meta, C.d_invjobs.p + C.inv_ptr[l], coefL, inv,
                                                    fm_ldl(fmode) ? 1 : 0, (CPX && fm_conj(fmode)) ? 1 : 0,
-                                                   fm_ldl(fmode) ? 1 : 0, lu ? 1 : 0, kch);
+                                                   fm_ldl(fmode) ? 1 : 0, lu ? 1 : 0, kch,
+                                                   C.tma ? hilo_of<T>(C.d_ihilo.p) : nullptr, C.ihilo_plane);
             nl++;
+            split_level(l);
             const int ntt = C.ttile_ptr[l + 1] - C.ttile_ptr[l];
             if (ntt) {
                 k_gemm_scatter<T><<<ntt, 256, 0, s>>>(C.meta, C.d_ttiles.p + C.ttile_ptr[l], C.d_tasks.p, coefL, coefU,
@@ -962,7 +1087,11 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                 const int ntc = C.tttile_ptr[l + 1] - C.tttile_ptr[l];
                 if (ntc) {
                     const int g = std::min(ntc, nsm);
-                    if (split)
+                    if (C.tma)
+                        k_gemm_scatter_tc_tma<true><<<g, TMA_THREADS, tma_smem_bytes<true>(), s>>>(
+                            C.meta, C.d_tttiles.p + C.tttile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
+                            scr, C.d_tmaps.p, C.d_mapidx.p);
+                    else if (split)
                         k_gemm_scatter_tc_persistent<true><<<g, TCP_THREADS, tcp_smem_bytes<true>(), s>>>(
                             C.meta, C.d_tttiles.p + C.tttile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
                             inv, scr);
@@ -974,7 +1103,8 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                 }
             }
             k_trsm_copyback<T><<<ntr, 256, 0, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], C.d_scroff.p, scr, coefL,
-                                                   coefU);
+                                                   coefU, C.tma ? hilo_of<T>(C.d_hilo.p) : nullptr, C.hilo_plane,
+                                                   C.coefnbr);
             nl++;
         } else if (ntr) {
             const size_t fixed = ((size_t)TRSM_TR * (mw + 1) + PB * PBL) * sizeof(T);
@@ -987,6 +1117,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                                         at(prof[1], C.trsm_ptr[l]));
             nl++;
         }
+        if (!(ntr && C.trsm_gemm)) split_level(l);   // the level's rows are final here
         // update GEMMs of the level: with lookahead the tiles whose target is
         // in the next level run here, the rest on stream2 once this level's
         // panels are final

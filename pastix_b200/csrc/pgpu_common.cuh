@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 
 namespace pgpu {
 
@@ -177,6 +178,14 @@ __device__ __forceinline__ void batched_copy(int total, int tid, int nt, Src src
             if (e < total) dst(e, r[u]);
         }
     }
+}
+
+// Round to TF32 (nearest, ties away from zero): the "hi" part of a 3xTF32
+// operand split x = hi + lo.
+__device__ __forceinline__ float tf32_round(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
 }
 
 // Shared-memory address and asynchronous global -> shared copies

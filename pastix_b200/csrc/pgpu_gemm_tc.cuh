@@ -125,12 +125,8 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Round to TF32 (nearest, ties away) -- the "hi" part of the 3xTF32 split.
-__device__ __forceinline__ float tf32_hi(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
-}
+// The "hi" part of the 3xTF32 split (TF32 rounding, pgpu_common.cuh).
+__device__ __forceinline__ float tf32_hi(float x) { return tf32_round(x); }
 
 __device__ __forceinline__ void sts128(uint32_t saddr, float4 v) {
     asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(saddr), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)

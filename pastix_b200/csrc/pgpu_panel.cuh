@@ -464,7 +464,8 @@ __host__ __device__ inline size_t tri_inverse_lb_offset(int nrow, size_t esz) {
 template <typename T>
 __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restrict__ jobs,
                                                      const T *__restrict__ coefL, T *__restrict__ inv,
-                                                     int unit, int cjp, int scale_d, int lu, int kch) {
+                                                     int unit, int cjp, int scale_d, int lu, int kch,
+                                                     T *__restrict__ ihilo, int64_t iplane) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int2 jbv = jobs[blockIdx.x];
     const int c = jbv.x, jb = jbv.y & 0xFFFFF, kind = jbv.y >> 20;
@@ -579,7 +580,16 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
         const int i = e / nb, q = e - i * nb;
         T v = X[i * PBL + q];
         if (scale_d) v = v * (T(1) / D[(int64_t)(jb + i) * ld + jb + i]);
-        Inv[(int64_t)(jb + i) * ld + jb + q] = v;
+        const int64_t o = (int64_t)(jb + i) * ld + jb + q;
+        Inv[o] = v;
+        if constexpr (std::is_same<T, float>::value) {
+            if (ihilo) {   // hi / lo planes of the tensor-core operand (3xTF32)
+                const int64_t io = (Inv - inv) + o;
+                const float hi = tf32_round(v);
+                ihilo[io] = hi;
+                ihilo[iplane + io] = v - hi;
+            }
+        }
     }
 }
 
@@ -588,18 +598,34 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
 // TRSM chunk {cblk, first row, panel, mode} of 32 rows.
 // For LU the U^t rows (panel 1) come from the second half of the cblk's
 // scratch (inv_span(h - w, ld) further) and go to the U coeftab.
+// hilo != nullptr (single precision, TMA operands): the rows' hi / lo split
+// is written too, at the coeftab offsets (U^t rows coefnbr further) of the
+// planes hilo[0..plane) and hilo[plane..2 plane).
 template <typename T>
 __global__ void k_trsm_copyback(Meta m, const int4 *__restrict__ chunks, const int64_t *__restrict__ scroff,
-                                const T *__restrict__ scr, T *__restrict__ coefL, T *__restrict__ coefU) {
+                                const T *__restrict__ scr, T *__restrict__ coefL, T *__restrict__ coefU,
+                                T *__restrict__ hilo, int64_t plane, int64_t coefnbr) {
     const int4 ch = chunks[blockIdx.x];
     const int c = ch.x, r0 = ch.y;
     const int w = m.width[c], h = m.height[c], ld = m.ld[c];
     const int nr = min(32, h - r0);
     const T *src = scr + scroff[c] + (ch.z ? inv_span(h - w, ld) : 0) + (int64_t)(r0 - w) * ld;
-    T *dst = (ch.z ? coefU : coefL) + m.coefoff[c] + (int64_t)r0 * ld;
+    const int64_t doff = m.coefoff[c] + (int64_t)r0 * ld;
+    T *dst = (ch.z ? coefU : coefL) + doff;
+    T *hdst = hilo ? hilo + doff + (ch.z ? coefnbr : 0) : nullptr;
     batched_copy(
         nr * w, threadIdx.x, blockDim.x, [&](int e) { const int i = e / w, j = e - i * w; return src[(int64_t)i * ld + j]; },
-        [&](int e, T v) { const int i = e / w, j = e - i * w; dst[(int64_t)i * ld + j] = v; });
+        [&](int e, T v) {
+            const int i = e / w, j = e - i * w;
+            dst[(int64_t)i * ld + j] = v;
+            if constexpr (std::is_same<T, float>::value) {
+                if (hdst) {
+                    const float hi = tf32_round(v);
+                    hdst[(int64_t)i * ld + j] = hi;
+                    hdst[plane + (int64_t)i * ld + j] = v - hi;
+                }
+            }
+        });
 }
 
 }  // namespace pgpu

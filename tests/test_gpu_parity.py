@@ -339,3 +339,32 @@ def test_wide_panel_kernel_matches_narrow(fact, make, mixed):
     if fact == "getrf":
         assert np.abs(U1 - U0).max() <= tol * np.abs(U0).max()
     s.close()
+
+
+@pytest.mark.parametrize("fact,make", [
+    ("potrf", lambda: M.diffusion_lognormal(26, 25, 24, 1.0, np.random.default_rng(12))),
+    ("getrf", lambda: M.convdiff_upwind(20, 18, 16, 10.0)),
+], ids=["potrf", "getrf"])
+@pytest.mark.parametrize("trsm_gemm", [1, 0], ids=["trsm_gemm", "trsm_rows"])
+def test_tma_operands_match_producer_split(fact, make, trsm_gemm):
+    """3xTF32 update and TRSM GEMMs with the operands split once per panel
+    into hi / lo planes and loaded by TMA (PGPU_TUNE_TC_TMA = 1) against the
+    producer warps splitting each tile (= 0): the same products, up to the
+    order of the scatter-add reductions."""
+    from pastix_b200 import autotune as AT
+    A = make()
+    ref, st = U.run_reference(A, fact, numfact=False)
+    s = _gpu_solver(A, st, fact, mixed=True)
+    assert AT.get_knob(s, "tc_tma") == 1
+    AT.set_knob(s, "trsm_gemm", trsm_gemm)
+    s.numfact(A.values)
+    L1, U1 = s.coeftab()
+    AT.set_knob(s, "tc_tma", 0)
+    s.numfact(A.values)
+    L0, U0 = s.coeftab()
+    assert np.abs(L1.astype(np.float64) - L0).max() <= 2e-6 * np.abs(L0).max()
+    if fact == "getrf":
+        assert np.abs(U1.astype(np.float64) - U0).max() <= 2e-6 * np.abs(U0).max()
+    st_ = s.stats()
+    assert st_["tc_ms"] > 0
+    s.close()
