@@ -1380,8 +1380,17 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
             PGPU_CHECK(mark(1));
-            k_fwd_off<T><<<nch, 256, off_smem(mw, true), s>>>(
-                C.meta, C.d_solve_chunks.p + C.solve_ptr[l], coefL, W, ldb, nrhs, SOLVE_ROWS_PER_CHUNK);
+            const size_t ysm = (size_t)round_up(mw, 16 / (int64_t)sizeof(T)) * nrhs * sizeof(T);
+            const int2 *chp = C.d_solve_chunks.p + C.solve_ptr[l];
+            if (nrhs == 1)
+                k_fwd_off_direct<T, 1><<<nch, 256, ysm, s>>>(C.meta, chp, coefL, W, ldb, SOLVE_ROWS_PER_CHUNK);
+            else if (nrhs == 2)
+                k_fwd_off_direct<T, 2><<<nch, 256, ysm, s>>>(C.meta, chp, coefL, W, ldb, SOLVE_ROWS_PER_CHUNK);
+            else if (nrhs == 4)
+                k_fwd_off_direct<T, 4><<<nch, 256, ysm, s>>>(C.meta, chp, coefL, W, ldb, SOLVE_ROWS_PER_CHUNK);
+            else
+                k_fwd_off<T><<<nch, 256, off_smem(mw, true), s>>>(C.meta, chp, coefL, W, ldb, nrhs,
+                                                                  SOLVE_ROWS_PER_CHUNK);
             nl++;
         }
     }
@@ -1403,9 +1412,16 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         const int nch = C.solve_ptr[l + 1] - C.solve_ptr[l];
         if (nch) {
             PGPU_CHECK(mark(3));
-            k_bwd_off<T><<<nch, 256, off_smem(mw, false), s>>>(
-                C.meta, C.d_solve_chunks.p + C.solve_ptr[l], coefU, W, ldb, nrhs, SOLVE_ROWS_PER_CHUNK,
-                lu ? 0 : cjp);
+            const size_t xsm = (size_t)SOLVE_ROWS_PER_CHUNK * nrhs * sizeof(T);
+            const int2 *chp = C.d_solve_chunks.p + C.solve_ptr[l];
+            const int bcj = lu ? 0 : cjp;
+            if (nrhs == 2)
+                k_bwd_off_direct<T, 2><<<nch, 256, xsm, s>>>(C.meta, chp, coefU, W, ldb, SOLVE_ROWS_PER_CHUNK, bcj);
+            else if (nrhs == 4)
+                k_bwd_off_direct<T, 4><<<nch, 256, xsm, s>>>(C.meta, chp, coefU, W, ldb, SOLVE_ROWS_PER_CHUNK, bcj);
+            else
+                k_bwd_off<T><<<nch, 256, off_smem(mw, false), s>>>(C.meta, chp, coefU, W, ldb, nrhs,
+                                                                   SOLVE_ROWS_PER_CHUNK, bcj);
             nl++;
         }
         int pch = 0;

@@ -357,6 +357,116 @@ __global__ void __launch_bounds__(256) k_bwd_off(Meta m, const int2 *__restrict_
 }
 
 // ---------------------------------------------------------------------------
+// Off-diagonal kernels for up to 4 right-hand sides, the panel rows read
+// straight from global memory in 16-byte vectors (no shared staging), so a
+// chunk costs about one memory latency:
+//   k_fwd_off_direct: one warp per RU rows at a time (all RU rows' loads in
+//     flight together), lanes across the columns, the cblk's solution in
+//     shared memory (zero padded); the row sums are reduced by shuffles and
+//     subtracted atomically from B at the rows' global indices;
+//   k_bwd_off_direct (2 or 4 right-hand sides): one thread per column,
+//     looping over the chunk's rows (coalesced across the threads), the
+//     solution at those rows gathered in shared memory; partial sums of the
+//     chunks meet atomically.  (One right-hand side keeps k_bwd_off: its
+//     16-byte staging wins when each loaded value feeds a single product.)
+// Same products as k_fwd_off / k_bwd_off.
+// ---------------------------------------------------------------------------
+template <typename T, int NR>
+__global__ void __launch_bounds__(256) k_fwd_off_direct(Meta m, const int2 *__restrict__ chunks,
+                                                        const T *__restrict__ coef, T *__restrict__ B, int ldb,
+                                                        int rows_per_chunk) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int VEC = 16 / sizeof(T), RU = 4;
+    const int2 ch = chunks[blockIdx.x];
+    const int c = ch.x, r0 = ch.y;
+    const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c], h = m.height[c];
+    const int wp = (w + VEC - 1) / VEC * VEC;
+    const int nr = min(h, r0 + rows_per_chunk) - r0;
+    T *y = reinterpret_cast<T *>(smem_raw);            // [wp][NR] (zero padded)
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    for (int e = tid; e < wp * NR; e += blockDim.x) {
+        const int j = e / NR, r = e - j * NR;
+        y[e] = j < w ? B[(int64_t)r * ldb + fc + j] : T(0);
+    }
+    __syncthreads();
+    const T *P = coef + m.coefoff[c] + (int64_t)r0 * ld;
+    const int *rows = m.rowidx + m.rowbase[c] + r0;
+    for (int i0 = warp * RU; i0 < nr; i0 += nw * RU) {
+        T acc[RU][NR];
+#pragma unroll
+        for (int u = 0; u < RU; u++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) acc[u][r] = T(0);
+        for (int k0 = lane * VEC; k0 < wp; k0 += 32 * VEC) {
+            T e[RU][VEC];
+#pragma unroll
+            for (int u = 0; u < RU; u++) {
+                // rows past the chunk read row i0 again (discarded below)
+                const int i = (i0 + u < nr) ? i0 + u : i0;
+                const uint4 v4 = __ldg(reinterpret_cast<const uint4 *>(P + (int64_t)i * ld + k0));
+                memcpy(e[u], &v4, 16);
+            }
+#pragma unroll
+            for (int q = 0; q < VEC; q++) {
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    const T yk = y[(k0 + q) * NR + r];
+#pragma unroll
+                    for (int u = 0; u < RU; u++) acc[u][r] += e[u][q] * yk;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < RU; u++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc[u][r] += shfl_xor_v(acc[u][r], o);
+            }
+        if (lane == 0)
+#pragma unroll
+            for (int u = 0; u < RU; u++)
+                if (i0 + u < nr)
+#pragma unroll
+                    for (int r = 0; r < NR; r++) atomic_sub(&B[(int64_t)r * ldb + rows[i0 + u]], acc[u][r]);
+    }
+}
+
+template <typename T, int NR>
+__global__ void __launch_bounds__(256) k_bwd_off_direct(Meta m, const int2 *__restrict__ chunks,
+                                                        const T *__restrict__ coef, T *__restrict__ B, int ldb,
+                                                        int rows_per_chunk, int cjp) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int2 ch = chunks[blockIdx.x];
+    const int c = ch.x, r0 = ch.y;
+    const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c], h = m.height[c];
+    const int nr = min(h, r0 + rows_per_chunk) - r0;
+    T *xr = reinterpret_cast<T *>(smem_raw);            // [rows][NR]: the solution at the chunk's rows
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int *rows = m.rowidx + m.rowbase[c] + r0;
+    for (int e = tid; e < nr * NR; e += nt) {
+        const int i = e / NR, r = e - i * NR;
+        xr[e] = B[(int64_t)r * ldb + rows[i]];
+    }
+    __syncthreads();
+    const T *P = coef + m.coefoff[c] + (int64_t)r0 * ld;
+    for (int j = tid; j < w; j += nt) {
+        T acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) acc[r] = T(0);
+#pragma unroll 8
+        for (int i = 0; i < nr; i++) {
+            T pv = P[(int64_t)i * ld + j];
+            if (cjp) pv = conj_v(pv);
+#pragma unroll
+            for (int r = 0; r < NR; r++) acc[r] += pv * xr[i * NR + r];
+        }
+#pragma unroll
+        for (int r = 0; r < NR; r++) atomic_sub(&B[(int64_t)r * ldb + fc + j], acc[r]);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Levels of narrow cblks (w <= 32, no diagonal-block inverse: the leaves of
 // the elimination tree, tens of thousands of them): one warp per cblk does
 // the diagonal solve and its off-diagonal rows in one launch, the solution
