@@ -111,18 +111,31 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
         // ---------------- TMA producer ----------------
         if (lane == 0) {
             int it = 0;
-            for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x) {
+            // operands of a tile: both maps, their row coordinates, k-blocks
+            struct Ops {
+                const CUtensorMap *ma, *mb;
+                int rowa, rowb, nk;
+            };
+            auto ops_of = [&](int ti) {
                 const int4 tl = tiles[ti];
                 const GemmTask t = tasks[tl.x];
-                const int K = m.width[t.c];
                 const bool trsm = (t.flags & 64) != 0;
                 const int mb = mapidx[t.c];
-                const CUtensorMap *ma = maps + mb + ((t.flags & 1) ? TMAP_U : TMAP_L);
-                const CUtensorMap *mbm =
-                    maps + mb + (trsm ? ((t.flags & 128) ? TMAP_I2 : TMAP_I) : ((t.flags & 2) ? TMAP_U : TMAP_L));
-                const int rowa = t.arow0 + tl.y * TC_BM;
-                const int rowb = (trsm ? 0 : m.browoff[t.b]) + tl.z * TC_BN;
-                const int nk = (K + TC_BK - 1) / TC_BK;
+                Ops o;
+                o.ma = maps + mb + ((t.flags & 1) ? TMAP_U : TMAP_L);
+                o.mb = maps + mb + (trsm ? ((t.flags & 128) ? TMAP_I2 : TMAP_I) : ((t.flags & 2) ? TMAP_U : TMAP_L));
+                o.rowa = t.arow0 + tl.y * TC_BM;
+                o.rowb = (trsm ? 0 : m.browoff[t.b]) + tl.z * TC_BN;
+                o.nk = (m.width[t.c] + TC_BK - 1) / TC_BK;
+                return o;
+            };
+            Ops nxt{};
+            if (blockIdx.x < ntiles) nxt = ops_of(blockIdx.x);
+            for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x) {
+                const Ops o = nxt;
+                if (ti + (int)gridDim.x < ntiles) nxt = ops_of(ti + gridDim.x);   // in flight during this tile
+                const CUtensorMap *ma = o.ma, *mbm = o.mb;
+                const int rowa = o.rowa, rowb = o.rowb, nk = o.nk;
                 bool ok = true;
                 for (int kb = 0; kb < nk; kb++, it++) {
                     const int s = it % S;
@@ -151,8 +164,12 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             int it = 0, tl = 0;
+            TcTileView nv{};
+            if (blockIdx.x < ntiles) nv = tc_tile_view(m, tiles[blockIdx.x], tasks, coefL, coefU, nullptr);
             for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x, tl++) {
-                const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU, nullptr);
+                const TcTileView v = nv;
+                if (ti + (int)gridDim.x < ntiles)   // the next tile's view loads while this one runs
+                    nv = tc_tile_view(m, tiles[ti + gridDim.x], tasks, coefL, coefU, nullptr);
                 const uint32_t idesc = tc_idesc(tc_mma_n(v.ncols));
                 const int ab = tl & 1;
                 const uint32_t acc = tmem + (uint32_t)(ab * 128);

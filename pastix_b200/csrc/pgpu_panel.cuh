@@ -121,24 +121,30 @@ __device__ __forceinline__ void warp_factor_tile(T *tile, int nb, typename real_
         const bool below = lane > k && lane < nb;
         if (below) a[k] = a[k] * inv;
         const T lik = a[k];
+        // (constant trip counts with j > k as a predicate: the nest unrolls
+        // completely, so a[] stays in registers)
         if (MODE == FM_GETRF) {
 #pragma unroll
-            for (int j = k + 1; j < PB; j++) {
-                const T ukj = shfl_v(a[j], k);
-                if (below) a[j] -= lik * ukj;
+            for (int j = 0; j < PB; j++) {
+                if (j > k) {
+                    const T ukj = shfl_v(a[j], k);
+                    if (below) a[j] -= lik * ukj;
+                }
             }
         } else {
             // a_ij -= l_ik op(l_jk) (Cholesky); a_ij -= l_ik d_k op(l_jk) (LDL; LDL^h takes the real part of d_k)
             const T ld = (MODE == FM_POTRF) ? lik : lik * (MODE == FM_HETRF ? T(real_v(dk)) : dk);
 #pragma unroll
-            for (int j = k + 1; j < PB; j++) {
-                const T ljk = shfl_v(a[k], j);
-                if (below && j <= lane) a[j] -= ld * cj<CJ>(ljk);
+            for (int j = 0; j < PB; j++) {
+                if (j > k) {
+                    const T ljk = shfl_v(a[k], j);
+                    if (below && j <= lane) a[j] -= ld * cj<CJ>(ljk);
+                }
             }
             if (MODE == FM_HETRF) {
 #pragma unroll
-                for (int j = k + 1; j < PB; j++)
-                    if (below && j == lane) a[j] = T(real_v(a[j]));
+                for (int j = 0; j < PB; j++)
+                    if (j > k && below && j == lane) a[j] = T(real_v(a[j]));
             }
         }
     }
