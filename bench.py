@@ -17,7 +17,8 @@ on the upwind LU otherwise stops with that error near 2e-12).
 
 Prints one JSON line (rank 0).  `value`: mixed-arm time-to-solution with the
 matrix values and b already in HBM (CUDA events on the library's stream);
-`e2e`: the same through the C ABI with host buffers (values, b in; x out).
+`e2e`: the same through the C ABI with host buffers (values, b in; x out;
+pinned host memory, allocated once before the timed steps).
 With --impl reference the reference's own CPU path (oracle/_ref, static
 scheduler, all host cores) is timed on a bounded sample (the same problem on
 a smaller grid) and scaled to the full problem by the ratio of factorization
@@ -233,14 +234,24 @@ def run_arm(A, st, b, mixed, steps, warmup, fact, refine, segments=None):
     wall = (time.perf_counter() - t0) / steps
     last = dict(st_)
     x = d_x.cpu().numpy().reshape(A.n, nrhs, order="F")
-    # e2e through the C ABI with host buffers
+    # e2e through the C ABI with host buffers: values and b in pinned host
+    # memory (allocated once, outside the timed region), x read back into a
+    # pinned buffer; every step copies them in and out
+    from pastix_b200.gpu import load, _p, _check
+    tdt = torch.complex128 if np.iscomplexobj(A.values) else torch.float64
+    h_vals = torch.empty(A.values.shape, dtype=tdt, pin_memory=True)
+    h_vals.numpy()[:] = A.values
+    h_b = torch.empty(A.n * nrhs, dtype=tdt, pin_memory=True)
+    h_b.numpy()[:] = np.asfortranarray(b).reshape(-1, order="F")
+    h_x = torch.zeros(A.n * nrhs, dtype=tdt, pin_memory=True)
     e2e = []
-    xh = None
     for _ in range(max(1, steps)):
         t = time.perf_counter()
-        s.numfact(A.values)
-        xh = s.solve_and_refine(b)
+        s.numfact(h_vals)
+        _check("pastix_gpu_solve_and_refine",
+               load().pastix_gpu_solve_and_refine(s._h, nrhs, _p(h_b), A.n, _p(h_x), A.n))
         e2e.append(time.perf_counter() - t)
+    xh = h_x.numpy().reshape(A.n, nrhs, order="F").copy()
     s.close()
     return {
         "device_s": float(np.median(per)) / 1e3, "device_s_all": [p / 1e3 for p in per], "wall_s": wall,

@@ -187,16 +187,24 @@ __device__ __forceinline__ void warp_factor_tile_smem(T *tile, int nb, typename 
         __syncwarp();
         if (lane > k && lane < nb) {
             const T lik = tile[lane * PBL + k];
-            if (MODE == FM_GETRF) {
-                for (int j = k + 1; j < nb; j++) tile[lane * PBL + j] -= lik * tile[k * PBL + j];
-            } else if (MODE == FM_POTRF) {
-                for (int j = k + 1; j <= lane; j++) tile[lane * PBL + j] -= lik * cj<CJ>(tile[j * PBL + k]);
-            } else {
-                // a_ij -= l_ik d_k op(l_jk); LDL^h takes the real part of d_k (zher)
-                const T ld = lik * (MODE == FM_HETRF ? T(real_v(dk)) : dk);
-                for (int j = k + 1; j <= lane; j++) tile[lane * PBL + j] -= ld * cj<CJ>(tile[j * PBL + k]);
-                if (MODE == FM_HETRF) tile[lane * PBL + lane] = T(real_v(tile[lane * PBL + lane]));
+            // 8 entries per batch: their loads are issued before the stores
+            // (the compiler cannot reorder shared-memory loads past stores)
+            const int jend = (MODE == FM_GETRF) ? nb - 1 : lane;
+            const T f = (MODE == FM_GETRF || MODE == FM_POTRF) ? lik : lik * (MODE == FM_HETRF ? T(real_v(dk)) : dk);
+            for (int j0 = k + 1; j0 <= jend; j0 += 8) {
+                T src[8], cur[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int j = min(j0 + u, jend);
+                    src[u] = (MODE == FM_GETRF) ? tile[k * PBL + j] : cj<CJ>(tile[j * PBL + k]);
+                    cur[u] = tile[lane * PBL + j];
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    if (j0 + u <= jend) tile[lane * PBL + j0 + u] = cur[u] - f * src[u];
             }
+            // LDL^h takes the real part of d_k (zher)
+            if (MODE == FM_HETRF) tile[lane * PBL + lane] = T(real_v(tile[lane * PBL + lane]));
         }
         __syncwarp();
     }

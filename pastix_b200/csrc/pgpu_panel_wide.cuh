@@ -32,7 +32,7 @@
 
 namespace pgpu {
 
-constexpr int WP_THREADS = 512;
+constexpr int WP_THREADS = 512, WP_WARPS = WP_THREADS / 32;
 
 // Tiles a thread owns: C tiles (rows of the block column) plus, for LU, R
 // tiles (columns of the row block); 4 x 4 entries each.
@@ -86,6 +86,20 @@ __host__ inline size_t wp_smem_bytes(int w, size_t esz, bool lu, bool ldl, int k
     return wp_tile_offset(w, esz, lu, ldl, kcb) + (size_t)(lu ? 2 : 1) * PB * (PB * esz + 16);
 }
 
+// The register tile factorization as a call of its own: the kernel's live
+// state is saved around the call, so the fully unrolled factorization gets
+// the register file to itself (inlined, it competes with the 512-thread
+// budget and runs about 1.5x slower).
+template <typename T, int MODE>
+__device__ __noinline__ void wp_factor_tile_call(T *Cb, int nb, typename real_of<T>::type crit, int *npiv, int *nneg,
+                                                 int *nbad) {
+    int a = 0, b = 0, c = 0;
+    warp_factor_tile<T, MODE>(Cb, nb, crit, a, b, c);
+    *npiv += a;
+    *nneg += b;
+    *nbad += c;
+}
+
 // Shared memory (elements of T): Ach[2][w + 16][kc + VK] chunk buffers of
 // the left columns, for LU Uch[2][w + 16][kc + VK] (the U rows above,
 // transposed), C[w][PBL], for LU R[w][PBL], for LDL d[w], then (16-byte
@@ -118,22 +132,21 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
     T *TA = reinterpret_cast<T *>(smem_raw + wp_tile_offset(w, sizeof(T), LU, LDL, kc * (int)sizeof(T)));
     T *TB = TA + PB * LDT;
     const R crit = R(*critp);
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint64_t t_start = prof ? global_ns() : 0;
     int npiv = 0, nneg = 0, nbad = 0;
 
     for (int jb = 0; jb < w; jb += PB) {
         const int nb = min(PB, w - jb), M = w - jb, MR = LU ? M - nb : 0;
         // 1. the block column (and the row block right of the tile), in flight during the update
-        for (int e = tid; e < M * nb; e += WP_THREADS) {
-            const int r = e / nb, j = e - r * nb;
-            cp_async_ca<sizeof(T)>(smem_u32(Cb + r * PBL + j), A + (int64_t)(jb + r) * ld + jb + j);
-        }
+        // (warp = row, lane = column: no index divisions)
+        if (lane < nb)
+            for (int r = warp; r < M; r += WP_WARPS)
+                cp_async_ca<sizeof(T)>(smem_u32(Cb + r * PBL + lane), A + (int64_t)(jb + r) * ld + jb + lane);
         if constexpr (LU)
-            for (int e = tid; e < MR * nb; e += WP_THREADS) {
-                const int j = e / MR, i = e - j * MR;
-                cp_async_ca<sizeof(T)>(smem_u32(Rb + i * PBL + j), A + (int64_t)(jb + j) * ld + jb + nb + i);
-            }
+            for (int j = warp; j < nb; j += WP_WARPS)
+                for (int i = lane; i < MR; i += 32)
+                    cp_async_ca<sizeof(T)>(smem_u32(Rb + i * PBL + j), A + (int64_t)(jb + j) * ld + jb + nb + i);
         cp_async_commit();
         // 2. left-looking update with the finished columns [0, jb)
         const int RG = wp_row_groups(M), RG2 = LU ? wp_row_groups(MR) : 0;
@@ -142,17 +155,16 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
         if (jb > 0) {
             auto stage = [&](int bf, int k0) {
                 T *dA = Ach + bf * bufsz;
-                const int pieces = kc / VK;
-                for (int e = tid; e < M * pieces; e += WP_THREADS) {
-                    const int r = e / pieces, pc = e - r * pieces;
+                const int lp = __ffs(kc / VK) - 1;   // 16-byte pieces per row: a power of two
+                for (int e = tid; e < (M << lp); e += WP_THREADS) {
+                    const int r = e >> lp, pc = e - (r << lp);
                     cp_async16(smem_u32(dA + r * S + pc * VK), A + (int64_t)(jb + r) * ld + k0 + pc * VK, true);
                 }
                 if (LU) {
                     T *dU = Uch + bf * bufsz;
-                    for (int e = tid; e < kc * M; e += WP_THREADS) {
-                        const int kk = e / M, i = e - kk * M;
-                        cp_async_ca<sizeof(T)>(smem_u32(dU + i * S + kk), A + (int64_t)(k0 + kk) * ld + jb + i);
-                    }
+                    for (int kk = warp; kk < kc; kk += WP_WARPS)
+                        for (int i = lane; i < M; i += 32)
+                            cp_async_ca<sizeof(T)>(smem_u32(dU + i * S + kk), A + (int64_t)(k0 + kk) * ld + jb + i);
                 }
             };
             // operand rows of each owned tile, as element offsets from Ach
@@ -240,7 +252,7 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
         }
         // 3. the tile, then the rows below it (and the columns of R)
         if (tid < 32) {
-            if constexpr (sizeof(T) == 4) warp_factor_tile<T, MODE>(Cb, nb, crit, npiv, nneg, nbad);
+            if constexpr (sizeof(T) == 4) wp_factor_tile_call<T, MODE>(Cb, nb, crit, &npiv, &nneg, &nbad);
             else warp_factor_tile_smem<T, MODE>(Cb, nb, crit, npiv, nneg, nbad);
             if (tid < nb) {
                 const T d = Cb[tid * PBL + tid];
@@ -248,11 +260,12 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
                 rdiag[tid] = T(1) / (MODE == FM_POTRF ? cj<CJ>(d) : d);
             }
             // the tile as 16-byte rows: TA = lower part (LU: U^t), TB = lower part (LU)
-            for (int e = tid; e < nb * nb; e += 32) {
-                const int j = e / nb, l = e - j * nb;
-                TA[j * LDT + l] = LU ? Cb[l * PBL + j] : Cb[j * PBL + l];
-                if (LU) TB[j * LDT + l] = Cb[j * PBL + l];
-            }
+            if (tid < nb)
+                for (int j = 0; j < nb; j++) {
+                    const int l = tid;
+                    TA[j * LDT + l] = LU ? Cb[l * PBL + j] : Cb[j * PBL + l];
+                    if (LU) TB[j * LDT + l] = Cb[j * PBL + l];
+                }
         }
         __syncthreads();
         for (int r = nb + tid; r < M; r += WP_THREADS) {
@@ -278,15 +291,12 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
             }
         __syncthreads();
         // 4. write back (the symmetric forms keep the tile's lower triangle only)
-        for (int e = tid; e < M * nb; e += WP_THREADS) {
-            const int r = e / nb, j = e - r * nb;
-            if (LU || r >= nb || j <= r) A[(int64_t)(jb + r) * ld + jb + j] = Cb[r * PBL + j];
-        }
+        if (lane < nb)
+            for (int r = warp; r < M; r += WP_WARPS)
+                if (LU || r >= nb || lane <= r) A[(int64_t)(jb + r) * ld + jb + lane] = Cb[r * PBL + lane];
         if constexpr (LU)
-            for (int e = tid; e < MR * nb; e += WP_THREADS) {
-                const int j = e / MR, i = e - j * MR;
-                A[(int64_t)(jb + j) * ld + jb + nb + i] = Rb[i * PBL + j];
-            }
+            for (int j = warp; j < nb; j += WP_WARPS)
+                for (int i = lane; i < MR; i += 32) A[(int64_t)(jb + j) * ld + jb + nb + i] = Rb[i * PBL + j];
         __syncthreads();
     }
     if (tid == 0) {
