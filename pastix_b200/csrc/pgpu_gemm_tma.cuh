@@ -62,15 +62,6 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
-// L2 prefetch of a box (no shared memory, no completion): issued S k-blocks
-// ahead of the loads, so that they find their data in L2.
-__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap *map, int c0, int c1, int c2) {
-    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
-                     reinterpret_cast<uint64_t>(map)),
-                 "r"(c0), "r"(c1), "r"(c2)
-                 : "memory");
-}
-
 template <bool SPLIT>
 __global__ void __launch_bounds__(TMA_THREADS, 1)
     k_gemm_scatter_tc_tma(Meta m, const int4 *__restrict__ tiles, int ntiles, const GemmTask *__restrict__ tasks,
@@ -139,30 +130,15 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                 return o;
             };
             Ops nxt{};
-            if (blockIdx.x < ntiles) {
-                nxt = ops_of(blockIdx.x);
-                for (int kb = 0; kb < S && kb < nxt.nk; kb++) {
-                    tma_prefetch_3d(nxt.ma, kb * TC_BK, nxt.rowa, 0);
-                    tma_prefetch_3d(nxt.mb, kb * TC_BK, nxt.rowb, 0);
-                }
-            }
+            if (blockIdx.x < ntiles) nxt = ops_of(blockIdx.x);
             for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x) {
                 const Ops o = nxt;
-                const bool more = ti + (int)gridDim.x < ntiles;
-                if (more) nxt = ops_of(ti + gridDim.x);   // in flight during this tile
+                if (ti + (int)gridDim.x < ntiles) nxt = ops_of(ti + gridDim.x);   // in flight during this tile
                 const CUtensorMap *ma = o.ma, *mbm = o.mb;
                 const int rowa = o.rowa, rowb = o.rowb, nk = o.nk;
                 bool ok = true;
                 for (int kb = 0; kb < nk; kb++, it++) {
                     const int s = it % S;
-                    // L2 prefetch S k-blocks ahead (into the next tile near the end of this one)
-                    if (kb + S < nk) {
-                        tma_prefetch_3d(ma, (kb + S) * TC_BK, rowa, 0);
-                        tma_prefetch_3d(mbm, (kb + S) * TC_BK, rowb, 0);
-                    } else if (more && kb + S - nk < nxt.nk) {
-                        tma_prefetch_3d(nxt.ma, (kb + S - nk) * TC_BK, nxt.rowa, 0);
-                        tma_prefetch_3d(nxt.mb, (kb + S - nk) * TC_BK, nxt.rowb, 0);
-                    }
                     if (it >= S && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((it / S - 1) & 1))) {
                         ok = false;
                         break;
