@@ -2013,12 +2013,9 @@ static int refine_cg_block(pastix_gpu_t &C, BlockOps<S> &V, const S *b, S *x, do
         }
         V.axpy(step, p, x);
         V.axpy(mstep, ap, r);
-        V.copy(r, z);
-        int rc = V.spsv(z);
-        if (rc) return rc;
-        V.dot(r, z, alpha2);
-        for (int c = 0; c < k; c++) beta[c] = active[c] ? alpha2[c] / beta[c] : HS(0.0);
-        V.xpby(z, beta, p);
+        // the stopping test only reads r: it runs before the preconditioner
+        // solve, which is skipped once every column has stopped (the
+        // reference solves once more and discards z; x and r are the same)
         V.norm(r, normr);
         V.measure(r, normr, normb, segb, res);
         any = false;
@@ -2028,6 +2025,13 @@ static int refine_cg_block(pastix_gpu_t &C, BlockOps<S> &V, const S *b, S *x, do
             active[c] = res[c] > eps && iters[c] < itermax;
             any |= active[c];
         }
+        if (!any) break;
+        V.copy(r, z);
+        int rc = V.spsv(z);
+        if (rc) return rc;
+        V.dot(r, z, alpha2);
+        for (int c = 0; c < k; c++) beta[c] = active[c] ? alpha2[c] / beta[c] : HS(0.0);
+        V.xpby(z, beta, p);
     }
     resid = res;
     return PASTIX_GPU_SUCCESS;
