@@ -19,6 +19,7 @@
 #include <cstring>
 #include <mutex>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 using namespace pgpu;
@@ -798,6 +799,44 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
             PGPU_CHECK(C.d_tmaps.upload(maps, C.stream));
             PGPU_CHECK(C.d_mapidx.upload(mapidx, C.stream));
             PGPU_CHECK(C.d_split.upload(split, C.stream));
+            // pairs of 128-row tiles (tm even, tm + 1) of one task and column block
+            // share their B tile in the TMA kernel: one entry {task, tm, tn, 1}
+            auto pair_range = [](const std::vector<int4> &in, int b, int e, std::vector<int4> &out) {
+                auto key = [](int t, int tm, int tn) { return ((int64_t)t << 32) | ((int64_t)tm << 16) | tn; };
+                std::unordered_map<int64_t, int> pos;
+                for (int i = b; i < e; i++) pos[key(in[i].x, in[i].y, in[i].z)] = i;
+                std::vector<char> used(std::max(0, e - b), 0);
+                for (int i = b; i < e; i++) {
+                    if (used[i - b]) continue;
+                    const int4 t = in[i];
+                    used[i - b] = 1;
+                    if ((t.y & 1) == 0) {
+                        auto it = pos.find(key(t.x, t.y + 1, t.z));
+                        if (it != pos.end() && !used[it->second - b]) {
+                            used[it->second - b] = 1;
+                            out.push_back(make_int4(t.x, t.y, t.z, 1));
+                            continue;
+                        }
+                    }
+                    out.push_back(make_int4(t.x, t.y, t.z, 0));
+                }
+            };
+            std::vector<int4> ptc, ptt;
+            std::vector<int> tc_ptr(C.nlevels + 1, 0), tt_ptr(C.nlevels + 1, 0), tc_crit(C.nlevels, 0);
+            for (int l = 0; l < C.nlevels; l++) {
+                const int b0 = C.tctile_ptr[l], bc = b0 + C.tctile_crit[l], b1 = C.tctile_ptr[l + 1];
+                pair_range(tctiles, b0, bc, ptc);
+                tc_crit[l] = (int)ptc.size() - tc_ptr[l];
+                pair_range(tctiles, bc, b1, ptc);
+                tc_ptr[l + 1] = (int)ptc.size();
+                pair_range(tttiles, C.tttile_ptr[l], C.tttile_ptr[l + 1], ptt);
+                tt_ptr[l + 1] = (int)ptt.size();
+            }
+            tctiles.swap(ptc);
+            tttiles.swap(ptt);
+            C.tctile_ptr.swap(tc_ptr);
+            C.tctile_crit.swap(tc_crit);
+            C.tttile_ptr.swap(tt_ptr);
         } else {
             C.split_ptr.assign(C.nlevels + 1, 0);
         }

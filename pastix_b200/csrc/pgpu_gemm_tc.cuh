@@ -426,7 +426,7 @@ __device__ __forceinline__ void mbar_arrive(uint32_t addr) {
 
 struct TcTileView {
     const float *A, *B;
-    int mrows, ncols, K, nk, flags, c, b, f, arow, j0, i0;
+    int mrows, ncols, K, nk, flags, c, b, f, arow, j0, i0, M, pair;
     int64_t out;
 };
 
@@ -453,6 +453,8 @@ __device__ __forceinline__ TcTileView tc_tile_view(const Meta &m, const int4 tl,
     v.mrows = min(TC_BM, t.M - i0);
     v.ncols = min(TC_BN, N - v.j0);
     v.nk = (v.K + TC_BK - 1) / TC_BK;
+    v.M = t.M;
+    v.pair = tl.w & 1;   // (TMA kernel) rows i0 .. i0 + 255: this tile and the next one of the task
     return v;
 }
 

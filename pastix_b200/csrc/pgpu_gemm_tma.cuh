@@ -40,9 +40,12 @@ constexpr int TMA_PROD_WARP = 4, TMA_MMA_WARP = 5;
 // operand maps per cblk: L panel, U panel (LU), first / second diagonal-block inverse
 enum { TMAP_L = 0, TMAP_U = 1, TMAP_I = 2, TMAP_I2 = 3, TMAP_KINDS = 4 };
 
+// A stage holds two A tiles (a pair of 128-row tiles of one task sharing the
+// B tile) and the B tile; hi and lo planes each for 3xTF32.
 template <bool SPLIT> struct TmaCfg;
-template <> struct TmaCfg<false> { static constexpr int STAGES = 6, TILES = 2; };
-template <> struct TmaCfg<true> { static constexpr int STAGES = 3, TILES = 4; };
+template <> struct TmaCfg<false> { static constexpr int STAGES = 4, TILES = 3, PL = 1; };
+template <> struct TmaCfg<true> { static constexpr int STAGES = 2, TILES = 6, PL = 2; };
+constexpr int TMA_TMEM_COLS = 512;   // two accumulator buffers x (two 128-column halves)
 template <bool SPLIT>
 constexpr int tma_smem_bytes() {
     return TmaCfg<SPLIT>::STAGES * TmaCfg<SPLIT>::TILES * TC_TILE_BYTES + TCP_EPI_BYTES + 1024;
@@ -67,13 +70,14 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
     k_gemm_scatter_tc_tma(Meta m, const int4 *__restrict__ tiles, int ntiles, const GemmTask *__restrict__ tasks,
                           float *__restrict__ coefL, float *__restrict__ coefU, Status *st, float *__restrict__ scr,
                           const CUtensorMap *__restrict__ maps, const int *__restrict__ mapidx) {
-    constexpr int S = TmaCfg<SPLIT>::STAGES, NT = TmaCfg<SPLIT>::TILES;
-    constexpr uint32_t STAGE_BYTES = (uint32_t)NT * TC_TILE_BYTES;
+    constexpr int S = TmaCfg<SPLIT>::STAGES, NT = TmaCfg<SPLIT>::TILES, PL = TmaCfg<SPLIT>::PL;
+    constexpr uint32_t BOX_BYTES = (uint32_t)PL * TC_TILE_BYTES;   // one operand box (hi [+ lo])
+    constexpr int QA1 = PL, QB = 2 * PL;                            // tile slots of A1 and B in a stage
     extern __shared__ __align__(16) unsigned char tc_smem_raw[];
     __shared__ __align__(8) uint64_t full[S], empty[S], accf[2], acce[2], drained;
     __shared__ uint32_t tmem_base_s;
     __shared__ int fail_s;
-    __shared__ int trow_s[TC_BM];
+    __shared__ int trow_s[2][TC_BM];
 
     const uint32_t raw = smem_u32(tc_smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -83,7 +87,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == TMA_MMA_WARP) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
-                     "r"(TCP_TMEM_COLS)
+                     "r"(TMA_TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -114,7 +118,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
             // operands of a tile: both maps, their row coordinates, k-blocks
             struct Ops {
                 const CUtensorMap *ma, *mb;
-                int rowa, rowb, nk;
+                int rowa, rowb, nk, pair;
             };
             auto ops_of = [&](int ti) {
                 const int4 tl = tiles[ti];
@@ -127,6 +131,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                 o.rowa = t.arow0 + tl.y * TC_BM;
                 o.rowb = (trsm ? 0 : m.browoff[t.b]) + tl.z * TC_BN;
                 o.nk = (m.width[t.c] + TC_BK - 1) / TC_BK;
+                o.pair = tl.w & 1;
                 return o;
             };
             Ops nxt{};
@@ -136,6 +141,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                 if (ti + (int)gridDim.x < ntiles) nxt = ops_of(ti + gridDim.x);   // in flight during this tile
                 const CUtensorMap *ma = o.ma, *mbm = o.mb;
                 const int rowa = o.rowa, rowb = o.rowb, nk = o.nk;
+                const uint32_t bytes = (o.pair ? 3u : 2u) * BOX_BYTES;
                 bool ok = true;
                 for (int kb = 0; kb < nk; kb++, it++) {
                     const int s = it % S;
@@ -143,9 +149,10 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                         ok = false;
                         break;
                     }
-                    mbar_arrive_expect_tx(smem_u32(&full[s]), STAGE_BYTES);
+                    mbar_arrive_expect_tx(smem_u32(&full[s]), bytes);
                     tma_load_3d(tile_addr(s, 0), ma, kb * TC_BK, rowa, 0, smem_u32(&full[s]));
-                    tma_load_3d(tile_addr(s, NT / 2), mbm, kb * TC_BK, rowb, 0, smem_u32(&full[s]));
+                    if (o.pair) tma_load_3d(tile_addr(s, QA1), ma, kb * TC_BK, rowa + TC_BM, 0, smem_u32(&full[s]));
+                    tma_load_3d(tile_addr(s, QB), mbm, kb * TC_BK, rowb, 0, smem_u32(&full[s]));
                 }
                 if (!ok) {
                     atomicExch(&fail_s, 1);
@@ -172,7 +179,8 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                     nv = tc_tile_view(m, tiles[ti + gridDim.x], tasks, coefL, coefU, nullptr);
                 const uint32_t idesc = tc_idesc(tc_mma_n(v.ncols));
                 const int ab = tl & 1;
-                const uint32_t acc = tmem + (uint32_t)(ab * 128);
+                const uint32_t acc = tmem + (uint32_t)(ab * 256), acc1 = acc + 128u;
+                const bool pair = v.pair != 0;
                 if (tl >= 2 && !mbar_wait(smem_u32(&acce[ab]), (uint32_t)((tl / 2 - 1) & 1))) {
                     atomicExch(&fail_s, 1);
                     break;
@@ -190,16 +198,22 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                     for (int kk = 0; kk < TC_BK / 8; kk++) {
                         const uint32_t first = (kb > 0 || kk > 0) ? 1u : 0u;
                         if (SPLIT) {
-                            const uint64_t ah = tc_sdesc(tile_addr(s, 0) + kk * 32),
-                                           al = tc_sdesc(tile_addr(s, 1) + kk * 32);
-                            const uint64_t bh = tc_sdesc(tile_addr(s, 2) + kk * 32),
-                                           bl = tc_sdesc(tile_addr(s, 3) + kk * 32);
-                            tc_mma(acc, al, bh, idesc, first);
-                            tc_mma(acc, ah, bl, idesc, 1u);
-                            tc_mma(acc, ah, bh, idesc, 1u);
+                            const uint64_t bh = tc_sdesc(tile_addr(s, QB) + kk * 32),
+                                           bl = tc_sdesc(tile_addr(s, QB + 1) + kk * 32);
+#pragma unroll
+                            for (int h = 0; h < 2; h++) {
+                                if (h == 1 && !pair) break;
+                                const uint64_t ah = tc_sdesc(tile_addr(s, h * QA1) + kk * 32),
+                                               al = tc_sdesc(tile_addr(s, h * QA1 + 1) + kk * 32);
+                                const uint32_t ac = h ? acc1 : acc;
+                                tc_mma(ac, al, bh, idesc, first);
+                                tc_mma(ac, ah, bl, idesc, 1u);
+                                tc_mma(ac, ah, bh, idesc, 1u);
+                            }
                         } else {
-                            tc_mma(acc, tc_sdesc(tile_addr(s, 0) + kk * 32), tc_sdesc(tile_addr(s, 1) + kk * 32),
-                                   idesc, first);
+                            const uint64_t bd = tc_sdesc(tile_addr(s, QB) + kk * 32);
+                            tc_mma(acc, tc_sdesc(tile_addr(s, 0) + kk * 32), bd, idesc, first);
+                            if (pair) tc_mma(acc1, tc_sdesc(tile_addr(s, QA1) + kk * 32), bd, idesc, first);
                         }
                     }
                     tc_commit(smem_u32(&empty[s]));
@@ -222,22 +236,30 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
             const int ab = tl & 1;
             const int myrow = warp * 32 + lane;
             const bool trsm = (v.flags & 64) != 0;
-            int tr = -1;
-            if (myrow < v.mrows && !trsm) tr = panel_row_of(m, v.f, m.rowidx[m.rowbase[v.c] + v.arow + myrow]);
+            const int nh = v.pair ? 2 : 1;
+            int tr[2] = {-1, -1};
+            for (int h = 0; h < nh; h++) {
+                const int row = h * TC_BM + myrow;     // row of the pair, from the first tile's first row
+                if (row < v.M - v.i0 && !trsm)
+                    tr[h] = panel_row_of(m, v.f, m.rowidx[m.rowbase[v.c] + v.arow + row]);
+            }
             if (!mbar_wait(smem_u32(&accf[ab]), (uint32_t)((tl / 2) & 1))) {
                 atomicExch(&fail_s, 1);
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            trow_s[myrow] = tr;
+            trow_s[0][myrow] = tr[0];
+            trow_s[1][myrow] = tr[1];
             __syncwarp();
             float *C = ((v.flags & 4) ? coefU : coefL) + m.coefoff[v.f];
             const int ldf = m.ld[v.f], wf = m.width[v.f];
             const int tcol0 = m.bfrow[v.b] + v.j0 - m.fcol[v.f];
             const bool lower_only = (v.flags & 8) != 0;
+            for (int h = 0; h < nh; h++)
             for (int cb = 0; cb < TC_BN; cb += 32) {
+                const int mrows = min(TC_BM, v.M - v.i0 - h * TC_BM);   // valid rows of this half
                 uint32_t r[32];
-                tc_ld32(tmem + (uint32_t)(ab * 128) + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, r);
+                tc_ld32(tmem + (uint32_t)(ab * 256 + h * 128) + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, r);
                 __syncwarp();
 #pragma unroll
                 for (int q = 0; q < 32; q++) E[lane * 33 + q] = __uint_as_float(r[q]);
@@ -245,10 +267,10 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                 const int j = cb + lane;
                 if (j < v.ncols && trsm) {
                     const int ldc = m.ld[v.c];
-                    float *O = scr + v.out + (int64_t)v.i0 * ldc + v.j0;
+                    float *O = scr + v.out + (int64_t)(v.i0 + h * TC_BM) * ldc + v.j0;
                     for (int rr = 0; rr < 32; rr++) {
                         const int i = warp * 32 + rr;
-                        if (i >= v.mrows) break;
+                        if (i >= mrows) break;
                         O[(int64_t)i * ldc + j] = E[rr * 33 + lane];
                     }
                 } else if (!trsm && cb < v.ncols) {
@@ -256,7 +278,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                     const int tcs = tcol0 + cb, a0 = tcs & ~3, o = tcs - a0;
                     for (int k = lane; k < 32 * 9; k += 32) {
                         const int rr = k / 9, g = k - rr * 9;
-                        const int t2 = trow_s[warp * 32 + rr];
+                        const int t2 = trow_s[h][warp * 32 + rr];
                         if (t2 < 0) continue;
                         float a[4];
                         bool any = false;
@@ -282,7 +304,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
     __syncthreads();
     if (warp == TMA_MMA_WARP) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCP_TMEM_COLS)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMA_TMEM_COLS)
                      : "memory");
     }
 }
