@@ -1427,6 +1427,8 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
                 k_fwd_off_direct<T, 2><<<nch, 256, ysm, s>>>(C.meta, chp, coefL, W, ldb, SOLVE_ROWS_PER_CHUNK);
             else if (nrhs == 4)
                 k_fwd_off_direct<T, 4><<<nch, 256, ysm, s>>>(C.meta, chp, coefL, W, ldb, SOLVE_ROWS_PER_CHUNK);
+            else if (nrhs == 8 && sizeof(T) <= 8)
+                k_fwd_off_direct<T, 8><<<nch, 256, ysm, s>>>(C.meta, chp, coefL, W, ldb, SOLVE_ROWS_PER_CHUNK);
             else
                 k_fwd_off<T><<<nch, 256, off_smem(mw, true), s>>>(C.meta, chp, coefL, W, ldb, nrhs,
                                                                   SOLVE_ROWS_PER_CHUNK);
@@ -1458,6 +1460,8 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
                 k_bwd_off_direct<T, 2><<<nch, 256, xsm, s>>>(C.meta, chp, coefU, W, ldb, SOLVE_ROWS_PER_CHUNK, bcj);
             else if (nrhs == 4)
                 k_bwd_off_direct<T, 4><<<nch, 256, xsm, s>>>(C.meta, chp, coefU, W, ldb, SOLVE_ROWS_PER_CHUNK, bcj);
+            else if (nrhs == 8)
+                k_bwd_off_direct<T, 8><<<nch, 256, xsm, s>>>(C.meta, chp, coefU, W, ldb, SOLVE_ROWS_PER_CHUNK, bcj);
             else
                 k_bwd_off<T><<<nch, 256, off_smem(mw, false), s>>>(C.meta, chp, coefU, W, ldb, nrhs,
                                                                    SOLVE_ROWS_PER_CHUNK, bcj);

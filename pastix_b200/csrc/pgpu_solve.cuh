@@ -95,7 +95,7 @@ __device__ void diag_solve_inverse(const T *__restrict__ Bi, const T *__restrict
     }
 }
 
-// Forward product with the inverse for up to 4 right-hand sides: one warp
+// Forward product with the inverse for 1, 2, 4 or 8 right-hand sides: one warp
 // per row n of Bi, lanes across k in 16-byte vectors read straight from
 // global memory (no staging), the warp's partial sums reduced by shuffles:
 // B[fc + n] = sum_{k <= n} op(Bi[n][k]) v[k] (times d_n for LDL).
@@ -220,6 +220,7 @@ __global__ void __launch_bounds__(1024) k_fwd_diag(Meta m, const int *__restrict
         case 1: diag_solve_inverse_fwd_warp<T, 1>(Bi, D, w, ld, ldl != 0, cjp != 0, y, B, ldb, fc); return;
         case 2: diag_solve_inverse_fwd_warp<T, 2>(Bi, D, w, ld, ldl != 0, cjp != 0, y, B, ldb, fc); return;
         case 4: diag_solve_inverse_fwd_warp<T, 4>(Bi, D, w, ld, ldl != 0, cjp != 0, y, B, ldb, fc); return;
+        case 8: diag_solve_inverse_fwd_warp<T, 8>(Bi, D, w, ld, ldl != 0, cjp != 0, y, B, ldb, fc); return;
         default: break;
         }
         diag_solve_inverse<T>(Bi, D, w, ld, nrhs, false, ldl != 0, cjp != 0, y, nullptr,
@@ -357,7 +358,7 @@ __global__ void __launch_bounds__(256) k_bwd_off(Meta m, const int2 *__restrict_
 }
 
 // ---------------------------------------------------------------------------
-// Off-diagonal kernels for up to 4 right-hand sides, the panel rows read
+// Off-diagonal kernels for 1, 2, 4 or 8 right-hand sides, the panel rows read
 // straight from global memory in 16-byte vectors (no shared staging), so a
 // chunk costs about one memory latency:
 //   k_fwd_off_direct: one warp per RU rows at a time (all RU rows' loads in
