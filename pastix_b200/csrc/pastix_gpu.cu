@@ -1084,8 +1084,23 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             const int wmw = C.lvl_wmaxw[l];
             const int kcb = wide_kcb(wmw, sizeof(T), lu, fm_ldl(fmode));
             if (!kwide || kcb == 0) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
-            kwide<<<npw, WP_THREADS, wp_smem_bytes(wmw, sizeof(T), lu, fm_ldl(fmode), kcb), s>>>(
-                C.meta, C.d_wjobs.p + C.pw_ptr[l], coefL, critp, kcb / (int)sizeof(T), C.d_status.p, prof[0]);
+            bool done = false;
+            if constexpr (std::is_same<T, float>::value) {
+                // single-precision LL^t / LDL^t: the lookahead form when its two block columns fit
+                static const bool la_off = getenv("PASTIX_GPU_WIDE_LA") && std::strcmp(getenv("PASTIX_GPU_WIDE_LA"), "0") == 0;
+                const size_t lsm = wpla_smem_bytes(wmw, fm_ldl(fmode));
+                if (!la_off && (fmode == FM_POTRF || fmode == FM_SYTRF) && lsm <= (size_t)WP_SMEM_LIMIT &&
+                    wp_row_groups(wmw) * 8 <= 2 * (WP_THREADS - 32)) {
+                    auto kla = fmode == FM_POTRF ? k_panel_wide_la<FM_POTRF> : k_panel_wide_la<FM_SYTRF>;
+                    PGPU_CHECK(cudaFuncSetAttribute(kla, cudaFuncAttributeMaxDynamicSharedMemorySize, WP_SMEM_LIMIT));
+                    kla<<<npw, WP_THREADS, lsm, s>>>(C.meta, C.d_wjobs.p + C.pw_ptr[l], coefL, critp, C.d_status.p,
+                                                     prof[0]);
+                    done = true;
+                }
+            }
+            if (!done)
+                kwide<<<npw, WP_THREADS, wp_smem_bytes(wmw, sizeof(T), lu, fm_ldl(fmode), kcb), s>>>(
+                    C.meta, C.d_wjobs.p + C.pw_ptr[l], coefL, critp, kcb / (int)sizeof(T), C.d_status.p, prof[0]);
             nl++;
         }
         if (npn) {

@@ -310,6 +310,213 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide(Meta m, const int2 *_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Lookahead form for single-precision LL^t / LDL^t (the 100^3 root chain's
+// case): while warp 0 factorizes the tile of block column jb, warps 1-15
+// already update block column jb + 32 with the finished columns [0, jb)
+// (chunks from global memory, a named barrier among those 480 threads);
+// after the row solves of block jb the last contribution, columns
+// [jb, jb + 32), comes from the just-solved block column, staged once in
+// the chunk layout (the "tail").  The same products as k_panel_wide, the
+// sums for an entry taken in the same chunk order.
+// Shared memory (floats): Ach[2][w + 16][36], C[2][w][PBL] (this block
+// column and the next), d[w] (LDL), TA[PB][36].
+// ---------------------------------------------------------------------------
+__host__ __device__ inline size_t wpla_tile_offset(int w, bool ldl) {
+    const size_t b = (2 * (size_t)(w + 16) * 36 + 2 * (size_t)w * PBL + (ldl ? (size_t)w : 0)) * sizeof(float);
+    return (b + 15) / 16 * 16;
+}
+__host__ inline size_t wpla_smem_bytes(int w, bool ldl) { return wpla_tile_offset(w, ldl) + (size_t)PB * 36 * 4; }
+
+__device__ __forceinline__ void wpla_bar_rest() { asm volatile("bar.sync 1, %0;" ::"n"(WP_THREADS - 32) : "memory"); }
+
+template <int MODE>
+__global__ void __launch_bounds__(WP_THREADS) k_panel_wide_la(Meta m, const int2 *__restrict__ jobs,
+                                                              float *__restrict__ coefL, const double *critp,
+                                                              Status *st, int64_t *prof) {
+    typedef float T;
+    constexpr bool LDL = fm_ldl(MODE);
+    constexpr int VK = 4, KC = 32, S = KC + VK, NTT = 2, GT = WP_THREADS - 32, LDT = PB + VK;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ T rdiag[PB];
+    const int2 job = jobs[blockIdx.x];
+    const int c = job.x;
+    const int w = m.width[c], ld = m.ld[c];
+    T *A = coefL + m.coefoff[c];
+    const int bufsz = (w + 16) * S;
+    T *Ach = reinterpret_cast<T *>(smem_raw);
+    T *Cbuf = Ach + 2 * bufsz;                         // C[2][w][PBL]
+    T *dsm = Cbuf + 2 * w * PBL;
+    T *TA = reinterpret_cast<T *>(smem_raw + wpla_tile_offset(w, LDL));
+    const T crit = T(*critp);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint64_t t_start = prof ? global_ns() : 0;
+    int npiv = 0, nneg = 0, nbad = 0;
+
+    // acc[t] += left rows (lo[t] + p ls) x right rows (ro[t] + 8 q S) over one chunk
+    auto chunk_fma = [&](const T *base, const int (&lo)[NTT], int ls, const int (&ro)[NTT], int tbase, int nthr,
+                         int ntiles, int k0, T (&acc)[NTT][4][4]) {
+#pragma unroll
+        for (int t = 0; t < NTT; t++) {
+            if (tbase + t * nthr >= ntiles) break;     // whole warps
+#pragma unroll 2
+            for (int kk = 0; kk < KC; kk += VK) {
+                T a[4][VK], b[4][VK];
+#pragma unroll
+                for (int p = 0; p < 4; p++) wp_lds16<T>(base + lo[t] + p * ls + kk, a[p]);
+#pragma unroll
+                for (int q = 0; q < 4; q++) wp_lds16<T>(base + ro[t] + q * 8 * S + kk, b[q]);
+#pragma unroll
+                for (int v = 0; v < VK; v++) {
+                    T dk = T(1);
+                    if (LDL) dk = dsm[k0 + kk + v];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const T bq = LDL ? b[q][v] * dk : b[q][v];
+#pragma unroll
+                        for (int p = 0; p < 4; p++) acc[t][p][q] += a[p][v] * bq;
+                    }
+                }
+            }
+        }
+    };
+    // tiles of thread tbase over mrows x 32: operand rows and zeroed accumulators
+    auto tiles_setup = [&](int tbase, int nthr, int rg, int (&lo)[NTT], int (&ro)[NTT], T (&acc)[NTT][4][4]) {
+#pragma unroll
+        for (int t = 0; t < NTT; t++) {
+            const int u = tbase + t * nthr;
+            lo[t] = (u >> 3) * S;
+            ro[t] = (u & 7) * S;
+#pragma unroll
+            for (int p = 0; p < 4; p++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[t][p][q] = T(0);
+        }
+    };
+    auto tiles_subtract = [&](T *D, int tbase, int nthr, int rg, int ntiles, int rows, int nbc, T (&acc)[NTT][4][4]) {
+#pragma unroll
+        for (int t = 0; t < NTT; t++) {
+            const int u = tbase + t * nthr;
+            if (u >= ntiles) break;
+            const int ti = u >> 3, tj = u & 7;
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                const int r = ti + p * rg;
+                if (r >= rows) continue;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int j = tj + 8 * q;
+                    if (j < nbc) D[r * PBL + j] -= acc[t][p][q];
+                }
+            }
+        }
+    };
+
+    // block column 0
+    {
+        const int nb0 = min(PB, w);
+        if (lane < nb0)
+            for (int r = warp; r < w; r += WP_WARPS)
+                cp_async_ca<4>(smem_u32(Cbuf + r * PBL + lane), A + (int64_t)r * ld + lane);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+    }
+    int cur = 0;
+    for (int jb = 0; jb < w; jb += PB) {
+        const int nb = min(PB, w - jb), M = w - jb;
+        T *Cc = Cbuf + cur * w * PBL, *Cn = Cbuf + (cur ^ 1) * w * PBL;
+        const int jn = jb + PB, Mn = w - jn, nbn = min(PB, w - jn);
+        const bool has_next = jn < w;
+        const int RGn = has_next ? wp_row_groups(Mn) : 0, ntn = RGn * 8;
+        if (warp == 0) {
+            // 1a. the tile of block jb
+            wp_factor_tile_call<T, MODE>(Cc, nb, crit, &npiv, &nneg, &nbad);
+            if (lane < nb) {
+                const T d = Cc[lane * PBL + lane];
+                if (LDL) dsm[jb + lane] = d;
+                rdiag[lane] = T(1) / d;
+                for (int j = 0; j < nb; j++) TA[j * LDT + lane] = Cc[j * PBL + lane];
+            }
+        } else if (has_next) {
+            // 1b. (warps 1-15) block column jn: load, and its update with the columns [0, jb)
+            const int gt = tid - 32, gw = warp - 1;
+            if (lane < nbn)
+                for (int r = gw; r < Mn; r += WP_WARPS - 1)
+                    cp_async_ca<4>(smem_u32(Cn + r * PBL + lane), A + (int64_t)(jn + r) * ld + jn + lane);
+            cp_async_commit();
+            if (jb > 0) {
+                int lo[NTT], ro[NTT];
+                T acc[NTT][4][4];
+                tiles_setup(gt, GT, RGn, lo, ro, acc);
+                auto stage = [&](int bf, int k0) {
+                    T *dA = Ach + bf * bufsz;
+                    for (int e = gt; e < (Mn << 3); e += GT) {
+                        const int r = e >> 3, pc = e & 7;
+                        cp_async16(smem_u32(dA + r * S + pc * VK), A + (int64_t)(jn + r) * ld + k0 + pc * VK, true);
+                    }
+                };
+                const int nck = jb / KC;
+                stage(0, 0);
+                cp_async_commit();
+                for (int ck = 0; ck < nck; ck++) {
+                    if (ck + 1 < nck) stage((ck + 1) & 1, (ck + 1) * KC);
+                    cp_async_commit();
+                    cp_async_wait<1>();
+                    wpla_bar_rest();
+                    chunk_fma(Ach + (ck & 1) * bufsz, lo, RGn * S, ro, gt, GT, ntn, ck * KC, acc);
+                    wpla_bar_rest();
+                }
+                cp_async_wait<0>();
+                wpla_bar_rest();
+                tiles_subtract(Cn, gt, GT, RGn, ntn, Mn, nbn, acc);
+            } else {
+                cp_async_wait<0>();
+            }
+        }
+        __syncthreads();
+        // 2. the rows below the tile
+        for (int r = nb + tid; r < M; r += WP_THREADS) {
+            T x[PB];
+#pragma unroll
+            for (int j = 0; j < PB; j++) x[j] = (j < nb) ? Cc[r * PBL + j] : T(0);
+            if (LDL) wp_solve_rows<T, false, true>(x, TA, LDT, rdiag, nb);
+            else wp_solve_rows<T, false, false>(x, TA, LDT, rdiag, nb);
+#pragma unroll
+            for (int j = 0; j < PB; j++)
+                if (j < nb) Cc[r * PBL + j] = LDL ? x[j] * rdiag[j] : x[j];
+        }
+        __syncthreads();
+        // 3. write back; the solved rows below the tile, staged as the tail chunk of block jn
+        if (lane < nb)
+            for (int r = warp; r < M; r += WP_WARPS) {
+                const T v = Cc[r * PBL + lane];
+                if (r >= nb || lane <= r) A[(int64_t)(jb + r) * ld + jb + lane] = v;
+                if (has_next && r >= PB) Ach[(r - PB) * S + lane] = v;
+            }
+        __syncthreads();
+        // 4. the tail: block jn -= (rows jn.. of block jb) op(rows jn..jn+32 of block jb D)^t
+        if (has_next) {
+            int lo[NTT], ro[NTT];
+            T acc[NTT][4][4];
+            tiles_setup(tid, WP_THREADS, RGn, lo, ro, acc);
+            chunk_fma(Ach, lo, RGn * S, ro, tid, WP_THREADS, ntn, jb, acc);
+            tiles_subtract(Cn, tid, WP_THREADS, RGn, ntn, Mn, nbn, acc);
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    if (tid == 0) {
+        if (npiv) atomicAdd(&st->nbpivots, npiv);
+        if (nneg) atomicAdd(&st->negpivots, nneg);
+        if (nbad) atomicAdd(&st->nonfinite, nbad);
+        if (prof) {
+            prof[2 * job.y] = (int64_t)t_start;
+            prof[2 * job.y + 1] = (int64_t)global_ns();
+        }
+    }
+}
+
 // Whether one CTA covers width w with its tile budget.
 __host__ inline bool wp_tiles_fit(int w, bool lu) {
     const int rg = wp_row_groups(w), rg2 = lu ? wp_row_groups(w > PB ? w - PB : 0) : 0;
