@@ -228,6 +228,8 @@ PASTIX_GPU_API int pastix_gpu_set_cblk_priority( pastix_gpu_t *ctx, const double
  *                             left-looking kernel (128; 0 disables it)
  *   PGPU_TUNE_TC_TMA          1 (default): 3xTF32 operands pre-split once per panel and
  *                             loaded by TMA; 0: split by producer warps per tile
+ *   PGPU_TUNE_TC_PAIR_MIN     TMA kernel: fewest tiles in a launch for pairing 128-row
+ *                             tiles that share their B tile (-1, default: 2 per SM)
  * Setting one invalidates the factorization plan (rebuilt by the next numfact).
  */
 #define PGPU_TUNE_MIXED_GEMM      0
@@ -239,7 +241,8 @@ PASTIX_GPU_API int pastix_gpu_set_cblk_priority( pastix_gpu_t *ctx, const double
 #define PGPU_TUNE_TC_MIN_MN       6
 #define PGPU_TUNE_WIDE_PANEL      7
 #define PGPU_TUNE_TC_TMA          8
-#define PGPU_TUNE_COUNT           9
+#define PGPU_TUNE_TC_PAIR_MIN     9
+#define PGPU_TUNE_COUNT           10
 PASTIX_GPU_API int pastix_gpu_set_tuning( pastix_gpu_t *ctx, int key, int64_t value );
 PASTIX_GPU_API int pastix_gpu_get_tuning( pastix_gpu_t *ctx, int key, int64_t *value );
 

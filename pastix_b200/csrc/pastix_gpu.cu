@@ -550,6 +550,7 @@ static void default_tuning(int64_t *t) {
     t[PGPU_TUNE_WIDE_PANEL] = e ? std::atoi(e) : 128;
     e = getenv("PASTIX_GPU_TC_TMA");
     t[PGPU_TUNE_TC_TMA] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
+    t[PGPU_TUNE_TC_PAIR_MIN] = -1;
 }
 static int mixed_gemm_mode(const pastix_gpu_t &C) { return (int)C.tune[PGPU_TUNE_MIXED_GEMM]; }
 
@@ -801,7 +802,16 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
             PGPU_CHECK(C.d_split.upload(split, C.stream));
             // pairs of 128-row tiles (tm even, tm + 1) of one task and column block
             // share their B tile in the TMA kernel: one entry {task, tm, tn, 1}
-            auto pair_range = [](const std::vector<int4> &in, int b, int e, std::vector<int4> &out) {
+            // (a launch with fewer tiles than two per SM keeps them single: pairs
+            // would leave SMs idle)
+            int nsm_plan = 148;
+            PGPU_CHECK(cudaDeviceGetAttribute(&nsm_plan, cudaDevAttrMultiProcessorCount, C.device));
+            const int64_t pmin = C.tune[PGPU_TUNE_TC_PAIR_MIN] >= 0 ? C.tune[PGPU_TUNE_TC_PAIR_MIN] : 2 * nsm_plan;
+            auto pair_range = [pmin](const std::vector<int4> &in, int b, int e, std::vector<int4> &out) {
+                if (e - b < pmin) {
+                    for (int i = b; i < e; i++) out.push_back(make_int4(in[i].x, in[i].y, in[i].z, 0));
+                    return;
+                }
                 auto key = [](int t, int tm, int tn) { return ((int64_t)t << 32) | ((int64_t)tm << 16) | tn; };
                 std::unordered_map<int64_t, int> pos;
                 for (int i = b; i < e; i++) pos[key(in[i].x, in[i].y, in[i].z)] = i;
@@ -2433,7 +2443,7 @@ extern "C" int pastix_gpu_set_tuning(pastix_gpu_t *ctx, int key, int64_t value) 
     if (!ctx || key < 0 || key >= PGPU_TUNE_COUNT) return PASTIX_GPU_ERR_BADPARAMETER;
     if (key == PGPU_TUNE_MIXED_GEMM && (value < MG_FP32 || value > MG_3XTF32)) return PASTIX_GPU_ERR_BADPARAMETER;
     if ((key == PGPU_TUNE_TRSM_GEMM_ROWS && value < 32) || (key == PGPU_TUNE_LA_RESERVED_SMS && value < 0) ||
-        (key == PGPU_TUNE_TC_MIN_MN && value < 0) || (key == PGPU_TUNE_WIDE_PANEL && value < 0))
+        (key == PGPU_TUNE_TC_MIN_MN && value < 0) || (key == PGPU_TUNE_WIDE_PANEL && value < 0) || (key == PGPU_TUNE_TC_PAIR_MIN && value < -1))
         return PASTIX_GPU_ERR_BADPARAMETER;
     ctx->tune[key] = value;
     ctx->plan_fact = -1;   // the next numfact rebuilds its launch lists (and graph)

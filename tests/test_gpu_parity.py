@@ -357,6 +357,7 @@ def test_tma_operands_match_producer_split(fact, make, trsm_gemm):
     s = _gpu_solver(A, st, fact, mixed=True)
     assert AT.get_knob(s, "tc_tma") == 1
     AT.set_knob(s, "trsm_gemm", trsm_gemm)
+    AT.set_knob(s, "tc_pair_min", 0)       # every launch pairs its 128-row tiles
     s.numfact(A.values)
     L1, U1 = s.coeftab()
     AT.set_knob(s, "tc_tma", 0)
