@@ -108,7 +108,9 @@ struct pastix_gpu_s {
     bool capturing = false;
     cudaGraph_t fact_graph = nullptr;
     cudaGraphExec_t fact_exec = nullptr;
-    int64_t graph_key[4] = {-1, -1, -1, -1};
+    std::vector<int> g_kinds, g_kinds2;   // the captured graph's timing marks (evpool, evpool2)
+    int g_used = 0, g_used2 = 0, g_nl = 0;
+    int64_t graph_key[5] = {-1, -1, -1, -1, -1};
     double thflops[2][3] = {{0}};   // [complex][POTRF, GETRF, LDL] algorithmic flops
 
     // ---- device structure ----
@@ -264,6 +266,8 @@ static double structure_flops(const pastix_gpu_t &C, int form, bool z) {
 // --------------------------------------------------------------------------
 // Structure handoff: device layout + level schedule.
 // --------------------------------------------------------------------------
+static void invalidate_graph(pastix_gpu_t &C);
+
 extern "C" int pastix_gpu_structure(pastix_gpu_t *ctx, int64_t n, int64_t cblknbr, const int64_t *cblktab,
                                     int64_t bloknbr, const int64_t *bloktab, int64_t brownbr,
                                     const int64_t *browtab, const int64_t *permtab, const int64_t *peritab) {
@@ -420,6 +424,7 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
         return PASTIX_GPU_ERR_BADPARAMETER;
     PGPU_CHECK(cudaSetDevice(ctx->device));
     auto &C = *ctx;
+    invalidate_graph(C);   // the value maps below are reallocated
     C.mtxtype = mtxtype;
     C.flttype = flttype;
     const int64_t nnz = colptr[n];
@@ -618,6 +623,16 @@ static bool wide_panel(const pastix_gpu_t &C, int w, size_t esz, bool lu, bool l
     return wmin > 0 && w >= wmin && esz <= 8 && wp_tiles_fit(w, lu) && wide_kcb(w, esz, lu, ldl) > 0;
 }
 
+// Forget the captured factorization graph (its nodes name the plan's and the
+// matrix's device buffers): called whenever those are rebuilt.
+static void invalidate_graph(pastix_gpu_t &C) {
+    if (C.fact_exec) cudaGraphExecDestroy(C.fact_exec);
+    if (C.fact_graph) cudaGraphDestroy(C.fact_graph);
+    C.fact_exec = nullptr;
+    C.fact_graph = nullptr;
+    for (int k = 0; k < 5; k++) C.graph_key[k] = -1;
+}
+
 static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     const bool use_tc = fp32 && !zc && tc_enabled(C) && (fmode == FM_POTRF || fmode == FM_GETRF);
     const bool lu = (fmode == FM_GETRF), ldl = fm_ldl(fmode);
@@ -627,6 +642,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     const int key = ((((fmode * 2 + (fp32 ? 1 : 0)) * 2 + (use_tc ? 1 : 0)) * 2 + (zc ? 1 : 0)) * 2 + (tgemm ? 1 : 0));
     // (set_tuning invalidates the plan, so the knobs need no place in the key)
     if (C.plan_fact == key) return PASTIX_GPU_SUCCESS;
+    invalidate_graph(C);   // the launch lists and workspaces the graph names are rebuilt
     const size_t esz = (fp32 ? 4 : 8) * (zc ? 2 : 1);
     const int fuse = tgemm ? std::min((int)C.tune[PGPU_TUNE_TRSM_GEMM_ROWS], fuse_rows_for(lu, esz))
                            : fuse_rows_for(lu, esz);
@@ -900,8 +916,9 @@ struct LaunchTimer {
     int used = 0;
     explicit LaunchTimer(pastix_gpu_t &c) : C(c), st(c.stream), pool(c.evpool) {}
     LaunchTimer(pastix_gpu_t &c, cudaStream_t s, std::vector<cudaEvent_t> &p) : C(c), st(s), pool(p) {}
+    // (inside a stream capture the record becomes an event node of the graph,
+    // so a replay times its launches alike)
     cudaError_t mark(int kind) {
-        if (C.capturing) return cudaSuccess;   // no timing inside a captured graph
         if (used >= (int)pool.size()) {
             cudaEvent_t e;
             cudaError_t r = cudaEventCreate(&e);
@@ -909,11 +926,15 @@ struct LaunchTimer {
             pool.push_back(e);
         }
         kinds.push_back(kind);
-        return cudaEventRecord(pool[used++], st);
+        // (in a capture a plain record only expresses a dependency; the
+        // external form makes it an event-record node of the graph)
+        return cudaEventRecordWithFlags(pool[used++], st, C.capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
     }
     // after the stream was synchronized: accumulate ms per kind (a mark of
     // kind -1 closes an interval without opening a timed one)
-    void collect(double *ms, int nkind) {
+    void collect(double *ms, int nkind) { collect_marks(pool, kinds, used, ms, nkind); }
+    static void collect_marks(const std::vector<cudaEvent_t> &pool, const std::vector<int> &kinds, int used,
+                              double *ms, int nkind) {
         for (int k = 0; k < nkind; k++) ms[k] = 0;
         for (int i = 0; i + 1 < used; i++) {
             float t = 0;
@@ -1016,7 +1037,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     const bool la = C.tune[PGPU_TUNE_LOOKAHEAD] != 0 && !C.record;
     LaunchTimer tm2(C, C.stream2, C.evpool2);
     if (la) {
-        while ((int)C.la_events.size() < 2 * C.nlevels + 1) {
+        while ((int)C.la_events.size() < 2 * C.nlevels + 2) {
             cudaEvent_t e;
             PGPU_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             C.la_events.push_back(e);
@@ -1202,8 +1223,11 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
         }
     }
     if (la && C.nlevels > 0) {
+        // join the second stream after its last timing mark (which is itself a
+        // graph node when the sequence is captured)
         PGPU_CHECK(tm2.mark(PH_END));
-        PGPU_CHECK(cudaStreamWaitEvent(s, C.la_events[2 * (C.nlevels - 1) + 1], 0));
+        PGPU_CHECK(cudaEventRecord(C.la_events[2 * C.nlevels + 1], C.stream2));
+        PGPU_CHECK(cudaStreamWaitEvent(s, C.la_events[2 * C.nlevels + 1], 0));
     }
     PGPU_CHECK(tm.mark(PH_END));
     PGPU_CHECK(cudaGetLastError());
@@ -1211,6 +1235,10 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     if (la && !C.capturing) {
         PGPU_CHECK(cudaStreamSynchronize(C.stream2));
         tm2.collect(C.side_ms, 4);
+    }
+    if (C.capturing) {   // the replays collect the second stream's marks after their synchronization
+        C.g_kinds2 = la ? tm2.kinds : std::vector<int>();
+        C.g_used2 = la ? tm2.used : 0;
     }
     *launches = nl;
     C.stats[7] = ngemm;
@@ -1283,14 +1311,20 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
         return mixed ? fill_and_factor<float, double>(C, fmode, &nl, tm)
                      : fill_and_factor<double, double>(C, fmode, &nl, tm);
     };
-    // PASTIX_GPU_GRAPH=1: capture the sequence once per (plan, coeftab,
-    // mode) and replay it; the per-phase timings are then not available
+    // PASTIX_GPU_GRAPH=1: the sequence is captured once per (plan, coeftab,
+    // mode, value buffer, pivot magnitude) as a CUDA graph and replayed by
+    // later calls (the first call of a new plan captures, instantiates and
+    // launches it).  The per-phase timings come from event nodes of the graph;
+    // with them the replay is no faster than direct launches at these sizes,
+    // so direct launches stay the default.
     const char *ge = getenv("PASTIX_GPU_GRAPH");
     const bool graph = ge && std::strcmp(ge, "1") == 0 && !C.record;
     bool replayed = false;
     if (graph) {
-        const int64_t key[4] = {C.plan_fact, (int64_t)(uintptr_t)C.d_coef.p, mixed * 8 + fmode,
-                                (int64_t)(uintptr_t)C.d_vals.p};
+        int64_t magn_bits;   // the static-pivot magnitude is a kernel argument of the graph
+        std::memcpy(&magn_bits, &C.dparm[PGPU_DPARM_EPSILON_MAGN_CTRL], sizeof(magn_bits));
+        const int64_t key[5] = {C.plan_fact, (int64_t)(uintptr_t)C.d_coef.p, mixed * 8 + fmode,
+                                (int64_t)(uintptr_t)C.d_vals.p, magn_bits};
         if (!C.fact_exec || std::memcmp(key, C.graph_key, sizeof(key)) != 0) {
             if (C.fact_exec) cudaGraphExecDestroy(C.fact_exec);
             if (C.fact_graph) cudaGraphDestroy(C.fact_graph);
@@ -1300,6 +1334,9 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
             C.capturing = true;
             rc = enqueue();
             C.capturing = false;
+            C.g_kinds = tm.kinds;
+            C.g_used = tm.used;
+            C.g_nl = nl;
             cudaGraph_t g = nullptr;
             const cudaError_t ec = cudaStreamEndCapture(s, &g);
             if (rc) {
@@ -1328,9 +1365,14 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     PGPU_CHECK(cudaEventElapsedTime(&ms, C.ev[0], C.ev[1]));
     C.stats[0] = launches + nl;
     C.stats[3] = ms;
+    if (replayed) {   // the graph's event nodes: main stream, then the lookahead stream
+        nl = C.g_nl;
+        LaunchTimer::collect_marks(C.evpool2, C.g_kinds2, C.g_used2, C.side_ms, 4);
+    }
     {
         double ph[4];
-        tm.collect(ph, 4);
+        if (replayed) LaunchTimer::collect_marks(C.evpool, C.g_kinds, C.g_used, ph, 4);
+        else tm.collect(ph, 4);
         C.stats[8] = ph[PH_DIAG];
         C.stats[9] = ph[PH_TRSM];
         C.stats[6] = ph[PH_GEMM] + ph[PH_TC] + C.side_ms[PH_GEMM] + C.side_ms[PH_TC];

@@ -276,19 +276,24 @@ def test_hetrf_gmres_refinement_reaches_1e12(mixed):
 
 @pytest.mark.parametrize("mixed", [False, True])
 def test_factorization_graph_replay_matches_direct(mixed, monkeypatch):
-    """PASTIX_GPU_GRAPH=1: the factorization sequence (norm, fill-in, every
-    level's panels, TRSMs and update GEMMs on both lookahead streams) is
-    captured once and replayed; its factors equal the directly launched
-    ones and a new set of values reuses the same graph."""
+    """The factorization sequence (norm, fill-in, every level's panels, TRSMs
+    and update GEMMs on both lookahead streams) captured once as a CUDA graph
+    and replayed (PASTIX_GPU_GRAPH=1; =0 launches kernel by kernel):
+    its factors equal the directly launched ones, a new set of values reuses
+    the same graph, and the per-phase timings come from its event nodes."""
     A = M.diffusion_lognormal(24, 23, 22, 1.0, np.random.default_rng(21))
     ref, st = U.run_reference(A, "potrf", numfact=False)
     s = _gpu_solver(A, st, "potrf", mixed=mixed)
+    monkeypatch.setenv("PASTIX_GPU_GRAPH", "0")   # launched kernel by kernel
     s.numfact(A.values)
+    assert s.stats()["graph_replayed"] == 0.0
     L0, _ = s.coeftab()
     monkeypatch.setenv("PASTIX_GPU_GRAPH", "1")
     s.numfact(A.values)                  # capture
     s.numfact(A.values)                  # replay
-    assert s.stats()["graph_replayed"] == 1.0
+    st_ = s.stats()
+    assert st_["graph_replayed"] == 1.0
+    assert st_["diag_ms"] > 0 and st_["gemm_ms"] > 0   # phase timings from the graph's event nodes
     L1, _ = s.coeftab()
     tol = 1e-12 if not mixed else 1e-5
     assert np.abs(L1.astype(np.float64) - L0).max() <= tol * np.abs(L0).max()
