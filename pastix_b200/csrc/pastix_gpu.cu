@@ -1467,8 +1467,13 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         const int mw = C.lvl_maxw[l];
         if (small_level(l)) {
             PGPU_CHECK(mark(0));
-            k_fwd_small<T><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], ncb, coefL, W, ldb,
-                                                        nrhs, (lu || ldl) ? 1 : 0);
+            const int *lc = C.d_lvl_cblks.p + C.lvl_ptr[l];
+            const int un = (lu || ldl) ? 1 : 0;
+            // right-hand sides 8 / 4 / 2 / 1 at a time in registers
+            if (nrhs % 8 == 0) k_fwd_small<T, 8><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, lc, ncb, coefL, W, ldb, nrhs, un);
+            else if (nrhs % 4 == 0) k_fwd_small<T, 4><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, lc, ncb, coefL, W, ldb, nrhs, un);
+            else if (nrhs % 2 == 0) k_fwd_small<T, 2><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, lc, ncb, coefL, W, ldb, nrhs, un);
+            else k_fwd_small<T, 1><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, lc, ncb, coefL, W, ldb, nrhs, un);
             nl++;
             continue;
         }
@@ -1512,8 +1517,16 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
         const int mw = C.lvl_maxw[l];
         if (small_level(l)) {
             PGPU_CHECK(mark(4));
-            k_bwd_small<T><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, C.d_lvl_cblks.p + C.lvl_ptr[l], ncb, coefL, coefU, W,
-                                                        ldb, nrhs, lu ? 1 : 0, ldl ? 1 : 0, lu ? 0 : cjp);
+            const int *lc = C.d_lvl_cblks.p + C.lvl_ptr[l];
+            const int up = lu ? 1 : 0, un = ldl ? 1 : 0, cj = lu ? 0 : cjp;
+            if (nrhs % 8 == 0)
+                k_bwd_small<T, 8><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, lc, ncb, coefL, coefU, W, ldb, nrhs, up, un, cj);
+            else if (nrhs % 4 == 0)
+                k_bwd_small<T, 4><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, lc, ncb, coefL, coefU, W, ldb, nrhs, up, un, cj);
+            else if (nrhs % 2 == 0)
+                k_bwd_small<T, 2><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, lc, ncb, coefL, coefU, W, ldb, nrhs, up, un, cj);
+            else
+                k_bwd_small<T, 1><<<cdiv(ncb, 8), 256, 0, s>>>(C.meta, lc, ncb, coefL, coefU, W, ldb, nrhs, up, un, cj);
             nl++;
             continue;
         }
@@ -2040,8 +2053,12 @@ struct BlockOps {
         const int grid = std::min(4096, cdiv((int64_t)n * k, 256));
         k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, k, C.d_peritab.p, x, n, xp, n, 0);
         if (beta != 0.0) k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, k, C.d_peritab.p, y, n, yp, n, 0);
-        k_spmv_multi<S><<<cdiv((int64_t)n * 32, 256), 256, 0, C.stream>>>(n, k, C.d_csr_ptr.p, C.d_csr_col.p, val,
-                                                                           alpha, xp, beta, yp);
+        if (C.csr_nnz <= (int64_t)16 * n)   // short rows: one thread per row
+            k_spmv_rows_multi<S><<<std::min(cdiv(n, 256), 8 * 148), 256, 0, C.stream>>>(
+                n, k, C.d_csr_ptr.p, C.d_csr_col.p, val, alpha, xp, beta, yp);
+        else
+            k_spmv_multi<S><<<cdiv((int64_t)n * 32, 256), 256, 0, C.stream>>>(n, k, C.d_csr_ptr.p, C.d_csr_col.p,
+                                                                               val, alpha, xp, beta, yp);
         k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, k, C.d_peritab.p, yp, n, y, n, 1);
         launches += 3 + (beta != 0.0);
     }

@@ -476,10 +476,12 @@ __global__ void __launch_bounds__(256) k_bwd_off_direct(Meta m, const int2 *__re
 // k_fwd_off (forward) and k_bwd_off + k_bwd_diag (backward) for these
 // cblks; the backward gather needs no atomics (one warp owns the cblk).
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int R>
 __global__ void __launch_bounds__(256) k_fwd_small(Meta m, const int *__restrict__ cblks, int ncb,
                                                    const T *__restrict__ coefL, T *__restrict__ B, int ldb, int nrhs,
                                                    int unit) {
+    // R right-hand sides at a time (nrhs a multiple of R), each one's
+    // operations in the same order as alone
     const int lane = threadIdx.x & 31;
     const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (q >= ncb) return;                                  // whole warps
@@ -488,31 +490,46 @@ __global__ void __launch_bounds__(256) k_fwd_small(Meta m, const int *__restrict
     const T *D = coefL + m.coefoff[c];
     const T dinv = (lane < w && !unit) ? T(1) / D[(int64_t)lane * ld + lane] : T(1);
     const int *rows = m.rowidx + m.rowbase[c];
-    for (int r = 0; r < nrhs; r++) {
-        T *Br = B + (int64_t)r * ldb;
-        T v = (lane < w) ? Br[fc + lane] : T(0);
+    for (int r0 = 0; r0 < nrhs; r0 += R) {
+        T v[R];
+#pragma unroll
+        for (int u = 0; u < R; u++) v[u] = (lane < w) ? B[(int64_t)(r0 + u) * ldb + fc + lane] : T(0);
         for (int j = 0; j < w; j++) {
-            if (lane == j) v = v * dinv;
-            const T xj = shfl_v(v, j);
-            if (lane > j && lane < w) v -= D[(int64_t)lane * ld + j] * xj;
+            const T lj = (lane > j && lane < w) ? D[(int64_t)lane * ld + j] : T(0);
+#pragma unroll
+            for (int u = 0; u < R; u++) {
+                if (lane == j) v[u] = v[u] * dinv;
+                const T xj = shfl_v(v[u], j);
+                if (lane > j && lane < w) v[u] -= lj * xj;
+            }
         }
-        if (lane < w) Br[fc + lane] = v;
+        if (lane < w)
+#pragma unroll
+            for (int u = 0; u < R; u++) B[(int64_t)(r0 + u) * ldb + fc + lane] = v[u];
         for (int i0 = w; i0 < h; i0 += 32) {
             const int i = i0 + lane;
             const T *row = D + (int64_t)i * ld;
-            T s = T(0);
+            T sacc[R];
+#pragma unroll
+            for (int u = 0; u < R; u++) sacc[u] = T(0);
             for (int j = 0; j < w; j++) {
-                const T xj = shfl_v(v, j);
-                if (i < h) s += row[j] * xj;
+                const T rj = (i < h) ? row[j] : T(0);
+#pragma unroll
+                for (int u = 0; u < R; u++) {
+                    const T xj = shfl_v(v[u], j);
+                    if (i < h) sacc[u] += rj * xj;
+                }
             }
-            if (i < h) atomic_sub(&Br[rows[i]], s);
+            if (i < h)
+#pragma unroll
+                for (int u = 0; u < R; u++) atomic_sub(&B[(int64_t)(r0 + u) * ldb + rows[i]], sacc[u]);
         }
     }
 }
 
 // upper != 0: U of the LU diagonal block (row-major upper part, non-unit),
 // P = the U^t panel (coefP); else op(L)^t with op = conj when cjp, P = L.
-template <typename T>
+template <typename T, int R>
 __global__ void __launch_bounds__(256) k_bwd_small(Meta m, const int *__restrict__ cblks, int ncb,
                                                    const T *__restrict__ coefL, const T *__restrict__ coefP,
                                                    T *__restrict__ B, int ldb, int nrhs, int upper, int unit,
@@ -530,30 +547,41 @@ __global__ void __launch_bounds__(256) k_bwd_small(Meta m, const int *__restrict
         const T d = D[(int64_t)lane * ld + lane];
         dinv = T(1) / (cjp ? conj_v(d) : d);
     }
-    for (int r = 0; r < nrhs; r++) {
-        T *Br = B + (int64_t)r * ldb;
+    for (int r0 = 0; r0 < nrhs; r0 += R) {
         // gather: x_j -= sum_i op(P[i][j]) x[row_i]
-        T s = T(0);
+        T sacc[R];
+#pragma unroll
+        for (int u = 0; u < R; u++) sacc[u] = T(0);
         if (lane < w)
             for (int i = w; i < h; i++) {
-                const T pv = P[(int64_t)i * ld + lane];
-                s += (cjp ? conj_v(pv) : pv) * Br[rows[i]];
+                T pv = P[(int64_t)i * ld + lane];
+                if (cjp) pv = conj_v(pv);
+                const int gi = rows[i];
+#pragma unroll
+                for (int u = 0; u < R; u++) sacc[u] += pv * B[(int64_t)(r0 + u) * ldb + gi];
             }
-        T v = (lane < w) ? Br[fc + lane] - s : T(0);
+        T v[R];
+#pragma unroll
+        for (int u = 0; u < R; u++) v[u] = (lane < w) ? B[(int64_t)(r0 + u) * ldb + fc + lane] - sacc[u] : T(0);
         for (int j = w - 1; j >= 0; j--) {
-            if (lane == j) v = v * dinv;
-            const T xj = shfl_v(v, j);
+            T dlj = T(0);
             if (lane < j) {
-                T dlj;
                 if (upper) dlj = D[(int64_t)lane * ld + j];
                 else {
                     dlj = D[(int64_t)j * ld + lane];
                     if (cjp) dlj = conj_v(dlj);
                 }
-                v -= dlj * xj;
+            }
+#pragma unroll
+            for (int u = 0; u < R; u++) {
+                if (lane == j) v[u] = v[u] * dinv;
+                const T xj = shfl_v(v[u], j);
+                if (lane < j) v[u] -= dlj * xj;
             }
         }
-        if (lane < w) Br[fc + lane] = v;
+        if (lane < w)
+#pragma unroll
+            for (int u = 0; u < R; u++) B[(int64_t)(r0 + u) * ldb + fc + lane] = v[u];
     }
 }
 
@@ -884,6 +912,34 @@ __global__ void k_scal_multi(int64_t n, int k, Coefs<double> a, S *__restrict__ 
 // y_c = alpha A x_c + beta y_c on the permuted CSR, one warp per row, all
 // columns from one pass over the row (same summation order per column as
 // k_spmv)
+// The same products with one thread per row (short rows, as the stencil
+// matrices have: a warp per row would leave most lanes idle); the row's
+// entries are summed in order.
+template <typename S>
+__global__ void k_spmv_rows_multi(int n, int k, const int64_t *__restrict__ rowptr, const int *__restrict__ col,
+                                  const S *__restrict__ val, double alpha, const S *__restrict__ x, double beta,
+                                  S *__restrict__ y) {
+    for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+        S s[MULTI_MAX];
+#pragma unroll
+        for (int c = 0; c < MULTI_MAX; c++) s[c] = S(0.0);
+        const int64_t q1 = rowptr[row + 1];
+        for (int64_t q = rowptr[row]; q < q1; q++) {
+            const S v = val[q];
+            const int cc = col[q];
+#pragma unroll
+            for (int c = 0; c < MULTI_MAX; c++)
+                if (c < k) s[c] += v * x[(int64_t)c * n + cc];
+        }
+#pragma unroll
+        for (int c = 0; c < MULTI_MAX; c++) {
+            if (c >= k) break;
+            S &yy = y[(int64_t)c * n + row];
+            yy = alpha * s[c] + (beta == 0.0 ? S(0.0) : beta * yy);
+        }
+    }
+}
+
 template <typename S>
 __global__ void k_spmv_multi(int n, int k, const int64_t *__restrict__ rowptr, const int *__restrict__ col,
                              const S *__restrict__ val, double alpha, const S *__restrict__ x, double beta,
