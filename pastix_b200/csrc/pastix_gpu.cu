@@ -122,6 +122,7 @@ struct pastix_gpu_s {
     // ---- factorization plan (per factotype) ----
     int plan_fact = -1;
     std::vector<int> tile_ptr, tctile_ptr, trsm_ptr, lvl_plrows, lvl_porows;
+    std::vector<int> stile_n;   // per level and part (next-level targets, others): warp tiles at the part's end
     // panel launches of a level: k_panel_factor over the narrow cblks and
     // k_panel_wide over the wide diagonal blocks, jobs {cblk, position in
     // lvl_cblks} (the position indexes the task records)
@@ -672,7 +673,11 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     std::vector<int2> pjobs, wjobs;
     C.tile_crit.assign(C.nlevels, 0);
     C.tctile_crit.assign(C.nlevels, 0);
-    std::vector<int4> lt[2], ltc[2];   // this level's FMA / tensor-core tiles: [0] next-level targets, [1] others
+    std::vector<int4> lt[2], ltc[2], lsm[2];   // this level's FMA (CTA / warp) and tensor-core tiles: [0] next-level targets, [1] others
+    // warp tiles for narrow FMA updates (not while recording task timings:
+    // those describe the CTA tiles)
+    const bool small_ok = !C.record && esz <= 8;
+    C.stile_n.assign(2 * C.nlevels, 0);
     for (int l = 0; l < C.nlevels; l++) {
         int64_t scr_lvl = 0;
         for (int k = 0; k < 2; k++) {
@@ -738,6 +743,10 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
                             }
                         return;
                     }
+                    if (small_ok && N <= GS_TN) {   // narrow update: one warp per 32 rows
+                        for (int tm = 0; tm < cdiv(M, GS_TM); tm++) lsm[crit].push_back(make_int4(id, tm, 0, 1));
+                        return;
+                    }
                     for (int tm = 0; tm < cdiv(M, GEMM_TM); tm++)
                         for (int tn = 0; tn < cdiv(N, GEMM_TN); tn++) {
                             if ((flags & 8) && tm < tn) continue;   // strictly upper tiles of the diagonal block
@@ -751,6 +760,12 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
                     if (b + 1 < b1) add(C.browoff[b + 1], 1 | 4);  // U side: A = U^T, B = L rows of b
                 }
             }
+        }
+        // each part: the CTA tiles, then the warp tiles (counted in stile_n)
+        for (int k = 0; k < 2; k++) {
+            C.stile_n[2 * l + k] = (int)lsm[k].size();
+            lt[k].insert(lt[k].end(), lsm[k].begin(), lsm[k].end());
+            lsm[k].clear();
         }
         C.tile_crit[l] = (int)lt[0].size();
         C.tctile_crit[l] = (int)ltc[0].size();
@@ -996,6 +1011,9 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     const int fuse = C.plan_fuse;   // rows the panel kernel solves itself (the plan's choice)
     PanelKernel<T> kpanel = panel_kernel<T>(fmode);
     if (!kpanel) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+    if constexpr (sizeof(T) <= 8)
+        PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        gs_smem_bytes<T>()));
     WideKernel<T> kwide = wide_kernel<T>(fmode);
     if (kwide)
         PGPU_CHECK(cudaFuncSetAttribute(kwide, cudaFuncAttributeMaxDynamicSharedMemorySize, WP_SMEM_LIMIT));
@@ -1057,14 +1075,26 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             }
         }
     };
-    auto launch_gemms = [&](cudaStream_t st, LaunchTimer &lt, int t0, int nt, int c0, int ntc, int gcap) -> int {
-        if (nt) {
+    auto launch_gemms = [&](cudaStream_t st, LaunchTimer &lt, int t0, int nt, int nw, int c0, int ntc,
+                            int gcap) -> int {
+        // tiles [t0, t0 + nt): CTA tiles, then nw warp tiles
+        if (nt - nw > 0) {
             PGPU_CHECK(lt.mark(PH_GEMM));
-            k_gemm_scatter<T><<<nt, 256, 0, st>>>(C.meta, C.d_tiles.p + t0, C.d_tasks.p, coefL, coefU, nullptr,
-                                                  nullptr, at(prof[2], t0));
+            k_gemm_scatter<T><<<nt - nw, 256, 0, st>>>(C.meta, C.d_tiles.p + t0, C.d_tasks.p, coefL, coefU, nullptr,
+                                                       nullptr, at(prof[2], t0));
             if (la) PGPU_CHECK(lt.mark(PH_END));
             nl++;
             ngemm++;
+        }
+        if constexpr (sizeof(T) <= 8) {
+            if (nw > 0) {
+                PGPU_CHECK(lt.mark(PH_GEMM));
+                k_gemm_scatter_small<T><<<cdiv(nw, GS_WARPS), GS_WARPS * 32, gs_smem_bytes<T>(), st>>>(
+                    C.meta, C.d_tiles.p + t0 + nt - nw, nw, C.d_tasks.p, coefL, coefU);
+                if (la) PGPU_CHECK(lt.mark(PH_END));
+                nl++;
+                ngemm++;
+            }
         }
         if constexpr (std::is_same<T, float>::value) {
             if (ntc) {
@@ -1209,16 +1239,21 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
         const int nti = C.tile_ptr[l + 1] - C.tile_ptr[l], ntc = C.tctile_ptr[l + 1] - C.tctile_ptr[l];
         if (la) {
             PGPU_CHECK(cudaEventRecord(C.la_events[2 * l], s));
-            int rc = launch_gemms(s, tm, C.tile_ptr[l], C.tile_crit[l], C.tctile_ptr[l], C.tctile_crit[l], nsm);
+            int rc = launch_gemms(s, tm, C.tile_ptr[l], C.tile_crit[l], C.stile_n[2 * l], C.tctile_ptr[l],
+                                  C.tctile_crit[l], nsm);
             if (rc) return rc;
             PGPU_CHECK(cudaStreamWaitEvent(C.stream2, C.la_events[2 * l], 0));
-            rc = launch_gemms(C.stream2, tm2, C.tile_ptr[l] + C.tile_crit[l], nti - C.tile_crit[l],
+            rc = launch_gemms(C.stream2, tm2, C.tile_ptr[l] + C.tile_crit[l], nti - C.tile_crit[l], C.stile_n[2 * l + 1],
                               C.tctile_ptr[l] + C.tctile_crit[l], ntc - C.tctile_crit[l],
                               std::max(1, nsm - (int)C.tune[PGPU_TUNE_LA_RESERVED_SMS]));
             if (rc) return rc;
             PGPU_CHECK(cudaEventRecord(C.la_events[2 * l + 1], C.stream2));
         } else {
-            const int rc = launch_gemms(s, tm, C.tile_ptr[l], nti, C.tctile_ptr[l], ntc, nsm);
+            // (one launch per kind: the warp tiles of both parts sit at the parts' ends)
+            int rc = launch_gemms(s, tm, C.tile_ptr[l], C.tile_crit[l], C.stile_n[2 * l], C.tctile_ptr[l], ntc, nsm);
+            if (rc) return rc;
+            rc = launch_gemms(s, tm, C.tile_ptr[l] + C.tile_crit[l], nti - C.tile_crit[l], C.stile_n[2 * l + 1], 0, 0,
+                              nsm);
             if (rc) return rc;
         }
     }

@@ -188,4 +188,80 @@ __global__ void __launch_bounds__(256) k_gemm_scatter(Meta m, const int4 *__rest
     }
 }
 
+// ---------------------------------------------------------------------------
+// Narrow update tasks (N <= 32 rows in block b: the leaves of 2D problems and
+// thin separators): one warp per 32-row slab of the task, lane i owning row
+// i's N outputs in registers.  The slab's A rows and B rows are staged per
+// 32-column chunk of K in the warp's shared memory (coalesced along k), then
+// C[i][j] += A[i][k] op(B[j][k]) in increasing k; the same flags as
+// k_gemm_scatter (U-side operands, D-scaled A for LDL, conjugated B,
+// lower-triangle-only targets) and the same scatter-add into the facing cblk.
+// ---------------------------------------------------------------------------
+constexpr int GS_TM = 32, GS_TN = 32, GS_WARPS = 8;
+template <typename T>
+constexpr int gs_smem_bytes() { return GS_WARPS * 2 * 32 * 33 * (int)sizeof(T); }
+
+template <typename T>
+__global__ void __launch_bounds__(GS_WARPS * 32) k_gemm_scatter_small(Meta m, const int4 *__restrict__ tiles,
+                                                                       int ntiles, const GemmTask *__restrict__ tasks,
+                                                                       T *__restrict__ coefL, T *__restrict__ coefU) {
+    extern __shared__ __align__(16) unsigned char gs_smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    T *As = reinterpret_cast<T *>(gs_smem_raw) + warp * 2 * 32 * 33;   // [k][i], stride 33
+    T *Bs = As + 32 * 33;                                               // [k][j]
+    const int ti = blockIdx.x * GS_WARPS + warp;
+    if (ti >= ntiles) return;                 // whole warps; only warp-level synchronization below
+    const int4 tl = tiles[ti];
+    const GemmTask t = tasks[tl.x];
+    const int c = t.c, b = t.b, f = t.f;
+    const int K = m.width[c], ld = m.ld[c];
+    const int N = m.blrow[b] - m.bfrow[b] + 1;
+    const int i0 = tl.y * GS_TM;
+    const int mrows = min(GS_TM, t.M - i0), ncols = min(GS_TN, N);
+    const T *A = ((t.flags & 1) ? coefU : coefL) + m.coefoff[c] + (int64_t)(t.arow0 + i0) * ld;
+    const T *Bm = ((t.flags & 2) ? coefU : coefL) + m.coefoff[c] + (int64_t)m.browoff[b] * ld;
+    const T *Dg = coefL + m.coefoff[c];
+    const bool scale_d = (t.flags & 16) != 0, conj_b = (t.flags & 32) != 0;
+    int tr = -1;
+    if (lane < mrows) tr = panel_row_of(m, f, m.rowidx[m.rowbase[c] + t.arow0 + i0 + lane]);
+    T acc[GS_TN];
+#pragma unroll
+    for (int j = 0; j < GS_TN; j++) acc[j] = T(0);
+    for (int k0 = 0; k0 < K; k0 += 32) {
+        const int kn = min(32, K - k0);
+        const T dk = (scale_d && lane < kn) ? Dg[(int64_t)(k0 + lane) * ld + k0 + lane] : T(1);
+        // lane = k: rows of A and B read along k (coalesced)
+        for (int i = 0; i < mrows; i++) {
+            T av = (lane < kn) ? A[(int64_t)i * ld + k0 + lane] : T(0);
+            if (scale_d) av = av * dk;
+            As[lane * 33 + i] = av;
+        }
+        for (int j = 0; j < ncols; j++) {
+            T bv = (lane < kn) ? Bm[(int64_t)j * ld + k0 + lane] : T(0);
+            if (conj_b) bv = conj_v(bv);
+            Bs[lane * 33 + j] = bv;
+        }
+        __syncwarp();
+        for (int kk = 0; kk < kn; kk++) {
+            const T a = As[kk * 33 + lane];
+#pragma unroll
+            for (int j = 0; j < GS_TN; j++)
+                if (j < ncols) acc[j] += a * Bs[kk * 33 + j];
+        }
+        __syncwarp();
+    }
+    if (tr < 0) return;
+    T *C = ((t.flags & 4) ? coefU : coefL) + m.coefoff[f];
+    const int ldf = m.ld[f], wf = m.width[f];
+    const int tcol0 = m.bfrow[b] - m.fcol[f];
+    const bool lower_only = (t.flags & 8) != 0;
+#pragma unroll
+    for (int j = 0; j < GS_TN; j++) {
+        if (j >= ncols) break;
+        const int tc = tcol0 + j;
+        if (lower_only && tr < wf && tc > tr) continue;
+        atomic_sub(&C[(int64_t)tr * ldf + tc], acc[j]);
+    }
+}
+
 }  // namespace pgpu
