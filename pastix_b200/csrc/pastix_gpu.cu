@@ -128,6 +128,8 @@ struct pastix_gpu_s {
     // lvl_cblks} (the position indexes the task records)
     std::vector<int> pn_ptr, pw_ptr, lvl_pmaxw, lvl_wmaxw;
     DArr<int2> d_pjobs, d_wjobs;
+    std::vector<int> ps_ptr;   // cblks of at most 32 columns: one warp each (k_panel_small)
+    DArr<int2> d_sjobs;
     DArr<int4> d_tiles, d_tctiles, d_trsm;
     double tc_flops = 0;   // update-GEMM flops on the tensor-core path
     DArr<GemmTask> d_tasks;
@@ -670,7 +672,8 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     C.lvl_wmaxw.assign(C.nlevels, 0);
     C.pn_ptr.assign(C.nlevels + 1, 0);
     C.pw_ptr.assign(C.nlevels + 1, 0);
-    std::vector<int2> pjobs, wjobs;
+    std::vector<int2> pjobs, wjobs, sjobs;
+    C.ps_ptr.assign(C.nlevels + 1, 0);
     C.tile_crit.assign(C.nlevels, 0);
     C.tctile_crit.assign(C.nlevels, 0);
     std::vector<int4> lt[2], ltc[2], lsm[2];   // this level's FMA (CTA / warp) and tensor-core tiles: [0] next-level targets, [1] others
@@ -691,6 +694,8 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
             if (rows == w && wide_panel(C, w, esz, lu, ldl)) {
                 wjobs.push_back(make_int2(c, q));
                 C.lvl_wmaxw[l] = std::max(C.lvl_wmaxw[l], w);
+            } else if (w <= PB && esz <= 8 && !C.record) {
+                sjobs.push_back(make_int2(c, q));   // one 32-column tile: one warp
             } else {
                 pjobs.push_back(make_int2(c, q));
                 C.lvl_plrows[l] = std::max(C.lvl_plrows[l], rows);
@@ -777,6 +782,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
         C.tctile_ptr[l + 1] = (int)tctiles.size();
         C.trsm_ptr[l + 1] = (int)trsm.size();
         C.pn_ptr[l + 1] = (int)pjobs.size();
+        C.ps_ptr[l + 1] = (int)sjobs.size();
         C.pw_ptr[l + 1] = (int)wjobs.size();
         C.inv_ptr[l + 1] = (int)invjobs.size();
         C.ttile_ptr[l + 1] = (int)ttiles.size();
@@ -906,6 +912,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     PGPU_CHECK(C.d_trsm.upload(trsm, s));
     PGPU_CHECK(C.d_tasks.upload(tasks, s));
     PGPU_CHECK(C.d_pjobs.upload(pjobs, s));
+    PGPU_CHECK(C.d_sjobs.upload(sjobs, s));
     PGPU_CHECK(C.d_wjobs.upload(wjobs, s));
     PGPU_CHECK(cudaStreamSynchronize(s));
     C.h_tiles.swap(tiles);
@@ -965,6 +972,24 @@ template <typename T>
 using PanelKernel = void (*)(Meta, const int2 *, T *, T *, const double *, int, int, int, Status *, int64_t *);
 template <typename T>
 using WideKernel = void (*)(Meta, const int2 *, T *, const double *, int, Status *, int64_t *);
+
+template <typename T>
+using SmallPanelKernel = void (*)(Meta, const int2 *, int, T *, T *, const double *, int, Status *);
+template <typename T>
+static SmallPanelKernel<T> panel_small_kernel(int fmode) {
+    if constexpr (sizeof(T) > 8) {
+        return nullptr;
+    } else {
+        switch (fmode) {
+        case FM_GETRF: return k_panel_small<T, FM_GETRF>;
+        case FM_SYTRF: return k_panel_small<T, FM_SYTRF>;
+        case FM_HETRF:
+            if constexpr (is_cplx<T>::value) return k_panel_small<T, FM_HETRF>;
+            return nullptr;
+        default: return k_panel_small<T, FM_POTRF>;
+        }
+    }
+}
 
 template <typename T>
 static WideKernel<T> wide_kernel(int fmode) {
@@ -1163,6 +1188,17 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                 kwide<<<npw, WP_THREADS, wp_smem_bytes(wmw, sizeof(T), lu, fm_ldl(fmode), kcb), s>>>(
                     C.meta, C.d_wjobs.p + C.pw_ptr[l], coefL, critp, kcb / (int)sizeof(T), C.d_status.p, prof[0]);
             nl++;
+        }
+        if constexpr (sizeof(T) <= 8) {
+            const int nps = C.ps_ptr[l + 1] - C.ps_ptr[l];
+            if (nps) {
+                auto ks = panel_small_kernel<T>(fmode);
+                if (!ks) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+                PGPU_CHECK(cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, ps_smem_bytes<T>(fmode == FM_GETRF)));
+                ks<<<cdiv(nps, PS_WARPS), PS_WARPS * 32, ps_smem_bytes<T>(fmode == FM_GETRF), s>>>(
+                    C.meta, C.d_sjobs.p + C.ps_ptr[l], nps, coefL, coefU, critp, fuse, C.d_status.p);
+                nl++;
+            }
         }
         if (npn) {
             const int pmw = C.lvl_pmaxw[l];

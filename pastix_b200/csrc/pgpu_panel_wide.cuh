@@ -517,6 +517,100 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide_la(Meta m, const int2
     }
 }
 
+// ---------------------------------------------------------------------------
+// Cblks of at most 32 columns (the leaves, ~10^5-10^6 of them in the
+// batched 2D problems): one warp per cblk.  The w x w diagonal block is one
+// tile, factorized in registers (warp_factor_tile), and the panel rows below
+// it are solved one lane per row with the row in registers -- the same
+// operations as k_panel_factor for such a cblk, without a 256-thread CTA per
+// leaf.
+// Shared memory per warp: X [PB][PB + VK] (the tile with row length PBL
+// while it is factorized, then TA, the tile as 16-byte rows for the row
+// solves), TB [PB][PB + VK] for LU, 1 / op(diagonal) [PB].
+// ---------------------------------------------------------------------------
+constexpr int PS_WARPS = 8;
+template <typename T>
+__host__ __device__ constexpr int ps_warp_elems(bool lu) { return (lu ? 2 : 1) * PB * (PB + 16 / (int)sizeof(T)) + PB; }
+template <typename T>
+constexpr int ps_smem_bytes(bool lu) { return PS_WARPS * ps_warp_elems<T>(lu) * (int)sizeof(T); }
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(PS_WARPS * 32) k_panel_small(Meta m, const int2 *__restrict__ jobs, int njobs,
+                                                               T *__restrict__ coefL, T *__restrict__ coefU,
+                                                               const double *critp, int fuse_rows, Status *st) {
+    typedef typename real_of<T>::type R;
+    constexpr bool LU = (MODE == FM_GETRF);
+    constexpr bool LDL = fm_ldl(MODE);
+    constexpr bool CJ = fm_conj(MODE);
+    constexpr int VK = 16 / sizeof(T), LDT = PB + VK;
+    static_assert(LDT >= PBL, "the tile fits in TA");
+    extern __shared__ __align__(16) unsigned char ps_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = blockIdx.x * PS_WARPS + warp;
+    if (q >= njobs) return;                        // whole warps; warp-level synchronization only
+    T *TA = reinterpret_cast<T *>(ps_raw) + (size_t)warp * ps_warp_elems<T>(LU);
+    T *tile = TA;
+    T *TB = TA + PB * LDT;
+    T *rdiag = TA + (LU ? 2 : 1) * PB * LDT;
+    const int c = jobs[q].x;
+    const int w = m.width[c], h = m.height[c], ld = m.ld[c];
+    const int rows = (h <= fuse_rows) ? h : w;
+    T *A = coefL + m.coefoff[c];
+    T *AU = coefU + m.coefoff[c];
+    const R crit = R(*critp);
+    int npiv = 0, nneg = 0, nbad = 0;
+    if (lane < w)
+        for (int i = 0; i < w; i++) tile[i * PBL + lane] = A[(int64_t)i * ld + lane];
+    __syncwarp();
+    warp_factor_tile<T, MODE>(tile, w, crit, npiv, nneg, nbad);
+    __syncwarp();
+    if (lane < w) {
+        for (int i = 0; i < w; i++)
+            if (LU || lane <= i) A[(int64_t)i * ld + lane] = tile[i * PBL + lane];
+        const T d = tile[lane * PBL + lane];
+        rdiag[lane] = T(1) / (MODE == FM_POTRF ? cj<CJ>(d) : d);
+        if (LU)
+            for (int j = 0; j < w; j++) TB[j * LDT + lane] = tile[j * PBL + lane];
+    }
+    {   // TA over the tile's storage: the whole tile goes through registers
+        T v[PB];
+#pragma unroll
+        for (int j = 0; j < PB; j++)
+            v[j] = (lane < w && j < w) ? (LU ? tile[lane * PBL + j] : tile[j * PBL + lane]) : T(0);
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < PB; j++)
+            if (lane < w && j < w) TA[j * LDT + lane] = v[j];
+    }
+    __syncwarp();
+    for (int r = w + lane; r < rows; r += 32) {
+        T x[PB];
+        T *row = A + (int64_t)r * ld;
+#pragma unroll
+        for (int j = 0; j < PB; j++) x[j] = (j < w) ? row[j] : T(0);
+        if (LU) wp_solve_rows<T, false, false>(x, TA, LDT, rdiag, w);
+        else if (LDL) wp_solve_rows<T, CJ, true>(x, TA, LDT, rdiag, w);
+        else wp_solve_rows<T, CJ, false>(x, TA, LDT, rdiag, w);
+#pragma unroll
+        for (int j = 0; j < PB; j++)
+            if (j < w) row[j] = LDL ? x[j] * rdiag[j] : x[j];
+        if constexpr (LU) {   // the U^t rows: x L^t = a (unit)
+            T *urow = AU + (int64_t)r * ld;
+#pragma unroll
+            for (int j = 0; j < PB; j++) x[j] = (j < w) ? urow[j] : T(0);
+            wp_solve_rows<T, false, true>(x, TB, LDT, rdiag, w);
+#pragma unroll
+            for (int j = 0; j < PB; j++)
+                if (j < w) urow[j] = x[j];
+        }
+    }
+    if (lane == 0) {
+        if (npiv) atomicAdd(&st->nbpivots, npiv);
+        if (nneg) atomicAdd(&st->negpivots, nneg);
+        if (nbad) atomicAdd(&st->nonfinite, nbad);
+    }
+}
+
 // Whether one CTA covers width w with its tile budget.
 __host__ inline bool wp_tiles_fit(int w, bool lu) {
     const int rg = wp_row_groups(w), rg2 = lu ? wp_row_groups(w > PB ? w - PB : 0) : 0;
