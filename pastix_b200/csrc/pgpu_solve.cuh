@@ -482,9 +482,12 @@ __global__ void __launch_bounds__(256) k_fwd_small(Meta m, const int *__restrict
                                                    int unit) {
     // R right-hand sides at a time (nrhs a multiple of R), each one's
     // operations in the same order as alone
+    constexpr int VK = 16 / sizeof(T);
+    __shared__ __align__(16) unsigned char xs_raw[8 * 32 * R * sizeof(T)];
     const int lane = threadIdx.x & 31;
     const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (q >= ncb) return;                                  // whole warps
+    T *xs = reinterpret_cast<T *>(xs_raw) + (threadIdx.x >> 5) * 32 * R;   // [32][R]: x of this cblk
     const int c = cblks[q];
     const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c], h = m.height[c];
     const T *D = coefL + m.coefoff[c];
@@ -506,24 +509,33 @@ __global__ void __launch_bounds__(256) k_fwd_small(Meta m, const int *__restrict
         if (lane < w)
 #pragma unroll
             for (int u = 0; u < R; u++) B[(int64_t)(r0 + u) * ldb + fc + lane] = v[u];
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < R; u++) xs[lane * R + u] = v[u];   // zero past w
+        __syncwarp();
+        // off-diagonal rows, lane = row: 16-byte loads of the row (rows are
+        // 16-byte aligned, ld >= w rounded to 4), x_j broadcast from shared
         for (int i0 = w; i0 < h; i0 += 32) {
             const int i = i0 + lane;
-            const T *row = D + (int64_t)i * ld;
+            const T *row = D + (int64_t)(i < h ? i : i0) * ld;
             T sacc[R];
 #pragma unroll
             for (int u = 0; u < R; u++) sacc[u] = T(0);
-            for (int j = 0; j < w; j++) {
-                const T rj = (i < h) ? row[j] : T(0);
+            for (int j0 = 0; j0 < w; j0 += VK) {
+                T e[VK];
+                const uint4 v4 = *reinterpret_cast<const uint4 *>(row + j0);
+                memcpy(e, &v4, 16);
 #pragma unroll
-                for (int u = 0; u < R; u++) {
-                    const T xj = shfl_v(v[u], j);
-                    if (i < h) sacc[u] += rj * xj;
-                }
+                for (int t = 0; t < VK; t++)
+                    if (j0 + t < w)
+#pragma unroll
+                        for (int u = 0; u < R; u++) sacc[u] += e[t] * xs[(j0 + t) * R + u];
             }
             if (i < h)
 #pragma unroll
                 for (int u = 0; u < R; u++) atomic_sub(&B[(int64_t)(r0 + u) * ldb + rows[i]], sacc[u]);
         }
+        __syncwarp();
     }
 }
 
@@ -534,9 +546,11 @@ __global__ void __launch_bounds__(256) k_bwd_small(Meta m, const int *__restrict
                                                    const T *__restrict__ coefL, const T *__restrict__ coefP,
                                                    T *__restrict__ B, int ldb, int nrhs, int upper, int unit,
                                                    int cjp) {
+    __shared__ __align__(16) unsigned char xs_raw[8 * 32 * R * sizeof(T)];
     const int lane = threadIdx.x & 31;
     const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (q >= ncb) return;
+    T *xs = reinterpret_cast<T *>(xs_raw) + (threadIdx.x >> 5) * 32 * R;   // [32][R]: x at 32 panel rows
     const int c = cblks[q];
     const int w = m.width[c], ld = m.ld[c], fc = m.fcol[c], h = m.height[c];
     const T *D = coefL + m.coefoff[c];
@@ -548,18 +562,32 @@ __global__ void __launch_bounds__(256) k_bwd_small(Meta m, const int *__restrict
         dinv = T(1) / (cjp ? conj_v(d) : d);
     }
     for (int r0 = 0; r0 < nrhs; r0 += R) {
-        // gather: x_j -= sum_i op(P[i][j]) x[row_i]
+        // gather: x_j -= sum_i op(P[i][j]) x[row_i]; the x of 32 rows at a
+        // time are fetched by the lanes (independent loads) into shared
+        // memory, then summed in increasing i as one lane per column
         T sacc[R];
 #pragma unroll
         for (int u = 0; u < R; u++) sacc[u] = T(0);
-        if (lane < w)
-            for (int i = w; i < h; i++) {
-                T pv = P[(int64_t)i * ld + lane];
-                if (cjp) pv = conj_v(pv);
-                const int gi = rows[i];
+        for (int i0 = w; i0 < h; i0 += 32) {
+            const int nr = min(32, h - i0);
+            if (lane < nr) {
+                const int gi = rows[i0 + lane];
 #pragma unroll
-                for (int u = 0; u < R; u++) sacc[u] += pv * B[(int64_t)(r0 + u) * ldb + gi];
+                for (int u = 0; u < R; u++) xs[lane * R + u] = B[(int64_t)(r0 + u) * ldb + gi];
             }
+            __syncwarp();
+            if (lane < w) {
+                const T *pr = P + (int64_t)i0 * ld + lane;
+#pragma unroll 4
+                for (int t = 0; t < nr; t++) {
+                    T pv = pr[(int64_t)t * ld];
+                    if (cjp) pv = conj_v(pv);
+#pragma unroll
+                    for (int u = 0; u < R; u++) sacc[u] += pv * xs[t * R + u];
+                }
+            }
+            __syncwarp();
+        }
         T v[R];
 #pragma unroll
         for (int u = 0; u < R; u++) v[u] = (lane < w) ? B[(int64_t)(r0 + u) * ldb + fc + lane] - sacc[u] : T(0);
@@ -719,12 +747,13 @@ __global__ void k_diag_scale(Meta m, const T *__restrict__ coefL, T *__restrict_
 template <typename Tin, typename Tout>
 __global__ void k_permute(int n, int nrhs, const int *__restrict__ peritab, const Tin *__restrict__ X,
                           int64_t ldx, Tout *__restrict__ Y, int64_t ldy, int backward) {
-    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t tot = (int64_t)n * nrhs;
-    for (; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-        int r = (int)(e / n), k = (int)(e - (int64_t)r * n);
-        if (!backward) Y[r * ldy + k] = (Tout)X[r * ldx + peritab[k]];
-        else Y[r * ldy + peritab[k]] = (Tout)X[r * ldx + k];
+    // one thread per row index: the permutation entry is read once for all
+    // right-hand sides, whose copies are independent loads in flight
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int p = peritab[k];
+        const int64_t src = backward ? k : p, dst = backward ? p : k;
+#pragma unroll 4
+        for (int r = 0; r < nrhs; r++) Y[r * ldy + dst] = (Tout)X[r * ldx + src];
     }
 }
 
