@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(256) k_bwd_off_direct(Meta m, const int2 *__re
 // cblks; the backward gather needs no atomics (one warp owns the cblk).
 // ---------------------------------------------------------------------------
 template <typename T, int R>
-__global__ void __launch_bounds__(256) k_fwd_small(Meta m, const int *__restrict__ cblks, int ncb,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_fwd_small(Meta m, const int *__restrict__ cblks, int ncb,
                                                    const T *__restrict__ coefL, T *__restrict__ B, int ldb, int nrhs,
                                                    int unit) {
     // R right-hand sides at a time (nrhs a multiple of R), each one's
@@ -542,7 +542,7 @@ __global__ void __launch_bounds__(256) k_fwd_small(Meta m, const int *__restrict
 // upper != 0: U of the LU diagonal block (row-major upper part, non-unit),
 // P = the U^t panel (coefP); else op(L)^t with op = conj when cjp, P = L.
 template <typename T, int R>
-__global__ void __launch_bounds__(256) k_bwd_small(Meta m, const int *__restrict__ cblks, int ncb,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_bwd_small(Meta m, const int *__restrict__ cblks, int ncb,
                                                    const T *__restrict__ coefL, const T *__restrict__ coefP,
                                                    T *__restrict__ B, int ldb, int nrhs, int upper, int unit,
                                                    int cjp) {
