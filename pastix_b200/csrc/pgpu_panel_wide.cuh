@@ -562,7 +562,7 @@ __global__ void __launch_bounds__(PS_WARPS * 32) k_panel_small(Meta m, const int
     if (lane < w)
         for (int i = 0; i < w; i++) tile[i * PBL + lane] = A[(int64_t)i * ld + lane];
     __syncwarp();
-    warp_factor_tile<T, MODE>(tile, w, crit, npiv, nneg, nbad);
+    warp_factor_tile_smem<T, MODE>(tile, w, crit, npiv, nneg, nbad);
     __syncwarp();
     if (lane < w) {
         for (int i = 0; i < w; i++)
