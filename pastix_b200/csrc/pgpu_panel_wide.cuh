@@ -520,7 +520,9 @@ __global__ void __launch_bounds__(WP_THREADS) k_panel_wide_la(Meta m, const int2
 // ---------------------------------------------------------------------------
 // Cblks of at most 32 columns (the leaves, ~10^5-10^6 of them in the
 // batched 2D problems): one warp per cblk.  The w x w diagonal block is one
-// tile, factorized in registers (warp_factor_tile), and the panel rows below
+// tile, factorized by the warp in shared memory (warp_factor_tile_smem: with
+// every warp of the SM in it, the fully unrolled register form misses in the
+// instruction cache), and the panel rows below
 // it are solved one lane per row with the row in registers -- the same
 // operations as k_panel_factor for such a cblk, without a 256-thread CTA per
 // leaf.
