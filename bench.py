@@ -425,7 +425,8 @@ def main():
         if rank == 0:
             print(json.dumps({"metric": METRIC, "arms": "mixed", "value": mixed["device_s"], "unit": "s",
                               "e2e_s": mixed["e2e_s"], "factor_ms": mixed["factor_ms"], "solve_ms": mixed["solve_ms"],
-                              "refine_ms": mixed["refine_ms"], "config": config}))
+                              "refine_ms": mixed["refine_ms"], "refine_iters": mixed["refine_iters"],
+                              "tc_ms": mixed["tc_ms_per_step"], "config": config}))
         return
     peaks = fma_peaks() if rank == 0 else {}
     barrier(pg)

@@ -215,6 +215,19 @@ PASTIX_GPU_API int pastix_gpu_task_times( pastix_gpu_t *ctx, int64_t *count, int
 PASTIX_GPU_API int pastix_gpu_set_cblk_priority( pastix_gpu_t *ctx, const double *prio );
 
 /*
+ * Phase timeline of the last numfact that launched its kernels directly (not
+ * a graph replay): one record per timed interval, info[3 r .. 3 r + 2] =
+ * {stream (0 main, 1 lookahead), phase (0 diagonal blocks, 1 panel TRSM,
+ * 2 FMA update GEMMs, 3 tensor-core update GEMMs), elimination-tree level}
+ * and times[2 r], times[2 r + 1] its start and end in ms from the start of
+ * the numfact (CUDA events).  With info or times NULL, *count receives the
+ * number of records; else up to *count are written.  The reference's
+ * counterpart is its kernel trace (kernels/kernels_trace.c), which times the
+ * CPU kernels.
+ */
+PASTIX_GPU_API int pastix_gpu_phase_log( pastix_gpu_t *ctx, int64_t *count, int64_t *info, double *times );
+
+/*
  * Kernel variants and launch shapes (the autotuner's knobs, no reference
  * counterpart; the reference's equivalents are compile-time block sizes):
  *   PGPU_TUNE_MIXED_GEMM      0 FP32 FMA, 1 TF32, 2 3xTF32 (default) update GEMMs

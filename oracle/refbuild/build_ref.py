@@ -9,8 +9,7 @@ Recipe (no reference build system is run):
      own spm stand-in (spm_standin.c) and config header;
   3. everything links into oracle/_ref/libpastix_ref.so against the
      LP64 OpenBLAS that ships with opencv-python-headless (cblas + LAPACKE
-     names), and the reference-facing driver oracle/refbuild/ref_driver.c
-     into oracle/_ref/pastix_ref_driver.
+     names).
 
 Nothing from the reference tree is copied into the repository: generated
 files and objects live only under the git-ignored oracle/_ref/.
@@ -26,7 +25,9 @@ ORACLE = os.path.dirname(HERE)
 OUT = os.path.join(ORACLE, "_ref")
 GEN = os.path.join(OUT, "gen")
 OBJ = os.path.join(OUT, "obj")
-REF = os.environ.get("PASTIX_REFERENCE_ROOT", "/root/reference")
+# the reference tree sits beside the repository (override: PASTIX_REFERENCE_ROOT)
+REF = os.environ.get("PASTIX_REFERENCE_ROOT",
+                     os.path.join(os.path.dirname(os.path.dirname(ORACLE)), "reference"))
 
 
 def find_openblas():
@@ -239,12 +240,7 @@ def main():
                                                  "-lm", "-pthread"]
     subprocess.check_call(cmd)
     build_hefix(units, blas)
-    drv = os.path.join(OUT, "pastix_ref_driver")
-    cmd = ["gcc"] + CFLAGS + includes() + [os.path.join(HERE, "ref_driver.c"), "-o", drv,
-                                           "-L" + OUT, "-lpastix_ref", "-Wl,-rpath,$ORIGIN",
-                                           blas, "-Wl,--disable-new-dtags", "-Wl,-rpath," + os.path.dirname(blas), "-lm"]
-    subprocess.check_call(cmd)
-    print("built", so, drv)
+    print("built", so)
     return 0
 
 

@@ -164,6 +164,12 @@ struct pastix_gpu_s {
     DArr<int64_t> d_seg;
     DArr<double> d_segss;               // per-system sums of squares
     std::vector<cudaEvent_t> evpool, evpool2;   // per-launch timing events (main, stream2)
+    // phase timeline of the last directly launched numfact (pastix_gpu_phase_log):
+    // {stream, phase, level} and {start, end} ms from the numfact's first event
+    std::vector<int> log_kinds2, log_levels2;
+    int log_used2 = 0;
+    std::vector<int64_t> phase_info;
+    std::vector<double> phase_times;
     DArr<double> d_fact_scal;          // [0] ||A||_F, [1] static-pivot threshold (device-side, no host trip)
     // per-task timings of the last numfact (learned cost model), when record
     bool record = false;
@@ -934,8 +940,9 @@ struct LaunchTimer {
     pastix_gpu_t &C;
     cudaStream_t st;
     std::vector<cudaEvent_t> &pool;
-    std::vector<int> kinds;
+    std::vector<int> kinds, levels;   // per mark: phase kind, factorization level (-1 outside the level loop)
     int used = 0;
+    int level = -1;
     explicit LaunchTimer(pastix_gpu_t &c) : C(c), st(c.stream), pool(c.evpool) {}
     LaunchTimer(pastix_gpu_t &c, cudaStream_t s, std::vector<cudaEvent_t> &p) : C(c), st(s), pool(p) {}
     // (inside a stream capture the record becomes an event node of the graph,
@@ -948,6 +955,7 @@ struct LaunchTimer {
             pool.push_back(e);
         }
         kinds.push_back(kind);
+        levels.push_back(level);
         // (in a capture a plain record only expresses a dependency; the
         // external form makes it an event-record node of the graph)
         return cudaEventRecordWithFlags(pool[used++], st, C.capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
@@ -1157,6 +1165,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     };
     for (int l = 0; l < C.nlevels; l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
+        tm.level = tm2.level = l;
         // the deferred updates into this level's cblks were issued on stream2 two levels back or earlier
         if (la && l >= 2) {
             PGPU_CHECK(tm.mark(PH_END));
@@ -1311,6 +1320,9 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
         C.g_kinds2 = la ? tm2.kinds : std::vector<int>();
         C.g_used2 = la ? tm2.used : 0;
     }
+    C.log_kinds2 = la ? tm2.kinds : std::vector<int>();
+    C.log_levels2 = la ? tm2.levels : std::vector<int>();
+    C.log_used2 = la ? tm2.used : 0;
     *launches = nl;
     C.stats[7] = ngemm;
     return PASTIX_GPU_SUCCESS;
@@ -1439,6 +1451,25 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     if (replayed) {   // the graph's event nodes: main stream, then the lookahead stream
         nl = C.g_nl;
         LaunchTimer::collect_marks(C.evpool2, C.g_kinds2, C.g_used2, C.side_ms, 4);
+    }
+    C.phase_info.clear();
+    C.phase_times.clear();
+    if (!replayed) {
+        // both streams' marks on one timeline: elapsed time from the numfact's first event
+        auto add = [&](int stream, const std::vector<cudaEvent_t> &pool, const std::vector<int> &kinds,
+                       const std::vector<int> &levels, int used) {
+            for (int i = 0; i + 1 < used; i++) {
+                if (kinds[i] < 0 || kinds[i] >= PH_END) continue;   // PH_END closes an untimed gap
+                float t0 = 0, t1 = 0;
+                if (cudaEventElapsedTime(&t0, C.ev[0], pool[i]) != cudaSuccess ||
+                    cudaEventElapsedTime(&t1, C.ev[0], pool[i + 1]) != cudaSuccess)
+                    continue;
+                C.phase_info.insert(C.phase_info.end(), {(int64_t)stream, (int64_t)kinds[i], (int64_t)levels[i]});
+                C.phase_times.insert(C.phase_times.end(), {(double)t0, (double)t1});
+            }
+        };
+        add(0, C.evpool, tm.kinds, tm.levels, tm.used);
+        add(1, C.evpool2, C.log_kinds2, C.log_levels2, C.log_used2);
     }
     {
         double ph[4];
@@ -2549,6 +2580,20 @@ static int task_records_impl(pastix_gpu_t *ctx, int64_t *count, int64_t *info, d
         }
     }
     *count = total;
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_phase_log(pastix_gpu_t *ctx, int64_t *count, int64_t *info, double *times) {
+    if (!ctx || !count) return PASTIX_GPU_ERR_BADPARAMETER;
+    const int64_t n = (int64_t)ctx->phase_times.size() / 2;
+    if (!info || !times) {
+        *count = n;
+        return PASTIX_GPU_SUCCESS;
+    }
+    const int64_t k = std::min<int64_t>(*count, n);
+    std::memcpy(info, ctx->phase_info.data(), 3 * k * sizeof(int64_t));
+    std::memcpy(times, ctx->phase_times.data(), 2 * k * sizeof(double));
+    *count = k;
     return PASTIX_GPU_SUCCESS;
 }
 

@@ -134,6 +134,22 @@ class Solver:
                 "tc_flops", "tc_timeouts", "graph_replayed", "reserved15"]
         return dict(zip(keys, s.tolist()))
 
+    def phase_log(self):
+        """Timeline of the last directly launched numfact: a list of
+        (stream, phase, level, start_ms, end_ms); phase 0 diagonal blocks,
+        1 panel TRSM, 2 FMA update GEMMs, 3 tensor-core update GEMMs."""
+        L = load()
+        if not hasattr(L, "_phase_log_ready"):
+            L.pastix_gpu_phase_log.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+            L._phase_log_ready = True
+        cnt = np.zeros(1, np.int64)
+        _check("pastix_gpu_phase_log", L.pastix_gpu_phase_log(self._h, _p(cnt), None, None))
+        info = np.zeros((max(int(cnt[0]), 1), 3), np.int64)
+        t = np.zeros((max(int(cnt[0]), 1), 2), np.float64)
+        _check("pastix_gpu_phase_log", L.pastix_gpu_phase_log(self._h, _p(cnt), _p(info), _p(t)))
+        k = int(cnt[0])
+        return [tuple(int(v) for v in info[i]) + (float(t[i, 0]), float(t[i, 1])) for i in range(k)]
+
     # -- structure / pattern -----------------------------------------------
     def set_structure(self, st):
         """st: dict with n, cblktab (cblknbr+1,4), bloktab (bloknbr,4), browtab, permtab, peritab."""

@@ -63,3 +63,44 @@ def test_analysis_rejects_bad_grid():
     A.grid = (5, 5, 4)
     with pytest.raises(G.PastixGpuError):
         _an().analyze(A)
+
+
+def _same_browtab(mine, ref):
+    """browtab equal as a set of facing blocks per cblk (the order inside a
+    cblk's segment follows the reference's insertion order, which the solve
+    and the update scatter do not depend on)."""
+    ct = mine["cblktab"]
+    seg = np.repeat(np.arange(ct.shape[0] - 1), np.diff(ct[:, 3]))
+    a = np.lexsort((mine["browtab"], seg))
+    b = np.lexsort((ref["browtab"], seg))
+    return np.array_equal(mine["browtab"][a], ref["browtab"][b])
+
+
+def _config_system(cid, which=0):
+    systems, meta = M.config(cid, scale=1.0, seed=0)
+    if cid == 4:
+        # the batch's smallest and largest sides, and one between
+        sides = [a.grid[0] for a in systems]
+        order = np.argsort(sides, kind="stable")
+        pick = {0: order[0], 1: order[-1], 2: order[len(order) // 2]}[which]
+        return systems[int(pick)], meta["fact"]
+    return systems[0], meta["fact"]
+
+
+@pytest.mark.skipif(not U.ref_available(), reason="reference oracle not built")
+@pytest.mark.parametrize("cid,which", [(1, 0), (2, 0), (3, 0), (5, 0), (4, 0), (4, 1), (4, 2)],
+                         ids=["C1_20^3", "C2_100^3", "C3_80^3_LU", "C5_60^3_LDLh", "C4_min_side", "C4_max_side",
+                              "C4_mid_side"])
+def test_analysis_matches_reference_at_benchmark_sizes(cid, which):
+    """The structure the benchmark factorizes is the reference's: ordering,
+    cblk/blok tables and browtab of the builder's analysis equal the
+    reference's own analysis of each benchmark configuration's matrix at its
+    full size (C2: 70 124 cblks)."""
+    A, fact = _config_system(cid, which)
+    ref, st = U.run_reference(A, fact, numfact=False)
+    g = U.gpu_structure(A, st)
+    ref.close()
+    mine = _an().analyze(A)
+    for k in ("permtab", "peritab", "cblktab", "bloktab"):
+        assert np.array_equal(mine[k], g[k]), k
+    assert _same_browtab(mine, g)
