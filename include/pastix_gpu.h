@@ -72,8 +72,11 @@ extern "C" {
 #define PGPU_GENERAL   111
 #define PGPU_SYMMETRIC 112
 #define PGPU_HERMITIAN 113
-/* spm_coeftype_t values of the input matrix */
+/* spm_coeftype_t / pastix_coeftype_t values (input matrix: DOUBLE or
+ * COMPLEX64; right-hand sides in the factor precision: FLOAT or COMPLEX32) */
+#define PGPU_FLOAT     2
 #define PGPU_DOUBLE    3
+#define PGPU_COMPLEX32 4
 #define PGPU_COMPLEX64 5
 /* pastix_refine_t (include/pastix/api.h:273-278) */
 #define PGPU_REFINE_GMRES 0
@@ -135,6 +138,28 @@ PASTIX_GPU_API int pastix_gpu_numfact( pastix_gpu_t *ctx, const void *values );
  * sopalin/sequential_ztrsm.c:536-552).
  */
 PASTIX_GPU_API int pastix_gpu_solve( pastix_gpu_t *ctx, int64_t nrhs, void *B, int64_t ldb );
+
+/*
+ * Solve steps on right-hand sides already permuted into the factorization's
+ * numbering (the pastix_rhs_t Bp of pastix_subtask_solve_adv,
+ * sopalin/pastix_task_solve.c:511): steps is a mask of
+ *   PGPU_SOLVE_FORWARD  the lower sweep, L y = b (unit L for LU and LDL),
+ *   PGPU_SOLVE_DIAG     the diagonal step of LDL^t / LDL^h (z = D^-1 y),
+ *   PGPU_SOLVE_BACKWARD the upper sweep (L^t / L^h x = z, or U x = y for LU).
+ * Each step replaces one call through the reference's solve tables:
+ * ztrsm_table (sopalin/sequential_ztrsm.c:536-552) for the sweeps and
+ * zdiag_table (sopalin/sequential_zdiag.c:298) for the diagonal.  B holds
+ * nrhs columns of leading dimension ldb in host or device memory; flttype is
+ * the arithmetic of B: PGPU_DOUBLE / PGPU_COMPLEX64 (cast to the factor
+ * precision and back on the device), or, for single-precision factors,
+ * PGPU_FLOAT / PGPU_COMPLEX32 (the reference's mixed solve hands the sweeps
+ * a single-precision copy of the right-hand sides).
+ */
+#define PGPU_SOLVE_FORWARD  1
+#define PGPU_SOLVE_DIAG     2
+#define PGPU_SOLVE_BACKWARD 4
+PASTIX_GPU_API int pastix_gpu_solve_steps( pastix_gpu_t *ctx, int steps, int64_t nrhs, void *B, int64_t ldb,
+                                           int flttype );
 
 /*
  * Allocation-free solve: A X = B in place for `nrhs` right-hand sides that

@@ -15,6 +15,11 @@ LIB = os.path.join(HERE, "_ref", "libpastix_ref.so")
 # the same build with the one-increment fix of core_zhetf2sp (see
 # oracle/refbuild/build_ref.py HEFIX): pins the LDL^h of complex matrices
 LIB_HEFIX = os.path.join(HERE, "_ref", "libpastix_ref_hefix.so")
+# the same reference sources with the GPU layer plugged into its sopalinFacto,
+# solve and refinement tables (pastix_b200/refplug/pastix_gpu_plug.c): not an
+# oracle, the drop-in under test
+LIB_GPUPLUG = os.path.join(HERE, "_ref", "libpastix_gpuplug.so")
+LIBS = {None: LIB, "hefix": LIB_HEFIX, "gpuplug": LIB_GPUPLUG}
 
 # include/pastix/api.h enumerations (iparm / dparm indices, values)
 IPARM = {k: i for i, k in enumerate("""VERBOSE IO_STRATEGY NNZEROS NNZEROS_BLOCK_LOCAL ALLOCATED_TERMS
@@ -46,14 +51,14 @@ _libs = {}
 
 
 def available(variant=None):
-    return os.path.exists(LIB_HEFIX if variant == "hefix" else LIB)
+    return os.path.exists(LIBS[variant])
 
 
 def lib(variant=None):
     if variant not in _libs:
         if not available(variant):
             raise RuntimeError("reference oracle not built: run oracle/refbuild/build_ref.py")
-        L = C.CDLL(LIB_HEFIX if variant == "hefix" else LIB)
+        L = C.CDLL(LIBS[variant])
         P, I64, I = C.c_void_p, C.c_int64, C.c_int
         L.ref_create.restype = P
         L.ref_create.argtypes = [I, I]

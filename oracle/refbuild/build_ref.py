@@ -204,6 +204,35 @@ def build_hefix(units, blas):
                            "-lm", "-pthread"])
 
 
+# Second build of the reference sources with the GPU layer plugged in
+# (pastix_b200/refplug/pastix_gpu_plug.c): the same objects, the plug, and
+# one --wrap per plug point, linked against pastix_b200/lib/libpastix_gpu.so.
+# The reference's own public API then factorizes, solves and refines on the
+# GPU (tests/test_dropin.py runs example/simple.c's call sequence on it).
+REPO = os.path.dirname(ORACLE)
+PLUG_SRC = os.path.join(REPO, "pastix_b200", "refplug", "pastix_gpu_plug.c")
+GPU_LIBDIR = os.path.join(REPO, "pastix_b200", "lib")
+PLUG_WRAPS = (["coeftabInit", "pastixFinalize"] +
+              ["sopalin_%s%s" % (p, f) for p in "sdcz" for f in ("potrf", "getrf", "sytrf", "trsm", "diag")] +
+              ["sopalin_chetrf", "sopalin_zhetrf"] +
+              ["%s_%s_smp" % (p, f) for p in "dz" for f in ("grad", "gmres")])
+
+
+def build_gpuplug(units, blas):
+    if not os.path.exists(os.path.join(GPU_LIBDIR, "libpastix_gpu.so")):
+        print("libpastix_gpu.so not built; skipping the GPU-plugged reference build")
+        return
+    obj = os.path.join(OBJ, "pastix_gpu_plug.o")
+    cmd = ["gcc"] + CFLAGS + includes() + ["-I" + os.path.join(REPO, "include"), "-c", PLUG_SRC, "-o", obj]
+    subprocess.check_call(cmd)
+    so = os.path.join(OUT, "libpastix_gpuplug.so")
+    wraps = ["-Wl,--wrap=" + w for w in PLUG_WRAPS]
+    subprocess.check_call(["gcc", "-shared", "-o", so] + [u[2] for u in units] + [obj] + wraps +
+                          ["-L" + GPU_LIBDIR, "-lpastix_gpu",
+                           "-Wl,-rpath,$ORIGIN/../../pastix_b200/lib", blas, "-Wl,-Bsymbolic",
+                           "-Wl,--disable-new-dtags", "-Wl,-rpath," + os.path.dirname(blas), "-lm", "-pthread"])
+
+
 def main():
     if not os.path.isdir(REF):
         print("reference tree not present; skipping the reference build")
@@ -240,6 +269,7 @@ def main():
                                                  "-lm", "-pthread"]
     subprocess.check_call(cmd)
     build_hefix(units, blas)
+    build_gpuplug(units, blas)
     print("built", so)
     return 0
 

@@ -184,6 +184,18 @@ struct pastix_gpu_s {
     // operand kind), split jobs {cblk, row, panel, -} per level
     bool tma = false;
     DArr<float> d_hilo, d_ihilo;
+    // 3xFP16 operands (mixed GEMM mode 3): FP16 hi / lo planes [2][h16_plane]
+    // of the source matrices, per-row inverse scales, and per operand map its
+    // first element (d_hoff) and first scale (d_hsbase)
+    bool h16 = false;
+    DArr<__half> d_h16;
+    DArr<float> d_hscale;
+    DArr<int64_t> d_hoff, d_hsbase;
+    int64_t h16_plane = 0;
+    // per task {target-row map base, A row-scale base, B row-scale base} and
+    // the target rows of the tensor-core update tasks (k_task_rowmap)
+    DArr<int64_t> d_taux;
+    DArr<int> d_tmap, d_tlist;
     int64_t hilo_plane = 0, ihilo_plane = 0;
     DArr<CUtensorMap> d_tmaps;
     DArr<int> d_mapidx;
@@ -546,11 +558,13 @@ static const int TRSM_TR = 32;   // panel rows per k_trsm_rows CTA
 // PGPU_TUNE_TRSM_GEMM (PASTIX_GPU_TRSM=rows disables the TRSM-as-GEMM path),
 // PGPU_TUNE_TRSM_GEMM_ROWS (256: panels taller than this take it),
 // PGPU_TUNE_TC_MIN_MN (8192: smallest M x N sent to the tensor cores).
-enum { MG_FP32 = 0, MG_TF32 = 1, MG_3XTF32 = 2 };
+enum { MG_FP32 = 0, MG_TF32 = 1, MG_3XTF32 = 2, MG_3XF16 = 3 };
 static void default_tuning(int64_t *t) {
     const char *e = getenv("PASTIX_GPU_MIXED_GEMM");
-    t[PGPU_TUNE_MIXED_GEMM] = (e && std::strcmp(e, "fp32") == 0) ? MG_FP32
-                              : (e && std::strcmp(e, "tf32") == 0) ? MG_TF32 : MG_3XTF32;
+    t[PGPU_TUNE_MIXED_GEMM] = (e && std::strcmp(e, "fp32") == 0)     ? MG_FP32
+                              : (e && std::strcmp(e, "tf32") == 0)   ? MG_TF32
+                              : (e && std::strcmp(e, "3xf16") == 0) ? MG_3XF16
+                                                                     : MG_3XTF32;
     e = getenv("PASTIX_GPU_TC_KERNEL");
     t[PGPU_TUNE_TC_KERNEL] = (e && std::strcmp(e, "tile") == 0) ? 0 : 1;
     e = getenv("PASTIX_GPU_LOOKAHEAD");
@@ -594,6 +608,20 @@ static bool encode_panel_map(CUtensorMap *map, float *base, int w, int rows, int
     const cuuint32_t box[3] = {(cuuint32_t)TC_BK, (cuuint32_t)TC_BM, (cuuint32_t)planes};
     const cuuint32_t estr[3] = {1, 1, 1};
     return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+// 3-D map {K = w, rows, 2 planes} over FP16 rows of ld16 halves, box
+// {64, 128, 2} (128-byte rows, SWIZZLE_128B): one box lands the hi and the lo
+// tile of a k-block.
+static bool encode_h16_map(CUtensorMap *map, __half *base, int w, int rows, int ld16, int64_t plane) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)w, (cuuint64_t)rows, 2};
+    const cuuint64_t strides[2] = {(cuuint64_t)ld16 * 2, (cuuint64_t)plane * 2};
+    const cuuint32_t box[3] = {64, (cuuint32_t)TC_BM, 2};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -797,10 +825,79 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     }
     // TMA operands (3xTF32, persistent kernel): hi/lo mirrors, tensor maps of
     // the source cblks, split jobs of their off-diagonal rows per level
-    C.tma = use_tc && mixed_gemm_mode(C) == MG_3XTF32 && C.tune[PGPU_TUNE_TC_KERNEL] != 0 && !C.record &&
+    C.tma = use_tc && (mixed_gemm_mode(C) == MG_3XTF32 || mixed_gemm_mode(C) == MG_3XF16) &&
+            C.tune[PGPU_TUNE_TC_KERNEL] != 0 && !C.record &&
             C.tune[PGPU_TUNE_TC_TMA] != 0 && tensor_map_encoder() != nullptr;
     C.split_ptr.assign(C.nlevels + 1, 0);
-    if (C.tma) {
+    C.h16 = C.tma && mixed_gemm_mode(C) == MG_3XF16;
+    std::vector<int> mapidx_h;        // (3xFP16) operand maps of each source cblk, for the task scale bases
+    std::vector<int64_t> hsbase_h;
+    if (C.h16) {
+        // 3xFP16: FP16 planes and row scales of the source matrices only (the
+        // panels and inverses that feed a tensor-core task), in level order
+        std::vector<char> src(C.cblknbr, 0);
+        for (const int4 &t : tctiles) src[tasks[t.x].c] = 1;
+        for (const int4 &t : tttiles) src[tasks[t.x].c] = 1;
+        std::vector<int> mapidx(C.cblknbr, -1);
+        std::vector<int64_t> hoff, hsbase;
+        int64_t hp = 0, sp = 0;
+        auto needed = [&](int c, int kind) {
+            return kind == TMAP_L || (kind == TMAP_U && lu) || (kind == TMAP_I && C.invoff[c] >= 0) ||
+                   (kind == TMAP_I2 && lu && C.invoff[c] >= 0);
+        };
+        for (int l = 0; l < C.nlevels; l++)
+            for (int q = C.lvl_ptr[l]; q < C.lvl_ptr[l + 1]; q++) {
+                const int c = C.lvl_cblks[q];
+                if (!src[c]) continue;
+                const int w = C.width[c];
+                mapidx[c] = (int)hoff.size();
+                for (int kind = 0; kind < TMAP_KINDS; kind++) {
+                    const bool nd = needed(c, kind);
+                    const int rows = kind < TMAP_I ? C.height[c] : w;
+                    hoff.push_back(nd ? hp : -1);
+                    hsbase.push_back(nd ? sp : -1);
+                    if (nd) {
+                        hp += round_up((int64_t)rows * ld16_of(w), 64);
+                        sp += rows;
+                    }
+                }
+            }
+        C.h16_plane = round_up(std::max<int64_t>(hp, 64), 64);
+        if (C.d_h16.n < (size_t)(2 * C.h16_plane)) PGPU_CHECK(C.d_h16.alloc(2 * C.h16_plane));
+        if (C.d_hscale.n < (size_t)std::max<int64_t>(sp, 1)) PGPU_CHECK(C.d_hscale.alloc(std::max<int64_t>(sp, 1)));
+        std::vector<CUtensorMap> maps(hoff.size());
+        if (!maps.empty()) std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+        std::vector<int4> split;
+        for (int l = 0; l < C.nlevels && C.tma; l++) {
+            for (int q = C.lvl_ptr[l]; q < C.lvl_ptr[l + 1]; q++) {
+                const int c = C.lvl_cblks[q];
+                if (mapidx[c] < 0) continue;
+                const int w = C.width[c], h = C.height[c];
+                for (int kind = 0; kind < TMAP_KINDS; kind++) {
+                    const int mi = mapidx[c] + kind;
+                    if (hoff[mi] < 0) continue;
+                    const int rows = kind < TMAP_I ? h : w;
+                    if (!encode_h16_map(&maps[mi], C.d_h16.p + hoff[mi], w, rows, ld16_of(w), C.h16_plane))
+                        C.tma = false;
+                    // panels: their off-diagonal rows; inverses: all rows
+                    for (int r0 = kind < TMAP_I ? w : 0; r0 < rows; r0 += 32) split.push_back(make_int4(c, r0, kind, 0));
+                }
+            }
+            C.split_ptr[l + 1] = (int)split.size();
+        }
+        if (C.tma) {
+            PGPU_CHECK(C.d_tmaps.upload(maps, C.stream));
+            PGPU_CHECK(C.d_mapidx.upload(mapidx, C.stream));
+            PGPU_CHECK(C.d_split.upload(split, C.stream));
+            PGPU_CHECK(C.d_hoff.upload(hoff, C.stream));
+            PGPU_CHECK(C.d_hsbase.upload(hsbase, C.stream));
+            mapidx_h.swap(mapidx);
+            hsbase_h.swap(hsbase);
+        } else {
+            C.h16 = false;
+            C.split_ptr.assign(C.nlevels + 1, 0);
+        }
+    } else if (C.tma) {
         std::vector<char> src(C.cblknbr, 0);
         for (const int4 &t : tctiles) src[tasks[t.x].c] = 1;
         for (const int4 &t : tttiles) src[tasks[t.x].c] = 1;
@@ -843,6 +940,12 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
             PGPU_CHECK(C.d_tmaps.upload(maps, C.stream));
             PGPU_CHECK(C.d_mapidx.upload(mapidx, C.stream));
             PGPU_CHECK(C.d_split.upload(split, C.stream));
+        } else {
+            C.split_ptr.assign(C.nlevels + 1, 0);
+        }
+    }
+    if (C.tma) {
+        {
             // pairs of 128-row tiles (tm even, tm + 1) of one task and column block
             // share their B tile in the TMA kernel: one entry {task, tm, tn, 1}
             // (a launch with fewer tiles than two per SM keeps them single: pairs
@@ -890,8 +993,6 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
             C.tctile_ptr.swap(tc_ptr);
             C.tctile_crit.swap(tc_crit);
             C.tttile_ptr.swap(tt_ptr);
-        } else {
-            C.split_ptr.assign(C.nlevels + 1, 0);
         }
     }
     if (tgemm) {
@@ -917,6 +1018,37 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     PGPU_CHECK(C.d_tctiles.upload(tctiles, s));
     PGPU_CHECK(C.d_trsm.upload(trsm, s));
     PGPU_CHECK(C.d_tasks.upload(tasks, s));
+    if (C.tma) {
+        // tensor-core tasks: target-row maps (built on the device) and scale bases
+        std::vector<int64_t> taux(3 * tasks.size(), 0);
+        std::vector<char> is_tc(tasks.size(), 0);
+        for (const int4 &t : tctiles) is_tc[t.x] = 1;
+        std::vector<int> tlist;
+        int64_t rows = 0;
+        for (size_t i = 0; i < tasks.size(); i++) {
+            const GemmTask &g = tasks[i];
+            const bool trsm = (g.flags & 64) != 0;
+            if (is_tc[i] && !trsm) {
+                taux[3 * i] = rows;
+                rows += g.M;
+                tlist.push_back((int)i);
+            }
+            if (C.h16 && (is_tc[i] || trsm) && mapidx_h[g.c] >= 0) {
+                const int mb = mapidx_h[g.c];
+                const int ka = (g.flags & 1) ? TMAP_U : TMAP_L;
+                const int kb = trsm ? ((g.flags & 128) ? TMAP_I2 : TMAP_I) : ((g.flags & 2) ? TMAP_U : TMAP_L);
+                taux[3 * i + 1] = hsbase_h[mb + ka] + g.arow0;
+                taux[3 * i + 2] = hsbase_h[mb + kb] + (trsm ? 0 : C.browoff[g.b]);
+            }
+        }
+        PGPU_CHECK(C.d_taux.upload(taux, s));
+        PGPU_CHECK(C.d_tlist.upload(tlist, s));
+        if (C.d_tmap.n < (size_t)std::max<int64_t>(rows, 1)) PGPU_CHECK(C.d_tmap.alloc(std::max<int64_t>(rows, 1)));
+        if (!tlist.empty())
+            k_task_rowmap<<<(int)tlist.size(), 256, 0, s>>>(C.meta, C.d_tasks.p, C.d_tlist.p, C.d_taux.p,
+                                                            C.d_tmap.p);
+        PGPU_CHECK(cudaGetLastError());
+    }
     PGPU_CHECK(C.d_pjobs.upload(pjobs, s));
     PGPU_CHECK(C.d_sjobs.upload(sjobs, s));
     PGPU_CHECK(C.d_wjobs.upload(wjobs, s));
@@ -1056,7 +1188,8 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     PGPU_CHECK(cudaFuncSetAttribute(kpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(ktrsm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(k_tri_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
-    const bool split = (mixed_gemm_mode(C) == MG_3XTF32);
+    // split products (3xTF32; the 3xFP16 mode without TMA operands falls back to it)
+    const bool split = (mixed_gemm_mode(C) == MG_3XTF32 || mixed_gemm_mode(C) == MG_3XF16);
     const bool persist = C.tune[PGPU_TUNE_TC_KERNEL] != 0 && !C.record;   // task timings need one tile per CTA
     int nsm = 148;
     if constexpr (std::is_same<T, float>::value) {
@@ -1070,6 +1203,8 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, tcp_smem_bytes<true>()));
         PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         tma_smem_bytes<true>()));
+        PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_tc_tma<true, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<true>()));
         PGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, C.device));
     }
     int64_t *prof[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -1101,7 +1236,13 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     auto split_level = [&](int l) {
         if constexpr (std::is_same<T, float>::value) {
             const int nsp = C.split_ptr[l + 1] - C.split_ptr[l];
-            if (C.tma && nsp) {
+            if (C.tma && C.h16 && nsp) {
+                k_split_rows_h16<<<nsp, 256, 0, s>>>(C.meta, C.d_split.p + C.split_ptr[l], coefL, coefU,
+                                                     reinterpret_cast<const float *>(C.d_inv.p), C.d_h16.p,
+                                                     C.h16_plane, C.d_hscale.p, C.d_hoff.p, C.d_hsbase.p,
+                                                     C.d_mapidx.p);
+                nl++;
+            } else if (C.tma && nsp) {
                 k_split_rows<<<nsp, 256, 0, s>>>(C.meta, C.d_split.p + C.split_ptr[l], coefL, coefU, C.d_hilo.p,
                                                  C.hilo_plane, C.coefnbr);
                 nl++;
@@ -1132,11 +1273,16 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
         if constexpr (std::is_same<T, float>::value) {
             if (ntc) {
                 PGPU_CHECK(lt.mark(PH_TC));
-                if (persist && C.tma) {
+                if (persist && C.tma && C.h16) {
+                    const int g = std::min(ntc, gcap);
+                    k_gemm_scatter_tc_tma<true, true><<<g, TMA_THREADS, tma_smem_bytes<true>(), st>>>(
+                        C.meta, C.d_tctiles.p + c0, ntc, C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr,
+                        C.d_tmaps.p, C.d_mapidx.p, C.d_tmap.p, C.d_taux.p, C.d_hscale.p);
+                } else if (persist && C.tma) {
                     const int g = std::min(ntc, gcap);
                     k_gemm_scatter_tc_tma<true><<<g, TMA_THREADS, tma_smem_bytes<true>(), st>>>(
                         C.meta, C.d_tctiles.p + c0, ntc, C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr,
-                        C.d_tmaps.p, C.d_mapidx.p);
+                        C.d_tmaps.p, C.d_mapidx.p, C.d_tmap.p, C.d_taux.p);
                 } else if (persist) {
                     const int g = std::min(ntc, gcap);
                     if (split)
@@ -1234,7 +1380,8 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             k_tri_inverse<T><<<nij, 256, ism, s>>>(C.meta, C.d_invjobs.p + C.inv_ptr[l], coefL, inv,
                                                    fm_ldl(fmode) ? 1 : 0, (CPX && fm_conj(fmode)) ? 1 : 0,
                                                    fm_ldl(fmode) ? 1 : 0, lu ? 1 : 0, kch,
-                                                   C.tma ? hilo_of<T>(C.d_ihilo.p) : nullptr, C.ihilo_plane);
+                                                   (C.tma && !C.h16) ? hilo_of<T>(C.d_ihilo.p) : nullptr,
+                                                   C.ihilo_plane);
             nl++;
             split_level(l);
             const int ntt = C.ttile_ptr[l + 1] - C.ttile_ptr[l];
@@ -1247,10 +1394,14 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                 const int ntc = C.tttile_ptr[l + 1] - C.tttile_ptr[l];
                 if (ntc) {
                     const int g = std::min(ntc, nsm);
-                    if (C.tma)
+                    if (C.tma && C.h16)
+                        k_gemm_scatter_tc_tma<true, true><<<g, TMA_THREADS, tma_smem_bytes<true>(), s>>>(
+                            C.meta, C.d_tttiles.p + C.tttile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
+                            scr, C.d_tmaps.p, C.d_mapidx.p, C.d_tmap.p, C.d_taux.p, C.d_hscale.p);
+                    else if (C.tma)
                         k_gemm_scatter_tc_tma<true><<<g, TMA_THREADS, tma_smem_bytes<true>(), s>>>(
                             C.meta, C.d_tttiles.p + C.tttile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
-                            scr, C.d_tmaps.p, C.d_mapidx.p);
+                            scr, C.d_tmaps.p, C.d_mapidx.p, C.d_tmap.p, C.d_taux.p);
                     else if (split)
                         k_gemm_scatter_tc_persistent<true><<<g, TCP_THREADS, tcp_smem_bytes<true>(), s>>>(
                             C.meta, C.d_tttiles.p + C.tttile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
@@ -1262,9 +1413,19 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                     nl++;
                 }
             }
-            k_trsm_copyback<T><<<ntr, 256, 0, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], C.d_scroff.p, scr, coefL,
-                                                   coefU, C.tma ? hilo_of<T>(C.d_hilo.p) : nullptr, C.hilo_plane,
-                                                   C.coefnbr);
+            bool copied = false;
+            if constexpr (std::is_same<T, float>::value) {
+                if (C.tma && C.h16) {
+                    k_trsm_copyback_h16<<<ntr, 256, 0, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], C.d_scroff.p, scr,
+                                                            coefL, coefU, C.d_h16.p, C.h16_plane, C.d_hscale.p,
+                                                            C.d_hoff.p, C.d_hsbase.p, C.d_mapidx.p);
+                    copied = true;
+                }
+            }
+            if (!copied)
+                k_trsm_copyback<T><<<ntr, 256, 0, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], C.d_scroff.p, scr, coefL,
+                                                       coefU, C.tma ? hilo_of<T>(C.d_hilo.p) : nullptr, C.hilo_plane,
+                                                       C.coefnbr);
             nl++;
         } else if (ntr) {
             const size_t fixed = ((size_t)TRSM_TR * (mw + 1) + PB * PBL) * sizeof(T);
@@ -1517,7 +1678,8 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
 // solve, sequential_zdiag.c; backward op(L)^t or U).
 // --------------------------------------------------------------------------
 template <typename T>
-static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
+// steps: PGPU_SOLVE_FORWARD | PGPU_SOLVE_DIAG | PGPU_SOLVE_BACKWARD (all three: a full solve)
+static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches, int steps = 7) {
     const int fm = C.fact_mode;
     const bool lu = (fm == FM_GETRF), ldl = fm_ldl(fm);
     const int cjp = fm_conj(fm) ? 1 : 0;
@@ -1564,7 +1726,7 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
     };
     // levels of narrow, short cblks: one warp per cblk, diagonal and off-diagonal parts in one launch
     auto small_level = [&](int l) { return C.lvl_maxw[l] <= 32 && C.lvl_maxh[l] <= SOLVE_SMALL_MAXH; };
-    for (int l = 0; l < C.nlevels; l++) {
+    for (int l = 0; l < ((steps & PGPU_SOLVE_FORWARD) ? C.nlevels : 0); l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
         if (small_level(l)) {
@@ -1609,12 +1771,12 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches) {
             nl++;
         }
     }
-    if (ldl) {
+    if (ldl && (steps & PGPU_SOLVE_DIAG)) {
         PGPU_CHECK(mark(2));
         k_diag_scale<T><<<std::min(C.cblknbr, 4096), 128, 0, s>>>(C.meta, coefL, W, ldb, nrhs);
         nl++;
     }
-    for (int l = C.nlevels - 1; l >= 0; l--) {
+    for (int l = (steps & PGPU_SOLVE_BACKWARD) ? C.nlevels - 1 : -1; l >= 0; l--) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
         if (small_level(l)) {
@@ -1687,21 +1849,25 @@ static int ensure_work(pastix_gpu_t &C) {
 }
 
 // Permute in (down-casting for single-precision factors), solve, permute out.
+// permuted: dB is already in the factorization's numbering (only the cast
+// to and from the factor precision happens around the solve steps)
 template <typename S, typename T>
-static int solve_block_t(pastix_gpu_t &C, S *dB, int64_t ldb, int nrhs, T *W, int *launches) {
+static int solve_block_t(pastix_gpu_t &C, S *dB, int64_t ldb, int nrhs, T *W, int *launches, int steps = 7,
+                         bool permuted = false) {
     // complex128 factors: at most 8 right-hand sides per pass (shared-memory staging of the solve kernels)
     if (sizeof(T) == 16 && nrhs > 8) {
-        int rc = solve_block_t<S, T>(C, dB, ldb, 8, W, launches);
+        int rc = solve_block_t<S, T>(C, dB, ldb, 8, W, launches, steps, permuted);
         if (rc) return rc;
-        return solve_block_t<S, T>(C, dB + 8 * ldb, ldb, nrhs - 8, W, launches);
+        return solve_block_t<S, T>(C, dB + 8 * ldb, ldb, nrhs - 8, W, launches, steps, permuted);
     }
     cudaStream_t s = C.stream;
     const int n = C.n;
     const int grid = std::min(4096, cdiv((int64_t)n * nrhs, 256));
-    k_permute<S, T><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, dB, ldb, W, n, 0);
-    int rc = solve_permuted<T>(C, W, nrhs, launches);
+    const int *perm = permuted ? nullptr : C.d_peritab.p;
+    k_permute<S, T><<<grid, 256, 0, s>>>(n, nrhs, perm, dB, ldb, W, n, 0);
+    int rc = solve_permuted<T>(C, W, nrhs, launches, steps);
     if (rc) return rc;
-    k_permute<T, S><<<grid, 256, 0, s>>>(n, nrhs, C.d_peritab.p, W, n, dB, ldb, 1);
+    k_permute<T, S><<<grid, 256, 0, s>>>(n, nrhs, perm, W, n, dB, ldb, 1);
     *launches += 2;
     PGPU_CHECK(cudaGetLastError());
     return PASTIX_GPU_SUCCESS;
@@ -1716,6 +1882,79 @@ static int solve_device_block(pastix_gpu_t &C, void *dB, int64_t ldb, int nrhs, 
     }
     if (C.coef_float) return solve_block_t<double, float>(C, (double *)dB, ldb, nrhs, (float *)W, launches);
     return solve_block_t<double, double>(C, (double *)dB, ldb, nrhs, (double *)W, launches);
+}
+
+// Solve steps on right-hand sides already in the factorization's numbering
+// (pastix_gpu_solve_steps): FP64 data goes through the cast of
+// solve_block_t, factor-precision data is solved in place in the work block.
+template <typename T>
+static int steps_native(pastix_gpu_t &C, int steps, int nr, char *db, int64_t dld, int *launches) {
+    cudaStream_t s = C.stream;
+    T *W = reinterpret_cast<T *>(C.d_work.p);
+    PGPU_CHECK(cudaMemcpy2DAsync(W, (size_t)C.n * sizeof(T), db, dld * sizeof(T), (size_t)C.n * sizeof(T), nr,
+                                 cudaMemcpyDeviceToDevice, s));
+    const int step_rhs = sizeof(T) == 16 ? 8 : nr;   // (complex128 factors: 8 at a time, as solve_block_t)
+    for (int r = 0; r < nr; r += step_rhs) {
+        int rc = solve_permuted<T>(C, W + (int64_t)r * C.n, std::min(step_rhs, nr - r), launches, steps);
+        if (rc) return rc;
+    }
+    PGPU_CHECK(cudaMemcpy2DAsync(db, dld * sizeof(T), W, (size_t)C.n * sizeof(T), (size_t)C.n * sizeof(T), nr,
+                                 cudaMemcpyDeviceToDevice, s));
+    return PASTIX_GPU_SUCCESS;
+}
+
+extern "C" int pastix_gpu_solve_steps(pastix_gpu_t *ctx, int steps, int64_t nrhs, void *B, int64_t ldb,
+                                      int flttype) {
+    if (!ctx || !B || nrhs <= 0 || ldb < ctx->n || steps <= 0 || steps > 7) return PASTIX_GPU_ERR_BADPARAMETER;
+    auto &C = *ctx;
+    if (C.fact_done < 0) return PASTIX_GPU_ERR_BADPARAMETER;
+    const bool zc = (C.flttype == PGPU_COMPLEX64);
+    const bool fp64_data = flttype == (zc ? PGPU_COMPLEX64 : PGPU_DOUBLE);
+    const bool native = C.coef_float && flttype == (zc ? PGPU_COMPLEX32 : PGPU_FLOAT);
+    if (!fp64_data && !native) return PASTIX_GPU_ERR_BADPARAMETER;
+    PGPU_CHECK(cudaSetDevice(C.device));
+    int rc = ensure_work(C);
+    if (rc) return rc;
+    cudaStream_t s = C.stream;
+    const bool dev = is_device_ptr(B);
+    int launches = 0;
+    PGPU_CHECK(cudaEventRecord(C.ev[2], s));
+    const size_t es = fp64_data ? rhs_esz(C) : coef_esz(C);
+    for (int64_t r0 = 0; r0 < nrhs; r0 += SOLVE_MAXRHS) {
+        const int nr = (int)std::min<int64_t>(SOLVE_MAXRHS, nrhs - r0);
+        char *hb = reinterpret_cast<char *>(B) + r0 * ldb * es;
+        char *db = hb;
+        int64_t dld = ldb;
+        if (!dev) {
+            db = reinterpret_cast<char *>(C.d_rhs.p);
+            dld = C.n;
+            PGPU_CHECK(cudaMemcpy2DAsync(db, C.n * es, hb, ldb * es, C.n * es, nr, cudaMemcpyHostToDevice, s));
+        }
+        if (fp64_data) {
+            if (zc)
+                rc = C.coef_float ? solve_block_t<cdouble, cfloat>(C, (cdouble *)db, dld, nr, (cfloat *)C.d_work.p,
+                                                                   &launches, steps, true)
+                                  : solve_block_t<cdouble, cdouble>(C, (cdouble *)db, dld, nr,
+                                                                    (cdouble *)C.d_work.p, &launches, steps, true);
+            else
+                rc = C.coef_float ? solve_block_t<double, float>(C, (double *)db, dld, nr, (float *)C.d_work.p,
+                                                                 &launches, steps, true)
+                                  : solve_block_t<double, double>(C, (double *)db, dld, nr, (double *)C.d_work.p,
+                                                                  &launches, steps, true);
+        } else {
+            rc = zc ? steps_native<cfloat>(C, steps, nr, db, dld, &launches)
+                    : steps_native<float>(C, steps, nr, db, dld, &launches);
+        }
+        if (rc) return rc;
+        if (!dev) PGPU_CHECK(cudaMemcpy2DAsync(hb, ldb * es, db, C.n * es, C.n * es, nr, cudaMemcpyDeviceToHost, s));
+    }
+    PGPU_CHECK(cudaEventRecord(C.ev[3], s));
+    PGPU_CHECK(cudaStreamSynchronize(s));
+    float ms = 0;
+    PGPU_CHECK(cudaEventElapsedTime(&ms, C.ev[2], C.ev[3]));
+    C.stats[1] = launches;
+    C.stats[4] = ms;
+    return PASTIX_GPU_SUCCESS;
 }
 
 extern "C" int pastix_gpu_solve(pastix_gpu_t *ctx, int64_t nrhs, void *B, int64_t ldb) {
@@ -2616,7 +2855,7 @@ extern "C" int pastix_gpu_set_cblk_priority(pastix_gpu_t *ctx, const double *pri
 
 extern "C" int pastix_gpu_set_tuning(pastix_gpu_t *ctx, int key, int64_t value) {
     if (!ctx || key < 0 || key >= PGPU_TUNE_COUNT) return PASTIX_GPU_ERR_BADPARAMETER;
-    if (key == PGPU_TUNE_MIXED_GEMM && (value < MG_FP32 || value > MG_3XTF32)) return PASTIX_GPU_ERR_BADPARAMETER;
+    if (key == PGPU_TUNE_MIXED_GEMM && (value < MG_FP32 || value > MG_3XF16)) return PASTIX_GPU_ERR_BADPARAMETER;
     if ((key == PGPU_TUNE_TRSM_GEMM_ROWS && value < 32) || (key == PGPU_TUNE_LA_RESERVED_SMS && value < 0) ||
         (key == PGPU_TUNE_TC_MIN_MN && value < 0) || (key == PGPU_TUNE_WIDE_PANEL && value < 0) || (key == PGPU_TUNE_TC_PAIR_MIN && value < -1))
         return PASTIX_GPU_ERR_BADPARAMETER;

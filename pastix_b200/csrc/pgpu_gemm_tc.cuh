@@ -68,6 +68,10 @@ __device__ __forceinline__ uint32_t tc_idesc(int n = TC_BN) {
     return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
 }
 __device__ __forceinline__ int tc_mma_n(int ncols) { return min(TC_BN, (ncols + 15) & ~15); }
+// The same for kind::f16 with FP16 A and B (format 0) and FP32 D.
+__device__ __forceinline__ uint32_t tc_idesc_f16(int n = TC_BN) {
+    return (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+}
 
 __device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
@@ -101,6 +105,18 @@ __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc, uint64_t b
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+        : "memory");
+}
+
+// kind::f16 (FP16 operands, K = 16 per instruction: 32 bytes of a 128-byte
+// swizzled row, the same descriptor step as the TF32 form's K = 8).
+__device__ __forceinline__ void tc_mma_f16(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                           uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
         : "memory");
 }

@@ -28,6 +28,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_fp16.h>
 
 #include "pgpu_common.cuh"
 #include "pgpu_factor.cuh"
@@ -35,8 +36,12 @@
 
 namespace pgpu {
 
-constexpr int TMA_THREADS = 192;
+// warps 0-3 and 6-9 write back the accumulators (two warps per TMEM lane
+// quarter, each taking every other 32-column chunk), warp 4 loads, warp 5
+// issues the MMAs
+constexpr int TMA_THREADS = 320, TMA_EPI_WARPS = 8;
 constexpr int TMA_PROD_WARP = 4, TMA_MMA_WARP = 5;
+constexpr int TMA_EPI_BYTES = TMA_EPI_WARPS * 32 * 33 * 4;
 // operand maps per cblk: L panel, U panel (LU), first / second diagonal-block inverse
 enum { TMAP_L = 0, TMAP_U = 1, TMAP_I = 2, TMAP_I2 = 3, TMAP_KINDS = 4 };
 
@@ -48,7 +53,7 @@ template <> struct TmaCfg<true> { static constexpr int STAGES = 2, TILES = 6, PL
 constexpr int TMA_TMEM_COLS = 512;   // two accumulator buffers x (two 128-column halves)
 template <bool SPLIT>
 constexpr int tma_smem_bytes() {
-    return TmaCfg<SPLIT>::STAGES * TmaCfg<SPLIT>::TILES * TC_TILE_BYTES + TCP_EPI_BYTES + 1024;
+    return TmaCfg<SPLIT>::STAGES * TmaCfg<SPLIT>::TILES * TC_TILE_BYTES + TMA_EPI_BYTES + 1024;
 }
 
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t addr, uint32_t bytes) {
@@ -65,24 +70,37 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
-template <bool SPLIT>
+// F16 (with SPLIT): "3xFP16" operands -- every row r of a source matrix
+// (panel rows, diagonal-block inverse rows) is scaled by a power of two
+// 2^e_r that brings its largest magnitude into [2^14, 2^15), then split into
+// hi = fp16(x 2^e_r) and lo = fp16(x 2^e_r - hi) (both round to nearest):
+// 11 + 11 significant bits, the precision of the 3xTF32 split, in half the
+// bytes, on the FP16 MMA rate (twice the TF32 rate).  The k-block is 64
+// halves (128 bytes, the same SWIZZLE_128B tile as 32 floats) and each MMA
+// covers K = 16.  The epilogue multiplies the accumulator by the rows'
+// inverse scales 2^-e_a 2^-e_b (hscale, one float per source row; hsbase
+// gives each operand map's first row there), exact powers of two.
+template <bool SPLIT, bool F16 = false>
 __global__ void __launch_bounds__(TMA_THREADS, 1)
     k_gemm_scatter_tc_tma(Meta m, const int4 *__restrict__ tiles, int ntiles, const GemmTask *__restrict__ tasks,
                           float *__restrict__ coefL, float *__restrict__ coefU, Status *st, float *__restrict__ scr,
-                          const CUtensorMap *__restrict__ maps, const int *__restrict__ mapidx) {
+                          const CUtensorMap *__restrict__ maps, const int *__restrict__ mapidx,
+                          const int *__restrict__ tmap, const int64_t *__restrict__ taux,
+                          const float *__restrict__ hscale = nullptr) {
+    static_assert(!F16 || SPLIT, "the FP16 operands are always split");
     constexpr int S = TmaCfg<SPLIT>::STAGES, NT = TmaCfg<SPLIT>::TILES, PL = TmaCfg<SPLIT>::PL;
+    constexpr int BK = F16 ? 64 : TC_BK;                              // elements per k-block (128 B per row)
     constexpr uint32_t BOX_BYTES = (uint32_t)PL * TC_TILE_BYTES;   // one operand box (hi [+ lo])
     constexpr int QA1 = PL, QB = 2 * PL;                            // tile slots of A1 and B in a stage
     extern __shared__ __align__(16) unsigned char tc_smem_raw[];
     __shared__ __align__(8) uint64_t full[S], empty[S], accf[2], acce[2], drained;
     __shared__ uint32_t tmem_base_s;
     __shared__ int fail_s;
-    __shared__ int trow_s[2][TC_BM];
 
     const uint32_t raw = smem_u32(tc_smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     unsigned char *sbase = tc_smem_raw + (base - raw);
-    float *epi = reinterpret_cast<float *>(sbase + S * NT * TC_TILE_BYTES);   // [4][32][33]
+    float *epi = reinterpret_cast<float *>(sbase + S * NT * TC_TILE_BYTES);   // [8][32][33]
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == TMA_MMA_WARP) {
@@ -98,7 +116,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(smem_u32(&accf[b]), 1);
-            mbar_init(smem_u32(&acce[b]), 4);
+            mbar_init(smem_u32(&acce[b]), TMA_EPI_WARPS);
         }
         mbar_init(smem_u32(&drained), 1);
         fail_s = 0;
@@ -130,7 +148,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                 o.mb = maps + mb + (trsm ? ((t.flags & 128) ? TMAP_I2 : TMAP_I) : ((t.flags & 2) ? TMAP_U : TMAP_L));
                 o.rowa = t.arow0 + tl.y * TC_BM;
                 o.rowb = (trsm ? 0 : m.browoff[t.b]) + tl.z * TC_BN;
-                o.nk = (m.width[t.c] + TC_BK - 1) / TC_BK;
+                o.nk = (m.width[t.c] + BK - 1) / BK;
                 o.pair = tl.w & 1;
                 return o;
             };
@@ -150,9 +168,9 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                         break;
                     }
                     mbar_arrive_expect_tx(smem_u32(&full[s]), bytes);
-                    tma_load_3d(tile_addr(s, 0), ma, kb * TC_BK, rowa, 0, smem_u32(&full[s]));
-                    if (o.pair) tma_load_3d(tile_addr(s, QA1), ma, kb * TC_BK, rowa + TC_BM, 0, smem_u32(&full[s]));
-                    tma_load_3d(tile_addr(s, QB), mbm, kb * TC_BK, rowb, 0, smem_u32(&full[s]));
+                    tma_load_3d(tile_addr(s, 0), ma, kb * BK, rowa, 0, smem_u32(&full[s]));
+                    if (o.pair) tma_load_3d(tile_addr(s, QA1), ma, kb * BK, rowa + TC_BM, 0, smem_u32(&full[s]));
+                    tma_load_3d(tile_addr(s, QB), mbm, kb * BK, rowb, 0, smem_u32(&full[s]));
                 }
                 if (!ok) {
                     atomicExch(&fail_s, 1);
@@ -177,7 +195,8 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                 const TcTileView v = nv;
                 if (ti + (int)gridDim.x < ntiles)   // the next tile's view loads while this one runs
                     nv = tc_tile_view(m, tiles[ti + gridDim.x], tasks, coefL, coefU, nullptr);
-                const uint32_t idesc = tc_idesc(tc_mma_n(v.ncols));
+                const uint32_t idesc = F16 ? tc_idesc_f16(tc_mma_n(v.ncols)) : tc_idesc(tc_mma_n(v.ncols));
+                const int vnk = F16 ? (v.K + BK - 1) / BK : v.nk;
                 const int ab = tl & 1;
                 const uint32_t acc = tmem + (uint32_t)(ab * 256), acc1 = acc + 128u;
                 const bool pair = v.pair != 0;
@@ -187,7 +206,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 bool ok = true;
-                for (int kb = 0; kb < v.nk; kb++, it++) {
+                for (int kb = 0; kb < vnk; kb++, it++) {
                     const int s = it % S;
                     if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((it / S) & 1))) {
                         ok = false;
@@ -206,9 +225,15 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                                 const uint64_t ah = tc_sdesc(tile_addr(s, h * QA1) + kk * 32),
                                                al = tc_sdesc(tile_addr(s, h * QA1 + 1) + kk * 32);
                                 const uint32_t ac = h ? acc1 : acc;
-                                tc_mma(ac, al, bh, idesc, first);
-                                tc_mma(ac, ah, bl, idesc, 1u);
-                                tc_mma(ac, ah, bh, idesc, 1u);
+                                if (F16) {
+                                    tc_mma_f16(ac, al, bh, idesc, first);
+                                    tc_mma_f16(ac, ah, bl, idesc, 1u);
+                                    tc_mma_f16(ac, ah, bh, idesc, 1u);
+                                } else {
+                                    tc_mma(ac, al, bh, idesc, first);
+                                    tc_mma(ac, ah, bl, idesc, 1u);
+                                    tc_mma(ac, ah, bh, idesc, 1u);
+                                }
                             }
                         } else {
                             const uint64_t bd = tc_sdesc(tile_addr(s, QB) + kk * 32);
@@ -229,47 +254,80 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
         }
     } else {
         // ---------------- epilogue (warps 0-3) ----------------
-        float *E = epi + warp * 32 * 33;
+        // The next tile's view, target rows and row scales are loaded while
+        // the current tile is written back (prep of tile t + 1 before the
+        // wait on tile t's accumulator): the epilogue's per-tile load chains
+        // stay off the path of the reductions.
+        const int ew = warp < 4 ? warp : warp - 2;   // epilogue warp 0..7
+        const int qw = warp & 3;                       // TMEM lane quarter (rows 32 qw .. 32 qw + 31)
+        const int grp = warp < 4 ? 0 : 1;              // column chunks 32 grp, 32 grp + 64
+        float *E = epi + ew * 32 * 33;
+        const int myrow = qw * 32 + lane;
+        struct EpiTile {
+            TcTileView v;
+            int tr[2];
+            float rs[2];
+            int64_t sb;
+        };
+        auto prep = [&](int ti, EpiTile &e) {
+            const int4 tl = tiles[ti];
+            e.v = tc_tile_view(m, tl, tasks, coefL, coefU, nullptr);
+            const bool trsm = (e.v.flags & 64) != 0;
+            const int64_t *ax = taux + 3 * (int64_t)tl.x;   // {row-map base, A scale base, B scale base}
+            const int64_t tb = ax[0];
+            const int64_t sa = F16 ? ax[1] : 0;
+            e.sb = F16 ? ax[2] + e.v.j0 : 0;
+            for (int h = 0; h < 2; h++) {
+                const int row = h * TC_BM + myrow;   // row of the pair, from the first tile's first row
+                const bool ok = (h == 0 || e.v.pair) && row < e.v.M - e.v.i0;
+                e.tr[h] = (ok && !trsm) ? tmap[tb + e.v.i0 + row] : -1;
+                e.rs[h] = (F16 && ok) ? hscale[sa + e.v.i0 + row] : 1.f;
+            }
+        };
+        EpiTile cur{}, nxt{};
+        if (blockIdx.x < ntiles) prep(blockIdx.x, cur);
         int tl = 0;
         for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x, tl++) {
-            const TcTileView v = tc_tile_view(m, tiles[ti], tasks, coefL, coefU, nullptr);
+            if (ti + (int)gridDim.x < ntiles) prep(ti + gridDim.x, nxt);
+            const TcTileView &v = cur.v;
             const int ab = tl & 1;
-            const int myrow = warp * 32 + lane;
             const bool trsm = (v.flags & 64) != 0;
             const int nh = v.pair ? 2 : 1;
-            int tr[2] = {-1, -1};
-            for (int h = 0; h < nh; h++) {
-                const int row = h * TC_BM + myrow;     // row of the pair, from the first tile's first row
-                if (row < v.M - v.i0 && !trsm)
-                    tr[h] = panel_row_of(m, v.f, m.rowidx[m.rowbase[v.c] + v.arow + row]);
-            }
             if (!mbar_wait(smem_u32(&accf[ab]), (uint32_t)((tl / 2) & 1))) {
                 atomicExch(&fail_s, 1);
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            trow_s[0][myrow] = tr[0];
-            trow_s[1][myrow] = tr[1];
-            __syncwarp();
+            const int trw[2] = {cur.tr[0], cur.tr[1]};   // each lane's row target, shuffled to the writers
+            const float rs[2] = {cur.rs[0], cur.rs[1]};
+            const int64_t sb = cur.sb;
             float *C = ((v.flags & 4) ? coefU : coefL) + m.coefoff[v.f];
             const int ldf = m.ld[v.f], wf = m.width[v.f];
             const int tcol0 = m.bfrow[v.b] + v.j0 - m.fcol[v.f];
             const bool lower_only = (v.flags & 8) != 0;
             for (int h = 0; h < nh; h++)
-            for (int cb = 0; cb < TC_BN; cb += 32) {
+            for (int cb = 32 * grp; cb < TC_BN; cb += 64) {
                 const int mrows = min(TC_BM, v.M - v.i0 - h * TC_BM);   // valid rows of this half
                 uint32_t r[32];
-                tc_ld32(tmem + (uint32_t)(ab * 256 + h * 128) + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, r);
+                tc_ld32(tmem + (uint32_t)(ab * 256 + h * 128) + ((uint32_t)(qw * 32) << 16) + (uint32_t)cb, r);
                 __syncwarp();
+                if (F16) {
+                    // column cb + lane's inverse scale, broadcast column by column
+                    const float cs = (cb + lane < v.ncols) ? hscale[sb + cb + lane] : 0.f;
 #pragma unroll
-                for (int q = 0; q < 32; q++) E[lane * 33 + q] = __uint_as_float(r[q]);
+                    for (int q = 0; q < 32; q++)
+                        E[lane * 33 + q] = __uint_as_float(r[q]) * rs[h] * __shfl_sync(0xffffffffu, cs, q);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 32; q++) E[lane * 33 + q] = __uint_as_float(r[q]);
+                }
                 __syncwarp();
                 const int j = cb + lane;
                 if (j < v.ncols && trsm) {
                     const int ldc = m.ld[v.c];
                     float *O = scr + v.out + (int64_t)(v.i0 + h * TC_BM) * ldc + v.j0;
                     for (int rr = 0; rr < 32; rr++) {
-                        const int i = warp * 32 + rr;
+                        const int i = qw * 32 + rr;
                         if (i >= mrows) break;
                         O[(int64_t)i * ldc + j] = E[rr * 33 + lane];
                     }
@@ -278,7 +336,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                     const int tcs = tcol0 + cb, a0 = tcs & ~3, o = tcs - a0;
                     for (int k = lane; k < 32 * 9; k += 32) {
                         const int rr = k / 9, g = k - rr * 9;
-                        const int t2 = trow_s[h][warp * 32 + rr];
+                        const int t2 = __shfl_sync(0xffffffffu, trw[h], rr);
                         if (t2 < 0) continue;
                         float a[4];
                         bool any = false;
@@ -297,6 +355,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&acce[ab]));
+            cur = nxt;
         }
     }
     if (tid == 0 && failed()) atomicAdd(&st->timeout, 1);
@@ -333,6 +392,140 @@ __global__ void k_split_rows(Meta m, const int4 *__restrict__ jobs, const float 
         reinterpret_cast<float4 *>(hi + (int64_t)i * ld)[q] = h4;
         reinterpret_cast<float4 *>(lo + (int64_t)i * ld)[q] = l4;
     }
+}
+
+// ---------------------------------------------------------------------------
+// 3xFP16 operands: per-row power-of-two scaling and hi / lo split.
+//
+// Row scale: the largest magnitude m of the row has binary exponent E
+// (2^E <= m < 2^(E+1)); e = 14 - E puts it in [2^14, 2^15), below the FP16
+// maximum 65504 and far above its normal minimum 2^-14.  e is clamped to
+// [-126, 126] so that 2^e and 2^-e are normal floats (an all-zero row keeps
+// e = 0).  The row's stored scale is 2^-e, which the GEMM epilogue applies.
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) << 23); }
+
+// One warp splits one row of w floats (src 16-byte aligned when w >= 4):
+// optional FP32 copy to dst, hi / lo halves at hi and hi + hplane, the
+// inverse scale at *sc.
+__device__ __forceinline__ void split_row_h16(const float *__restrict__ src, int w, float *__restrict__ dst,
+                                              __half *__restrict__ hi, int64_t hplane, float *__restrict__ sc,
+                                              int lane) {
+    const int wv = w >> 2;
+    float mx = 0.f;
+    for (int q = lane; q < wv; q += 32) {
+        const float4 x = reinterpret_cast<const float4 *>(src)[q];
+        mx = fmaxf(mx, fmaxf(fmaxf(fabsf(x.x), fabsf(x.y)), fmaxf(fabsf(x.z), fabsf(x.w))));
+    }
+    for (int j = 4 * wv + lane; j < w; j += 32) mx = fmaxf(mx, fabsf(src[j]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    int e = 0;
+    if (mx > 0.f) {
+        const int E = ((__float_as_int(mx) >> 23) & 0xff) - 127;
+        e = max(-126, min(126, 14 - E));
+    }
+    const float s = pow2f(e);
+    if (lane == 0) *sc = pow2f(-e);
+    __half *lo = hi + hplane;
+    for (int q = lane; q < wv; q += 32) {
+        const float4 x = reinterpret_cast<const float4 *>(src)[q];
+        if (dst) reinterpret_cast<float4 *>(dst)[q] = x;
+        const float y[4] = {x.x * s, x.y * s, x.z * s, x.w * s};
+        __half h[4], l[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            h[u] = __float2half_rn(y[u]);
+            l[u] = __float2half_rn(y[u] - __half2float(h[u]));
+        }
+        reinterpret_cast<__half2 *>(hi)[2 * q] = __halves2half2(h[0], h[1]);
+        reinterpret_cast<__half2 *>(hi)[2 * q + 1] = __halves2half2(h[2], h[3]);
+        reinterpret_cast<__half2 *>(lo)[2 * q] = __halves2half2(l[0], l[1]);
+        reinterpret_cast<__half2 *>(lo)[2 * q + 1] = __halves2half2(l[2], l[3]);
+    }
+    for (int j = 4 * wv + lane; j < w; j += 32) {
+        const float x = src[j];
+        if (dst) dst[j] = x;
+        const float y = x * s;
+        const __half h = __float2half_rn(y);
+        hi[j] = h;
+        lo[j] = __float2half_rn(y - __half2float(h));
+    }
+}
+
+// Target rows of the tensor-core update tasks, once per plan: for task
+// tlist[blockIdx.x] and each row i of its M rows, the panel row of the facing
+// cblk that source row arow0 + i lands in (kernels/core_zgemmsp.c:170-250
+// walks the facing blocks for this).  tmap[taux[3 task] + i].
+__global__ void k_task_rowmap(Meta m, const GemmTask *__restrict__ tasks, const int *__restrict__ tlist,
+                              const int64_t *__restrict__ taux, int *__restrict__ tmap) {
+    const int id = tlist[blockIdx.x];
+    const GemmTask t = tasks[id];
+    const int64_t base = taux[3 * (int64_t)id];
+    const int *rows = m.rowidx + m.rowbase[t.c] + t.arow0;
+    for (int i = threadIdx.x; i < t.M; i += blockDim.x) tmap[base + i] = panel_row_of(m, t.f, rows[i]);
+}
+
+// Layout of the FP16 planes: per operand map (mapidx[c] + kind) the first
+// element in the planes (hoff, rows of ld16 = round_up(w_c, 8) halves) and the
+// first row in hscale (hsbase).
+__host__ __device__ inline int ld16_of(int w) { return (w + 7) & ~7; }
+
+// Split jobs {cblk, first row, kind (TMAP_*), -}: rows [r0, r0 + 32) of the
+// source matrix of that kind (L / U panel rows, or the rows of the first /
+// second diagonal-block inverse), one warp per row.
+__global__ void __launch_bounds__(256) k_split_rows_h16(Meta m, const int4 *__restrict__ jobs,
+                                                        const float *__restrict__ coefL,
+                                                        const float *__restrict__ coefU,
+                                                        const float *__restrict__ inv, __half *__restrict__ h16,
+                                                        int64_t hplane, float *__restrict__ hscale,
+                                                        const int64_t *__restrict__ hoff,
+                                                        const int64_t *__restrict__ hsbase,
+                                                        const int *__restrict__ mapidx) {
+    const int4 jb = jobs[blockIdx.x];
+    const int c = jb.x, r0 = jb.y, kind = jb.z;
+    const int w = m.width[c], ld = m.ld[c], l16 = ld16_of(w);
+    const int rows = kind < TMAP_I ? m.height[c] : w;
+    const float *src = kind == TMAP_L ? coefL + m.coefoff[c]
+                       : kind == TMAP_U ? coefU + m.coefoff[c]
+                                        : inv + m.invoff[c] + (kind == TMAP_I2 ? inv_span(w, ld) : 0);
+    const int mi = mapidx[c] + kind;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r1 = min(r0 + 32, rows);
+    for (int i = r0 + warp; i < r1; i += blockDim.x >> 5)
+        split_row_h16(src + (int64_t)i * ld, w, nullptr, h16 + hoff[mi] + (int64_t)i * l16, hplane,
+                      hscale + hsbase[mi] + i, lane);
+}
+
+// TRSM copy-back with the FP16 split: rows [r0, r0 + 32) of the level's
+// TRSM output (chunks {cblk, r0, side, -} as k_trsm_copyback) into the panel
+// and, when the cblk is a tensor-core source, into its FP16 planes.
+__global__ void __launch_bounds__(256) k_trsm_copyback_h16(Meta m, const int4 *__restrict__ chunks,
+                                                           const int64_t *__restrict__ scroff,
+                                                           const float *__restrict__ scr, float *__restrict__ coefL,
+                                                           float *__restrict__ coefU, __half *__restrict__ h16,
+                                                           int64_t hplane, float *__restrict__ hscale,
+                                                           const int64_t *__restrict__ hoff,
+                                                           const int64_t *__restrict__ hsbase,
+                                                           const int *__restrict__ mapidx) {
+    const int4 ch = chunks[blockIdx.x];
+    const int c = ch.x, r0 = ch.y;
+    const int w = m.width[c], h = m.height[c], ld = m.ld[c], l16 = ld16_of(w);
+    const int nr = min(32, h - r0);
+    const float *src = scr + scroff[c] + (ch.z ? inv_span(h - w, ld) : 0) + (int64_t)(r0 - w) * ld;
+    float *dst = (ch.z ? coefU : coefL) + m.coefoff[c] + (int64_t)r0 * ld;
+    const int mb = mapidx[c];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (mb < 0) {   // not a tensor-core source: the FP32 rows only
+        for (int e = threadIdx.x; e < nr * w; e += blockDim.x) {
+            const int i = e / w, j = e - i * w;
+            dst[(int64_t)i * ld + j] = src[(int64_t)i * ld + j];
+        }
+        return;
+    }
+    const int mi = mb + (ch.z ? TMAP_U : TMAP_L);
+    for (int i = warp; i < nr; i += blockDim.x >> 5)
+        split_row_h16(src + (int64_t)i * ld, w, dst + (int64_t)i * ld, h16 + hoff[mi] + (int64_t)(r0 + i) * l16,
+                      hplane, hscale + hsbase[mi] + r0 + i, lane);
 }
 
 }  // namespace pgpu

@@ -750,7 +750,7 @@ __global__ void k_permute(int n, int nrhs, const int *__restrict__ peritab, cons
     // one thread per row index: the permutation entry is read once for all
     // right-hand sides, whose copies are independent loads in flight
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int p = peritab[k];
+        const int p = peritab ? peritab[k] : k;   // no table: the identity (a cast copy)
         const int64_t src = backward ? k : p, dst = backward ? p : k;
 #pragma unroll 4
         for (int r = 0; r < nrhs; r++) Y[r * ldy + dst] = (Tout)X[r * ldx + src];

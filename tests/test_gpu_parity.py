@@ -99,12 +99,19 @@ def test_mixed_factor_matches_reference_mixed(name, make, fact, fp32_gemm):
     assert np.abs(Lg.astype(np.float64) - Lr)[mask].max() <= MIXED_TOL * np.abs(Lr).max()
 
 
-@pytest.mark.parametrize("name,make,fact", [CASES[4], CASES[6]] + LARGE,
-                         ids=[CASES[4][0], CASES[6][0]] + [c[0] for c in LARGE])
-def test_mixed_default_tensor_core_factor_matches_reference_mixed(name, make, fact):
-    """The default mixed factorization (update and TRSM GEMMs on tcgen05 with
-    split products) against the reference's own single-precision factors, at
-    the FMA path's accuracy: the split keeps the products at FP32 accuracy."""
+TC_CASES = [CASES[4], ("cd20x18x16", lambda: M.convdiff_upwind(20, 18, 16, 10.0), "getrf")] + LARGE
+
+
+@pytest.mark.parametrize("mode", ["default", "3xf16", "3xtf32"])
+@pytest.mark.parametrize("name,make,fact", TC_CASES, ids=[c[0] for c in TC_CASES])
+def test_mixed_tensor_core_factor_matches_reference_mixed(name, make, fact, mode, monkeypatch):
+    """The mixed factorization with its update and TRSM GEMMs on tcgen05 with
+    split products (the default mode, and each split form: 3xFP16 with per-row
+    power-of-two scales, 3xTF32) against the reference's own single-precision
+    factors, at the FMA path's accuracy: the splits keep the products at FP32
+    accuracy."""
+    if mode != "default":
+        monkeypatch.setenv("PASTIX_GPU_MIXED_GEMM", mode)
     A = make()
     ref, st = U.run_reference(A, fact, mixed=True, nthreads=NTH)
     g = U.gpu_structure(A, st)
@@ -147,7 +154,7 @@ def fp32_gemm(monkeypatch):
     monkeypatch.setenv("PASTIX_GPU_MIXED_GEMM", "fp32")
 
 
-@pytest.mark.parametrize("mode,tol", [("3xtf32", MIXED_TOL), ("tf32", 5e-3)])
+@pytest.mark.parametrize("mode,tol", [("3xtf32", MIXED_TOL), ("3xf16", MIXED_TOL), ("tf32", 5e-3)])
 def test_tf32_tensor_core_factor_and_refinement(mode, tol, monkeypatch):
     """The mixed factorization's large update GEMMs run on tcgen05 with TF32
     operands (one product, or the 3xTF32 split): the factor stays within that
