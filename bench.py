@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--scale", type=float, default=1.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-scale", type=float, default=1.0)
+    # skip the learned cost model's measured-time evaluation (after the timed steps)
+    p.add_argument("--no-cost-model", action="store_true")
     # --arms mixed: only the mixed arm, no peak measurement (the command the
     # ncu launch lists and captures in profiles/ are taken on)
     p.add_argument("--arms", default="both", choices=["both", "mixed"])
@@ -263,6 +265,63 @@ def run_arm(A, st, b, mixed, steps, warmup, fact, refine, segments=None):
         "fact_gflops": float(dp[G.DPARM_FACT_FLOPS]), "thflops": float(dp[G.DPARM_FACT_THFLOPS]),
         "x": x, "x_e2e": xh,
     }
+
+
+def cost_model_eval(cfg, A, st, fact, mixed_values, systems=None, structs=None, nrhs=8):
+    """The learned cost model judged by measured time (after the timed
+    steps): the network and the flop model are fitted on the recorded task
+    timings of smaller problems of the same family, their held-out
+    prediction errors compared on another size, then the factorization of
+    this workload is timed with its level launches ordered by each model's
+    per-cblk cost and in plain cblk order; for the batch of independent
+    systems the LPT shards of 8 ranks chosen by each model are also run one
+    after the other and their makespans compared."""
+    from pastix_b200 import costmodel as CM
+    from pastix_b200 import gpu as G
+    fam = {1: (2, 0.3, 0.4, 0.35), 2: (2, 0.3, 0.4, 0.35), 3: (3, 0.2, 0.25, 0.22), 5: (5, 0.25, 0.3, 0.27)}
+    if cfg == 4:
+        rng = np.random.default_rng(11)
+        train = [M.diffusion_lognormal(int(q), int(q), 1, 0.5, rng) for q in rng.integers(32, 257, 48)]
+        test = [M.diffusion_lognormal(int(q), int(q), 1, 0.5, rng) for q in rng.integers(32, 257, 16)]
+    else:
+        c0, s1, s2, s3 = fam[cfg]
+        train = M.config(c0, scale=s1, seed=5)[0] + M.config(c0, scale=s2, seed=6)[0]
+        test = M.config(c0, scale=s3, seed=7)[0]
+    mixed = True
+    mlp, flop = CM.train_models(train, fact, mixed)
+    e_mlp, e_flop = CM.heldout_errors([mlp, flop], test, fact, mixed)
+    out = {"train": "recorded task timings of %d %s" % (len(train), "2D systems" if cfg == 4 else "smaller grids"),
+           "heldout_median_abs_log_err": {"mlp": e_mlp, "flop_model": e_flop}}
+    # level-launch order inside the factorization of this workload
+    s = G.Solver(device=0)
+    s.set_iparm(G.IPARM_FACTORIZATION, G.FACT[fact])
+    s.set_iparm(G.IPARM_MIXED, 1)
+    s.set_structure(st)
+    s.set_spm(A)
+    s.numfact(mixed_values)
+    esz = 4 * (2 if np.iscomplexobj(A.values) else 1)
+    cplx = np.iscomplexobj(A.values)
+    # (the recorded plan: real single-precision LL^t / LU updates on the tensor cores)
+    info = CM.plan_tasks(st, fact, esz, use_tc=not cplx and fact in ("potrf", "getrf"), complex_=cplx)
+    nc = st["cblktab"].shape[0] - 1
+    out["numfact_ms"] = {
+        "cblk_order": CM.numfact_ms_with_priority(s, None, mixed_values),
+        "mlp_priority": CM.numfact_ms_with_priority(s, CM.cblk_costs(info, mlp.predict(info), nc), mixed_values),
+        "flop_priority": CM.numfact_ms_with_priority(s, CM.cblk_costs(info, flop.predict(info), nc), mixed_values)}
+    s.close()
+    if cfg == 4 and systems is not None:
+        from pastix_b200 import batch as B
+        c_mlp = CM.system_costs(structs, mlp, fact, 4, use_tc=True)
+        c_flop = np.array([B.system_flops(t) for t in structs])
+        p_mlp, _ = B.shard(c_mlp, 8)
+        p_flop, _ = B.shard(c_flop, 8)
+        m_mlp, t_mlp = CM.shard_makespan_ms(systems, structs, p_mlp, fact, True, nrhs)
+        m_flop, t_flop = CM.shard_makespan_ms(systems, structs, p_flop, fact, True, nrhs)
+        out["lpt_8_shards_ms"] = {"mlp": {"makespan": m_mlp, "shards": t_mlp},
+                                  "flop_model": {"makespan": m_flop, "shards": t_flop},
+                                  "how": "each rank's shard (numfact + solve + CG) run on this GPU in turn"}
+    mlp.close()
+    return out
 
 
 def errors_batch(systems, offs, b, x, xtrue):
@@ -491,6 +550,12 @@ def main():
         "analysis_s": t_an, "peaks": peaks,
     }
     line["clocks"] = clk.summary()
+    if not args.no_cost_model:
+        try:
+            line["cost_model"] = cost_model_eval(cfg, A, st, fact, A.values, systems if batch else None,
+                                                 all_structs if batch else None, nrhs)
+        except Exception as e:
+            line["cost_model"] = {"error": str(e)}
     if world == 1 and not args.no_cpu_baseline and batch:
         nth = os.cpu_count() or 1
         v, k, t_s, err = cpu_reference_batch(systems, nrhs, fact, refine, True, nth, 20.0, total_flops)

@@ -255,7 +255,7 @@ PASTIX_GPU_API int pastix_gpu_phase_log( pastix_gpu_t *ctx, int64_t *count, int6
 /*
  * Kernel variants and launch shapes (the autotuner's knobs, no reference
  * counterpart; the reference's equivalents are compile-time block sizes):
- *   PGPU_TUNE_MIXED_GEMM      0 FP32 FMA, 1 TF32, 2 3xTF32 (default) update GEMMs
+ *   PGPU_TUNE_MIXED_GEMM      0 FP32 FMA, 1 TF32, 2 3xTF32 (default), 3 3xFP16 update GEMMs
  *   PGPU_TUNE_TC_KERNEL       1 persistent warp-specialized (default), 0 one tile per CTA
  *   PGPU_TUNE_LOOKAHEAD       1 (default): deferred update GEMMs on a second stream
  *   PGPU_TUNE_LA_RESERVED_SMS SMs left to the critical path by the second stream (16)
@@ -268,6 +268,8 @@ PASTIX_GPU_API int pastix_gpu_phase_log( pastix_gpu_t *ctx, int64_t *count, int6
  *                             loaded by TMA; 0: split by producer warps per tile
  *   PGPU_TUNE_TC_PAIR_MIN     TMA kernel: fewest tiles in a launch for pairing 128-row
  *                             tiles that share their B tile (-1, default: 2 per SM)
+ *   PGPU_TUNE_DMMA            1 (default): real FP64 update / TRSM GEMMs large enough
+ *                             for a 128 x 64 tile on the FP64 tensor cores (DMMA); 0: FMA tiles
  * Setting one invalidates the factorization plan (rebuilt by the next numfact).
  */
 #define PGPU_TUNE_MIXED_GEMM      0
@@ -280,7 +282,8 @@ PASTIX_GPU_API int pastix_gpu_phase_log( pastix_gpu_t *ctx, int64_t *count, int6
 #define PGPU_TUNE_WIDE_PANEL      7
 #define PGPU_TUNE_TC_TMA          8
 #define PGPU_TUNE_TC_PAIR_MIN     9
-#define PGPU_TUNE_COUNT           10
+#define PGPU_TUNE_DMMA            10
+#define PGPU_TUNE_COUNT           11
 PASTIX_GPU_API int pastix_gpu_set_tuning( pastix_gpu_t *ctx, int key, int64_t value );
 PASTIX_GPU_API int pastix_gpu_get_tuning( pastix_gpu_t *ctx, int key, int64_t *value );
 

@@ -284,3 +284,74 @@ def system_costs(structs, model, fact="potrf", esz=8, use_tc=False):
         info = plan_tasks(st, fact, esz, use_tc)
         out.append(float(model.predict(info).sum()))
     return np.array(out)
+
+
+# --- judged by measured time ---------------------------------------------------
+def record_batch(systems, fact="potrf", mixed=False):
+    """Task records (info, ns) of one factorization of `systems` merged into
+    one forest, recording on (one task per CTA; the second of two runs)."""
+    from . import batch as B
+    bs = B.BatchSolver(systems, fact=fact, mixed=mixed)
+    try:
+        record_tasks(bs.solver)
+        bs.solver.numfact(bs.values())
+        bs.solver.numfact(bs.values())
+        return task_records(bs.solver)
+    finally:
+        bs.close()
+
+
+def train_models(train_systems, fact="potrf", mixed=False, hidden=32, steps=2000, seed=3):
+    """The network and the flop model fitted on the same recorded tasks."""
+    info, ns = record_batch(train_systems, fact, mixed)
+    mlp = MLPCostModel(hidden=hidden, seed=seed)
+    mlp.fit(info, ns, steps=steps, lr=3e-3)
+    flop = FlopModel().fit(info, ns)
+    return mlp, flop
+
+
+def heldout_errors(models, test_systems, fact="potrf", mixed=False):
+    """Median |log(pred / measured)| of each model on systems it was not
+    trained on."""
+    info, ns = record_batch(test_systems, fact, mixed)
+    return [log_error(m.predict(info), ns) for m in models]
+
+
+def numfact_ms_with_priority(solver, prio, values, repeats=3):
+    """Median device time of the factorization with the level launches
+    ordered by `prio` (per-cblk cost; None: cblk order)."""
+    set_cblk_priority(solver, prio)
+    solver.numfact(values)                         # plan rebuilt with the new order
+    t = []
+    for _ in range(repeats):
+        solver.numfact(values)
+        t.append(solver.stats()["numfact_ms"])
+    set_cblk_priority(solver, None)
+    return float(np.median(t))
+
+
+def shard_makespan_ms(systems, structs, parts, fact="potrf", mixed=True, nrhs=8, repeats=2):
+    """Measured per-shard time-to-solution (numfact + solve + refinement,
+    device ms) of each rank's shard run on this GPU one after the other, and
+    the makespan (the slowest shard): what an LPT assignment decides."""
+    from . import batch as B
+    from . import matrices as M
+    times = []
+    for p in parts:
+        if len(p) == 0:
+            times.append(0.0)
+            continue
+        bs = B.BatchSolver([systems[i] for i in p], fact=fact, mixed=mixed, structs=[structs[i] for i in p])
+        try:
+            rhs = [M.rhs_from_xtrue(systems[i], nrhs, np.random.default_rng(1000 + int(i)))[1] for i in p]
+            b = bs.stack(rhs)
+            best = []
+            for _ in range(repeats + 1):
+                bs.solver.numfact(bs.values())
+                bs.solver.solve_and_refine(b)
+                st = bs.solver.stats()
+                best.append(st["numfact_ms"] + st["solve_ms"] + st["refine_ms"])
+            times.append(float(np.median(best[1:])))
+        finally:
+            bs.close()
+    return max(times), times

@@ -8,6 +8,7 @@
 #include "pgpu_gemm_tc.cuh"
 #include "pgpu_panel_wide.cuh"
 #include "pgpu_gemm_tma.cuh"
+#include "pgpu_gemm_f64.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -579,6 +580,8 @@ static void default_tuning(int64_t *t) {
     e = getenv("PASTIX_GPU_TC_TMA");
     t[PGPU_TUNE_TC_TMA] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
     t[PGPU_TUNE_TC_PAIR_MIN] = -1;
+    e = getenv("PASTIX_GPU_DMMA");
+    t[PGPU_TUNE_DMMA] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
 }
 static int mixed_gemm_mode(const pastix_gpu_t &C) { return (int)C.tune[PGPU_TUNE_MIXED_GEMM]; }
 
@@ -672,6 +675,10 @@ static void invalidate_graph(pastix_gpu_t &C) {
 
 static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     const bool use_tc = fp32 && !zc && tc_enabled(C) && (fmode == FM_POTRF || fmode == FM_GETRF);
+    // real FP64: the large update and TRSM GEMMs on the FP64 tensor cores (DMMA),
+    // planned like the single-precision tensor-core tiles (128 x 64 tiles)
+    const bool use_dmma = !fp32 && !zc && C.tune[PGPU_TUNE_DMMA] != 0 && !C.record;
+    const int tbm = use_tc ? TC_BM : DG_BM, tbn = use_tc ? TC_BN : DG_BN;
     const bool lu = (fmode == FM_GETRF), ldl = fm_ldl(fmode);
     // panels taller than TRSM_GEMM_ROWS: inverse of the diagonal block, then the
     // off-diagonal rows times it as a GEMM (tensor cores in single precision)
@@ -683,7 +690,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     const size_t esz = (fp32 ? 4 : 8) * (zc ? 2 : 1);
     const int fuse = tgemm ? std::min((int)C.tune[PGPU_TUNE_TRSM_GEMM_ROWS], fuse_rows_for(lu, esz))
                            : fuse_rows_for(lu, esz);
-    const bool tc_trsm = tgemm && fp32 && !zc && tc_enabled(C);
+    const bool tc_trsm = tgemm && ((fp32 && !zc && tc_enabled(C)) || use_dmma);
     std::vector<int2> invjobs;
     std::vector<int4> ttiles, tttiles;
     int64_t inv_elems = 0, scr_max = 0;
@@ -756,7 +763,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
                     GemmTask g{c, C.fblok[c], c, w, h - w, side ? (64 | 128 | 1) : 64, 0};
                     g.out = C.scroff[c] + (side ? inv_span(h - w, C.ld[c]) : 0);
                     tasks.push_back(g);
-                    const int bm = tc_trsm ? TC_BM : GEMM_TM, bn = tc_trsm ? TC_BN : GEMM_TN;
+                    const int bm = tc_trsm ? tbm : GEMM_TM, bn = tc_trsm ? tbn : GEMM_TN;
                     for (int tm = 0; tm < cdiv(h - w, bm); tm++)
                         for (int tn = 0; tn < cdiv(w, bn); tn++)
                             (tc_trsm ? tttiles : ttiles).push_back(make_int4(id, tm, tn, 0));
@@ -773,11 +780,11 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
                     const int id = (int)tasks.size();
                     tasks.push_back(GemmTask{c, b, f, arow0, M, flags});
                     gflops += fma_flops * M * N * w;
-                    if (use_tc && tc_task(C, M, N, w)) {
+                    if ((use_tc || use_dmma) && tc_task(C, M, N, w)) {
                         tcflops += 2.0 * M * N * w;
-                        for (int tm = 0; tm < cdiv(M, TC_BM); tm++)
-                            for (int tn = 0; tn < cdiv(N, TC_BN); tn++) {
-                                if ((flags & 8) && tm < tn) continue;
+                        for (int tm = 0; tm < cdiv(M, tbm); tm++)
+                            for (int tn = 0; tn < cdiv(N, tbn); tn++) {
+                                if ((flags & 8) && (int64_t)(tm + 1) * tbm <= (int64_t)tn * tbn) continue;
                                 ltc[crit].push_back(make_int4(id, tm, tn, 0));
                             }
                         return;
@@ -1018,7 +1025,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     PGPU_CHECK(C.d_tctiles.upload(tctiles, s));
     PGPU_CHECK(C.d_trsm.upload(trsm, s));
     PGPU_CHECK(C.d_tasks.upload(tasks, s));
-    if (C.tma) {
+    if (C.tma || use_dmma) {
         // tensor-core tasks: target-row maps (built on the device) and scale bases
         std::vector<int64_t> taux(3 * tasks.size(), 0);
         std::vector<char> is_tc(tasks.size(), 0);
@@ -1207,6 +1214,9 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<true>()));
         PGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, C.device));
     }
+    if constexpr (std::is_same<T, double>::value)
+        PGPU_CHECK(cudaFuncSetAttribute(k_gemm_scatter_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        dg_smem_bytes()));
     int64_t *prof[4] = {nullptr, nullptr, nullptr, nullptr};
     if (C.record) {
         const size_t cnt[4] = {(size_t)C.cblknbr, (size_t)C.trsm_ptr[C.nlevels], (size_t)C.tile_ptr[C.nlevels],
@@ -1265,6 +1275,16 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                 PGPU_CHECK(lt.mark(PH_GEMM));
                 k_gemm_scatter_small<T><<<cdiv(nw, GS_WARPS), GS_WARPS * 32, gs_smem_bytes<T>(), st>>>(
                     C.meta, C.d_tiles.p + t0 + nt - nw, nw, C.d_tasks.p, coefL, coefU);
+                if (la) PGPU_CHECK(lt.mark(PH_END));
+                nl++;
+                ngemm++;
+            }
+        }
+        if constexpr (std::is_same<T, double>::value) {
+            if (ntc) {   // FP64 tensor cores (DMMA)
+                PGPU_CHECK(lt.mark(PH_TC));
+                k_gemm_scatter_dmma<<<ntc, DG_THREADS, dg_smem_bytes(), st>>>(
+                    C.meta, C.d_tctiles.p + c0, C.d_tasks.p, coefL, coefU, nullptr, nullptr, C.d_tmap.p, C.d_taux.p);
                 if (la) PGPU_CHECK(lt.mark(PH_END));
                 nl++;
                 ngemm++;
@@ -1389,6 +1409,15 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                 k_gemm_scatter<T><<<ntt, 256, 0, s>>>(C.meta, C.d_ttiles.p + C.ttile_ptr[l], C.d_tasks.p, coefL, coefU,
                                                       inv, scr, nullptr);
                 nl++;
+            }
+            if constexpr (std::is_same<T, double>::value) {
+                const int ntc = C.tttile_ptr[l + 1] - C.tttile_ptr[l];
+                if (ntc) {
+                    k_gemm_scatter_dmma<<<ntc, DG_THREADS, dg_smem_bytes(), s>>>(
+                        C.meta, C.d_tttiles.p + C.tttile_ptr[l], C.d_tasks.p, coefL, coefU, inv, scr, C.d_tmap.p,
+                        C.d_taux.p);
+                    nl++;
+                }
             }
             if constexpr (std::is_same<T, float>::value) {
                 const int ntc = C.tttile_ptr[l + 1] - C.tttile_ptr[l];
@@ -1641,7 +1670,7 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
         C.stats[6] = ph[PH_GEMM] + ph[PH_TC] + C.side_ms[PH_GEMM] + C.side_ms[PH_TC];
         C.stats[10] = C.plan_gemm_flops;
         C.stats[11] = ph[PH_TC] + C.side_ms[PH_TC];
-        C.stats[12] = mixed ? C.tc_flops : 0.0;
+        C.stats[12] = C.tc_flops;   // tensor-core (tcgen05, or FP64 DMMA) task flops
         C.stats[13] = st.timeout;
         C.stats[14] = replayed ? 1.0 : 0.0;
     }

@@ -57,6 +57,9 @@ def test_factor_matches_reference(name, make, fact):
     Lr, Ur = U.ref_coeftab_1d(ref, st, lay)
     s = _gpu_solver(A, st, fact)
     s.numfact(A.values)
+    if name in [c[0] for c in LARGE]:
+        # the large update and TRSM GEMMs ran on the FP64 tensor cores (DMMA)
+        assert s.stats()["tc_flops"] > 0.5 * s.stats()["gemm_flops"], s.stats()
     Lg, Ug = s.coeftab()
     mask = U.lower_mask(lay) if fact == "potrf" else np.ones(lay.off[-1], bool)
     scale = np.abs(Lr).max()
@@ -419,4 +422,29 @@ def test_tma_operands_match_producer_split(fact, make, trsm_gemm):
         assert np.abs(U1.astype(np.float64) - U0).max() <= 2e-6 * np.abs(U0).max()
     st_ = s.stats()
     assert st_["tc_ms"] > 0
+    s.close()
+
+
+DMMA_CASES = LARGE + [("sytrf20", LDL_CASES[0][1], "sytrf")]
+
+
+@pytest.mark.parametrize("name,make,fact", DMMA_CASES, ids=[c[0] for c in DMMA_CASES])
+def test_fp64_dmma_matches_fma_tiles(name, make, fact, monkeypatch):
+    """FP64 update and TRSM GEMMs on the FP64 tensor cores (DMMA, default)
+    against the FMA tiles (PGPU_TUNE_DMMA = 0): the same factors to the
+    rounding of their summation orders."""
+    from pastix_b200 import autotune as AT
+    A = make()
+    ref, st = U.run_reference(A, fact, numfact=False, nthreads=NTH)
+    s = _gpu_solver(A, st, fact)
+    s.numfact(A.values)
+    assert s.stats()["tc_flops"] > 0
+    L1, U1 = s.coeftab()
+    AT.set_knob(s, "dmma", 0)
+    s.numfact(A.values)
+    assert s.stats()["tc_flops"] == 0
+    L0, U0 = s.coeftab()
+    assert np.abs(L1 - L0).max() <= 1e-13 * np.abs(L0).max()
+    if fact == "getrf":
+        assert np.abs(U1 - U0).max() <= 1e-13 * np.abs(U0).max()
     s.close()
