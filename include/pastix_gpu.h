@@ -112,8 +112,9 @@ PASTIX_GPU_API int pastix_gpu_structure( pastix_gpu_t *ctx, int64_t n,
 /*
  * Hand over the pattern of the user's matrix (0-based CSC; Symmetric and
  * Hermitian matrices give one triangle).  Builds the device-side bcsc
- * equivalents: the fill-in map into the coeftab and the permuted matrix the
- * refinement multiplies by.  Replaces pastix_subtask_spm2bcsc
+ * equivalents on the device: the fill-in map into the coeftab and the
+ * permuted matrix the refinement multiplies by (its device time is
+ * stats[15] of pastix_gpu_stats).  Replaces pastix_subtask_spm2bcsc
  * (sopalin/pastix_task_sopalin.c:93) / bcscInit (bcsc/bcsc.c:1887).
  */
 PASTIX_GPU_API int pastix_gpu_spm( pastix_gpu_t *ctx, int mtxtype, int flttype, int64_t n,
@@ -182,7 +183,10 @@ PASTIX_GPU_API int pastix_gpu_solve_steps( pastix_gpu_t *ctx, int steps, int64_t
  * stream capture.  All calls share the one array and it keeps the contents of
  * the last call (nothing needs clearing: every element used is written first),
  * so calls that overlap on the GPU -- from two contexts, threads or streams on
- * the same device -- race and must be serialized by the caller.
+ * the same device -- race and must be serialized by the caller.  The address
+ * is kept for the life of the process: a reset of the device (cudaDeviceReset,
+ * or the primary context released and created again) invalidates it, so no
+ * call may follow such a reset.
  * Returns when the solution is in dB.
  */
 #define PASTIX_GPU_NOALLOC_SCRATCH_BYTES ( (size_t)16 << 20 )
@@ -255,7 +259,7 @@ PASTIX_GPU_API int pastix_gpu_phase_log( pastix_gpu_t *ctx, int64_t *count, int6
 /*
  * Kernel variants and launch shapes (the autotuner's knobs, no reference
  * counterpart; the reference's equivalents are compile-time block sizes):
- *   PGPU_TUNE_MIXED_GEMM      0 FP32 FMA, 1 TF32, 2 3xTF32 (default), 3 3xFP16 update GEMMs
+ *   PGPU_TUNE_MIXED_GEMM      0 FP32 FMA, 1 TF32, 2 3xTF32, 3 3xFP16 (default) update GEMMs
  *   PGPU_TUNE_TC_KERNEL       1 persistent warp-specialized (default), 0 one tile per CTA
  *   PGPU_TUNE_LOOKAHEAD       1 (default): deferred update GEMMs on a second stream
  *   PGPU_TUNE_LA_RESERVED_SMS SMs left to the critical path by the second stream (16)
@@ -264,8 +268,8 @@ PASTIX_GPU_API int pastix_gpu_phase_log( pastix_gpu_t *ctx, int64_t *count, int6
  *   PGPU_TUNE_TC_MIN_MN       smallest M x N update sent to the tensor cores (8192)
  *   PGPU_TUNE_WIDE_PANEL      narrowest diagonal block factorized by the 512-thread
  *                             left-looking kernel (128; 0 disables it)
- *   PGPU_TUNE_TC_TMA          1 (default): 3xTF32 operands pre-split once per panel and
- *                             loaded by TMA; 0: split by producer warps per tile
+ *   PGPU_TUNE_TC_TMA          1 (default): split operands (3xFP16 / 3xTF32) pre-split once per
+ *                             panel and loaded by TMA; 0: 3xTF32 split by producer warps per tile
  *   PGPU_TUNE_TC_PAIR_MIN     TMA kernel: fewest tiles in a launch for pairing 128-row
  *                             tiles that share their B tile (-1, default: 2 per SM)
  *   PGPU_TUNE_DMMA            1 (default): real FP64 update / TRSM GEMMs large enough
@@ -311,15 +315,18 @@ PASTIX_GPU_API int pastix_gpu_coeftab( pastix_gpu_t *ctx, void *L, void *U );
  *   stats[7] update-GEMM launches inside numfact
  *   stats[8] diagonal-factorization ms, stats[9] panel-TRSM ms inside numfact
  *   stats[10] algorithmic flops of the update GEMMs (sum of 2 M N K)
- *   stats[11] ms of the tensor-core (tcgen05) update-GEMM launches (part of stats[6])
+ *   stats[11] ms of the tensor-core update-GEMM launches (part of stats[6]): tcgen05
+ *             for single precision, DMMA for real FP64
  *   stats[12] algorithmic flops of the GEMM tasks that ran on the tensor cores
  *   stats[13] tensor-core tiles whose bounded MMA wait timed out (0 when healthy)
  *   stats[14] 1 when the factorization replayed a captured CUDA graph
- *   stats[15] reserved
+ *   stats[15] ms of the last pastix_gpu_spm (device-side pattern setup: uploads,
+ *             fill map, permuted CSR)
  * (16 doubles)
  * The single-precision (mixed) factorization runs its large update GEMMs on
- * the tensor cores with TF32 operands; environment PASTIX_GPU_MIXED_GEMM=fp32
- * keeps them on FP32 FMA instead.
+ * the tensor cores with split FP16 operands (3xFP16); environment
+ * PASTIX_GPU_MIXED_GEMM=3xtf32 | tf32 | fp32 selects the 3xTF32 split, one
+ * TF32 product, or FMA tiles instead.
  */
 PASTIX_GPU_API int pastix_gpu_stats( pastix_gpu_t *ctx, double *stats );
 

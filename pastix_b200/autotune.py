@@ -10,7 +10,7 @@ library's CUDA events), by coordinate descent over a small candidate space:
   la_reserved_sms  SMs the lookahead stream leaves to the critical path
   wide_panel       narrowest diagonal block given to the left-looking
                    512-thread panel kernel (0: none)
-  mixed_gemm       3xTF32 vs one TF32 product (objective "solve": the
+  mixed_gemm       3xFP16 vs 3xTF32 vs one TF32 product (objective "solve": the
                    refinement's extra iterations are part of the cost)
 
 `tune` returns the chosen values and every measurement; `TuningCache`
@@ -79,7 +79,7 @@ def tune(solver, values, b=None, space=None, reps=2, objective="numfact", rounds
     (best settings, best time, list of (settings, time) measured)."""
     space = dict(DEFAULT_SPACE if space is None else space)
     if objective == "solve" and "mixed_gemm" not in space:
-        space["mixed_gemm"] = [2, 1]
+        space["mixed_gemm"] = [3, 2, 1]
     meas = measure_fn or (lambda: measure(solver, values, b, reps, objective))
     best = {k: get_knob(solver, k) for k in space}
     for k, v in best.items():

@@ -9,6 +9,9 @@
 #include "pgpu_panel_wide.cuh"
 #include "pgpu_gemm_tma.cuh"
 #include "pgpu_gemm_f64.cuh"
+#include "pgpu_spm.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include <cudaTypedefs.h>
 
@@ -423,16 +426,6 @@ extern "C" int pastix_gpu_structure(pastix_gpu_t *ctx, int64_t n, int64_t cblknb
     return PASTIX_GPU_SUCCESS;
 }
 
-// Panel row of global row r in cblk c (host mirror of panel_row_of).
-static int host_panel_row(const pastix_gpu_t &C, int c, int r) {
-    int lo = C.fblok[c], hi = C.fblok[c + 1] - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (C.bfrow[mid] <= r) lo = mid; else hi = mid - 1;
-    }
-    if (r < C.bfrow[lo] || r > C.blrow[lo]) return -1;
-    return C.browoff[lo] + (r - C.bfrow[lo]);
-}
 
 // --------------------------------------------------------------------------
 // Pattern handoff: fill-in map (bcsc -> coeftab) and the permuted CSR.
@@ -450,82 +443,73 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
     C.mtxtype = mtxtype;
     C.flttype = flttype;
     const int64_t nnz = colptr[n];
+    if (nnz < 0 || 2 * nnz > (int64_t)INT32_MAX) return PASTIX_GPU_ERR_BADPARAMETER;
     C.nnz = nnz;
-    std::vector<int> perm(n);
-    for (int k = 0; k < n; k++) perm[C.peritab[k]] = k;
-    std::vector<int64_t> dst(nnz);
-    std::vector<int8_t> wgt(nnz);
     const bool sym = (mtxtype != PGPU_GENERAL);
     // a Hermitian entry that lands in the other triangle is stored conjugated
     const bool herm = (mtxtype == PGPU_HERMITIAN && flttype == PGPU_COMPLEX64);
-    // permuted full matrix as (row, col, src) triplets
-    std::vector<int64_t> rcount(n + 1, 0);
-    for (int64_t j = 0; j < n; j++) {
-        for (int64_t k = colptr[j]; k < colptr[j + 1]; k++) {
-            int64_t i = rowptr[k];
-            if (i < 0 || i >= n) return PASTIX_GPU_ERR_BADPARAMETER;
-            int pi = perm[i], pj = perm[j];
-            wgt[k] = (sym && i != j) ? 2 : 1;
-            rcount[pi + 1]++;
-            if (sym && i != j) rcount[pj + 1]++;
-            bool flip = false;
-            if (sym && pi < pj) {
-                std::swap(pi, pj);
-                flip = herm;
-            }
-            int64_t d;
-            if (pi >= pj) {
-                int c = C.col2cblk[pj];
-                int pr = host_panel_row(C, c, pi);
-                if (pr < 0) return PASTIX_GPU_ERR_BADPARAMETER;
-                d = C.coefoff[c] + (int64_t)pr * C.ld[c] + (pj - C.fcol[c]);
-            } else {
-                // general, upper entry A(pi, pj), pi < pj
-                int c = C.col2cblk[pi];
-                if (C.col2cblk[pj] == c) {
-                    // inside the diagonal block: kept in L's square
-                    d = C.coefoff[c] + (int64_t)(pi - C.fcol[c]) * C.ld[c] + (pj - C.fcol[c]);
-                } else {
-                    int pr = host_panel_row(C, c, pj);
-                    if (pr < 0) return PASTIX_GPU_ERR_BADPARAMETER;
-                    d = C.coefnbr + C.coefoff[c] + (int64_t)pr * C.ld[c] + (pi - C.fcol[c]);
-                }
-            }
-            dst[k] = flip ? ~d : d;
-        }
-    }
-    for (int64_t i = 0; i < n; i++) rcount[i + 1] += rcount[i];
-    const int64_t fnnz = rcount[n];
-    std::vector<int> ccol(fnnz);
-    std::vector<int64_t> csrc(fnnz);
-    {
-        std::vector<int64_t> pos(rcount.begin(), rcount.end() - 1);
-        for (int64_t j = 0; j < n; j++) {
-            for (int64_t k = colptr[j]; k < colptr[j + 1]; k++) {
-                int64_t i = rowptr[k];
-                int pi = perm[i], pj = perm[j];
-                int64_t q = pos[pi]++;
-                ccol[q] = pj;
-                csrc[q] = k;
-                if (sym && i != j) {
-                    q = pos[pj]++;
-                    ccol[q] = pi;
-                    csrc[q] = herm ? ~k : k;
-                }
-            }
-        }
-    }
     cudaStream_t s = C.stream;
-    PGPU_CHECK(C.d_fill_dst.upload(dst, s));
-    PGPU_CHECK(C.d_wgt.upload(wgt, s));
-    PGPU_CHECK(C.d_csr_ptr.upload(rcount, s));
-    PGPU_CHECK(C.d_csr_col.upload(ccol, s));
-    PGPU_CHECK(C.d_csr_src.upload(csrc, s));
+    PGPU_CHECK(cudaEventRecord(C.ev[4], s));
+    // the pattern, the ordering and the column -> cblk map go to the device;
+    // the maps are built there (k_spm_maps, a stable radix sort by row, k_spm_csr)
+    std::vector<int> perm(n);
+    for (int k = 0; k < n; k++) perm[C.peritab[k]] = k;
+    DArr<int64_t> d_colptr, d_rowptr, d_slot, d_sslot;
+    DArr<int> d_perm, d_c2c, d_key, d_skey, d_colof, d_bad;
+    DArr<unsigned char> d_tmp;
+    {
+        std::vector<int64_t> cp(colptr, colptr + n + 1), rp(rowptr, rowptr + nnz);
+        PGPU_CHECK(d_colptr.upload(cp, s));
+        PGPU_CHECK(d_rowptr.upload(rp, s));
+        PGPU_CHECK(d_perm.upload(perm, s));
+        PGPU_CHECK(d_c2c.upload(C.col2cblk, s));
+        PGPU_CHECK(cudaStreamSynchronize(s));   // (the host vectors leave scope)
+    }
+    const int64_t ns = 2 * std::max<int64_t>(nnz, 1);
+    PGPU_CHECK(C.d_fill_dst.alloc(std::max<int64_t>(nnz, 1)));
+    PGPU_CHECK(C.d_wgt.alloc(std::max<int64_t>(nnz, 1)));
+    PGPU_CHECK(d_key.alloc(ns));
+    PGPU_CHECK(d_skey.alloc(ns));
+    PGPU_CHECK(d_slot.alloc(ns));
+    PGPU_CHECK(d_sslot.alloc(ns));
+    PGPU_CHECK(d_colof.alloc(std::max<int64_t>(nnz, 1)));
+    PGPU_CHECK(d_bad.alloc(1));
+    PGPU_CHECK(cudaMemsetAsync(d_bad.p, 0, sizeof(int), s));
+    SpmMaps sm{(int)n, nnz, sym ? 1 : 0, herm ? 1 : 0, d_colptr.p, d_rowptr.p, d_perm.p, d_c2c.p, C.coefnbr,
+                C.d_fill_dst.p, C.d_wgt.p, d_key.p, d_slot.p, d_colof.p, d_bad.p};
+    if (n > 0) k_spm_maps<<<cdiv(n * 32, 256), 256, 0, s>>>(C.meta, sm);
+    // stable sort of the slots by permuted row (rows < n, absent mirrors = n)
+    int bits = 1;
+    while (((int64_t)1 << bits) <= n) bits++;
+    size_t tmp_bytes = 0;
+    PGPU_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_key.p, d_skey.p, d_slot.p, d_sslot.p,
+                                               (int)(2 * nnz), 0, bits, s));
+    PGPU_CHECK(d_tmp.alloc(std::max<size_t>(tmp_bytes, 1)));
+    PGPU_CHECK(cub::DeviceRadixSort::SortPairs(d_tmp.p, tmp_bytes, d_key.p, d_skey.p, d_slot.p, d_sslot.p,
+                                               (int)(2 * nnz), 0, bits, s));
+    PGPU_CHECK(C.d_csr_ptr.alloc(n + 1));
+    k_spm_rowptr<<<std::max(1, std::min(4096, cdiv(n + 1, 256))), 256, 0, s>>>((int)n, 2 * nnz, d_skey.p,
+                                                                               C.d_csr_ptr.p);
+    int64_t fnnz = 0;
+    int bad = 0;
+    PGPU_CHECK(cudaMemcpyAsync(&fnnz, C.d_csr_ptr.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    PGPU_CHECK(cudaMemcpyAsync(&bad, d_bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PGPU_CHECK(cudaStreamSynchronize(s));
+    if (bad) return PASTIX_GPU_ERR_BADPARAMETER;
+    PGPU_CHECK(C.d_csr_col.alloc(std::max<int64_t>(fnnz, 1)));
+    PGPU_CHECK(C.d_csr_src.alloc(std::max<int64_t>(fnnz, 1)));
+    if (fnnz > 0)
+        k_spm_csr<<<(int)std::min<int64_t>(4096, (fnnz + 255) / 256), 256, 0, s>>>(
+            fnnz, d_sslot.p, d_colof.p, d_rowptr.p, d_perm.p, herm ? 1 : 0, C.d_csr_col.p, C.d_csr_src.p);
     const int ncomp = (flttype == PGPU_COMPLEX64) ? 2 : 1;
     C.csr_nnz = fnnz;
-    PGPU_CHECK(C.d_csr_val.alloc(fnnz * ncomp));
-    PGPU_CHECK(C.d_vals.alloc(nnz * ncomp));
+    PGPU_CHECK(C.d_csr_val.alloc(std::max<int64_t>(fnnz, 1) * ncomp));
+    PGPU_CHECK(C.d_vals.alloc(std::max<int64_t>(nnz, 1) * ncomp));
+    PGPU_CHECK(cudaEventRecord(C.ev[5], s));
     PGPU_CHECK(cudaStreamSynchronize(s));
+    float ms = 0;
+    PGPU_CHECK(cudaEventElapsedTime(&ms, C.ev[4], C.ev[5]));
+    C.stats[15] = ms;   // device time of the pattern setup (uploads, maps, sort)
     C.have_spm = true;
     C.fact_done = -1;
     return PASTIX_GPU_SUCCESS;
@@ -550,9 +534,10 @@ static const int TRSM_TR = 32;   // panel rows per k_trsm_rows CTA
 
 // Single-precision update GEMMs large enough for a 128 x 128 tensor-core tile
 // go to the tcgen05 kernel.  Tuning PGPU_TUNE_MIXED_GEMM selects the operand
-// mode: 3xTF32 (default; split products, about FP32 accuracy), TF32 (one
-// product) or FP32 (no tensor cores: FMA tiles only); its default comes from
-// PASTIX_GPU_MIXED_GEMM = 3xtf32 | tf32 | fp32.  The other knobs and their
+// mode: 3xFP16 (default; per-row power-of-two scaled FP16 hi/lo split, about
+// FP32 accuracy), 3xTF32 (the same split in TF32), TF32 (one product) or FP32
+// (no tensor cores: FMA tiles only); its default comes from
+// PASTIX_GPU_MIXED_GEMM = 3xf16 | 3xtf32 | tf32 | fp32.  The other knobs and their
 // environment defaults: PGPU_TUNE_TC_KERNEL (PASTIX_GPU_TC_KERNEL=tile: one
 // tile per CTA instead of the persistent kernel), PGPU_TUNE_LOOKAHEAD
 // (PASTIX_GPU_LOOKAHEAD=0 disables it), PGPU_TUNE_LA_RESERVED_SMS (16),
@@ -562,10 +547,10 @@ static const int TRSM_TR = 32;   // panel rows per k_trsm_rows CTA
 enum { MG_FP32 = 0, MG_TF32 = 1, MG_3XTF32 = 2, MG_3XF16 = 3 };
 static void default_tuning(int64_t *t) {
     const char *e = getenv("PASTIX_GPU_MIXED_GEMM");
-    t[PGPU_TUNE_MIXED_GEMM] = (e && std::strcmp(e, "fp32") == 0)     ? MG_FP32
-                              : (e && std::strcmp(e, "tf32") == 0)   ? MG_TF32
-                              : (e && std::strcmp(e, "3xf16") == 0) ? MG_3XF16
-                                                                     : MG_3XTF32;
+    t[PGPU_TUNE_MIXED_GEMM] = (e && std::strcmp(e, "fp32") == 0)      ? MG_FP32
+                              : (e && std::strcmp(e, "tf32") == 0)    ? MG_TF32
+                              : (e && std::strcmp(e, "3xtf32") == 0) ? MG_3XTF32
+                                                                      : MG_3XF16;
     e = getenv("PASTIX_GPU_TC_KERNEL");
     t[PGPU_TUNE_TC_KERNEL] = (e && std::strcmp(e, "tile") == 0) ? 0 : 1;
     e = getenv("PASTIX_GPU_LOOKAHEAD");
@@ -1674,8 +1659,11 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
         C.stats[13] = st.timeout;
         C.stats[14] = replayed ? 1.0 : 0.0;
     }
-    if (st.timeout) {
+    if (st.timeout || st.drain_timeout) {
         fprintf(stderr, "pastix_gpu: %d tensor-core GEMM tiles timed out waiting for their MMAs\n", st.timeout);
+        if (st.drain_timeout)
+            fprintf(stderr, "pastix_gpu: %d CTAs gave up waiting for their own TMA loads after a time-out: the "
+                            "factorization's results are undefined\n", st.drain_timeout);
         C.fact_done = -1;
         return PASTIX_GPU_ERR_INTERNAL;
     }
@@ -1757,6 +1745,7 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches, int st
     auto small_level = [&](int l) { return C.lvl_maxw[l] <= 32 && C.lvl_maxh[l] <= SOLVE_SMALL_MAXH; };
     for (int l = 0; l < ((steps & PGPU_SOLVE_FORWARD) ? C.nlevels : 0); l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
+        tm.level = l;
         const int mw = C.lvl_maxw[l];
         if (small_level(l)) {
             PGPU_CHECK(mark(0));
@@ -1808,6 +1797,7 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches, int st
     for (int l = (steps & PGPU_SOLVE_BACKWARD) ? C.nlevels - 1 : -1; l >= 0; l--) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
+        tm.level = l;
         if (small_level(l)) {
             PGPU_CHECK(mark(4));
             const int *lc = C.d_lvl_cblks.p + C.lvl_ptr[l];
@@ -1857,6 +1847,19 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches, int st
         tm.collect(ms, 5);
         fprintf(stderr, "pastix_gpu solve profile (nrhs %d, %d levels): fwd_diag %.3f fwd_off %.3f diag %.3f "
                         "bwd_off %.3f bwd_diag %.3f ms\n", nrhs, C.nlevels, ms[0], ms[1], ms[2], ms[3], ms[4]);
+        if (getenv("PASTIX_GPU_SOLVE_PROFILE")[0] == '2') {   // per level: fwd_diag fwd_off bwd_off bwd_diag
+            std::vector<double> lv(5 * (size_t)C.nlevels, 0.0);
+            for (int i = 0; i + 1 < tm.used; i++) {
+                float t = 0;
+                if (tm.kinds[i] >= 0 && tm.kinds[i] < 5 && tm.levels[i] >= 0 &&
+                    cudaEventElapsedTime(&t, C.evpool[i], C.evpool[i + 1]) == cudaSuccess)
+                    lv[5 * (size_t)tm.levels[i] + tm.kinds[i]] += t;
+            }
+            for (int l = 0; l < C.nlevels; l++)
+                fprintf(stderr, "  level %d ncblk %d maxw %d: %.4f %.4f %.4f %.4f ms\n", l,
+                        C.lvl_ptr[l + 1] - C.lvl_ptr[l], C.lvl_maxw[l], lv[5 * l + 0], lv[5 * l + 1], lv[5 * l + 3],
+                        lv[5 * l + 4]);
+        }
     }
     *launches += nl;
     return PASTIX_GPU_SUCCESS;

@@ -55,6 +55,8 @@ struct Status {
     int nonfinite;     // NaN/Inf met on a diagonal
     int overflow;      // FP32 down-cast overflow in the mixed fill-in
     int timeout;       // a bounded wait inside a kernel gave up (tile skipped)
+    int drain_timeout; // after a time-out, waiting for a CTA's own TMA loads in flight gave up too: the
+                       // launch's results are undefined (its shared memory may still receive those bytes)
 };
 
 // Complex scalar (interleaved re, im: the layout of pastix_complex64_t /

@@ -178,10 +178,13 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                 }
             }
             if (failed()) {
-                // the loads still in flight land before the CTA leaves
+                // the loads still in flight land before the CTA leaves; if one
+                // of these waits gives up as well, the CTA may leave with bulk
+                // copies still writing its shared memory: recorded apart, and the
+                // host treats the whole factorization as failed
                 for (int j = 1; j <= S && it - j >= 0; j++) {
                     const int k = it - j;
-                    mbar_wait(smem_u32(&full[k % S]), (uint32_t)((k / S) & 1));
+                    if (!mbar_wait(smem_u32(&full[k % S]), (uint32_t)((k / S) & 1))) atomicAdd(&st->drain_timeout, 1);
                 }
             }
         }

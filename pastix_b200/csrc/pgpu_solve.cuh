@@ -104,39 +104,63 @@ __device__ void diag_solve_inverse_fwd_warp(const T *__restrict__ Bi, const T *_
                                             bool ldl, bool cjp, const T *__restrict__ v, T *__restrict__ Bg,
                                             int64_t ldb, int fc) {
     constexpr int VEC = 16 / sizeof(T);
+    // RU rows per warp at a time (n0, n0 + nw, ...): their loads are in flight
+    // together, so a warp waits one memory latency per RU rows (RU bounded so
+    // that the 1024-thread kernel stays within its 64 registers)
+    constexpr int RU = sizeof(T) * NR <= 8 ? 4 : (sizeof(T) * NR <= 16 ? 2 : 1);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int n = warp; n < w; n += nw) {
-        const T *row = Bi + (int64_t)n * ld;
-        T acc[NR];
+    for (int n0 = warp; n0 < w; n0 += nw * RU) {
+        const int nlast = min(w - 1, n0 + (RU - 1) * nw);
+        T acc[RU][NR];
 #pragma unroll
-        for (int r = 0; r < NR; r++) acc[r] = T(0);
-        for (int k0 = lane * VEC; k0 <= n; k0 += 32 * VEC) {
-            const uint4 u = __ldg(reinterpret_cast<const uint4 *>(row + k0));
-            T e[VEC];
-            memcpy(e, &u, 16);
+        for (int t = 0; t < RU; t++)
 #pragma unroll
-            for (int q = 0; q < VEC; q++) {
-                const int k = k0 + q;
-                if (k <= n) {
-                    const T b = cjp ? conj_v(e[q]) : e[q];
+            for (int r = 0; r < NR; r++) acc[t][r] = T(0);
+        for (int k0 = lane * VEC; k0 <= nlast; k0 += 32 * VEC) {
+            uint4 u[RU];
 #pragma unroll
-                    for (int r = 0; r < NR; r++) acc[r] += b * v[k * NR + r];
+            for (int t = 0; t < RU; t++) {
+                const int n = n0 + t * nw;
+                u[t] = (n < w && k0 <= n) ? __ldg(reinterpret_cast<const uint4 *>(Bi + (int64_t)n * ld + k0))
+                                          : make_uint4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int t = 0; t < RU; t++) {
+                const int n = n0 + t * nw;
+                T e[VEC];
+                memcpy(e, &u[t], 16);
+#pragma unroll
+                for (int q = 0; q < VEC; q++) {
+                    const int k = k0 + q;
+                    if (k <= n) {
+                        const T b = cjp ? conj_v(e[q]) : e[q];
+#pragma unroll
+                        for (int r = 0; r < NR; r++) acc[t][r] += b * v[k * NR + r];
+                    }
                 }
             }
         }
 #pragma unroll
-        for (int r = 0; r < NR; r++) {
+        for (int t = 0; t < RU; t++)
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc[r] += shfl_xor_v(acc[r], o);
-        }
-        if (lane == 0) {
-            T d = T(1);
-            if (ldl) {
-                d = D[(int64_t)n * ld + n];
-                if (cjp) d = conj_v(d);
+            for (int r = 0; r < NR; r++) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc[t][r] += shfl_xor_v(acc[t][r], o);
             }
+        if (lane == 0) {
 #pragma unroll
-            for (int r = 0; r < NR; r++) Bg[(int64_t)r * ldb + fc + n] = ldl ? acc[r] * d : acc[r];
+            for (int t = 0; t < RU; t++) {
+                const int n = n0 + t * nw;
+                if (n < w) {
+                    T d = T(1);
+                    if (ldl) {
+                        d = D[(int64_t)n * ld + n];
+                        if (cjp) d = conj_v(d);
+                    }
+#pragma unroll
+                    for (int r = 0; r < NR; r++) Bg[(int64_t)r * ldb + fc + n] = ldl ? acc[t][r] * d : acc[t][r];
+                }
+            }
         }
     }
 }

@@ -131,7 +131,7 @@ class Solver:
         _check("pastix_gpu_stats", load().pastix_gpu_stats(self._h, _p(s)))
         keys = ["numfact_launches", "solve_launches", "refine_launches", "numfact_ms", "solve_ms",
                 "refine_ms", "gemm_ms", "gemm_launches", "diag_ms", "trsm_ms", "gemm_flops", "tc_ms",
-                "tc_flops", "tc_timeouts", "graph_replayed", "reserved15"]
+                "tc_flops", "tc_timeouts", "graph_replayed", "spm_ms"]
         return dict(zip(keys, s.tolist()))
 
     def phase_log(self):

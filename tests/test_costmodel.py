@@ -132,3 +132,37 @@ def test_learned_model_beats_flop_model_on_held_out_systems():
     for b_ in (bs1, bs2):
         b_.close()
     mlp.close()
+
+
+@pytest.mark.gpu
+def test_learned_model_judged_by_measured_time():
+    """What the trained network gains, measured: (1) its held-out prediction
+    error against the flop model's; (2) the factorization time with the level
+    launches ordered by its per-cblk costs, by the flop model's, and in cblk
+    order; (3) the makespan of the 4-rank LPT shards of a batch chosen with
+    its system costs and with flop counts, each shard run on the GPU.  The
+    differences are reported as measured, a gain or not; the test fails only
+    if a measurement is missing or the network predicts worse than flops."""
+    rng = np.random.default_rng(17)
+    train = [M.diffusion_lognormal(int(q), int(q), 1, 0.5, rng) for q in rng.integers(32, 200, 24)]
+    test = [M.diffusion_lognormal(int(q), int(q), 1, 0.5, rng) for q in rng.integers(32, 200, 12)]
+    batch = [M.diffusion_lognormal(int(q), int(q), 1, 0.5, rng) for q in rng.integers(32, 257, 24)]
+    mlp, flop = CM.train_models(train, "potrf", mixed=True)
+    e_mlp, e_flop = CM.heldout_errors([mlp, flop], test, "potrf", mixed=True)
+    structs = [analysis.analyze(a) for a in batch]
+    bs = B.BatchSolver(batch, fact="potrf", mixed=True, structs=structs)
+    info = CM.plan_tasks(bs.struct, "potrf", 4, use_tc=True)
+    nc = bs.struct["cblktab"].shape[0] - 1
+    t_order = CM.numfact_ms_with_priority(bs.solver, None, bs.values())
+    t_mlp = CM.numfact_ms_with_priority(bs.solver, CM.cblk_costs(info, mlp.predict(info), nc), bs.values())
+    t_flop = CM.numfact_ms_with_priority(bs.solver, CM.cblk_costs(info, flop.predict(info), nc), bs.values())
+    bs.close()
+    c_mlp = CM.system_costs(structs, mlp, "potrf", 4, use_tc=True)
+    c_flop = np.array([B.system_flops(t) for t in structs])
+    m_mlp, _ = CM.shard_makespan_ms(batch, structs, B.shard(c_mlp, 4)[0], "potrf", True, nrhs=8)
+    m_flop, _ = CM.shard_makespan_ms(batch, structs, B.shard(c_flop, 4)[0], "potrf", True, nrhs=8)
+    mlp.close()
+    print("held-out |log err| mlp %.3f flop %.3f; numfact ms: cblk order %.3f, mlp order %.3f, flop order %.3f; "
+          "LPT makespan ms (4 shards): mlp %.3f flop %.3f" % (e_mlp, e_flop, t_order, t_mlp, t_flop, m_mlp, m_flop))
+    assert all(np.isfinite(v) and v > 0 for v in (t_order, t_mlp, t_flop, m_mlp, m_flop))
+    assert e_mlp < e_flop

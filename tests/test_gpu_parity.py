@@ -400,12 +400,13 @@ def test_wide_panel_kernel_matches_narrow(fact, make, mixed):
     ("getrf", lambda: M.convdiff_upwind(20, 18, 16, 10.0)),
 ], ids=["potrf", "getrf"])
 @pytest.mark.parametrize("trsm_gemm", [1, 0], ids=["trsm_gemm", "trsm_rows"])
-def test_tma_operands_match_producer_split(fact, make, trsm_gemm):
+def test_tma_operands_match_producer_split(fact, make, trsm_gemm, monkeypatch):
     """3xTF32 update and TRSM GEMMs with the operands split once per panel
     into hi / lo planes and loaded by TMA (PGPU_TUNE_TC_TMA = 1) against the
     producer warps splitting each tile (= 0): the same products, up to the
     order of the scatter-add reductions."""
     from pastix_b200 import autotune as AT
+    monkeypatch.setenv("PASTIX_GPU_MIXED_GEMM", "3xtf32")   # the same arithmetic on both paths
     A = make()
     ref, st = U.run_reference(A, fact, numfact=False)
     s = _gpu_solver(A, st, fact, mixed=True)

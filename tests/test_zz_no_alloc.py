@@ -10,6 +10,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from pastix_b200 import matrices as M
+
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12          # FP64 solves, relative max-norm (the tolerance of the GPU parity tests)
@@ -61,6 +63,46 @@ def test_noalloc_solve_matches_solve_on_two_calls(mixed):
         x = new.cpu().numpy().reshape(A.n, nrhs, order="F")
         r = b - A.to_scipy_full() @ x
         assert np.abs(r).max() <= (2e-2 if mixed else 1e-10) * np.abs(b).max()
+    s.close()
+
+
+@pytest.mark.parametrize("fact,make", [
+    ("getrf", lambda: M.convdiff_upwind(10, 9, 8, 10.0)),
+    ("potrf", lambda: M.magnetic_laplacian(8, 7, 6, -0.5, np.random.default_rng(4))),
+], ids=["getrf_real", "potrf_complex"])
+def test_noalloc_many_rhs_in_chunks(fact, make):
+    """20 right-hand sides: two chunks of the scratch (16, then 4, the second
+    starting 16 columns into B), on LU factors and on complex factors (solved
+    8 columns at a time), against pastix_gpu_solve, twice in a row."""
+    import torch
+    from pastix_b200 import analysis
+    from pastix_b200 import gpu as G
+    A = make()
+    st = analysis.analyze(A)
+    s = G.Solver()
+    s.set_iparm(G.IPARM_FACTORIZATION, G.FACT[fact])
+    s.set_structure(st)
+    s.set_spm(A)
+    s.numfact(A.values)
+    L = _lib()
+    nrhs = 20
+    cplx = np.iscomplexobj(A.values)
+    for call in range(2):
+        rng = np.random.default_rng(200 + call)
+        b = rng.uniform(-1.0, 1.0, (A.n, nrhs))
+        if cplx:
+            b = b + 1j * rng.uniform(-1.0, 1.0, (A.n, nrhs))
+        flat = np.asfortranarray(b).ravel(order="F")
+        ref = torch.from_numpy(flat.copy()).cuda()
+        new = torch.from_numpy(flat.copy()).cuda()
+        torch.cuda.synchronize()
+        assert L.pastix_gpu_solve(s._h, nrhs, C.c_void_p(ref.data_ptr()), A.n) == 0
+        assert L.pastix_gpu_solve_noalloc(s._h, nrhs, C.c_void_p(new.data_ptr()), A.n) == 0
+        torch.cuda.synchronize()
+        err = (new - ref).abs().max().item() / ref.abs().max().item()
+        assert err <= TOL, (call, err)
+        x = new.cpu().numpy().reshape(A.n, nrhs, order="F")
+        assert np.abs(b - A.to_scipy_full() @ x).max() <= 1e-10 * np.abs(b).max()
     s.close()
 
 
