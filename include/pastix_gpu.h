@@ -344,6 +344,17 @@ typedef struct pastix_gpu_analysis_s pastix_gpu_analysis_t;
 PASTIX_GPU_API int pastix_gpu_analyze_grid( pastix_gpu_analysis_t **an, int64_t nx, int64_t ny, int64_t nz,
                                             int64_t n, const int64_t *colptr, const int64_t *rowptr,
                                             const int64_t *iparm );
+/*
+ * The same tables read from files instead of computed: the SolverMatrix as
+ * the reference's solverSave writes it (blend/solver_io.c:261; the format
+ * solverLoad reads back, :45) and the ordering as pastixOrderSave writes it
+ * (order/order_io.c:293).  A saved analysis is handed to the GPU layer without
+ * running it again (refactorizations of the same pattern; the re-entry of
+ * pastix_subtask_bcsc2ctab, sopalin/pastix_task_sopalin.c:213).  Returns
+ * PASTIX_GPU_ERR_BADPARAMETER for a missing, malformed or inconsistent file.
+ */
+PASTIX_GPU_API int pastix_gpu_analysis_load( pastix_gpu_analysis_t **an, const char *solver_file,
+                                             const char *order_file );
 /* sizes[0..4] = n, cblknbr, bloknbr, brownbr, supernodes of the ordering */
 PASTIX_GPU_API int pastix_gpu_analysis_sizes( const pastix_gpu_analysis_t *an, int64_t *sizes );
 /* cblktab (cblknbr+1) x 4, bloktab bloknbr x 4, browtab, permtab/peritab (n),

@@ -81,6 +81,7 @@ def lib(variant=None):
         L.ref_order_dump.argtypes = [P, P, P]
         L.ref_coeftab_dump.argtypes = [P, P, P]
         L.ref_destroy.argtypes = [P]
+        L.ref_save_structure.argtypes = [P, C.c_char_p, C.c_char_p]
         _libs[variant] = L
     return _libs[variant]
 
@@ -198,6 +199,13 @@ class RefSolver:
         Uc = np.zeros(size, dt) if st["factotype"] == FACT["getrf"] else None
         lib(self.variant).ref_coeftab_dump(self.h, _ptr(Lc), _ptr(Uc))
         return Lc, Uc
+
+    def save_structure(self, solver_path, order_path):
+        """The reference's solverSave into solver_path, the ordering in its
+        ordering_save format into order_path (ref_glue.c)."""
+        rc = lib(self.variant).ref_save_structure(self.h, str(solver_path).encode(), str(order_path).encode())
+        if rc:
+            raise RuntimeError("save_structure failed: %d" % rc)
 
     def close(self):
         if self.h:

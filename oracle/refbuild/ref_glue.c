@@ -120,6 +120,36 @@ int ref_refine( ref_handle_t *h, int64_t nrhs, void *B, int64_t ldb, void *X, in
  * out[5]=gemmmax out[6]=offdmax out[7]=blokmax out[8]=colmax out[9]=factotype
  * out[10]=flttype out[11]=nb2dcblk out[12]=cblkmin2d out[13]=cblkmax1d
  */
+/*
+ * Save the analysis: the SolverMatrix by the reference's own solverSave
+ * (blend/solver_io.c:261) into solver_path, and the ordering into order_path
+ * in the format of the reference's ordering_save (order/order_io.c:199:
+ * "1", cblknbr, vertnbr, then rangtab, permtab and treetab, eight values per
+ * line).  The reference's pastixOrderSave (order/order_io.c:293) writes only
+ * when pastix_data->procnbr == 0, the total number of processes, which is
+ * never the case, so its format is written here.
+ */
+int ref_save_structure( ref_handle_t *h, const char *solver_path, const char *order_path )
+{
+    FILE *f = fopen( solver_path, "w" );
+    if ( !f ) return 1;
+    int rc = solverSave( h->pd->solvmatr, f );
+    fclose( f );
+    if ( rc ) return rc;
+    const pastix_order_t *o = h->pd->ordemesh;
+    f = fopen( order_path, "w" );
+    if ( !f ) return 1;
+    fprintf( f, "1\n%ld\t%ld\n", (long)o->cblknbr, (long)o->vertnbr );
+    for ( pastix_int_t k = 0; k <= o->cblknbr; k++ )
+        fprintf( f, "%ld%c", (long)o->rangtab[k], ( ( k & 7 ) == 7 || k == o->cblknbr ) ? '\n' : '\t' );
+    for ( pastix_int_t k = 0; k < o->vertnbr; k++ )
+        fprintf( f, "%ld%c", (long)o->permtab[k], ( ( k & 7 ) == 7 || k == o->vertnbr - 1 ) ? '\n' : '\t' );
+    for ( pastix_int_t k = 0; k < o->cblknbr; k++ )
+        fprintf( f, "%ld%c", (long)o->treetab[k], ( ( k & 7 ) == 7 || k == o->cblknbr - 1 ) ? '\n' : '\t' );
+    fclose( f );
+    return 0;
+}
+
 int ref_struct_sizes( ref_handle_t *h, int64_t *out )
 {
     SolverMatrix *s = h->pd->solvmatr;

@@ -19,6 +19,7 @@ def _lib():
         L.pastix_gpu_analyze_grid.argtypes = [C.POINTER(P), I64, I64, I64, I64, P, P, P]
         L.pastix_gpu_analysis_sizes.argtypes = [P, P]
         L.pastix_gpu_analysis_export.argtypes = [P, P, P, P, P, P, P, P]
+        L.pastix_gpu_analysis_load.argtypes = [C.POINTER(P), C.c_char_p, C.c_char_p]
         L.pastix_gpu_analysis_free.argtypes = [C.POINTER(P)]
         L.pastix_gpu_analysis_free.restype = None
         L._analysis_ready = True
@@ -41,6 +42,21 @@ def analyze(system, iparm=None):
     h = C.c_void_p()
     rc = L.pastix_gpu_analyze_grid(C.byref(h), nx, ny, nz, system.n, G._p(colptr), G._p(rowptr), G._p(ip))
     G._check("pastix_gpu_analyze_grid", rc)
+    return _export(L, h)
+
+
+def load(solver_file, order_file):
+    """The structure of a saved analysis: the reference's solverSave file and
+    its ordering file (pastixOrderSave), read by pastix_gpu_analysis_load;
+    same dict as analyze()."""
+    L = _lib()
+    h = C.c_void_p()
+    rc = L.pastix_gpu_analysis_load(C.byref(h), str(solver_file).encode(), str(order_file).encode())
+    G._check("pastix_gpu_analysis_load", rc)
+    return _export(L, h)
+
+
+def _export(L, h):
     try:
         sz = np.zeros(5, np.int64)
         L.pastix_gpu_analysis_sizes(h, G._p(sz))

@@ -20,8 +20,10 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <memory>
 #include <vector>
 
 namespace {
@@ -643,6 +645,102 @@ extern "C" int pastix_gpu_analyze_grid(pastix_gpu_analysis_t **out, int64_t nx, 
     split_symbol(s, bmin, bmax);
     an->symb = std::move(s);
     *out = an;
+    return PASTIX_GPU_SUCCESS;
+}
+
+// Structure handoff through files: the SolverMatrix written by the
+// reference's solverSave (blend/solver_io.c:261: header "2", then cblknbr,
+// bloknbr, nodenbr, baseval, one {fcolnum, lcolnum, first blok} line per
+// cblk and one {frownum, lrownum, fcblknm} line per blok; what follows --
+// coefficient offsets, tasks -- is not needed on the GPU) and the ordering
+// written by pastixOrderSave (order/order_io.c:199 ordering_save: header
+// "1", then cblknbr, vertnbr, rangtab, permtab, treetab).  The owner cblk of
+// each blok follows from the cblks' first bloks, the blocks facing each cblk
+// (browtab) from the bloks' facing cblks.
+static bool read_ints(FILE *f, I count, VI &out) {
+    out.resize(count);
+    for (I k = 0; k < count; k++) {
+        long v;
+        if (fscanf(f, "%ld", &v) != 1) return false;
+        out[k] = v;
+    }
+    return true;
+}
+
+extern "C" int pastix_gpu_analysis_load(pastix_gpu_analysis_t **out, const char *solver_file,
+                                        const char *order_file) {
+    if (!out || !solver_file || !order_file) return PASTIX_GPU_ERR_BADPARAMETER;
+    *out = nullptr;
+    std::unique_ptr<pastix_gpu_analysis_t> an(new pastix_gpu_analysis_t());
+    // the ordering
+    FILE *fo = fopen(order_file, "r");
+    if (!fo) return PASTIX_GPU_ERR_BADPARAMETER;
+    VI hdr;
+    bool ok = read_ints(fo, 3, hdr) && hdr[0] == 1 && hdr[1] > 0 && hdr[2] > 0;
+    Ordering &o = an->order;
+    if (ok) {
+        o.cblknbr = hdr[1];
+        o.n = hdr[2];
+        ok = read_ints(fo, o.cblknbr + 1, o.rangtab) && read_ints(fo, o.n, o.permtab) &&
+             read_ints(fo, o.cblknbr, o.treetab);
+    }
+    fclose(fo);
+    if (!ok) return PASTIX_GPU_ERR_BADPARAMETER;
+    const I obase = o.rangtab[0];
+    if (obase != 0 && obase != 1) return PASTIX_GPU_ERR_BADPARAMETER;
+    for (auto &v : o.rangtab) v -= obase;
+    for (auto &v : o.permtab) v -= obase;
+    o.peritab.assign(o.n, -1);
+    for (I i = 0; i < o.n; i++) {
+        if (o.permtab[i] < 0 || o.permtab[i] >= o.n || o.peritab[o.permtab[i]] >= 0) return PASTIX_GPU_ERR_BADPARAMETER;
+        o.peritab[o.permtab[i]] = i;
+    }
+    an->ocblknbr = o.cblknbr;
+    // the solver matrix
+    FILE *fs = fopen(solver_file, "r");
+    if (!fs) return PASTIX_GPU_ERR_BADPARAMETER;
+    Symbol &sy = an->symb;
+    ok = read_ints(fs, 5, hdr) && hdr[0] == 2 && hdr[1] > 0 && hdr[2] >= hdr[1] && hdr[3] == o.n &&
+         (hdr[4] == 0 || hdr[4] == 1);
+    VI ctab, btab;
+    if (ok) {
+        sy.cblknbr = hdr[1];
+        sy.bloknbr = hdr[2];
+        sy.nodenbr = hdr[3];
+        ok = read_ints(fs, 3 * sy.cblknbr, ctab) && read_ints(fs, 3 * sy.bloknbr, btab);
+    }
+    fclose(fs);
+    if (!ok) return PASTIX_GPU_ERR_BADPARAMETER;
+    const I base = hdr[4];
+    sy.fcol.resize(sy.cblknbr);
+    sy.lcol.resize(sy.cblknbr);
+    sy.bloknum.resize(sy.cblknbr + 1);
+    for (I c = 0; c < sy.cblknbr; c++) {
+        sy.fcol[c] = ctab[3 * c] - base;
+        sy.lcol[c] = ctab[3 * c + 1] - base;
+        sy.bloknum[c] = ctab[3 * c + 2];
+    }
+    sy.bloknum[sy.cblknbr] = sy.bloknbr;
+    sy.frow.resize(sy.bloknbr);
+    sy.lrow.resize(sy.bloknbr);
+    sy.fcblk.resize(sy.bloknbr);
+    sy.lcblk.resize(sy.bloknbr);
+    for (I b = 0; b < sy.bloknbr; b++) {
+        sy.frow[b] = btab[3 * b] - base;
+        sy.lrow[b] = btab[3 * b + 1] - base;
+        sy.fcblk[b] = btab[3 * b + 2] - base;
+    }
+    for (I c = 0; c < sy.cblknbr; c++) {
+        if (sy.bloknum[c] < 0 || sy.bloknum[c] >= sy.bloknum[c + 1] || sy.lcol[c] < sy.fcol[c])
+            return PASTIX_GPU_ERR_BADPARAMETER;
+        for (I b = sy.bloknum[c]; b < sy.bloknum[c + 1]; b++) {
+            if (sy.fcblk[b] < 0 || sy.fcblk[b] >= sy.cblknbr) return PASTIX_GPU_ERR_BADPARAMETER;
+            sy.lcblk[b] = c;
+        }
+    }
+    if (sy.lcol[sy.cblknbr - 1] + 1 != o.n) return PASTIX_GPU_ERR_BADPARAMETER;
+    sy.build_rowtab();
+    *out = an.release();
     return PASTIX_GPU_SUCCESS;
 }
 

@@ -104,3 +104,34 @@ def test_analysis_matches_reference_at_benchmark_sizes(cid, which):
     for k in ("permtab", "peritab", "cblktab", "bloktab"):
         assert np.array_equal(mine[k], g[k]), k
     assert _same_browtab(mine, g)
+
+
+@pytest.mark.skipif(not U.ref_available(), reason="reference oracle not built")
+@pytest.mark.parametrize("make,fact", [(lambda: M.laplacian_7pt(20), "potrf"),
+                                       (lambda: M.convdiff_upwind(14, 12, 9, 10.0), "getrf"),
+                                       (lambda: M.laplacian_7pt(40, 33, 1), "potrf")],
+                         ids=["lap20", "cd14x12x9", "lap2d_40x33"])
+def test_saved_analysis_loads_as_the_reference_structure(make, fact, tmp_path):
+    """The reference writes its analysis (its solverSave, and the ordering in
+    the format of its ordering_save); the GPU layer's loader
+    (pastix_gpu_analysis_load) reads the files back into the tables it hands
+    to pastix_gpu_structure: the same ordering, cblks, bloks and facing blocks
+    as the reference's SolverMatrix in memory."""
+    A = make()
+    ref, st = U.run_reference(A, fact, numfact=False)
+    g = U.gpu_structure(A, st)
+    ref.save_structure(tmp_path / "solvergen", tmp_path / "ordergen")
+    ref.close()
+    loaded = _an().load(tmp_path / "solvergen", tmp_path / "ordergen")
+    for k in ("permtab", "peritab", "cblktab", "bloktab"):
+        assert np.array_equal(loaded[k], g[k]), k
+    assert _same_browtab(loaded, g)
+
+
+def test_saved_analysis_rejects_bad_files(tmp_path):
+    from pastix_b200 import gpu as G
+    (tmp_path / "bad").write_text("7\n1 2 3\n")
+    with pytest.raises(G.PastixGpuError):
+        _an().load(tmp_path / "bad", tmp_path / "bad")
+    with pytest.raises(G.PastixGpuError):
+        _an().load(tmp_path / "missing", tmp_path / "missing")

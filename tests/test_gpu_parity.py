@@ -449,3 +449,29 @@ def test_fp64_dmma_matches_fma_tiles(name, make, fact, monkeypatch):
     if fact == "getrf":
         assert np.abs(U1 - U0).max() <= 1e-13 * np.abs(U0).max()
     s.close()
+
+
+def test_factorization_from_a_saved_analysis(tmp_path):
+    """Structure handoff through files: the reference's saved analysis
+    (solverSave + ordering file) loaded by pastix_gpu_analysis_load drives a
+    factorization and solve equal to the reference's."""
+    from pastix_b200 import analysis
+    A = M.diffusion_lognormal(18, 17, 16, 1.0, np.random.default_rng(31))
+    ref, st = U.run_reference(A, "potrf", nthreads=NTH)
+    ref.save_structure(tmp_path / "solvergen", tmp_path / "ordergen")
+    g = analysis.load(tmp_path / "solvergen", tmp_path / "ordergen")
+    from pastix_b200 import gpu as G
+    s = G.Solver()
+    s.set_iparm(G.IPARM_FACTORIZATION, G.FACT["potrf"])
+    s.set_structure(g)
+    s.set_spm(A)
+    s.numfact(A.values)
+    lay = U.layout_of(U.gpu_structure(A, st))
+    Lr, _ = U.ref_coeftab_1d(ref, st, lay)
+    Lg, _ = s.coeftab()
+    mask = U.lower_mask(lay)
+    assert np.abs(Lg - Lr)[mask].max() <= 1e-12 * np.abs(Lr).max()
+    x, b = M.rhs_from_xtrue(A, 2, np.random.default_rng(3))
+    assert np.abs(s.solve(b) - ref.solve(b)).max() <= 1e-11 * np.abs(x).max()
+    s.close()
+    ref.close()
