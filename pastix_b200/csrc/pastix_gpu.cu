@@ -663,7 +663,10 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     // real FP64: the large update and TRSM GEMMs on the FP64 tensor cores (DMMA),
     // planned like the single-precision tensor-core tiles (128 x 64 tiles)
     const bool use_dmma = !fp32 && !zc && C.tune[PGPU_TUNE_DMMA] != 0 && !C.record;
-    const int tbm = use_tc ? TC_BM : DG_BM, tbn = use_tc ? TC_BN : DG_BN;
+    // tile shape of the tensor-core lists: tcgen05 tiles in single precision
+    // (update tiles of LL^t / LU, and the TRSM tiles of every real form,
+    // LDL^t included), DMMA tiles in FP64
+    const int tbm = fp32 ? TC_BM : DG_BM, tbn = fp32 ? TC_BN : DG_BN;
     const bool lu = (fmode == FM_GETRF), ldl = fm_ldl(fmode);
     // panels taller than TRSM_GEMM_ROWS: inverse of the diagonal block, then the
     // off-diagonal rows times it as a GEMM (tensor cores in single precision)
@@ -1006,6 +1009,18 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     C.meta.invoff = C.d_invoff.p;
     C.trsm_gemm = tgemm;
     cudaStream_t s = C.stream;
+    // every tensor-core tile must start inside its task (a tile past the task
+    // would hand the MMA an empty or negative width)
+    for (const std::vector<int4> *lst : {&tctiles, &tttiles})
+        for (const int4 &t : *lst) {
+            const GemmTask &g = tasks[t.x];
+            const int N = (g.flags & 64) ? C.width[g.c] : C.blrow[g.b] - C.bfrow[g.b] + 1;
+            if ((int64_t)t.y * tbm >= g.M || (int64_t)t.z * tbn >= N ||
+                ((t.w & 1) && (int64_t)(t.y + 1) * tbm >= g.M)) {
+                fprintf(stderr, "pastix_gpu: tensor-core tile outside its task (plan error)\n");
+                return PASTIX_GPU_ERR_INTERNAL;
+            }
+        }
     PGPU_CHECK(C.d_tiles.upload(tiles, s));
     PGPU_CHECK(C.d_tctiles.upload(tctiles, s));
     PGPU_CHECK(C.d_trsm.upload(trsm, s));

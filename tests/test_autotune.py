@@ -45,7 +45,7 @@ def test_gpu_tuning_knobs_and_search():
     with pytest.raises(G.PastixGpuError):
         AT.set_knob(s, "mixed_gemm", 7)
     x, b = M.rhs_from_xtrue(A, 1, np.random.default_rng(5))
-    space = {"trsm_gemm_rows": [128, 256], "la_reserved_sms": [0, 16], "mixed_gemm": [2, 1]}
+    space = {"trsm_gemm_rows": [128, 256], "la_reserved_sms": [0, 16], "mixed_gemm": [3, 2, 1]}
     best, t, log = AT.tune(s, A.values, b, space=space, objective="solve")
     assert all(best[k] in v for k, v in space.items()) and t > 0 and len(log) >= 4
     for k, v in best.items():
