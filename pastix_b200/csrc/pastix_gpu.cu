@@ -200,6 +200,7 @@ struct pastix_gpu_s {
     // the target rows of the tensor-core update tasks (k_task_rowmap)
     DArr<int64_t> d_taux;
     DArr<int> d_tmap, d_tlist;
+    DArr<TcDesc> d_tcdesc, d_ttdesc;   // per tensor-core tile (update, TRSM): k_gemm_scatter_tc_tma's records
     int64_t hilo_plane = 0, ihilo_plane = 0;
     DArr<CUtensorMap> d_tmaps;
     DArr<int> d_mapidx;
@@ -825,7 +826,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
             C.tune[PGPU_TUNE_TC_TMA] != 0 && tensor_map_encoder() != nullptr;
     C.split_ptr.assign(C.nlevels + 1, 0);
     C.h16 = C.tma && mixed_gemm_mode(C) == MG_3XF16;
-    std::vector<int> mapidx_h;        // (3xFP16) operand maps of each source cblk, for the task scale bases
+    std::vector<int> mapidx_h;        // operand maps of each source cblk (TMA modes), for the tile descriptors
     std::vector<int64_t> hsbase_h;
     if (C.h16) {
         // 3xFP16: FP16 planes and row scales of the source matrices only (the
@@ -934,6 +935,7 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
         if (C.tma) {
             PGPU_CHECK(C.d_tmaps.upload(maps, C.stream));
             PGPU_CHECK(C.d_mapidx.upload(mapidx, C.stream));
+            mapidx_h = mapidx;
             PGPU_CHECK(C.d_split.upload(split, C.stream));
         } else {
             C.split_ptr.assign(C.nlevels + 1, 0);
@@ -1049,6 +1051,49 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
             }
         }
         PGPU_CHECK(C.d_taux.upload(taux, s));
+        if (C.tma) {
+            // one descriptor per tensor-core tile (k_gemm_scatter_tc_tma reads no task tables)
+            auto make_desc = [&](const int4 &t) {
+                const GemmTask &g = tasks[t.x];
+                const bool trsm = (g.flags & 64) != 0;
+                const int c = g.c, w = C.width[c];
+                const int N = trsm ? w : C.blrow[g.b] - C.bfrow[g.b] + 1;
+                const int i0 = t.y * TC_BM, j0 = t.z * TC_BN;
+                const int mb = mapidx_h[c];
+                TcDesc d;
+                std::memset(&d, 0, sizeof(d));
+                d.mapa = mb + ((g.flags & 1) ? TMAP_U : TMAP_L);
+                d.mapb = mb + (trsm ? ((g.flags & 128) ? TMAP_I2 : TMAP_I) : ((g.flags & 2) ? TMAP_U : TMAP_L));
+                d.rowa = g.arow0 + i0;
+                d.rowb = (trsm ? 0 : C.browoff[g.b]) + j0;
+                d.nk = cdiv(w, C.h16 ? 64 : TC_BK);
+                d.ncols = std::min(TC_BN, N - j0);
+                d.pair = t.w & 1;
+                d.flags = g.flags;
+                d.mrows = g.M - i0;
+                if (trsm) {
+                    d.ldo = C.ld[c];
+                    d.off = g.out + (int64_t)i0 * C.ld[c] + j0;
+                } else {
+                    const int f = g.f;
+                    d.ldo = C.ld[f];
+                    d.wf = C.width[f];
+                    d.tcol = C.bfrow[g.b] + j0 - C.fcol[f];
+                    d.off = ((g.flags & 4) ? C.coefnbr : 0) + C.coefoff[f];
+                    d.rmap = taux[3 * (size_t)t.x] + i0;
+                }
+                if (C.h16) {
+                    d.sa = taux[3 * (size_t)t.x + 1] + i0;
+                    d.sb = taux[3 * (size_t)t.x + 2] + j0;
+                }
+                return d;
+            };
+            std::vector<TcDesc> dtc(tctiles.size()), dtt(tttiles.size());
+            for (size_t i = 0; i < tctiles.size(); i++) dtc[i] = make_desc(tctiles[i]);
+            for (size_t i = 0; i < tttiles.size(); i++) dtt[i] = make_desc(tttiles[i]);
+            PGPU_CHECK(C.d_tcdesc.upload(dtc, s));
+            PGPU_CHECK(C.d_ttdesc.upload(dtt, s));
+        }
         PGPU_CHECK(C.d_tlist.upload(tlist, s));
         if (C.d_tmap.n < (size_t)std::max<int64_t>(rows, 1)) PGPU_CHECK(C.d_tmap.alloc(std::max<int64_t>(rows, 1)));
         if (!tlist.empty())
@@ -1296,13 +1341,12 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                 if (persist && C.tma && C.h16) {
                     const int g = std::min(ntc, gcap);
                     k_gemm_scatter_tc_tma<true, true><<<g, TMA_THREADS, tma_smem_bytes<true>(), st>>>(
-                        C.meta, C.d_tctiles.p + c0, ntc, C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr,
-                        C.d_tmaps.p, C.d_mapidx.p, C.d_tmap.p, C.d_taux.p, C.d_hscale.p);
+                        C.d_tcdesc.p + c0, ntc, coefL, C.d_status.p, nullptr, C.d_tmaps.p, C.d_tmap.p,
+                        C.d_hscale.p);
                 } else if (persist && C.tma) {
                     const int g = std::min(ntc, gcap);
                     k_gemm_scatter_tc_tma<true><<<g, TMA_THREADS, tma_smem_bytes<true>(), st>>>(
-                        C.meta, C.d_tctiles.p + c0, ntc, C.d_tasks.p, coefL, coefU, C.d_status.p, nullptr,
-                        C.d_tmaps.p, C.d_mapidx.p, C.d_tmap.p, C.d_taux.p);
+                        C.d_tcdesc.p + c0, ntc, coefL, C.d_status.p, nullptr, C.d_tmaps.p, C.d_tmap.p);
                 } else if (persist) {
                     const int g = std::min(ntc, gcap);
                     if (split)
@@ -1425,12 +1469,11 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                     const int g = std::min(ntc, nsm);
                     if (C.tma && C.h16)
                         k_gemm_scatter_tc_tma<true, true><<<g, TMA_THREADS, tma_smem_bytes<true>(), s>>>(
-                            C.meta, C.d_tttiles.p + C.tttile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
-                            scr, C.d_tmaps.p, C.d_mapidx.p, C.d_tmap.p, C.d_taux.p, C.d_hscale.p);
+                            C.d_ttdesc.p + C.tttile_ptr[l], ntc, coefL, C.d_status.p, scr, C.d_tmaps.p, C.d_tmap.p,
+                            C.d_hscale.p);
                     else if (C.tma)
                         k_gemm_scatter_tc_tma<true><<<g, TMA_THREADS, tma_smem_bytes<true>(), s>>>(
-                            C.meta, C.d_tttiles.p + C.tttile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,
-                            scr, C.d_tmaps.p, C.d_mapidx.p, C.d_tmap.p, C.d_taux.p);
+                            C.d_ttdesc.p + C.tttile_ptr[l], ntc, coefL, C.d_status.p, scr, C.d_tmaps.p, C.d_tmap.p);
                     else if (split)
                         k_gemm_scatter_tc_persistent<true><<<g, TCP_THREADS, tcp_smem_bytes<true>(), s>>>(
                             C.meta, C.d_tttiles.p + C.tttile_ptr[l], ntc, C.d_tasks.p, coefL, coefU, C.d_status.p,

@@ -70,6 +70,31 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
+// Everything the three roles need for one tile, built on the host when the
+// plan is made: the kernel reads one 96-byte record per tile (loaded one or
+// two tiles ahead) instead of walking tile -> task -> cblk tables through
+// chains of dependent loads before it can issue a tile's loads or MMAs.
+struct __align__(16) TcDesc {
+    int mapa, mapb, rowa, rowb;   // tensor maps (indices into maps) and row coordinates of A and B
+    int nk, ncols, pair, flags;   // k-blocks, valid columns, paired 128-row tiles, task flags (64: TRSM)
+    int mrows, ldo, wf, tcol;     // rows from the tile's first; target (or output) row stride, target
+                                  // cblk width (lower-triangle rule), first target column
+    int pad[4];
+    int64_t off;                  // target panel offset from coefL, or (TRSM) output offset in scr
+    int64_t rmap;                 // row-map index of the tile's first row (update tiles)
+    int64_t sa, sb;               // 3xFP16: scale index of the first A row, of the first B row
+};
+static_assert(sizeof(TcDesc) == 96, "TcDesc is six 16-byte vectors");
+
+__device__ __forceinline__ TcDesc tc_desc_load(const TcDesc *p) {
+    TcDesc d;
+    const int4 *s = reinterpret_cast<const int4 *>(p);
+    int4 *o = reinterpret_cast<int4 *>(&d);
+#pragma unroll
+    for (int k = 0; k < 6; k++) o[k] = __ldg(s + k);
+    return d;
+}
+
 // F16 (with SPLIT): "3xFP16" operands -- every row r of a source matrix
 // (panel rows, diagonal-block inverse rows) is scaled by a power of two
 // 2^e_r that brings its largest magnitude into [2^14, 2^15), then split into
@@ -82,11 +107,9 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
 // gives each operand map's first row there), exact powers of two.
 template <bool SPLIT, bool F16 = false>
 __global__ void __launch_bounds__(TMA_THREADS, 1)
-    k_gemm_scatter_tc_tma(Meta m, const int4 *__restrict__ tiles, int ntiles, const GemmTask *__restrict__ tasks,
-                          float *__restrict__ coefL, float *__restrict__ coefU, Status *st, float *__restrict__ scr,
-                          const CUtensorMap *__restrict__ maps, const int *__restrict__ mapidx,
-                          const int *__restrict__ tmap, const int64_t *__restrict__ taux,
-                          const float *__restrict__ hscale = nullptr) {
+    k_gemm_scatter_tc_tma(const TcDesc *__restrict__ desc, int ntiles, float *__restrict__ coefL, Status *st,
+                          float *__restrict__ scr, const CUtensorMap *__restrict__ maps,
+                          const int *__restrict__ tmap, const float *__restrict__ hscale = nullptr) {
     static_assert(!F16 || SPLIT, "the FP16 operands are always split");
     constexpr int S = TmaCfg<SPLIT>::STAGES, NT = TmaCfg<SPLIT>::TILES, PL = TmaCfg<SPLIT>::PL;
     constexpr int BK = F16 ? 64 : TC_BK;                              // elements per k-block (128 B per row)
@@ -133,31 +156,12 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
         // ---------------- TMA producer ----------------
         if (lane == 0) {
             int it = 0;
-            // operands of a tile: both maps, their row coordinates, k-blocks
-            struct Ops {
-                const CUtensorMap *ma, *mb;
-                int rowa, rowb, nk, pair;
-            };
-            auto ops_of = [&](int ti) {
-                const int4 tl = tiles[ti];
-                const GemmTask t = tasks[tl.x];
-                const bool trsm = (t.flags & 64) != 0;
-                const int mb = mapidx[t.c];
-                Ops o;
-                o.ma = maps + mb + ((t.flags & 1) ? TMAP_U : TMAP_L);
-                o.mb = maps + mb + (trsm ? ((t.flags & 128) ? TMAP_I2 : TMAP_I) : ((t.flags & 2) ? TMAP_U : TMAP_L));
-                o.rowa = t.arow0 + tl.y * TC_BM;
-                o.rowb = (trsm ? 0 : m.browoff[t.b]) + tl.z * TC_BN;
-                o.nk = (m.width[t.c] + BK - 1) / BK;
-                o.pair = tl.w & 1;
-                return o;
-            };
-            Ops nxt{};
-            if (blockIdx.x < ntiles) nxt = ops_of(blockIdx.x);
+            TcDesc nx{};
+            if (blockIdx.x < ntiles) nx = tc_desc_load(desc + blockIdx.x);
             for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x) {
-                const Ops o = nxt;
-                if (ti + (int)gridDim.x < ntiles) nxt = ops_of(ti + gridDim.x);   // in flight during this tile
-                const CUtensorMap *ma = o.ma, *mbm = o.mb;
+                const TcDesc o = nx;
+                if (ti + (int)gridDim.x < ntiles) nx = tc_desc_load(desc + ti + gridDim.x);   // for the next tile
+                const CUtensorMap *ma = maps + o.mapa, *mbm = maps + o.mapb;
                 const int rowa = o.rowa, rowb = o.rowb, nk = o.nk;
                 const uint32_t bytes = (o.pair ? 3u : 2u) * BOX_BYTES;
                 bool ok = true;
@@ -192,14 +196,13 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             int it = 0, tl = 0;
-            TcTileView nv{};
-            if (blockIdx.x < ntiles) nv = tc_tile_view(m, tiles[blockIdx.x], tasks, coefL, coefU, nullptr);
+            TcDesc nx{};
+            if (blockIdx.x < ntiles) nx = tc_desc_load(desc + blockIdx.x);
             for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x, tl++) {
-                const TcTileView v = nv;
-                if (ti + (int)gridDim.x < ntiles)   // the next tile's view loads while this one runs
-                    nv = tc_tile_view(m, tiles[ti + gridDim.x], tasks, coefL, coefU, nullptr);
+                const TcDesc v = nx;
+                if (ti + (int)gridDim.x < ntiles) nx = tc_desc_load(desc + ti + gridDim.x);   // for the next tile
                 const uint32_t idesc = F16 ? tc_idesc_f16(tc_mma_n(v.ncols)) : tc_idesc(tc_mma_n(v.ncols));
-                const int vnk = F16 ? (v.K + BK - 1) / BK : v.nk;
+                const int vnk = v.nk;
                 const int ab = tl & 1;
                 const uint32_t acc = tmem + (uint32_t)(ab * 256), acc1 = acc + 128u;
                 const bool pair = v.pair != 0;
@@ -266,33 +269,38 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
         const int grp = warp < 4 ? 0 : 1;              // column chunks 32 grp, 32 grp + 64
         float *E = epi + ew * 32 * 33;
         const int myrow = qw * 32 + lane;
+        // two stages: the descriptor of tile t + 2 is loaded while tile t is
+        // written back, and the row targets / scales of tile t + 1 (which need
+        // its descriptor) are requested then too
         struct EpiTile {
-            TcTileView v;
+            TcDesc d;
             int tr[2];
-            float rs[2];
-            int64_t sb;
+            float rs[2], cs[2];
         };
-        auto prep = [&](int ti, EpiTile &e) {
-            const int4 tl = tiles[ti];
-            e.v = tc_tile_view(m, tl, tasks, coefL, coefU, nullptr);
-            const bool trsm = (e.v.flags & 64) != 0;
-            const int64_t *ax = taux + 3 * (int64_t)tl.x;   // {row-map base, A scale base, B scale base}
-            const int64_t tb = ax[0];
-            const int64_t sa = F16 ? ax[1] : 0;
-            e.sb = F16 ? ax[2] + e.v.j0 : 0;
+        auto prep = [&](const TcDesc &d, EpiTile &e) {
+            e.d = d;
+            const bool trsm = (d.flags & 64) != 0;
             for (int h = 0; h < 2; h++) {
                 const int row = h * TC_BM + myrow;   // row of the pair, from the first tile's first row
-                const bool ok = (h == 0 || e.v.pair) && row < e.v.M - e.v.i0;
-                e.tr[h] = (ok && !trsm) ? tmap[tb + e.v.i0 + row] : -1;
-                e.rs[h] = (F16 && ok) ? hscale[sa + e.v.i0 + row] : 1.f;
+                const bool ok = (h == 0 || d.pair) && row < d.mrows;
+                e.tr[h] = (ok && !trsm) ? tmap[d.rmap + row] : -1;
+                e.rs[h] = (F16 && ok) ? hscale[d.sa + row] : 1.f;
+                // this warp's two 32-column chunks: column 32 grp + 64 h + lane
+                const int col = 32 * grp + 64 * h + lane;
+                e.cs[h] = (F16 && col < d.ncols) ? hscale[d.sb + col] : 0.f;
             }
         };
         EpiTile cur{}, nxt{};
-        if (blockIdx.x < ntiles) prep(blockIdx.x, cur);
+        TcDesc dn{};
+        if (blockIdx.x < ntiles) prep(tc_desc_load(desc + blockIdx.x), cur);
+        if (blockIdx.x + (int)gridDim.x < ntiles) dn = tc_desc_load(desc + blockIdx.x + gridDim.x);
         int tl = 0;
         for (int ti = blockIdx.x; ti < ntiles && !failed(); ti += gridDim.x, tl++) {
-            if (ti + (int)gridDim.x < ntiles) prep(ti + gridDim.x, nxt);
-            const TcTileView &v = cur.v;
+            if (ti + (int)gridDim.x < ntiles) {
+                prep(dn, nxt);
+                if (ti + 2 * (int)gridDim.x < ntiles) dn = tc_desc_load(desc + ti + 2 * gridDim.x);
+            }
+            const TcDesc &v = cur.d;
             const int ab = tl & 1;
             const bool trsm = (v.flags & 64) != 0;
             const int nh = v.pair ? 2 : 1;
@@ -303,23 +311,23 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int trw[2] = {cur.tr[0], cur.tr[1]};   // each lane's row target, shuffled to the writers
             const float rs[2] = {cur.rs[0], cur.rs[1]};
-            const int64_t sb = cur.sb;
-            float *C = ((v.flags & 4) ? coefU : coefL) + m.coefoff[v.f];
-            const int ldf = m.ld[v.f], wf = m.width[v.f];
-            const int tcol0 = m.bfrow[v.b] + v.j0 - m.fcol[v.f];
+            const float csr[2] = {cur.cs[0], cur.cs[1]};
+            float *C = coefL + v.off;
+            const int ldf = v.ldo, wf = v.wf;
+            const int tcol0 = v.tcol;
             const bool lower_only = (v.flags & 8) != 0;
             for (int h = 0; h < nh; h++)
             for (int cb = 32 * grp; cb < TC_BN; cb += 64) {
-                const int mrows = min(TC_BM, v.M - v.i0 - h * TC_BM);   // valid rows of this half
+                const int mrows = min(TC_BM, v.mrows - h * TC_BM);   // valid rows of this half
                 uint32_t r[32];
                 tc_ld32(tmem + (uint32_t)(ab * 256 + h * 128) + ((uint32_t)(qw * 32) << 16) + (uint32_t)cb, r);
                 __syncwarp();
                 if (F16) {
-                    // column cb + lane's inverse scale, broadcast column by column
-                    const float cs = (cb + lane < v.ncols) ? hscale[sb + cb + lane] : 0.f;
+                    // column cb + lane's inverse scale (loaded with the tile), broadcast column by column
+                    const float cs = (cb - 32 * grp) ? csr[1] : csr[0], rsh = h ? rs[1] : rs[0];
 #pragma unroll
                     for (int q = 0; q < 32; q++)
-                        E[lane * 33 + q] = __uint_as_float(r[q]) * rs[h] * __shfl_sync(0xffffffffu, cs, q);
+                        E[lane * 33 + q] = __uint_as_float(r[q]) * rsh * __shfl_sync(0xffffffffu, cs, q);
                 } else {
 #pragma unroll
                     for (int q = 0; q < 32; q++) E[lane * 33 + q] = __uint_as_float(r[q]);
@@ -327,8 +335,8 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                 __syncwarp();
                 const int j = cb + lane;
                 if (j < v.ncols && trsm) {
-                    const int ldc = m.ld[v.c];
-                    float *O = scr + v.out + (int64_t)(v.i0 + h * TC_BM) * ldc + v.j0;
+                    const int ldc = v.ldo;
+                    float *O = scr + v.off + (int64_t)h * TC_BM * ldc;
                     for (int rr = 0; rr < 32; rr++) {
                         const int i = qw * 32 + rr;
                         if (i >= mrows) break;
@@ -339,7 +347,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                     const int tcs = tcol0 + cb, a0 = tcs & ~3, o = tcs - a0;
                     for (int k = lane; k < 32 * 9; k += 32) {
                         const int rr = k / 9, g = k - rr * 9;
-                        const int t2 = __shfl_sync(0xffffffffu, trw[h], rr);
+                        const int t2 = __shfl_sync(0xffffffffu, h ? trw[1] : trw[0], rr);
                         if (t2 < 0) continue;
                         float a[4];
                         bool any = false;
