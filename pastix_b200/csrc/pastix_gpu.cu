@@ -10,12 +10,14 @@
 #include "pgpu_gemm_tma.cuh"
 #include "pgpu_gemm_f64.cuh"
 #include "pgpu_spm.cuh"
+#include "pgpu_solve_flow.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <queue>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -201,6 +203,24 @@ struct pastix_gpu_s {
     DArr<int64_t> d_taux;
     DArr<int> d_tmap, d_tlist;
     DArr<TcDesc> d_tcdesc, d_ttdesc;   // per tensor-core tile (update, TRSM): k_gemm_scatter_tc_tma's records
+    // dataflow solve of runs of levels whose cblks all hold a diagonal-block
+    // inverse (k_solve_flow): runs {first level, end level}, per run the task
+    // ranges (forward, backward), the per-cblk counters (5 x cblknbr) and their
+    // per-launch increments (4 x cblknbr), epochs and ticket bases, the Y and Z
+    // blocks (n x FLOW_MAXRHS each), the largest width of a run's cblk
+    std::vector<int2> flow_runs;
+    std::vector<int> flow_tptr[2];    // per run: first task
+    DArr<int> d_flow_off[2];          // per run: 2 x (G + 1) offsets of the CTAs' tasks in the two lists
+    int flow_G = 0;
+    DArr<FlowTask> d_flow_tasks[2];
+    DArr<unsigned long long> d_flow_cnt;
+    DArr<int> d_flow_need;
+    DArr<FlowState> d_flow_state;
+    DArr<unsigned char> d_flowY, d_flowZ;
+    DArr<unsigned long long> d_flow_stamps;   // per-task times of the last launch (PASTIX_GPU_SOLVE_PROFILE=3)
+    std::vector<unsigned long long> flow_epoch[2];
+    int flow_maxw = 0;
+    bool flow_used = false;
     int64_t hilo_plane = 0, ihilo_plane = 0;
     DArr<CUtensorMap> d_tmaps;
     DArr<int> d_mapidx;
@@ -257,6 +277,8 @@ extern "C" int pastix_gpu_init(pastix_gpu_t **pctx, int device, const int64_t *i
     PGPU_CHECK(ctx->d_partial.alloc(1024));
     PGPU_CHECK(ctx->d_scalar.alloc(16));
     PGPU_CHECK(ctx->d_fact_scal.alloc(4));
+    PGPU_CHECK(ctx->d_flow_state.alloc(1));
+    PGPU_CHECK(cudaMemset(ctx->d_flow_state.p, 0, sizeof(FlowState)));
     *pctx = ctx;
     return PASTIX_GPU_SUCCESS;
 }
@@ -568,6 +590,8 @@ static void default_tuning(int64_t *t) {
     t[PGPU_TUNE_TC_PAIR_MIN] = -1;
     e = getenv("PASTIX_GPU_DMMA");
     t[PGPU_TUNE_DMMA] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
+    e = getenv("PASTIX_GPU_SOLVE_CHAIN");
+    t[PGPU_TUNE_SOLVE_CHAIN] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
 }
 static int mixed_gemm_mode(const pastix_gpu_t &C) { return (int)C.tune[PGPU_TUNE_MIXED_GEMM]; }
 
@@ -657,6 +681,191 @@ static void invalidate_graph(pastix_gpu_t &C) {
     C.fact_exec = nullptr;
     C.fact_graph = nullptr;
     for (int k = 0; k < 5; k++) C.graph_key[k] = -1;
+}
+
+// Clears the dataflow solve's counters, ticket counters, error flag and Z
+// (a new plan, or a solve whose waits gave up).
+static int flow_reset(pastix_gpu_t &C) {
+    if (C.d_flow_cnt.n) PGPU_CHECK(cudaMemsetAsync(C.d_flow_cnt.p, 0, C.d_flow_cnt.n * sizeof(unsigned long long), C.stream));
+    if (C.d_flowZ.n) PGPU_CHECK(cudaMemsetAsync(C.d_flowZ.p, 0, C.d_flowZ.n, C.stream));
+    PGPU_CHECK(cudaMemsetAsync(C.d_flow_state.p, 0, sizeof(FlowState), C.stream));
+    for (int d = 0; d < 2; d++) C.flow_epoch[d].assign(C.flow_runs.size(), 0);
+    return PASTIX_GPU_SUCCESS;
+}
+
+// Runs of consecutive levels the dataflow solve takes (k_solve_flow): levels
+// that are not solved one warp per cblk and whose cblks all hold the inverse
+// of their diagonal block (and narrow enough for one stage's vector part of
+// FLOW_MAXRHS right-hand sides, complex128: 2).  Tasks of at most
+// FLOW_MAXROWS rows (fewer where a row is long: one staging buffer), in two
+// lists per direction -- critical: the diagonal tasks and the updates of a
+// cblk of the next level; the others -- each sorted by one key that is a
+// dependency order (a task waits only for tasks with smaller keys):
+//   forward, by deadline: D(c): 2 lev(c); O(c, f): 2 lev(f) - 1 (just before
+//            D(f)), or 2 lb when f lies above the run; older sources first;
+//   backward, by the point where the input exists, with depth
+//            d = (last level of the run) - lev:  E(c): 2 d(c) + 1;
+//            G(c, f): 2 d(f) + 2 (after x_f), or 0 when f lies above the run;
+//            the nearest source first.
+// (Forward, the deadline order keeps each level's inputs together; backward,
+// the input order lets gathers run as soon as x_f exists: each measured the
+// faster for its direction.)  Each record carries the task's deadline -- the
+// key of the task that needs it (backward G: 2 d(c)) -- by which the fetch
+// warp chooses between the heads of its two lists.  List task i goes to CTA
+// i mod G (G: one CTA per SM); the lists are stored CTA by CTA.  Y and Z for
+// up to FLOW_MAXRHS right-hand sides are allocated here, with the plan (the
+// allocation-free solve allocates nothing).
+static int build_flow_plan(pastix_gpu_t &C, size_t esz, bool lu) {
+    C.flow_runs.clear();
+    C.flow_maxw = 0;
+    if (!C.trsm_gemm) return PASTIX_GPU_SUCCESS;
+    const int nc = C.cblknbr;
+    std::vector<char> ok(C.nlevels, 0);
+    for (int l = 0; l < C.nlevels; l++) {
+        bool all = !(C.lvl_maxw[l] <= 32 && C.lvl_maxh[l] <= SOLVE_SMALL_MAXH) && C.lvl_ptr[l + 1] > C.lvl_ptr[l];
+        for (int q = C.lvl_ptr[l]; q < C.lvl_ptr[l + 1] && all; q++) {
+            const int c = C.lvl_cblks[q];
+            const size_t vmax = (size_t)std::max(C.width[c], FLOW_MAXROWS) * (esz <= 8 ? FLOW_MAXRHS : 2) * esz;
+            all = C.invoff[c] >= 0 && vmax + 16 <= (size_t)FLOW_VEC_BYTES && (size_t)C.ld[c] * esz <= (size_t)FLOW_STAGE;
+        }
+        ok[l] = all;
+    }
+    for (int l = 0; l < C.nlevels;) {
+        if (!ok[l]) {
+            l++;
+            continue;
+        }
+        int e = l;
+        while (e < C.nlevels && ok[e]) e++;
+        C.flow_runs.push_back(make_int2(l, e));
+        l = e;
+    }
+    if (C.flow_runs.empty()) return PASTIX_GPU_SUCCESS;
+    std::vector<int> runid(nc, -1);
+    for (size_t r = 0; r < C.flow_runs.size(); r++)
+        for (int q = C.lvl_ptr[C.flow_runs[r].x]; q < C.lvl_ptr[C.flow_runs[r].y]; q++) {
+            runid[C.lvl_cblks[q]] = (int)r;
+            C.flow_maxw = std::max(C.flow_maxw, C.width[C.lvl_cblks[q]]);
+        }
+    std::vector<int> need(4 * (size_t)nc, 0);   // nd, noin, ngo, ned
+    int G = 0;   // CTAs of a launch: one per SM
+    PGPU_CHECK(cudaDeviceGetAttribute(&G, cudaDevAttrMultiProcessorCount, C.device));
+    int *nd = need.data(), *noin = nd + nc, *ngo = noin + nc, *ned = ngo + nc;
+    C.flow_G = G;
+    std::vector<FlowTask> all[2];
+    std::vector<int> offs[2];
+    for (int d = 0; d < 2; d++) C.flow_tptr[d].assign(1, 0);
+    for (size_t r = 0; r < C.flow_runs.size(); r++) {
+        const int la = C.flow_runs[r].x, lb = C.flow_runs[r].y;
+        auto lev = [&](int c) { return C.cblk_level[c]; };
+        // the factor rows of a task: D / E rows of the inverse (forward LU: the
+        // second, unit-lower one), O / G rows of the panel (backward LU: U^t)
+        auto task = [&](int kind, bool fwd, int flag, int nr, int c, int r0, int f) {
+            FlowTask t;
+            t.hdr = kind | (flag << 3) | (nr << 4);
+            t.c = c;
+            t.r0 = r0;
+            t.f = f;
+            t.w = C.width[c];
+            t.ld = C.ld[c];
+            t.fc = C.fcol[c];
+            t.need = 0;   // (set once every task of the run is counted)
+            if (kind == FLOW_D) {
+                t.src = C.invoff[c] + (fwd && lu ? inv_span(C.width[c], C.ld[c]) : 0) + (int64_t)r0 * C.ld[c];
+                t.aux = C.coefoff[c];
+            } else {
+                t.src = (!fwd && lu ? C.coefnbr : 0) + C.coefoff[c] + (int64_t)r0 * C.ld[c];
+                t.aux = C.rowbase[c] + r0;
+            }
+            return t;
+        };
+        struct Keyed {
+            int key, sec, seq;   // list order: key, then sec, then creation
+            FlowTask t;
+            bool high;           // critical list
+            int deadline;        // the key of the task that needs it (stored in the record)
+        };
+        std::vector<Keyed> fw, bw;
+        for (int l = la; l < lb; l++)
+            for (int q = C.lvl_ptr[l]; q < C.lvl_ptr[l + 1]; q++) {
+                const int c = C.lvl_cblks[q];
+                const int w = C.width[c];
+                const int R = std::max(1, std::min(FLOW_MAXROWS, (int)((size_t)FLOW_STAGE / ((size_t)C.ld[c] * esz))));
+                const int dc = lb - 1 - l;
+                for (int n0 = 0; n0 < w; n0 += R) {
+                    const int nr = std::min(R, w - n0);
+                    fw.push_back({2 * l, 0, (int)fw.size(), task(FLOW_D, true, 0, nr, c, n0, 0), true, 2 * l});
+                    bw.push_back({2 * dc + 1, 0, (int)bw.size(), task(FLOW_D, false, 0, nr, c, n0, 0), true,
+                                  2 * dc + 1});
+                    nd[c]++;
+                    ned[c]++;
+                }
+                // off-diagonal rows, in runs of blocks facing the same cblk
+                for (int b = C.fblok[c] + 1; b < C.fblok[c + 1];) {
+                    const int f = C.bfcblk[b];
+                    int e = b;
+                    while (e < C.fblok[c + 1] && C.bfcblk[e] == f) e++;
+                    const int ra = C.browoff[b], rb = C.browoff[e - 1] + C.blrow[e - 1] - C.bfrow[e - 1] + 1;
+                    const bool in = runid[f] == (int)r;
+                    const bool next = in && lev(f) == l + 1;
+                    const int df = lb - 1 - lev(f);
+                    for (int r0 = ra; r0 < rb; r0 += R) {
+                        const int nr = std::min(R, rb - r0);
+                        const int fkey = in ? 2 * lev(f) - 1 : 2 * lb;
+                        fw.push_back({fkey, l, (int)fw.size(), task(FLOW_O, true, in ? 1 : 0, nr, c, r0, f), next, fkey});
+                        bw.push_back({in ? 2 * df + 2 : 0, dc, (int)bw.size(),
+                                      task(FLOW_O, false, in ? 1 : 0, nr, c, r0, f), next, 2 * dc});
+                        if (in) noin[f]++;
+                        ngo[c]++;
+                    }
+                    b = e;
+                }
+            }
+        for (int d = 0; d < 2; d++) {
+            std::vector<Keyed> &v = d ? bw : fw;
+            std::stable_sort(v.begin(), v.end(), [](const Keyed &x, const Keyed &y) {
+                if (x.high != y.high) return x.high;   // critical list first
+                return x.key != y.key ? x.key < y.key : (x.sec != y.sec ? x.sec < y.sec : x.seq < y.seq);
+            });
+            int nh = 0;
+            for (const Keyed &k : v) nh += k.high ? 1 : 0;
+            // each list CTA by CTA: list task i goes to CTA i mod G, the CTA's tasks contiguous and in
+            // list order; offsets: G + 1 for the critical list, then G + 1 for the other
+            for (int part = 0; part < 2; part++) {
+                const int b = part ? nh : 0, n = part ? (int)v.size() - nh : nh;
+                offs[d].push_back(part ? nh : 0);
+                for (int q = 0; q < G; q++) {
+                    for (int i = q; i < n; i += G) {
+                        FlowTask t = v[b + i].t;
+                        const int kind = t.hdr & 7, flag = (t.hdr >> 3) & 1;
+                        t.hdr |= v[b + i].deadline << 10;
+                        if (d == 0) t.need = kind == FLOW_D ? noin[t.c] : nd[t.c];
+                        else t.need = kind == FLOW_D ? ngo[t.c] : flag;
+                        all[d].push_back(t);
+                    }
+                    offs[d].push_back((int)all[d].size() - C.flow_tptr[d].back());
+                }
+            }
+            C.flow_tptr[d].push_back((int)all[d].size());
+        }
+    }
+    for (int d = 0; d < 2; d++) PGPU_CHECK(C.d_flow_off[d].upload(offs[d], C.stream));
+    for (int d = 0; d < 2; d++) PGPU_CHECK(C.d_flow_tasks[d].upload(all[d], C.stream));
+    PGPU_CHECK(C.d_flow_need.upload(need, C.stream));
+    if (C.d_flow_cnt.n < 5 * (size_t)nc) {
+        C.d_flow_cnt.release();
+        PGPU_CHECK(C.d_flow_cnt.alloc(5 * (size_t)nc));
+    }
+    const size_t vbytes = (size_t)C.n * FLOW_MAXRHS * esz;
+    if (C.d_flowY.n < vbytes) {
+        C.d_flowY.release();
+        PGPU_CHECK(C.d_flowY.alloc(vbytes));
+    }
+    if (C.d_flowZ.n < vbytes) {
+        C.d_flowZ.release();
+        PGPU_CHECK(C.d_flowZ.alloc(vbytes));
+    }
+    return flow_reset(C);
 }
 
 static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
@@ -1104,6 +1313,10 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
     PGPU_CHECK(C.d_pjobs.upload(pjobs, s));
     PGPU_CHECK(C.d_sjobs.upload(sjobs, s));
     PGPU_CHECK(C.d_wjobs.upload(wjobs, s));
+    {
+        int rc = build_flow_plan(C, esz, lu);
+        if (rc) return rc;
+    }
     PGPU_CHECK(cudaStreamSynchronize(s));
     C.h_tiles.swap(tiles);
     C.h_tctiles.swap(tctiles);
@@ -1752,6 +1965,124 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
 // sopalin/pastix_task_solve.c:600-650 (forward L; for LDL the diagonal
 // solve, sequential_zdiag.c; backward op(L)^t or U).
 // --------------------------------------------------------------------------
+// One launch of the dataflow solve over run `run`, forward or backward: a
+// cooperative launch (every CTA resident), one CTA per SM.
+template <typename T, int NR>
+static int flow_launch(pastix_gpu_t &C, bool fwd, int run, const T *coefL, const T *inv, T *W, int ldb, bool ldl,
+                       int cjp) {
+    const int dir = fwd ? 0 : 1;
+    auto kern = fwd ? k_solve_flow<T, NR, true> : k_solve_flow<T, NR, false>;
+    const int vec_elems = (int)align16_elems<T>((size_t)std::max(C.flow_maxw, FLOW_MAXROWS) * NR);
+    const size_t smem = (size_t)FLOW_S * FLOW_STAGE + (size_t)FLOW_S * vec_elems * sizeof(T);
+    if ((size_t)vec_elems * sizeof(T) > (size_t)FLOW_VEC_BYTES) return PASTIX_GPU_ERR_INTERNAL;
+    static size_t attr[2] = {0, 0};   // dynamic shared memory the kernel is set up for
+    if (attr[dir] < smem) {
+        PGPU_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr[dir] = smem;
+    }
+    int nsm = 0, per = 0;
+    PGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, C.device));
+    PGPU_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, FLOW_THREADS, smem));
+    if (per < 1) return PASTIX_GPU_ERR_INTERNAL;
+    const unsigned long long nc = (unsigned long long)C.cblknbr;
+    FlowArgs<T> a;
+    a.m = C.meta;
+    if (nsm != C.flow_G) return PASTIX_GPU_ERR_INTERNAL;   // (the schedule is for this many CTAs)
+    a.tasks = C.d_flow_tasks[dir].p + C.flow_tptr[dir][run];
+    a.ntasks = C.flow_tptr[dir][run + 1] - C.flow_tptr[dir][run];
+    a.off = C.d_flow_off[dir].p + (size_t)run * 2 * (nsm + 1);
+    a.epoch = ++C.flow_epoch[dir][run];
+    a.fs = C.d_flow_state.p;
+    unsigned long long *cnt = C.d_flow_cnt.p;
+    const int *need = C.d_flow_need.p;
+    a.k = FlowCounters{cnt, cnt + nc, cnt + 2 * nc, cnt + 3 * nc, cnt + 4 * nc,
+                       need, need + nc, need + 2 * nc, need + 3 * nc};
+    a.coef = coefL;
+    a.inv = inv;
+    a.B = W;
+    a.Y = reinterpret_cast<T *>(C.d_flowY.p);
+    a.Z = reinterpret_cast<T *>(C.d_flowZ.p);
+    a.ldb = ldb;
+    a.ldl = ldl ? 1 : 0;
+    a.cjp = cjp;
+    a.vec_elems = vec_elems;
+    // PASTIX_GPU_SOLVE_PROFILE=3: per-task times, summarized per level on stderr (diagnostics)
+    static const bool tprof = getenv("PASTIX_GPU_SOLVE_PROFILE") && getenv("PASTIX_GPU_SOLVE_PROFILE")[0] == '3';
+    a.stamps = nullptr;
+    if (tprof) {
+        const size_t ns = 2 * (size_t)a.ntasks + (size_t)nsm * FRT_N;
+        if (C.d_flow_stamps.n < ns) PGPU_CHECK(C.d_flow_stamps.alloc(ns));
+        PGPU_CHECK(cudaMemsetAsync(C.d_flow_stamps.p, 0, ns * 8, C.stream));
+        a.stamps = C.d_flow_stamps.p;
+    }
+    void *args[] = {&a};
+    PGPU_CHECK(cudaLaunchCooperativeKernel((const void *)kern, dim3(nsm), dim3(FLOW_THREADS), args, smem, C.stream));
+    C.flow_used = true;
+    if (tprof) {
+        // per level of the run: first start and last signal of its D / E tasks and of the O / G tasks of its
+        // cblks, in microseconds from the first task's start
+        std::vector<unsigned long long> t(2 * (size_t)a.ntasks + (size_t)nsm * FRT_N);
+        std::vector<FlowTask> tk(a.ntasks);
+        PGPU_CHECK(cudaMemcpyAsync(t.data(), a.stamps, t.size() * 8, cudaMemcpyDeviceToHost, C.stream));
+        PGPU_CHECK(cudaMemcpyAsync(tk.data(), a.tasks, tk.size() * sizeof(FlowTask), cudaMemcpyDeviceToHost, C.stream));
+        PGPU_CHECK(cudaStreamSynchronize(C.stream));
+        unsigned long long t0 = ~0ull, t1 = 0;
+        for (int i = 0; i < a.ntasks; i++) {
+            t0 = std::min(t0, t[2 * i]);
+            t1 = std::max(t1, t[2 * i + 1]);
+        }
+        const int la = C.flow_runs[run].x, lb = C.flow_runs[run].y;
+        std::vector<double> lo(4 * (size_t)(lb - la), 1e30), hi(4 * (size_t)(lb - la), 0);
+        for (int i = 0; i < a.ntasks; i++) {
+            const int l = C.cblk_level[tk[i].c] - la, kd = (tk[i].hdr & 7) == FLOW_D ? 0 : 1;
+            lo[4 * l + 2 * kd] = std::min(lo[4 * l + 2 * kd], (t[2 * i] - t0) * 1e-3);
+            hi[4 * l + 2 * kd + 1] = std::max(hi[4 * l + 2 * kd + 1], (t[2 * i + 1] - t0) * 1e-3);
+        }
+        fprintf(stderr, "pastix_gpu dataflow %s levels %d..%d: %d tasks, %.1f us; per level (us): diag first..last, off first..last\n",
+                fwd ? "forward" : "backward", la, lb - 1, a.ntasks, (t1 - t0) * 1e-3);
+        for (int l = 0; l < lb - la; l++)
+            fprintf(stderr, "  %d  %.1f..%.1f  %.1f..%.1f\n", la + l, lo[4 * l], hi[4 * l + 1], lo[4 * l + 2], hi[4 * l + 3]);
+        double rt[FRT_N] = {0};
+        for (int q = 0; q < nsm; q++)
+            for (int j = 0; j < FRT_N; j++) rt[j] += t[2 * (size_t)a.ntasks + (size_t)q * FRT_N + j] / (double)nsm;
+        fprintf(stderr, "  role waits, mean kcycles per CTA: fetch/empty %.1f fetch/ready %.1f vector/record %.1f "
+                        "compute/full %.1f signal/done %.1f compute busy %.1f total %.1f\n",
+                rt[FRT_F_EMPTY] * 1e-3, rt[FRT_F_READY] * 1e-3, rt[FRT_V_RECV] * 1e-3, rt[FRT_C_FULL] * 1e-3,
+                rt[FRT_S_DONE] * 1e-3, rt[FRT_C_BUSY] * 1e-3, rt[FRT_TOTAL] * 1e-3);
+    }
+    return PASTIX_GPU_SUCCESS;
+}
+
+template <typename T>
+static int flow_launch_nr(pastix_gpu_t &C, int nrhs, bool fwd, int run, const T *coefL, const T *inv, T *W,
+                          int ldb, bool ldl, int cjp) {
+    switch (nrhs) {
+    case 1: return flow_launch<T, 1>(C, fwd, run, coefL, inv, W, ldb, ldl, cjp);
+    case 2: return flow_launch<T, 2>(C, fwd, run, coefL, inv, W, ldb, ldl, cjp);
+    case 4:
+        if constexpr (sizeof(T) <= 8) return flow_launch<T, 4>(C, fwd, run, coefL, inv, W, ldb, ldl, cjp);
+        return PASTIX_GPU_ERR_INTERNAL;
+    default: return PASTIX_GPU_ERR_INTERNAL;
+    }
+}
+
+// A wait of the dataflow solve that gave up (FlowState::err): the solve's
+// results are undefined; its counters are cleared for the next one.
+static int flow_check(pastix_gpu_t &C) {
+    if (!C.flow_used) return PASTIX_GPU_SUCCESS;
+    C.flow_used = false;
+    FlowState fs;
+    PGPU_CHECK(cudaMemcpy(&fs, C.d_flow_state.p, sizeof(fs), cudaMemcpyDeviceToHost));
+    if (fs.err) {
+        fprintf(stderr, "pastix_gpu: a wait of the dataflow solve timed out (%d)\n", fs.err);
+        int rc = flow_reset(C);
+        if (rc) return rc;
+        PGPU_CHECK(cudaStreamSynchronize(C.stream));
+        return PASTIX_GPU_ERR_INTERNAL;
+    }
+    return PASTIX_GPU_SUCCESS;
+}
+
 template <typename T>
 // steps: PGPU_SOLVE_FORWARD | PGPU_SOLVE_DIAG | PGPU_SOLVE_BACKWARD (all three: a full solve)
 static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches, int steps = 7) {
@@ -1801,10 +2132,28 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches, int st
     };
     // levels of narrow, short cblks: one warp per cblk, diagonal and off-diagonal parts in one launch
     auto small_level = [&](int l) { return C.lvl_maxw[l] <= 32 && C.lvl_maxh[l] <= SOLVE_SMALL_MAXH; };
+    // runs of levels with diagonal-block inverses: one dataflow launch each way
+    const bool flow = inv && C.tune[PGPU_TUNE_SOLVE_CHAIN] != 0 &&
+                      (nrhs == 1 || nrhs == 2 || (nrhs == 4 && sizeof(T) <= 8)) && nrhs <= FLOW_MAXRHS;
+    auto flow_run_at = [&](int l, bool first) {
+        if (flow)
+            for (size_t r = 0; r < C.flow_runs.size(); r++)
+                if ((first ? C.flow_runs[r].x : C.flow_runs[r].y - 1) == l) return (int)r;
+        return -1;
+    };
     for (int l = 0; l < ((steps & PGPU_SOLVE_FORWARD) ? C.nlevels : 0); l++) {
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         tm.level = l;
         const int mw = C.lvl_maxw[l];
+        const int run = flow_run_at(l, true);
+        if (run >= 0) {
+            PGPU_CHECK(mark(0));
+            int rc = flow_launch_nr<T>(C, nrhs, true, run, coefL, inv, W, ldb, ldl, cjp);
+            if (rc) return rc;
+            nl++;
+            l = C.flow_runs[run].y - 1;
+            continue;
+        }
         if (small_level(l)) {
             PGPU_CHECK(mark(0));
             const int *lc = C.d_lvl_cblks.p + C.lvl_ptr[l];
@@ -1856,6 +2205,15 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches, int st
         const int ncb = C.lvl_ptr[l + 1] - C.lvl_ptr[l];
         const int mw = C.lvl_maxw[l];
         tm.level = l;
+        const int run = flow_run_at(l, false);
+        if (run >= 0) {
+            PGPU_CHECK(mark(4));
+            int rc = flow_launch_nr<T>(C, nrhs, false, run, coefL, inv, W, ldb, ldl, lu ? 0 : cjp);
+            if (rc) return rc;
+            nl++;
+            l = C.flow_runs[run].x;
+            continue;
+        }
         if (small_level(l)) {
             PGPU_CHECK(mark(4));
             const int *lc = C.d_lvl_cblks.p + C.lvl_ptr[l];
@@ -2044,7 +2402,7 @@ extern "C" int pastix_gpu_solve_steps(pastix_gpu_t *ctx, int steps, int64_t nrhs
     PGPU_CHECK(cudaEventElapsedTime(&ms, C.ev[2], C.ev[3]));
     C.stats[1] = launches;
     C.stats[4] = ms;
-    return PASTIX_GPU_SUCCESS;
+    return flow_check(C);
 }
 
 extern "C" int pastix_gpu_solve(pastix_gpu_t *ctx, int64_t nrhs, void *B, int64_t ldb) {
@@ -2083,7 +2441,7 @@ extern "C" int pastix_gpu_solve(pastix_gpu_t *ctx, int64_t nrhs, void *B, int64_
     C.stats[1] = launches;
     C.stats[4] = ms;
     C.dparm[PGPU_DPARM_SOLV_TIME] = ms * 1e-3;
-    return PASTIX_GPU_SUCCESS;
+    return flow_check(C);
 }
 
 // --------------------------------------------------------------------------
@@ -2147,7 +2505,7 @@ extern "C" int pastix_gpu_solve_noalloc(pastix_gpu_t *ctx, int64_t nrhs, void *d
     }
     PGPU_CHECK(cudaGetLastError());
     PGPU_CHECK(cudaStreamSynchronize(s));
-    return PASTIX_GPU_SUCCESS;
+    return flow_check(C);
 }
 
 // --------------------------------------------------------------------------
@@ -2771,7 +3129,7 @@ static int refine_impl(pastix_gpu_t &C, int64_t nrhs, const void *B, int64_t ldb
     C.iparm[PGPU_IPARM_NBITER] = maxit;
     C.dparm[PGPU_DPARM_RELATIVE_ERROR] = maxres;
     C.dparm[PGPU_DPARM_REFINE_TIME] = ms * 1e-3;
-    return PASTIX_GPU_SUCCESS;
+    return flow_check(C);
 }
 
 extern "C" int pastix_gpu_refine(pastix_gpu_t *ctx, int64_t nrhs, const void *B, int64_t ldb, void *X,

@@ -451,6 +451,51 @@ def test_fp64_dmma_matches_fma_tiles(name, make, fact, monkeypatch):
     s.close()
 
 
+# persistent solve (runs of levels whose cblks all hold a diagonal-block
+# inverse, one cooperative launch per direction) for 1, 2 and 4 right-hand
+# sides, real and complex, LL^t / LU / LDL^t / LDL^h, FP64 and mixed factors
+CHAIN_CASES = [
+    ("diff26_d1", CASES[4][1], "potrf", None, False, 1),
+    ("diff26_d2", CASES[4][1], "potrf", None, False, 2),
+    ("diff26_s1", CASES[4][1], "potrf", None, True, 1),
+    ("diff26_s4", CASES[4][1], "potrf", None, True, 4),
+    ("cd32_d1", LARGE[1][1], "getrf", None, False, 1),
+    ("cd32_s2", LARGE[1][1], "getrf", None, True, 2),
+    ("sytrf_d4", LDL_CASES[0][1], "sytrf", None, False, 4),
+    ("hetrf_z24_1", LDL_CASES[6][1], "hetrf", "hefix", False, 1),
+    ("hetrf_z24_2", LDL_CASES[6][1], "hetrf", "hefix", False, 2),
+    ("hetrf_z24_s4", LDL_CASES[6][1], "hetrf", "hefix", True, 4),
+]
+
+
+@pytest.mark.parametrize("name,make,fact,variant,mixed,nrhs", CHAIN_CASES, ids=[c[0] for c in CHAIN_CASES])
+def test_persistent_solve_matches_reference(name, make, fact, variant, mixed, nrhs):
+    """The persistent solve (PGPU_TUNE_SOLVE_CHAIN = 1, default) takes fewer
+    launches than the per-level kernels and gives the same solution: FP64
+    factors to 1e-11 of the reference's solve and 1e-12 of the per-level
+    solve; single-precision factors to 1e-5 of the per-level solve (the
+    summation orders differ)."""
+    from pastix_b200 import autotune as AT
+    A = make()
+    ref, st = U.run_reference(A, fact, variant=variant, nthreads=NTH, numfact=not mixed)
+    s = _gpu_solver(A, st, fact, mixed=mixed)
+    s.numfact(A.values)
+    x, b = M.rhs_from_xtrue(A, nrhs, np.random.default_rng(41))
+    assert AT.get_knob(s, "solve_chain") == 1
+    xg = s.solve(b)
+    n_on = s.stats()["solve_launches"]
+    AT.set_knob(s, "solve_chain", 0)
+    x0 = s.solve(b)
+    n_off = s.stats()["solve_launches"]
+    assert n_on < n_off, (n_on, n_off)
+    tol = 1e-5 if mixed else 1e-12
+    assert np.abs(xg - x0).max() <= tol * np.abs(x0).max()
+    if not mixed:
+        xr = ref.solve(b)
+        assert np.abs(xg - xr).max() <= 1e-11 * np.abs(xr).max()
+    s.close()
+
+
 def test_factorization_from_a_saved_analysis(tmp_path):
     """Structure handoff through files: the reference's saved analysis
     (solverSave + ordering file) loaded by pastix_gpu_analysis_load drives a
