@@ -153,6 +153,26 @@ def errors(A, b, x, xtrue):
     return {"backward_error": bwd, "relative_residual": rel, "forward_error": fwd}
 
 
+def factor_nnz(st):
+    """Entries of the factor's lower part (diagonal blocks as triangles) and of
+    the diagonal blocks (the solve reads their inverses whole)."""
+    cb, bl = np.asarray(st["cblktab"]), np.asarray(st["bloktab"])
+    nc = cb.shape[0] - 1
+    w = (cb[:nc, 1] - cb[:nc, 0] + 1).astype(np.int64)
+    h = np.bincount(bl[:, 2], weights=(bl[:, 1] - bl[:, 0] + 1), minlength=nc).astype(np.int64)
+    return int((h * w).sum() - (w * (w - 1) // 2).sum()), int((w * w).sum())
+
+
+def measured_peaks():
+    """HBM GB/s and dense BF16 TFLOP/s of this pool's B200s: the driver-measured
+    file when present, else the earlier measurement on this pool."""
+    try:
+        pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return {"hbm_gbs": float(pk["hbm_gbs"]), "bf16_tflops": float(pk["bf16_tflops"]), "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
 def fma_peaks():
     import ctypes as C
     lib = C.CDLL(os.path.join(ROOT, "pastix_b200", "lib", "libpgpu_peak.so"))
@@ -511,11 +531,15 @@ def main():
     tc_ach = (mixed["tc_flops_per_step"] / (mixed["tc_ms_per_step"] * 1e-3) / 1e12
               if mixed["tc_ms_per_step"] > 0 else None)
     peak_tf32 = peaks.get("tf32_cublas_tflops")
-    bf16_peak = None
-    try:
-        bf16_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]
-    except Exception:
-        bf16_peak = 1590.0
+    mp = measured_peaks()
+    bf16_peak = mp["bf16_tflops"]
+    # solve: algorithmic bytes of one FP32 solve -- the factor read twice (forward, backward) and
+    # the right-hand side in and out in FP64 -- over the measured solve time; the diagonal blocks'
+    # inverses, read whole instead of their triangles, are reported apart
+    nnz_l, nnz_diag = factor_nnz(st) if not batch else (None, None)
+    solve_bytes = (2 * nnz_l * 4 + 2 * A.n * nrhs * 8) if nnz_l else None
+    # (at most: every diagonal block read whole, w^2 instead of w (w + 1) / 2, in both sweeps)
+    inv_extra = (nnz_diag - A.n) * 4 if nnz_diag else None
     g64 = fp64["gemm_flops_per_step"] / (fp64["gemm_ms_per_step"] * 1e-3) / 1e12
     peak64 = peaks.get("fp64_fma_tflops")
     line = {
@@ -534,13 +558,28 @@ def main():
                   "refine_iters": mixed["refine_iters"], "fact_gflops": mixed["fact_gflops"], "errors": err_m,
                   "wall_s": mixed["wall_s"], "device_s_all": mixed["device_s_all"]},
         "mixed_speedup_vs_fp64": fp64_v / value,
+        # the mixed solution against the FP64 arm's (which the GPU parity tests hold to 1e-11 of the
+        # reference's own solve)
+        "forward_error_vs_fp64": float(np.abs(mixed["x"] - fp64["x"]).max() / np.abs(fp64["x"]).max()),
+        "roofline_solve": ({"bound": "hbm", "kernel": "one FP32 supernodal solve (forward + backward; "
+                                                       "k_solve_flow on the levels with inverses)",
+                            "achieved": solve_bytes / (mixed["solve_ms"] * 1e-3) / 1e9, "peak": mp["hbm_gbs"],
+                            "unit": "GB/s",
+                            "frac": solve_bytes / (mixed["solve_ms"] * 1e-3) / 1e9 / mp["hbm_gbs"],
+                            "peak_source": mp["source"], "algorithmic_bytes": solve_bytes, "nnz_l": nnz_l,
+                            "inverse_extra_bytes": inv_extra, "solve_ms": mixed["solve_ms"]}
+                           if solve_bytes else None),
         "roofline": {"bound": "tensor",
-                     "kernel": "k_gemm_scatter_tc_tma<3xFP16> (tcgen05 update + TRSM GEMM, scatter-add epilogue)",
-                     "achieved": tc_ach, "peak": peak_tf32, "unit": "TFLOP/s",
-                     "frac": tc_ach / peak_tf32 if (peak_tf32 and tc_ach) else None, "traffic": None,
-                     "peak_source": "measured cuBLAS TF32 GEMM 8192^3 on this GPU (torch.matmul, allow_tf32); "
-                                    "MEASURED_PEAKS.json has BF16 only (%.1f TFLOP/s)" % bf16_peak,
-                     "frac_of_bf16_measured": tc_ach / bf16_peak if (bf16_peak and tc_ach) else None,
+                     "kernel": "k_gemm_scatter_tc_tma<3xFP16> (tcgen05 kind::f16 update + TRSM GEMM, "
+                               "scatter-add epilogue)",
+                     "achieved": tc_ach, "peak": bf16_peak, "unit": "TFLOP/s",
+                     "frac": tc_ach / bf16_peak if (bf16_peak and tc_ach) else None, "traffic": None,
+                     "peak_source": "dense BF16/FP16 tensor rate, %s (%s)" % (
+                         mp["source"], "MEASURED_PEAKS.json" if mp["source"] == "measured" else
+                         "no MEASURED_PEAKS.json: the earlier measurement on this pool"),
+                     # 3xFP16: three FP16 MMAs (lo.hi, hi.lo, hi.hi) per algorithmic product
+                     "issued_frac": 3 * tc_ach / bf16_peak if (bf16_peak and tc_ach) else None,
+                     "tf32_cublas_tflops": peak_tf32,
                      "algorithmic_flops_per_step": mixed["tc_flops_per_step"],
                      "tc_ms_per_step": mixed["tc_ms_per_step"],
                      "all_gemm": {"achieved": g_ach, "algorithmic_flops_per_step": mixed["gemm_flops_per_step"],

@@ -1452,7 +1452,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     auto ktrsm = (CPX && fm_conj(fmode)) ? k_trsm_rows<T, TRSM_TR, CPX> : k_trsm_rows<T, TRSM_TR, false>;
     PGPU_CHECK(cudaFuncSetAttribute(kpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
     PGPU_CHECK(cudaFuncSetAttribute(ktrsm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
-    PGPU_CHECK(cudaFuncSetAttribute(k_tri_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT));
+    PGPU_CHECK(cudaFuncSetAttribute(k_tri_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, WP_SMEM_LIMIT));
     // split products (3xTF32; the 3xFP16 mode without TMA operands falls back to it)
     const bool split = (mixed_gemm_mode(C) == MG_3XTF32 || mixed_gemm_mode(C) == MG_3XF16);
     const bool persist = C.tune[PGPU_TUNE_TC_KERNEL] != 0 && !C.record;   // task timings need one tile per CTA
@@ -1649,16 +1649,22 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             // X[w][33] + a 32-row strip of L, kch columns wide (as wide as fits, a multiple of 32)
             const size_t xs = tri_inverse_lb_offset(mw, sizeof(T));
             const int vk = std::max<int>(1, 16 / (int)sizeof(T));
-            if (xs + (size_t)PB * (PB + vk) * sizeof(T) > (size_t)SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
-            int kch = (int)std::min<size_t>(round_up(mw, PB), ((SMEM_LIMIT - xs) / ((size_t)PB * sizeof(T)) - vk));
+            if (xs + (size_t)PB * (PB + vk) * sizeof(T) > (size_t)WP_SMEM_LIMIT) return PASTIX_GPU_ERR_NOTIMPLEMENTED;
+            int kch = (int)std::min<size_t>(round_up(mw, PB), ((WP_SMEM_LIMIT - xs) / ((size_t)PB * sizeof(T)) - vk));
             kch = std::max(PB, kch / PB * PB);
-            const size_t ism = xs + (size_t)PB * (kch + vk) * sizeof(T);
+            size_t ism = xs + (size_t)PB * (kch + vk) * sizeof(T);
+            // bulk-copied, double-buffered strips and tiles where they fit (rows of L; the U^t
+            // columns of LU's first inverse keep the staged loads)
+            const int slb = (int)round_up(mw, PB) + vk;
+            const size_t bsm = xs + 2 * ((size_t)PB * slb + (size_t)PB * (PB + vk)) * sizeof(T);
+            const int bulk_lb = bsm <= (size_t)WP_SMEM_LIMIT ? slb : 0;
+            if (bulk_lb) ism = std::max(ism, bsm);
             PGPU_CHECK(tm.mark(PH_TRSM));
             k_tri_inverse<T><<<nij, 256, ism, s>>>(C.meta, C.d_invjobs.p + C.inv_ptr[l], coefL, inv,
                                                    fm_ldl(fmode) ? 1 : 0, (CPX && fm_conj(fmode)) ? 1 : 0,
                                                    fm_ldl(fmode) ? 1 : 0, lu ? 1 : 0, kch,
                                                    (C.tma && !C.h16) ? hilo_of<T>(C.d_ihilo.p) : nullptr,
-                                                   C.ihilo_plane);
+                                                   C.ihilo_plane, bulk_lb, C.d_status.p);
             nl++;
             split_level(l);
             const int ntt = C.ttile_ptr[l + 1] - C.ttile_ptr[l];

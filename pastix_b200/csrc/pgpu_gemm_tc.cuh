@@ -73,26 +73,6 @@ __device__ __forceinline__ uint32_t tc_idesc_f16(int n = TC_BN) {
     return (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
 }
 
-__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
-}
-
-// Bounded wait on an mbarrier phase; false on time-out (about 2 s).
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
-    const long long t0 = clock64();
-    while (true) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(addr), "r"(parity)
-            : "memory");
-        if (done) return true;
-        if (clock64() - t0 > 4000000000LL) return false;
-    }
-}
 
 
 __device__ __forceinline__ void tc_fence_async_smem() {
@@ -436,9 +416,6 @@ __device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, 
                  : "memory");
 }
 
-__device__ __forceinline__ void mbar_arrive(uint32_t addr) {
-    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
-}
 
 struct TcTileView {
     const float *A, *B;

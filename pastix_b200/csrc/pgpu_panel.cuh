@@ -475,12 +475,22 @@ __host__ __device__ inline size_t tri_inverse_lb_offset(int nrow, size_t esz) {
     return ((size_t)nrow * PBL * esz + 15) / 16 * 16;
 }
 
+// bulk_lb > 0 (the rows of L, not the U^t columns): the 32-row strip left of
+// each tile and the tile itself arrive by bulk asynchronous copies, one per
+// row (the rows are contiguous in the row-major panel), into two buffers of
+// PB rows x bulk_lb (strip) and PB rows x (PB + VK) (tile): the copies of
+// the next tile row are in flight while the current one is computed.  A
+// copy that does not land within the bounded wait is counted in
+// Status::timeout and the factorization reported failed.
 template <typename T>
 __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restrict__ jobs,
                                                      const T *__restrict__ coefL, T *__restrict__ inv,
                                                      int unit, int cjp, int scale_d, int lu, int kch,
-                                                     T *__restrict__ ihilo, int64_t iplane) {
+                                                     T *__restrict__ ihilo, int64_t iplane, int bulk_lb,
+                                                     Status *st) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t tmb[2];
+    __shared__ int tfail;
     const int2 jbv = jobs[blockIdx.x];
     const int c = jbv.x, jb = jbv.y & 0xFFFFF, kind = jbv.y >> 20;
     const int w = m.width[c], ld = m.ld[c];
@@ -498,8 +508,110 @@ __global__ void __launch_bounds__(256) k_tri_inverse(Meta m, const int2 *__restr
         const int i = e / PB, q = e - i * PB;
         X[i * PBL + q] = (i == q && q < nb) ? T(1) : T(0);
     }
+    if (bulk_lb > 0 && !tr) {
+        constexpr int TLB = PB + VK;   // tile rows, 16-byte multiples
+        const int slb = bulk_lb;
+        auto strip = [&](int b) { return Lb + (size_t)b * (PB * (size_t)slb + PB * TLB); };
+        auto tile = [&](int b) { return strip(b) + (size_t)PB * slb; };
+        if (tid == 0) {
+            mbar_init(smem_u32(&tmb[0]), 1);
+            mbar_init(smem_u32(&tmb[1]), 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            tfail = 0;
+        }
+        __syncthreads();
+        // thread 0: rows ib .. ib + nbi of L, columns jb .. ib (the strip) and ib .. (the tile)
+        auto issue = [&](int b, int ib) {
+            const int nbi = min(PB, w - ib), kn = ib - jb, tcols = (nbi + VK - 1) / VK * VK;
+            const uint32_t bytes = (uint32_t)((size_t)nbi * (kn + tcols) * sizeof(T));
+            mbar_arrive_expect_tx(smem_u32(&tmb[b]), bytes);
+            for (int r = 0; r < nbi; r++) {
+                const T *row = D + (int64_t)(ib + r) * ld;
+                if (kn)
+                    bulk_g2s(smem_u32(strip(b) + (size_t)r * slb), row + jb, (uint32_t)(kn * sizeof(T)),
+                             smem_u32(&tmb[b]));
+                bulk_g2s(smem_u32(tile(b) + (size_t)r * TLB), row + ib, (uint32_t)(tcols * sizeof(T)),
+                         smem_u32(&tmb[b]));
+            }
+        };
+        if (tid == 0) issue(0, jb);
+        int stp = 0;
+        for (int ib = jb; ib < w; ib += PB, stp++) {
+            const int b = stp & 1, nbi = min(PB, w - ib), kn = ib - jb;
+            // the other buffer was last read by the previous step (synchronized at its end)
+            if (tid == 0 && ib + PB < w) issue(b ^ 1, ib + PB);
+            if (!mbar_wait(smem_u32(&tmb[b]), (uint32_t)((stp >> 1) & 1))) tfail = 1;
+            __syncthreads();
+            if (tfail) {
+                if (tid == 0) {
+                    // this step's copies and, when issued, the next step's land before the CTA leaves
+                    atomicAdd(&st->timeout, 1);
+                    if (!mbar_wait(smem_u32(&tmb[b]), (uint32_t)((stp >> 1) & 1))) atomicAdd(&st->drain_timeout, 1);
+                    if (ib + PB < w && !mbar_wait(smem_u32(&tmb[b ^ 1]), (uint32_t)(((stp + 1) >> 1) & 1)))
+                        atomicAdd(&st->drain_timeout, 1);
+                }
+                break;
+            }
+            const T *Ls = strip(b), *Lt = tile(b);
+            if (kn > 0) {
+                // X[ib..] -= L[ib.., jb..ib) X[jb..ib): thread = rows r4..r4+3 of the strip, column q
+                const int q = tid & 31, r4 = (tid >> 5) * 4;
+                T acc[4] = {T(0), T(0), T(0), T(0)};
+                for (int k = 0; k < kn; k += VK) {
+                    T lv[4][VK];
+#pragma unroll
+                    for (int p = 0; p < 4; p++) {
+                        const uint4 u = *reinterpret_cast<const uint4 *>(Ls + (r4 + p) * slb + k);
+                        memcpy(lv[p], &u, 16);
+                    }
+#pragma unroll
+                    for (int v = 0; v < VK; v++) {
+                        const T xv = X[(k + v) * PBL + q];
+#pragma unroll
+                        for (int p = 0; p < 4; p++) acc[p] += (cjp ? conj_v(lv[p][v]) : lv[p][v]) * xv;
+                    }
+                }
+                if (q < nb)
+#pragma unroll
+                    for (int p = 0; p < 4; p++)
+                        if (r4 + p < nbi) X[(kn + r4 + p) * PBL + q] -= acc[p];
+            }
+            __syncthreads();
+            {
+                // X[ib..ib+nbi) = L_tile^{-1} X[ib..ib+nbi): warp w solves columns w, w + 8, .. (lane = row)
+                const int warp = tid >> 5, lane = tid & 31;
+                T y[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int q = warp + 8 * u;
+                    y[u] = (lane < nbi && q < nb) ? X[(kn + lane) * PBL + q] : T(0);
+                }
+                T dg = lane < nbi ? Lt[lane * TLB + lane] : T(1);
+                if (cjp) dg = conj_v(dg);
+                const T rinv = (!unit && lane < nbi) ? T(1) / dg : T(1);
+#pragma unroll
+                for (int k = 0; k < PB; k++) {
+                    if (k >= nbi) break;
+                    T lrk = (lane > k && lane < nbi) ? Lt[lane * TLB + k] : T(0);
+                    if (cjp) lrk = conj_v(lrk);
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        if (lane == k && !unit) y[u] = y[u] * rinv;
+                        const T xk = shfl_v(y[u], k);
+                        if (lane > k) y[u] -= lrk * xk;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int q = warp + 8 * u;
+                    if (lane < nbi && q < nb) X[(kn + lane) * PBL + q] = y[u];
+                }
+            }
+            __syncthreads();
+        }
+    }
     __syncthreads();
-    for (int ib = jb; ib < w; ib += PB) {
+    for (int ib = (bulk_lb > 0 && !tr) ? w : jb; ib < w; ib += PB) {
         const int nbi = min(PB, w - ib);
         // (1) X[ib..] -= L[ib.., jb..ib) X[jb..ib), kch columns of L at a time
         for (int kc0 = jb; kc0 < ib; kc0 += kch) {

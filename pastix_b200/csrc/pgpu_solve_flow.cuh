@@ -107,13 +107,6 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes) {
     asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(bytes) : "memory");
 }
 
-// Bulk asynchronous copy global -> this CTA's shared memory (16-byte aligned
-// addresses, size a multiple of 16), completing on mbar.
-__device__ __forceinline__ void flow_bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t mbar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(mbar)
-                 : "memory");
-}
 
 // Shared-memory loads by address in the shared window (the compute role reads
 // its staged rows and vectors only through these, so that every one is an
@@ -316,7 +309,7 @@ __global__ void __launch_bounds__(FLOW_THREADS, 1) k_solve_flow(FlowArgs<T> a) {
                     const uint32_t bytes = (uint32_t)(((q.hdr >> 4) & 63) * (size_t)q.ld * sizeof(T));
                     const T *src = ((q.hdr & 7) == FLOW_D ? a.inv : a.coef) + q.src;
                     mbar_expect_tx(smem_u32(&full[s]), bytes);
-                    flow_bulk_load(smem_u32(data(s)), src, bytes, smem_u32(&full[s]));
+                    bulk_g2s(smem_u32(data(s)), src, bytes, smem_u32(&full[s]));
                     mbar_arrive(smem_u32(&recv[s]));
                 }
             }
