@@ -284,7 +284,7 @@ def run_arm(A, st, b, mixed, steps, warmup, fact, refine, segments=None):
         "refine_iters": iters[-1], "factor_ms": last["numfact_ms"], "solve_ms": last["solve_ms"],
         "refine_ms": last["refine_ms"], "diag_ms": last["diag_ms"], "trsm_ms": last["trsm_ms"],
         "fact_gflops": float(dp[G.DPARM_FACT_FLOPS]), "thflops": float(dp[G.DPARM_FACT_THFLOPS]),
-        "x": x, "x_e2e": xh, "spm_ms": spm_ms,
+        "x": x, "x_e2e": xh, "spm_ms": spm_ms, "graph_replayed": bool(last.get("graph_replayed", 0.0)),
     }
 
 
@@ -587,6 +587,7 @@ def main():
         "e2e": {"value": e2e_v, "unit": "s", "h2d_bytes_per_step": int(A.values.nbytes + b.nbytes),
                 "d2h_bytes_per_step": int(b.nbytes), "errors": err_e},
         "gpu_launches": int(mixed["launches"]),
+        "factor_graph_replayed": mixed["graph_replayed"],
         "spm_setup_ms": mixed["spm_ms"],
         "analysis_s": t_an, "peaks": peaks,
     }

@@ -278,6 +278,9 @@ PASTIX_GPU_API int pastix_gpu_phase_log( pastix_gpu_t *ctx, int64_t *count, int6
  *                             diagonal-block inverse go through one dataflow launch per
  *                             direction (per-cblk counters instead of per-level launches;
  *                             1, 2 or 4 right-hand sides, complex128: 1 or 2); 0: per-level launches
+ *   PGPU_TUNE_GRAPH           -1 (default): the factorization captured as a CUDA graph and
+ *                             replayed when the factor holds at most 2^24 coefficients
+ *                             (launch-bound sizes); 1 always; 0 never
  * Setting one invalidates the factorization plan (rebuilt by the next numfact).
  */
 #define PGPU_TUNE_MIXED_GEMM      0
@@ -292,7 +295,8 @@ PASTIX_GPU_API int pastix_gpu_phase_log( pastix_gpu_t *ctx, int64_t *count, int6
 #define PGPU_TUNE_TC_PAIR_MIN     9
 #define PGPU_TUNE_DMMA            10
 #define PGPU_TUNE_SOLVE_CHAIN     11
-#define PGPU_TUNE_COUNT           12
+#define PGPU_TUNE_GRAPH           12
+#define PGPU_TUNE_COUNT           13
 PASTIX_GPU_API int pastix_gpu_set_tuning( pastix_gpu_t *ctx, int key, int64_t value );
 PASTIX_GPU_API int pastix_gpu_get_tuning( pastix_gpu_t *ctx, int key, int64_t *value );
 

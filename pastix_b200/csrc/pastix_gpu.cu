@@ -592,6 +592,8 @@ static void default_tuning(int64_t *t) {
     t[PGPU_TUNE_DMMA] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
     e = getenv("PASTIX_GPU_SOLVE_CHAIN");
     t[PGPU_TUNE_SOLVE_CHAIN] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
+    e = getenv("PASTIX_GPU_GRAPH");
+    t[PGPU_TUNE_GRAPH] = e ? (std::strcmp(e, "1") == 0 ? 1 : 0) : -1;
 }
 static int mixed_gemm_mode(const pastix_gpu_t &C) { return (int)C.tune[PGPU_TUNE_MIXED_GEMM]; }
 
@@ -1846,14 +1848,18 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
         return mixed ? fill_and_factor<float, double>(C, fmode, &nl, tm)
                      : fill_and_factor<double, double>(C, fmode, &nl, tm);
     };
-    // PASTIX_GPU_GRAPH=1: the sequence is captured once per (plan, coeftab,
-    // mode, value buffer, pivot magnitude) as a CUDA graph and replayed by
-    // later calls (the first call of a new plan captures, instantiates and
-    // launches it).  The per-phase timings come from event nodes of the graph;
-    // with them the replay is no faster than direct launches at these sizes,
-    // so direct launches stay the default.
-    const char *ge = getenv("PASTIX_GPU_GRAPH");
-    const bool graph = ge && std::strcmp(ge, "1") == 0 && !C.record;
+    // Graph replay (PGPU_TUNE_GRAPH): the sequence is captured once per
+    // (plan, coeftab, mode, value buffer, pivot magnitude) as a CUDA graph and
+    // replayed by later calls (the first call of a new plan captures,
+    // instantiates and launches it).  The per-phase timings come from event
+    // nodes of the graph.  Measured on one B200: the replay wins where the
+    // launches outweigh the work (20^3 Laplacian: numfact 1.31 -> 1.23 ms,
+    // time-to-solution end to end 2.54 -> 2.24 ms), is even on the 512 2D
+    // systems (30.2 vs 30.6 ms) and loses on the large 3-D problems (80^3 LU:
+    // 40.7 vs 44.2 ms); by default (-1) it is used for factors of at most
+    // 2^24 coefficients.
+    const int64_t gt = C.tune[PGPU_TUNE_GRAPH];
+    const bool graph = !C.record && (gt == 1 || (gt < 0 && C.coefnbr <= ((int64_t)1 << 24)));
     bool replayed = false;
     if (graph) {
         int64_t magn_bits;   // the static-pivot magnitude is a kernel argument of the graph
@@ -3311,7 +3317,8 @@ extern "C" int pastix_gpu_set_tuning(pastix_gpu_t *ctx, int key, int64_t value) 
     if (!ctx || key < 0 || key >= PGPU_TUNE_COUNT) return PASTIX_GPU_ERR_BADPARAMETER;
     if (key == PGPU_TUNE_MIXED_GEMM && (value < MG_FP32 || value > MG_3XF16)) return PASTIX_GPU_ERR_BADPARAMETER;
     if ((key == PGPU_TUNE_TRSM_GEMM_ROWS && value < 32) || (key == PGPU_TUNE_LA_RESERVED_SMS && value < 0) ||
-        (key == PGPU_TUNE_TC_MIN_MN && value < 0) || (key == PGPU_TUNE_WIDE_PANEL && value < 0) || (key == PGPU_TUNE_TC_PAIR_MIN && value < -1))
+        (key == PGPU_TUNE_TC_MIN_MN && value < 0) || (key == PGPU_TUNE_WIDE_PANEL && value < 0) || (key == PGPU_TUNE_TC_PAIR_MIN && value < -1) ||
+        (key == PGPU_TUNE_GRAPH && (value < -1 || value > 1)))
         return PASTIX_GPU_ERR_BADPARAMETER;
     ctx->tune[key] = value;
     ctx->plan_fact = -1;   // the next numfact rebuilds its launch lists (and graph)

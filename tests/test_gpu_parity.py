@@ -327,17 +327,23 @@ def test_hetrf_gmres_refinement_reaches_1e12(mixed):
 def test_factorization_graph_replay_matches_direct(mixed, monkeypatch):
     """The factorization sequence (norm, fill-in, every level's panels, TRSMs
     and update GEMMs on both lookahead streams) captured once as a CUDA graph
-    and replayed (PASTIX_GPU_GRAPH=1; =0 launches kernel by kernel):
+    and replayed (PGPU_TUNE_GRAPH = 1; 0 launches kernel by kernel; the
+    default, -1, captures factors of at most 2^24 coefficients, as here):
     its factors equal the directly launched ones, a new set of values reuses
     the same graph, and the per-phase timings come from its event nodes."""
+    from pastix_b200 import autotune as AT
     A = M.diffusion_lognormal(24, 23, 22, 1.0, np.random.default_rng(21))
     ref, st = U.run_reference(A, "potrf", numfact=False)
     s = _gpu_solver(A, st, "potrf", mixed=mixed)
-    monkeypatch.setenv("PASTIX_GPU_GRAPH", "0")   # launched kernel by kernel
+    assert AT.get_knob(s, "graph") == -1
+    s.numfact(A.values)                  # (default: captured, this size)
+    s.numfact(A.values)
+    assert s.stats()["graph_replayed"] == 1.0
+    AT.set_knob(s, "graph", 0)           # launched kernel by kernel
     s.numfact(A.values)
     assert s.stats()["graph_replayed"] == 0.0
     L0, _ = s.coeftab()
-    monkeypatch.setenv("PASTIX_GPU_GRAPH", "1")
+    AT.set_knob(s, "graph", 1)
     s.numfact(A.values)                  # capture
     s.numfact(A.values)                  # replay
     st_ = s.stats()
