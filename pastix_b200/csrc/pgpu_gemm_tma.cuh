@@ -419,6 +419,58 @@ __device__ __forceinline__ void split_row_h16(const float *__restrict__ src, int
                                               __half *__restrict__ hi, int64_t hplane, float *__restrict__ sc,
                                               int lane) {
     const int wv = w >> 2;
+    constexpr int RV = 4;   // rows of up to 32 RV float4 stay in registers: read once, all loads in flight
+    if (wv <= 32 * RV) {
+        float4 x[RV];
+        float mx = 0.f;
+#pragma unroll
+        for (int u = 0; u < RV; u++) {
+            const int q = lane + 32 * u;
+            x[u] = q < wv ? __ldg(reinterpret_cast<const float4 *>(src) + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        const int jt = 4 * wv + lane;   // the tail (w % 4 columns), one per lane
+        const float xt = jt < w ? src[jt] : 0.f;
+#pragma unroll
+        for (int u = 0; u < RV; u++)
+            mx = fmaxf(mx, fmaxf(fmaxf(fabsf(x[u].x), fabsf(x[u].y)), fmaxf(fabsf(x[u].z), fabsf(x[u].w))));
+        mx = fmaxf(mx, fabsf(xt));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        int e = 0;
+        if (mx > 0.f) {
+            const int E = ((__float_as_int(mx) >> 23) & 0xff) - 127;
+            e = max(-126, min(126, 14 - E));
+        }
+        const float s = pow2f(e);
+        if (lane == 0) *sc = pow2f(-e);
+        __half *lo = hi + hplane;
+#pragma unroll
+        for (int u = 0; u < RV; u++) {
+            const int q = lane + 32 * u;
+            if (q < wv) {
+                if (dst) reinterpret_cast<float4 *>(dst)[q] = x[u];
+                const float y[4] = {x[u].x * s, x[u].y * s, x[u].z * s, x[u].w * s};
+                __half h[4], l[4];
+#pragma unroll
+                for (int v = 0; v < 4; v++) {
+                    h[v] = __float2half_rn(y[v]);
+                    l[v] = __float2half_rn(y[v] - __half2float(h[v]));
+                }
+                reinterpret_cast<__half2 *>(hi)[2 * q] = __halves2half2(h[0], h[1]);
+                reinterpret_cast<__half2 *>(hi)[2 * q + 1] = __halves2half2(h[2], h[3]);
+                reinterpret_cast<__half2 *>(lo)[2 * q] = __halves2half2(l[0], l[1]);
+                reinterpret_cast<__half2 *>(lo)[2 * q + 1] = __halves2half2(l[2], l[3]);
+            }
+        }
+        if (jt < w) {
+            if (dst) dst[jt] = xt;
+            const float y = xt * s;
+            const __half h = __float2half_rn(y);
+            hi[jt] = h;
+            lo[jt] = __float2half_rn(y - __half2float(h));
+        }
+        return;
+    }
     float mx = 0.f;
     for (int q = lane; q < wv; q += 32) {
         const float4 x = reinterpret_cast<const float4 *>(src)[q];
