@@ -968,6 +968,14 @@ static int build_fact_plan(pastix_gpu_t &C, int fmode, bool fp32, bool zc) {
                         for (int tn = 0; tn < cdiv(w, bn); tn++)
                             (tc_trsm ? tttiles : ttiles).push_back(make_int4(id, tm, tn, 0));
                 }
+            } else if (h > fuse && h == w && tgemm) {
+                // a wide cblk without off-diagonal rows (a root): the inverse alone, for
+                // the solve's products with it (no TRSM)
+                const int sides = lu ? 2 : 1;
+                C.invoff[c] = inv_elems;
+                inv_elems += sides * inv_span(w, C.ld[c]);
+                for (int kind = 0; kind < sides; kind++)
+                    for (int jb = 0; jb < w; jb += PB) invjobs.push_back(make_int2(c, jb + (kind << 20)));
             }
             const int b1 = C.fblok[c + 1];
             for (int b = C.fblok[c] + 1; b < b1; b++) {
@@ -1644,10 +1652,12 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             nl++;
         }
         const int ntr = C.trsm_ptr[l + 1] - C.trsm_ptr[l];
-        if (ntr && C.trsm_gemm) {
+        const int nij = C.inv_ptr[l + 1] - C.inv_ptr[l];
+        // (a level of roots may hold inverses and no TRSM rows)
+        const bool inv_block = (ntr || nij) && C.trsm_gemm;
+        if (inv_block) {
             T *inv = reinterpret_cast<T *>(C.d_inv.p);
             T *scr = reinterpret_cast<T *>(C.d_scr.p);
-            const int nij = C.inv_ptr[l + 1] - C.inv_ptr[l];
             // X[w][33] + a 32-row strip of L, kch columns wide (as wide as fits, a multiple of 32)
             const size_t xs = tri_inverse_lb_offset(mw, sizeof(T));
             const int vk = std::max<int>(1, 16 / (int)sizeof(T));
@@ -1709,17 +1719,18 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
             bool copied = false;
             if constexpr (std::is_same<T, float>::value) {
                 if (C.tma && C.h16) {
-                    k_trsm_copyback_h16<<<ntr, 256, 0, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], C.d_scroff.p, scr,
-                                                            coefL, coefU, C.d_h16.p, C.h16_plane, C.d_hscale.p,
-                                                            C.d_hoff.p, C.d_hsbase.p, C.d_mapidx.p);
+                    if (ntr)
+                        k_trsm_copyback_h16<<<ntr, 256, 0, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], C.d_scroff.p,
+                                                                scr, coefL, coefU, C.d_h16.p, C.h16_plane,
+                                                                C.d_hscale.p, C.d_hoff.p, C.d_hsbase.p, C.d_mapidx.p);
                     copied = true;
                 }
             }
-            if (!copied)
+            if (!copied && ntr)
                 k_trsm_copyback<T><<<ntr, 256, 0, s>>>(C.meta, C.d_trsm.p + C.trsm_ptr[l], C.d_scroff.p, scr, coefL,
                                                        coefU, C.tma ? hilo_of<T>(C.d_hilo.p) : nullptr, C.hilo_plane,
                                                        C.coefnbr);
-            nl++;
+            if (ntr) nl++;
         } else if (ntr) {
             const size_t fixed = ((size_t)TRSM_TR * (mw + 1) + PB * PBL) * sizeof(T);
             const int pch = (int)std::min<size_t>(mw, (SMEM_LIMIT - std::min<size_t>(fixed, SMEM_LIMIT)) /
@@ -1731,7 +1742,7 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
                                         at(prof[1], C.trsm_ptr[l]));
             nl++;
         }
-        if (!(ntr && C.trsm_gemm)) split_level(l);   // the level's rows are final here
+        if (!inv_block) split_level(l);   // the level's rows are final here
         // update GEMMs of the level: with lookahead the tiles whose target is
         // in the next level run here, the rest on stream2 once this level's
         // panels are final
