@@ -274,7 +274,7 @@ PASTIX_GPU_API int pastix_gpu_phase_log( pastix_gpu_t *ctx, int64_t *count, int6
  *                             tiles that share their B tile (-1, default: 2 per SM)
  *   PGPU_TUNE_DMMA            1 (default): real FP64 update / TRSM GEMMs large enough
  *                             for a 128 x 64 tile on the FP64 tensor cores (DMMA); 0: FMA tiles
- *   PGPU_TUNE_SOLVE_CHAIN     1 (default): runs of solve levels whose cblks all hold a
+ *   PGPU_TUNE_SOLVE_FLOW      1 (default): runs of solve levels whose cblks all hold a
  *                             diagonal-block inverse go through one dataflow launch per
  *                             direction (per-cblk counters instead of per-level launches;
  *                             1, 2 or 4 right-hand sides, complex128: 1 or 2); 0: per-level launches
@@ -294,7 +294,7 @@ PASTIX_GPU_API int pastix_gpu_phase_log( pastix_gpu_t *ctx, int64_t *count, int6
 #define PGPU_TUNE_TC_TMA          8
 #define PGPU_TUNE_TC_PAIR_MIN     9
 #define PGPU_TUNE_DMMA            10
-#define PGPU_TUNE_SOLVE_CHAIN     11
+#define PGPU_TUNE_SOLVE_FLOW      11
 #define PGPU_TUNE_GRAPH           12
 #define PGPU_TUNE_COUNT           13
 PASTIX_GPU_API int pastix_gpu_set_tuning( pastix_gpu_t *ctx, int key, int64_t value );

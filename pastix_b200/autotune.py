@@ -27,7 +27,7 @@ from . import gpu as G
 
 KNOBS = {"mixed_gemm": 0, "tc_kernel": 1, "lookahead": 2, "la_reserved_sms": 3, "trsm_gemm": 4,
          "trsm_gemm_rows": 5, "tc_min_mn": 6, "wide_panel": 7, "tc_tma": 8, "tc_pair_min": 9,
-         "dmma": 10, "solve_chain": 11, "graph": 12}
+         "dmma": 10, "solve_flow": 11, "graph": 12}
 
 DEFAULT_SPACE = {
     "trsm_gemm_rows": [128, 256, 512],

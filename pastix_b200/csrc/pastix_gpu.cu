@@ -590,8 +590,8 @@ static void default_tuning(int64_t *t) {
     t[PGPU_TUNE_TC_PAIR_MIN] = -1;
     e = getenv("PASTIX_GPU_DMMA");
     t[PGPU_TUNE_DMMA] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
-    e = getenv("PASTIX_GPU_SOLVE_CHAIN");
-    t[PGPU_TUNE_SOLVE_CHAIN] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
+    e = getenv("PASTIX_GPU_SOLVE_FLOW");
+    t[PGPU_TUNE_SOLVE_FLOW] = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
     e = getenv("PASTIX_GPU_GRAPH");
     t[PGPU_TUNE_GRAPH] = e ? (std::strcmp(e, "1") == 0 ? 1 : 0) : -1;
 }
@@ -2156,7 +2156,7 @@ static int solve_permuted(pastix_gpu_t &C, T *W, int nrhs, int *launches, int st
     // levels of narrow, short cblks: one warp per cblk, diagonal and off-diagonal parts in one launch
     auto small_level = [&](int l) { return C.lvl_maxw[l] <= 32 && C.lvl_maxh[l] <= SOLVE_SMALL_MAXH; };
     // runs of levels with diagonal-block inverses: one dataflow launch each way
-    const bool flow = inv && C.tune[PGPU_TUNE_SOLVE_CHAIN] != 0 &&
+    const bool flow = inv && C.tune[PGPU_TUNE_SOLVE_FLOW] != 0 &&
                       (nrhs == 1 || nrhs == 2 || (nrhs == 4 && sizeof(T) <= 8)) && nrhs <= FLOW_MAXRHS;
     auto flow_run_at = [&](int l, bool first) {
         if (flow)

@@ -457,10 +457,10 @@ def test_fp64_dmma_matches_fma_tiles(name, make, fact, monkeypatch):
     s.close()
 
 
-# persistent solve (runs of levels whose cblks all hold a diagonal-block
-# inverse, one cooperative launch per direction) for 1, 2 and 4 right-hand
-# sides, real and complex, LL^t / LU / LDL^t / LDL^h, FP64 and mixed factors
-CHAIN_CASES = [
+# dataflow solve (runs of levels whose cblks all hold a diagonal-block
+# inverse, one launch per direction) for 1, 2 and 4 right-hand sides, real
+# and complex, LL^t / LU / LDL^t / LDL^h, FP64 and mixed factors
+FLOW_CASES = [
     ("diff26_d1", CASES[4][1], "potrf", None, False, 1),
     ("diff26_d2", CASES[4][1], "potrf", None, False, 2),
     ("diff26_s1", CASES[4][1], "potrf", None, True, 1),
@@ -474,9 +474,9 @@ CHAIN_CASES = [
 ]
 
 
-@pytest.mark.parametrize("name,make,fact,variant,mixed,nrhs", CHAIN_CASES, ids=[c[0] for c in CHAIN_CASES])
-def test_persistent_solve_matches_reference(name, make, fact, variant, mixed, nrhs):
-    """The persistent solve (PGPU_TUNE_SOLVE_CHAIN = 1, default) takes fewer
+@pytest.mark.parametrize("name,make,fact,variant,mixed,nrhs", FLOW_CASES, ids=[c[0] for c in FLOW_CASES])
+def test_dataflow_solve_matches_reference(name, make, fact, variant, mixed, nrhs):
+    """The dataflow solve (PGPU_TUNE_SOLVE_FLOW = 1, default) takes fewer
     launches than the per-level kernels and gives the same solution: FP64
     factors to 1e-11 of the reference's solve and 1e-12 of the per-level
     solve; single-precision factors to 1e-5 of the per-level solve (the
@@ -487,10 +487,10 @@ def test_persistent_solve_matches_reference(name, make, fact, variant, mixed, nr
     s = _gpu_solver(A, st, fact, mixed=mixed)
     s.numfact(A.values)
     x, b = M.rhs_from_xtrue(A, nrhs, np.random.default_rng(41))
-    assert AT.get_knob(s, "solve_chain") == 1
+    assert AT.get_knob(s, "solve_flow") == 1
     xg = s.solve(b)
     n_on = s.stats()["solve_launches"]
-    AT.set_knob(s, "solve_chain", 0)
+    AT.set_knob(s, "solve_flow", 0)
     x0 = s.solve(b)
     n_off = s.stats()["solve_launches"]
     assert n_on < n_off, (n_on, n_off)
