@@ -163,6 +163,14 @@ def factor_nnz(st):
     return int((h * w).sum() - (w * (w - 1) // 2).sum()), int((w * w).sum())
 
 
+# DRAM bytes of the tensor-core update kernel over one factorization of the
+# 100^3 lognormal diffusion problem (LL^t, 3xFP16): one-pass ncu capture of all
+# 228 launches of a numfact (profiles/k_gemm_scatter_tc_tma_c2_dram.md).  About
+# 82 GB of the 90 GB are the scatter-add targets' partial sums (40.8 GB of
+# reductions, each target line read and written back); the operands are ~4 GB.
+TC_DRAM_BYTES_100CUBE = {"read": 53332129280, "write": 37116627968, "launches": 228}
+
+
 def measured_peaks():
     """HBM GB/s and dense BF16 TFLOP/s of this pool's B200s: the driver-measured
     file when present, else the earlier measurement on this pool."""
@@ -573,7 +581,13 @@ def main():
                      "kernel": "k_gemm_scatter_tc_tma<3xFP16> (tcgen05 kind::f16 update + TRSM GEMM, "
                                "scatter-add epilogue)",
                      "achieved": tc_ach, "peak": bf16_peak, "unit": "TFLOP/s",
-                     "frac": tc_ach / bf16_peak if (bf16_peak and tc_ach) else None, "traffic": None,
+                     "frac": tc_ach / bf16_peak if (bf16_peak and tc_ach) else None,
+                     # DRAM bytes per step of the kernel (ncu capture of this workload; other
+                     # configurations were not captured)
+                     "traffic": (TC_DRAM_BYTES_100CUBE["read"] + TC_DRAM_BYTES_100CUBE["write"]) if cfg == 2 else None,
+                     "traffic_rate_gbs": ((TC_DRAM_BYTES_100CUBE["read"] + TC_DRAM_BYTES_100CUBE["write"]) /
+                                          (mixed["tc_ms_per_step"] * 1e-3) / 1e9)
+                                         if (cfg == 2 and mixed["tc_ms_per_step"]) else None,
                      "peak_source": "dense BF16/FP16 tensor rate, %s (%s)" % (
                          mp["source"], "MEASURED_PEAKS.json" if mp["source"] == "measured" else
                          "no MEASURED_PEAKS.json: the earlier measurement on this pool"),

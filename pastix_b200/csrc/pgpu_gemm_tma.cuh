@@ -14,9 +14,10 @@
 // cover the coeftab itself, {K, rows, 1}.  Rows and columns past the panel
 // are zero-filled by the TMA unit.
 //
-// Roles (192 threads, one CTA per SM walking the level's tiles):
-//   warps 0-3: epilogue (TMEM -> registers -> shared transpose -> 16-byte
-//              vector reductions into the target), as the persistent kernel;
+// Roles (320 threads, one CTA per SM walking the level's tiles):
+//   warps 0-3, 6-9: epilogue (TMEM -> registers -> a swizzled 32 x 32 shared
+//              buffer per warp -> 16-byte vector reductions along the target
+//              rows);
 //   warp 4, lane 0: TMA producer -- per k-block waits for a free stage,
 //              announces the stage's bytes on its mbarrier and issues the A
 //              and B box loads;
@@ -29,6 +30,7 @@
 
 #include <cuda.h>
 #include <cuda_fp16.h>
+#include <type_traits>
 
 #include "pgpu_common.cuh"
 #include "pgpu_factor.cuh"
@@ -41,7 +43,7 @@ namespace pgpu {
 // issues the MMAs
 constexpr int TMA_THREADS = 320, TMA_EPI_WARPS = 8;
 constexpr int TMA_PROD_WARP = 4, TMA_MMA_WARP = 5;
-constexpr int TMA_EPI_BYTES = TMA_EPI_WARPS * 32 * 33 * 4;
+constexpr int TMA_EPI_BYTES = TMA_EPI_WARPS * 32 * 32 * 4;   // a swizzled 32 x 32 float buffer per warp
 // operand maps per cblk: L panel, U panel (LU), first / second diagonal-block inverse
 enum { TMAP_L = 0, TMAP_U = 1, TMAP_I = 2, TMAP_I2 = 3, TMAP_KINDS = 4 };
 
@@ -120,7 +122,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
     const uint32_t raw = smem_u32(tc_smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     unsigned char *sbase = tc_smem_raw + (base - raw);
-    float *epi = reinterpret_cast<float *>(sbase + S * NT * TC_TILE_BYTES);   // [8][32][33]
+    float *epi = reinterpret_cast<float *>(sbase + S * NT * TC_TILE_BYTES);   // [8][32][32]
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == TMA_MMA_WARP) {
@@ -264,7 +266,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
         const int ew = warp < 4 ? warp : warp - 2;   // epilogue warp 0..7
         const int qw = warp & 3;                       // TMEM lane quarter (rows 32 qw .. 32 qw + 31)
         const int grp = warp < 4 ? 0 : 1;              // column chunks 32 grp, 32 grp + 64
-        float *E = epi + ew * 32 * 33;
+        float *E = epi + ew * 32 * 32;
         const int myrow = qw * 32 + lane;
         // two stages: the descriptor of tile t + 2 is loaded while tile t is
         // written back, and the row targets / scales of tile t + 1 (which need
@@ -313,22 +315,31 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
             const int ldf = v.ldo, wf = v.wf;
             const int tcol0 = v.tcol;
             const bool lower_only = (v.flags & 8) != 0;
+            // the update subtracts: the sign rides on the row scale
+            const float sgn = trsm ? 1.f : -1.f;
             for (int h = 0; h < nh; h++)
             for (int cb = 32 * grp; cb < TC_BN; cb += 64) {
                 const int mrows = min(TC_BM, v.mrows - h * TC_BM);   // valid rows of this half
                 uint32_t r[32];
                 tc_ld32(tmem + (uint32_t)(ab * 256 + h * 128) + ((uint32_t)(qw * 32) << 16) + (uint32_t)cb, r);
                 __syncwarp();
+                // this lane's row (TMEM lane) as eight 16-byte groups, group g at
+                // slot g ^ (row & 7): conflict-free both for the row-wise stores
+                // here and for the loads along a row / down a column below
+                float x[32];
                 if (F16) {
                     // column cb + lane's inverse scale (loaded with the tile), broadcast column by column
-                    const float cs = (cb - 32 * grp) ? csr[1] : csr[0], rsh = h ? rs[1] : rs[0];
+                    const float cs = (cb - 32 * grp) ? csr[1] : csr[0], rsh = (h ? rs[1] : rs[0]) * sgn;
 #pragma unroll
-                    for (int q = 0; q < 32; q++)
-                        E[lane * 33 + q] = __uint_as_float(r[q]) * rsh * __shfl_sync(0xffffffffu, cs, q);
+                    for (int q = 0; q < 32; q++) x[q] = __uint_as_float(r[q]) * rsh * __shfl_sync(0xffffffffu, cs, q);
                 } else {
 #pragma unroll
-                    for (int q = 0; q < 32; q++) E[lane * 33 + q] = __uint_as_float(r[q]);
+                    for (int q = 0; q < 32; q++) x[q] = __uint_as_float(r[q]) * sgn;
                 }
+#pragma unroll
+                for (int g = 0; g < 8; g++)
+                    *reinterpret_cast<float4 *>(E + lane * 32 + ((g ^ (lane & 7)) << 2)) =
+                        make_float4(x[4 * g], x[4 * g + 1], x[4 * g + 2], x[4 * g + 3]);
                 __syncwarp();
                 const int j = cb + lane;
                 if (j < v.ncols && trsm) {
@@ -337,25 +348,51 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
                     for (int rr = 0; rr < 32; rr++) {
                         const int i = qw * 32 + rr;
                         if (i >= mrows) break;
-                        O[(int64_t)i * ldc + j] = E[rr * 33 + lane];
+                        O[(int64_t)i * ldc + j] = E[rr * 32 + ((((lane >> 2) ^ (rr & 7)) << 2) | (lane & 3))];
                     }
                 } else if (!trsm && cb < v.ncols) {
                     const int nvalid = min(32, v.ncols - cb);
-                    const int tcs = tcol0 + cb, a0 = tcs & ~3, o = tcs - a0;
-                    for (int k = lane; k < 32 * 9; k += 32) {
-                        const int rr = k / 9, g = k - rr * 9;
-                        const int t2 = __shfl_sync(0xffffffffu, h ? trw[1] : trw[0], rr);
-                        if (t2 < 0) continue;
-                        float a[4];
-                        bool any = false;
+                    const int tcs = tcol0 + cb, a0 = tcs & ~3;
+                    const int trh = h ? trw[1] : trw[0];
+                    // target group g (columns a0 + 4 g ..) takes source columns 4 g - O ..
+                    // 4 g + 3 - O: the tail of group g - 1 and the head of group g, the
+                    // offset O = tcs mod 4 a compile-time constant per branch
+                    auto reduce = [&](auto oc) {
+                        constexpr int O = decltype(oc)::value;
+                        for (int k = lane; k < 32 * 9; k += 32) {
+                            const int rr = k / 9, g = k - rr * 9;
+                            const int t2 = __shfl_sync(0xffffffffu, trh, rr);
+                            if (t2 < 0 || (O == 0 && g == 8)) continue;
+                            const float *Er = E + rr * 32;
+                            const int sw = rr & 7;
+                            float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
+                            if (O > 0 && g >= 1) lo = *reinterpret_cast<const float4 *>(Er + (((g - 1) ^ sw) << 2));
+                            if (g <= 7) hi = *reinterpret_cast<const float4 *>(Er + ((g ^ sw) << 2));
+                            float a[4];
+                            if (O == 0) { a[0] = hi.x; a[1] = hi.y; a[2] = hi.z; a[3] = hi.w; }
+                            if (O == 1) { a[0] = lo.w; a[1] = hi.x; a[2] = hi.y; a[3] = hi.z; }
+                            if (O == 2) { a[0] = lo.z; a[1] = lo.w; a[2] = hi.x; a[3] = hi.y; }
+                            if (O == 3) { a[0] = lo.y; a[1] = lo.z; a[2] = lo.w; a[3] = hi.x; }
+                            const int j0 = 4 * g - O;   // source column of a[0]
+                            if (j0 < 0 || j0 + 3 >= nvalid || lower_only) {
+                                bool any = false;
 #pragma unroll
-                        for (int u = 0; u < 4; u++) {
-                            const int jj = 4 * g + u - o, tc = a0 + 4 * g + u;
-                            const bool ok = jj >= 0 && jj < nvalid && !(lower_only && t2 < wf && tc > t2);
-                            a[u] = ok ? -E[rr * 33 + (ok ? jj : 0)] : 0.f;
-                            any |= ok;
+                                for (int u = 0; u < 4; u++) {
+                                    const int jj = j0 + u, tc = a0 + 4 * g + u;
+                                    const bool ok = jj >= 0 && jj < nvalid && !(lower_only && t2 < wf && tc > t2);
+                                    a[u] = ok ? a[u] : 0.f;
+                                    any |= ok;
+                                }
+                                if (!any) continue;
+                            }
+                            red_add_v4(&C[(int64_t)t2 * ldf + a0 + 4 * g], a[0], a[1], a[2], a[3]);
                         }
-                        if (any) red_add_v4(&C[(int64_t)t2 * ldf + a0 + 4 * g], a[0], a[1], a[2], a[3]);
+                    };
+                    switch (tcs - a0) {
+                        case 0: reduce(std::integral_constant<int, 0>{}); break;
+                        case 1: reduce(std::integral_constant<int, 1>{}); break;
+                        case 2: reduce(std::integral_constant<int, 2>{}); break;
+                        default: reduce(std::integral_constant<int, 3>{}); break;
                     }
                 }
                 __syncwarp();
