@@ -169,11 +169,16 @@ struct pastix_gpu_s {
     std::vector<int64_t> seg;           // batch: first unknown of each system (+ n), empty if none
     DArr<int64_t> d_seg;
     DArr<double> d_segss;               // per-system sums of squares
-    std::vector<cudaEvent_t> evpool, evpool2;   // per-launch timing events (main, stream2)
+    std::vector<cudaEvent_t> evpool, evpool2;   // per-launch timing events (solves; the numfact's stream2)
+    std::vector<cudaEvent_t> evpoolf;           // the numfact's main-stream timing events
     // phase timeline of the last directly launched numfact (pastix_gpu_phase_log):
     // {stream, phase, level} and {start, end} ms from the numfact's first event
-    std::vector<int> log_kinds2, log_levels2;
-    int log_used2 = 0;
+    std::vector<int> log_kinds, log_levels, log_kinds2, log_levels2;
+    int log_used = 0, log_used2 = 0;
+    // the numfact's per-phase times and timeline are read from its events when
+    // first asked for (pastix_gpu_stats / pastix_gpu_phase_log), not between the
+    // numfact and the next call: 1 direct launch, 2 graph replay, 0 collected
+    int fact_marks_pending = 0;
     std::vector<int64_t> phase_info;
     std::vector<double> phase_times;
     DArr<double> d_fact_scal;          // [0] ||A||_F, [1] static-pivot threshold (device-side, no host trip)
@@ -1776,11 +1781,8 @@ static int run_factor(pastix_gpu_t &C, int fmode, int *launches, LaunchTimer &tm
     }
     PGPU_CHECK(tm.mark(PH_END));
     PGPU_CHECK(cudaGetLastError());
-    std::fill(C.side_ms, C.side_ms + 4, 0.0);
-    if (la && !C.capturing) {
-        PGPU_CHECK(cudaStreamSynchronize(C.stream2));
-        tm2.collect(C.side_ms, 4);
-    }
+    // (the second stream's marks are read with the main stream's, after the
+    // numfact, which ends on the main stream after it joined the second)
     if (C.capturing) {   // the replays collect the second stream's marks after their synchronization
         C.g_kinds2 = la ? tm2.kinds : std::vector<int>();
         C.g_used2 = la ? tm2.used : 0;
@@ -1815,6 +1817,46 @@ static int fill_and_factor(pastix_gpu_t &C, int fmode, int *nl, LaunchTimer &tm)
     return run_factor<T>(C, fmode, nl, tm);
 }
 
+// The last numfact's per-phase device times (stats 6, 8, 9, 11) and its
+// phase timeline, from the timing events of both streams.  Called when they
+// are first asked for rather than at the end of the numfact: reading a few
+// hundred events costs about a millisecond of host time, which would
+// otherwise sit between the factorization and the next call's launches.  The
+// numfact's events (evpoolf, evpool2, ev[0]) are recorded only by numfact.
+static void fact_marks_collect(pastix_gpu_t &C) {
+    if (!C.fact_marks_pending) return;
+    const bool replayed = C.fact_marks_pending == 2;
+    C.fact_marks_pending = 0;
+    if (replayed) LaunchTimer::collect_marks(C.evpool2, C.g_kinds2, C.g_used2, C.side_ms, 4);
+    else LaunchTimer::collect_marks(C.evpool2, C.log_kinds2, C.log_used2, C.side_ms, 4);
+    C.phase_info.clear();
+    C.phase_times.clear();
+    if (!replayed) {
+        // both streams' marks on one timeline: elapsed time from the numfact's first event
+        auto add = [&](int stream, const std::vector<cudaEvent_t> &pool, const std::vector<int> &kinds,
+                       const std::vector<int> &levels, int used) {
+            for (int i = 0; i + 1 < used; i++) {
+                if (kinds[i] < 0 || kinds[i] >= PH_END) continue;   // PH_END closes an untimed gap
+                float t0 = 0, t1 = 0;
+                if (cudaEventElapsedTime(&t0, C.ev[0], pool[i]) != cudaSuccess ||
+                    cudaEventElapsedTime(&t1, C.ev[0], pool[i + 1]) != cudaSuccess)
+                    continue;
+                C.phase_info.insert(C.phase_info.end(), {(int64_t)stream, (int64_t)kinds[i], (int64_t)levels[i]});
+                C.phase_times.insert(C.phase_times.end(), {(double)t0, (double)t1});
+            }
+        };
+        add(0, C.evpoolf, C.log_kinds, C.log_levels, C.log_used);
+        add(1, C.evpool2, C.log_kinds2, C.log_levels2, C.log_used2);
+    }
+    double ph[4];
+    if (replayed) LaunchTimer::collect_marks(C.evpoolf, C.g_kinds, C.g_used, ph, 4);
+    else LaunchTimer::collect_marks(C.evpoolf, C.log_kinds, C.log_used, ph, 4);
+    C.stats[8] = ph[PH_DIAG];
+    C.stats[9] = ph[PH_TRSM];
+    C.stats[6] = ph[PH_GEMM] + ph[PH_TC] + C.side_ms[PH_GEMM] + C.side_ms[PH_TC];
+    C.stats[11] = ph[PH_TC] + C.side_ms[PH_TC];
+}
+
 extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     if (!ctx || !values) return PASTIX_GPU_ERR_BADPARAMETER;
     auto &C = *ctx;
@@ -1842,7 +1884,8 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
                                is_device_ptr(values) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
     int launches = 4;
     int nl = 0;
-    LaunchTimer tm(C);
+    C.fact_marks_pending = 0;
+    LaunchTimer tm(C, s, C.evpoolf);
     auto enqueue = [&]() -> int {
         if (zc) dev_norm_and_crit<cdouble>(C, C.dparm[PGPU_DPARM_EPSILON_MAGN_CTRL]);
         else dev_norm_and_crit<double>(C, C.dparm[PGPU_DPARM_EPSILON_MAGN_CTRL]);
@@ -1917,42 +1960,17 @@ extern "C" int pastix_gpu_numfact(pastix_gpu_t *ctx, const void *values) {
     PGPU_CHECK(cudaEventElapsedTime(&ms, C.ev[0], C.ev[1]));
     C.stats[0] = launches + nl;
     C.stats[3] = ms;
-    if (replayed) {   // the graph's event nodes: main stream, then the lookahead stream
-        nl = C.g_nl;
-        LaunchTimer::collect_marks(C.evpool2, C.g_kinds2, C.g_used2, C.side_ms, 4);
-    }
-    C.phase_info.clear();
-    C.phase_times.clear();
-    if (!replayed) {
-        // both streams' marks on one timeline: elapsed time from the numfact's first event
-        auto add = [&](int stream, const std::vector<cudaEvent_t> &pool, const std::vector<int> &kinds,
-                       const std::vector<int> &levels, int used) {
-            for (int i = 0; i + 1 < used; i++) {
-                if (kinds[i] < 0 || kinds[i] >= PH_END) continue;   // PH_END closes an untimed gap
-                float t0 = 0, t1 = 0;
-                if (cudaEventElapsedTime(&t0, C.ev[0], pool[i]) != cudaSuccess ||
-                    cudaEventElapsedTime(&t1, C.ev[0], pool[i + 1]) != cudaSuccess)
-                    continue;
-                C.phase_info.insert(C.phase_info.end(), {(int64_t)stream, (int64_t)kinds[i], (int64_t)levels[i]});
-                C.phase_times.insert(C.phase_times.end(), {(double)t0, (double)t1});
-            }
-        };
-        add(0, C.evpool, tm.kinds, tm.levels, tm.used);
-        add(1, C.evpool2, C.log_kinds2, C.log_levels2, C.log_used2);
-    }
-    {
-        double ph[4];
-        if (replayed) LaunchTimer::collect_marks(C.evpool, C.g_kinds, C.g_used, ph, 4);
-        else tm.collect(ph, 4);
-        C.stats[8] = ph[PH_DIAG];
-        C.stats[9] = ph[PH_TRSM];
-        C.stats[6] = ph[PH_GEMM] + ph[PH_TC] + C.side_ms[PH_GEMM] + C.side_ms[PH_TC];
-        C.stats[10] = C.plan_gemm_flops;
-        C.stats[11] = ph[PH_TC] + C.side_ms[PH_TC];
-        C.stats[12] = C.tc_flops;   // tensor-core (tcgen05, or FP64 DMMA) task flops
-        C.stats[13] = st.timeout;
-        C.stats[14] = replayed ? 1.0 : 0.0;
-    }
+    if (replayed) nl = C.g_nl;
+    // per-phase times (stats 6, 8, 9, 11) and the timeline: read from the
+    // events when first asked for (fact_marks_collect)
+    C.log_kinds = tm.kinds;
+    C.log_levels = tm.levels;
+    C.log_used = tm.used;
+    C.fact_marks_pending = replayed ? 2 : 1;
+    C.stats[10] = C.plan_gemm_flops;
+    C.stats[12] = C.tc_flops;   // tensor-core (tcgen05, or FP64 DMMA) task flops
+    C.stats[13] = st.timeout;
+    C.stats[14] = replayed ? 1.0 : 0.0;
     if (st.timeout || st.drain_timeout) {
         fprintf(stderr, "pastix_gpu: %d tensor-core GEMM tiles timed out waiting for their MMAs\n", st.timeout);
         if (st.drain_timeout)
@@ -3295,6 +3313,7 @@ static int task_records_impl(pastix_gpu_t *ctx, int64_t *count, int64_t *info, d
 
 extern "C" int pastix_gpu_phase_log(pastix_gpu_t *ctx, int64_t *count, int64_t *info, double *times) {
     if (!ctx || !count) return PASTIX_GPU_ERR_BADPARAMETER;
+    fact_marks_collect(*ctx);
     const int64_t n = (int64_t)ctx->phase_times.size() / 2;
     if (!info || !times) {
         *count = n;
@@ -3399,6 +3418,7 @@ extern "C" int pastix_gpu_coeftab(pastix_gpu_t *ctx, void *L, void *U) {
 
 extern "C" int pastix_gpu_stats(pastix_gpu_t *ctx, double *stats) {
     if (!ctx || !stats) return PASTIX_GPU_ERR_BADPARAMETER;
+    fact_marks_collect(*ctx);
     std::memcpy(stats, ctx->stats, sizeof(ctx->stats));
     return PASTIX_GPU_SUCCESS;
 }
@@ -3411,6 +3431,7 @@ extern "C" void pastix_gpu_finalize(pastix_gpu_t **pctx) {
     for (auto &e : C->ev) cudaEventDestroy(e);
     for (auto &e : C->evpool) cudaEventDestroy(e);
     for (auto &e : C->evpool2) cudaEventDestroy(e);
+    for (auto &e : C->evpoolf) cudaEventDestroy(e);
     for (auto &e : C->la_events) cudaEventDestroy(e);
     if (C->fact_exec) cudaGraphExecDestroy(C->fact_exec);
     if (C->fact_graph) cudaGraphDestroy(C->fact_graph);
