@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
             if (!mbar_wait(smem_u32(&drained), 0u)) atomicExch(&fail_s, 1);
         }
     } else {
-        // ---------------- epilogue (warps 0-3) ----------------
+        // ---------------- epilogue (warps 0-3 and 6-9) ----------------
         // The next tile's view, target rows and row scales are loaded while
         // the current tile is written back (prep of tile t + 1 before the
         // wait on tile t's accumulator): the epilogue's per-tile load chains
