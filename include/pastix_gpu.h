@@ -113,7 +113,7 @@ PASTIX_GPU_API int pastix_gpu_structure( pastix_gpu_t *ctx, int64_t n,
  * Hand over the pattern of the user's matrix (0-based CSC; Symmetric and
  * Hermitian matrices give one triangle).  Builds the device-side bcsc
  * equivalents on the device: the fill-in map into the coeftab and the
- * permuted matrix the refinement multiplies by (its device time is
+ * full matrix in CSR (user numbering) the refinement multiplies by (its device time is
  * stats[15] of pastix_gpu_stats).  Replaces pastix_subtask_spm2bcsc
  * (sopalin/pastix_task_sopalin.c:93) / bcscInit (bcsc/bcsc.c:1887).
  */
@@ -330,7 +330,7 @@ PASTIX_GPU_API int pastix_gpu_coeftab( pastix_gpu_t *ctx, void *L, void *U );
  *   stats[13] tensor-core tiles whose bounded MMA wait timed out (0 when healthy)
  *   stats[14] 1 when the factorization replayed a captured CUDA graph
  *   stats[15] ms of the last pastix_gpu_spm (device-side pattern setup: uploads,
- *             fill map, permuted CSR)
+ *             fill map, CSR)
  * (16 doubles)
  * The single-precision (mixed) factorization runs its large update GEMMs on
  * the tensor cores with split FP16 operands (3xFP16); environment

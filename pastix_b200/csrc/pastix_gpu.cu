@@ -528,7 +528,7 @@ extern "C" int pastix_gpu_spm(pastix_gpu_t *ctx, int mtxtype, int flttype, int64
     PGPU_CHECK(C.d_csr_src.alloc(std::max<int64_t>(fnnz, 1)));
     if (fnnz > 0)
         k_spm_csr<<<(int)std::min<int64_t>(4096, (fnnz + 255) / 256), 256, 0, s>>>(
-            fnnz, d_sslot.p, d_colof.p, d_rowptr.p, d_perm.p, herm ? 1 : 0, C.d_csr_col.p, C.d_csr_src.p);
+            fnnz, d_sslot.p, d_colof.p, d_rowptr.p, herm ? 1 : 0, C.d_csr_col.p, C.d_csr_src.p);
     const int ncomp = (flttype == PGPU_COMPLEX64) ? 2 : 1;
     C.csr_nnz = fnnz;
     PGPU_CHECK(C.d_csr_val.alloc(std::max<int64_t>(fnnz, 1) * ncomp));
@@ -2594,19 +2594,14 @@ struct VecOps {
         k_scal<S><<<1024, 256, 0, C.stream>>>(C.n, a, x);
         launches++;
     }
-    // y = alpha A x + beta y, in the user numbering: the CSR is permuted, so
-    // work on permuted copies held in d_gm.
+    // y = alpha A x + beta y in the user numbering, the CSR's own (x and y
+    // are distinct vectors at every call)
     void spmv(double alpha, const S *x, double beta, S *y) {
         const int n = C.n;
-        S *xp = reinterpret_cast<S *>(C.d_gm.p), *yp = xp + n;
         const S *val = reinterpret_cast<const S *>(C.d_csr_val.p);
-        const int grid = cdiv(n, 256);
-        k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, x, n, xp, n, 0);
-        if (beta != 0.0) k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, y, n, yp, n, 0);
-        k_spmv<S><<<cdiv((int64_t)n * 32, 256), 256, 0, C.stream>>>(n, C.d_csr_ptr.p, C.d_csr_col.p, val, alpha, xp,
-                                                                     beta, yp);
-        k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, 1, C.d_peritab.p, yp, n, y, n, 1);
-        launches += 3 + (beta != 0.0);
+        k_spmv<S><<<cdiv((int64_t)n * 32, 256), 256, 0, C.stream>>>(n, C.d_csr_ptr.p, C.d_csr_col.p, val, alpha, x,
+                                                                     beta, y);
+        launches++;
     }
     int spsv(S *z) { return solve_device_block(C, z, C.n, 1, C.d_work.p, &launches); }
     // per-system 2-norms of x (batch segments)
@@ -2876,21 +2871,18 @@ struct BlockOps {
     void copy(const S *x, S *y) {
         cudaMemcpyAsync(y, x, (size_t)C.n * k * sizeof(S), cudaMemcpyDeviceToDevice, C.stream);
     }
+    // (the CSR is in the user numbering, as the vectors: no permutation; x
+    // and y are distinct vectors at every call)
     void spmv(double alpha, const S *x, double beta, S *y) {
         const int n = C.n;
-        S *xp = reinterpret_cast<S *>(C.d_gm.p), *yp = xp + (size_t)n * k;
         const S *val = reinterpret_cast<const S *>(C.d_csr_val.p);
-        const int grid = std::min(4096, cdiv((int64_t)n * k, 256));
-        k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, k, C.d_peritab.p, x, n, xp, n, 0);
-        if (beta != 0.0) k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, k, C.d_peritab.p, y, n, yp, n, 0);
         if (C.csr_nnz <= (int64_t)16 * n)   // short rows: one thread per row
             k_spmv_rows_multi<S><<<std::min(cdiv(n, 256), 8 * 148), 256, 0, C.stream>>>(
-                n, k, C.d_csr_ptr.p, C.d_csr_col.p, val, alpha, xp, beta, yp);
+                n, k, C.d_csr_ptr.p, C.d_csr_col.p, val, alpha, x, beta, y);
         else
             k_spmv_multi<S><<<cdiv((int64_t)n * 32, 256), 256, 0, C.stream>>>(n, k, C.d_csr_ptr.p, C.d_csr_col.p,
-                                                                               val, alpha, xp, beta, yp);
-        k_permute<S, S><<<grid, 256, 0, C.stream>>>(n, k, C.d_peritab.p, yp, n, y, n, 1);
-        launches += 3 + (beta != 0.0);
+                                                                               val, alpha, x, beta, y);
+        launches++;
     }
     int spsv(S *z) { return solve_device_block(C, z, C.n, k, C.d_work.p, &launches); }
     // per column: ||r_c|| / ||b_c||, or with batch segments the largest

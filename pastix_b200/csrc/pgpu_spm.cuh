@@ -5,11 +5,12 @@
 //     P A P^t for symmetric / Hermitian matrices, L or U^t for general ones;
 //     ~offset when a Hermitian value must be conjugated) and its Frobenius
 //     weight (2 for a mirrored off-diagonal entry);
-//   * the permuted full matrix P A P^t in CSR for the refinement's SpMV: its
-//     entries are generated in the user's entry order (entry k gives slot 2k,
-//     its symmetric mirror slot 2k + 1) and stably sorted by permuted row, so
-//     the rows list their entries in the order a column-by-column pass visits
-//     them (deterministic SpMV sums).
+//   * the full matrix A in CSR, in the user's numbering, for the refinement's
+//     SpMV (which works on vectors in that numbering, so it needs no
+//     permutation around it): its entries are generated in the user's entry
+//     order (entry k gives slot 2k, its symmetric mirror slot 2k + 1) and
+//     stably sorted by row, so the rows list their entries in the order a
+//     column-by-column pass visits them (deterministic SpMV sums).
 #pragma once
 
 #include "pgpu_common.cuh"
@@ -26,7 +27,7 @@ struct SpmMaps {
     int64_t coefnbr;
     int64_t *fill_dst;                // [nnz]
     int8_t *wgt;                      // [nnz]
-    int *key;                         // [2 nnz] permuted row of each slot (n: no entry)
+    int *key;                         // [2 nnz] CSR row of each slot (n: no entry)
     int64_t *slot;                    // [2 nnz] slot index 2k / 2k + 1
     int *colof;                       // [nnz] user column of entry k
     int *bad;                         // set when an entry is outside the matrix or the structure
@@ -54,8 +55,8 @@ __global__ void __launch_bounds__(256) k_spm_maps(Meta m, SpmMaps s) {
         int pi = s.perm[i], pj = pj0;
         const bool off = (i != j);
         s.wgt[k] = (s.sym && off) ? 2 : 1;
-        s.key[2 * k] = pi;                                  // the entry, in row perm[i]
-        s.key[2 * k + 1] = (s.sym && off) ? pj : s.n;       // its mirror, in row perm[j]
+        s.key[2 * k] = (int)i;                              // the entry, in row i
+        s.key[2 * k + 1] = (s.sym && off) ? j : s.n;        // its mirror, in row j
         bool flip = false;
         if (s.sym && pi < pj) {
             const int t = pi;
@@ -87,15 +88,15 @@ __global__ void __launch_bounds__(256) k_spm_maps(Meta m, SpmMaps s) {
 
 // after the sort: CSR columns and value sources of the sorted slots
 __global__ void k_spm_csr(int64_t fnnz, const int64_t *__restrict__ slot, const int *__restrict__ colof,
-                          const int64_t *__restrict__ rowptr, const int *__restrict__ perm, int herm,
-                          int *__restrict__ ccol, int64_t *__restrict__ csrc) {
+                          const int64_t *__restrict__ rowptr, int herm, int *__restrict__ ccol,
+                          int64_t *__restrict__ csrc) {
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < fnnz; q += (int64_t)gridDim.x * blockDim.x) {
         const int64_t sl = slot[q], k = sl >> 1;
-        if ((sl & 1) == 0) {   // the entry itself, in row perm[i]: column perm[j]
-            ccol[q] = perm[colof[k]];
+        if ((sl & 1) == 0) {   // the entry itself, in row i: column j
+            ccol[q] = colof[k];
             csrc[q] = k;
-        } else {               // its mirror, in row perm[j]: column perm[i] (conjugated if Hermitian)
-            ccol[q] = perm[rowptr[k]];
+        } else {               // its mirror, in row j: column i (conjugated if Hermitian)
+            ccol[q] = (int)rowptr[k];
             csrc[q] = herm ? ~k : k;
         }
     }
